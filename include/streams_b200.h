@@ -1,0 +1,186 @@
+/*
+ * streams_b200.h -- C ABI of the B200 (sm_100a) backend for the per-Runge-Kutta-stage
+ * right-hand side and update of the STREAmS-2 Cartesian compressible Navier-Stokes solver.
+ *
+ * Everything here is plain C: opaque handles, POD structs, host or device pointers and
+ * sizes.  A Fortran solver object binds it with ISO_C_BINDING exactly as the HIP backend
+ * binds its C++ wrappers (code/src/singleideal/kernels_amd.F90:1658-1677, passing
+ * `type(c_ptr), value` arrays and `value` scalars).
+ *
+ * Conventions
+ *   - Every entry point returns 0 on success and a negative STREAMS_B200_E* code on error.
+ *     Nothing calls exit(); the message of the last failure on a context is returned by
+ *     streams_b200_last_error(ctx) (streams_b200_global_error() when no context exists).
+ *   - The conserved field w is the reference's field%w array: w(1-ng:nx+ng, 1-ng:ny+ng,
+ *     1-ng:nz+ng, 1:5), Fortran order (i fastest, variable slowest), REAL64
+ *     (code/src/field.F90:404-454).
+ *   - A context owns all of its device memory and one CUDA stream.  Calls on one context
+ *     are not reentrant; distinct contexts may be driven from distinct host threads.
+ *   - The device path computes in FP64 (precision = 0) or in the mixed form (precision = 1:
+ *     FP32 flux and viscous arithmetic with compensated flux-difference sums; FP64 state,
+ *     RK register, temperature recovery and reductions).
+ */
+#ifndef STREAMS_B200_H
+#define STREAMS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STREAMS_B200_ABI_VERSION 1
+
+/* error codes */
+#define STREAMS_B200_OK 0
+#define STREAMS_B200_EINVAL -1      /* invalid argument or unsupported option */
+#define STREAMS_B200_ECUDA -2       /* a CUDA runtime call failed */
+#define STREAMS_B200_ENOMEM -3      /* device allocation failed or over budget */
+#define STREAMS_B200_ENAN -4        /* NaN detected in a reduction (the reference's "boom") */
+#define STREAMS_B200_ETIMEOUT -5    /* a bounded device wait gave up */
+#define STREAMS_B200_ENODEV -6      /* no usable sm_100 device */
+
+/*
+ * Solver parameters.  Field names follow equation_singleideal_object
+ * (code/src/singleideal/singleideal.F90:36-280) after initialize() has run, so the
+ * Fortran side fills this struct from equation_base%... one to one.
+ */
+typedef struct streams_b200_params {
+  /* sizes: interior cells of the (single) block and ghost layers (field%nx, ny, nz, grid%ng) */
+  int nx, ny, nz, ng;
+  /* numerics (singleideal.F90:489-545) */
+  int ep_order;             /* central order; lmax = ep_order/2 (2, 4, 6, 8) */
+  int nkeep;                /* KEEP(n) variant: 0 internal-energy split, <0 enthalpy split, >0 KEEP(n) */
+  int weno_scheme;          /* WENO order = 2*weno_scheme-1 (1..4) */
+  int weno_version;         /* 0 Jiang-Shu, 1 WENO-Z (weno_scheme 3 only) */
+  int flux_splitting;       /* 0 Roe characteristic splitting (the only one on the device path) */
+  int conservative_viscous; /* 1 conservative 2nd-order viscous form (the only one on the device path) */
+  double sensor_threshold;  /* Ducros threshold; <0 full WENO, >1 full central */
+  /* boundary conditions (bctags after the periodic normalisation, singleideal.F90:379-403) */
+  int bctags[6];            /* xmin xmax ymin ymax zmin zmax: 0 periodic, 6 viscous wall */
+  int force_zero_flux[6];   /* bc_preproc (singleideal.F90:4703-4750) */
+  int eul_imin, eul_imax, eul_jmin, eul_jmax, eul_kmin, eul_kmax;
+  int is_y_staggered;       /* staggered y walls (channel) */
+  /* fluid (set_fluid_prop, singleideal.F90:2685-2774) */
+  int visc_model;           /* 0 inviscid, 1 power law, 2 Sutherland */
+  int calorically_perfect;  /* 1 constant cp (the only one on the device path) */
+  double mu0, t0, rgas0, rho0, u0, l0;
+  double sutherland_s, t_ref_dim, powerlaw_vtexp, prandtl;
+  double cp0, cv0;          /* cp_coeff(0), cv_coeff(0) */
+  double cp_last, cv_last;  /* cp_coeff(indx_cp_r+1), cv_coeff(indx_cp_r+1) */
+  /* channel forcing (force_rhs / force_var, singleideal_cpu.F90:845-933) */
+  int channel_case;
+  double theta_wall, t_wall, t_bulk_target, volchan;
+  /* time integration (runge_kutta_initialize, singleideal.F90:4773-4795) */
+  int nrk;
+  double rhork[4], gamrk[4];
+  double cfl;               /* >0 CFL number, <0 fixed time step -cfl */
+  /* arithmetic of the device path: 0 = FP64, 1 = mixed (FP32 fluxes, FP64 state) */
+  int precision;
+} streams_b200_params;
+
+/*
+ * One-dimensional grid data of the block (field%x, y, z, yn and the metrics of
+ * set_local_grid, code/src/field.F90:456-516).  Host pointers; copied at create time.
+ */
+typedef struct streams_b200_grid {
+  const double* x;          /* x(1-ng:nx+ng)   nx+2*ng values */
+  const double* y;          /* y(1-ng:ny+ng)   ny+2*ng values */
+  const double* z;          /* z(1-ng:nz+ng)   nz+2*ng values */
+  const double* yn;         /* yn(1:ny+1)      cell faces in y */
+  const double* dcsidx;     /* dcsidx(1:nx) */
+  const double* detady;     /* detady(1:ny) */
+  const double* dzitdz;     /* dzitdz(1:nz) */
+  const double* dcsidxs;    /* dcsidxs(1:nx) */
+  const double* detadys;    /* detadys(1:ny) */
+  const double* dzitdzs;    /* dzitdzs(1:nz) */
+  const double* coeff_deriv1; /* coeff_deriv1(1:4,1:4), Fortran order (l fastest) */
+  const int* ep_ord_x;      /* ep_ord_change(i,*,*,1), i = 0..nx */
+  const int* ep_ord_y;      /* ep_ord_change(*,j,*,2), j = 0..ny */
+  const int* ep_ord_z;      /* ep_ord_change(*,*,k,3), k = 0..nz */
+} streams_b200_grid;
+
+typedef struct streams_b200_ctx streams_b200_ctx;
+
+/* Library identification. */
+int streams_b200_abi_version(void);
+const char* streams_b200_global_error(void);
+
+/*
+ * Create a context: validates the parameters, allocates the device state and uploads the grid.
+ * Replaces equation_singleideal_gpu_object%initialize / base_gpu%initialize
+ * (code/src/singleideal/singleideal_gpu.F90 initialize; code/src/base_gpu.F90:2033-2064).
+ */
+int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g, streams_b200_ctx** out);
+int streams_b200_destroy(streams_b200_ctx* ctx);
+const char* streams_b200_last_error(const streams_b200_ctx* ctx);
+
+/* Bytes of device memory a context with these parameters allocates (admission control). */
+long long streams_b200_footprint_bytes(const streams_b200_params* p);
+
+/*
+ * Field transfer.  Replace base_gpu%copy_from_field / copy_to_field
+ * (code/src/base_gpu.F90).  The host array is w(1-ng:nx+ng,1-ng:ny+ng,1-ng:nz+ng,5).
+ * The _device variants take a device pointer with the same layout.
+ */
+int streams_b200_copy_from_field(streams_b200_ctx* ctx, const double* w_host);
+int streams_b200_copy_to_field(streams_b200_ctx* ctx, double* w_host);
+int streams_b200_copy_from_device(streams_b200_ctx* ctx, const double* w_dev);
+int streams_b200_copy_to_device(streams_b200_ctx* ctx, double* w_dev);
+
+/*
+ * Preamble of run() (code/src/singleideal/singleideal_cpu.F90:1542-1557): update_ghost,
+ * compute_aux, visflx(mode=2) for the initial Ducros sensor, bcswap_var of the sensor,
+ * zero_flux.  Call once after the initial field is uploaded.
+ */
+int streams_b200_init_run(streams_b200_ctx* ctx);
+
+/*
+ * compute_aux(central=1, ghost=0) + compute_dt (singleideal_cpu.F90:1476-1517);
+ * the new time step is kept on the device and also returned in *dt (may be NULL).
+ */
+int streams_b200_compute_dt(streams_b200_ctx* ctx, double* dt);
+
+/* Set the device time step explicitly (cfl < 0 runs, or a host-imposed dt). */
+int streams_b200_set_dt(streams_b200_ctx* ctx, double dt);
+
+/*
+ * One Runge-Kutta step = nrk stages of the RHS and update, with the channel bulk
+ * forcing, ghost fills and the stage-3 sensor update.  Replaces rk_sync
+ * (code/src/singleideal/singleideal_cpu.F90:332-409).  Uses the device time step.
+ */
+int streams_b200_rk_sync(streams_b200_ctx* ctx);
+
+/*
+ * Advance nsteps time steps without host synchronisation: each step recomputes dt when
+ * (icyc - icyc0) % iter_dt_recompute == 0 (the run() loop, singleideal_cpu.F90:1576-1590),
+ * then runs rk_sync and accumulates the time on the device.  Not captured if nsteps == 0.
+ */
+int streams_b200_advance(streams_b200_ctx* ctx, int nsteps, int iter_dt_recompute, int icyc_start, int icyc0);
+
+/* Read device scalars: out[0..6] = dt, time, dpdx, rhobulk, ubulk, tbulk, tbdiff. */
+int streams_b200_get_scalars(streams_b200_ctx* ctx, double out[7]);
+int streams_b200_set_time(streams_b200_ctx* ctx, double time);
+
+/*
+ * compute_residual (singleideal_cpu.F90:1339-1364): out[0..6] = residual_rhou (sqrt of the
+ * mean of (fln_2/dt)^2), rhomin, rhomax, tmin, tmax, pmin, pmax.  Returns STREAMS_B200_ENAN
+ * (after filling out) when the residual is NaN.
+ */
+int streams_b200_compute_residual(streams_b200_ctx* ctx, double out[7]);
+
+/* Fraction of WENO faces per direction (count_weno, singleideal_cpu.F90:1389-1429). */
+int streams_b200_count_weno(streams_b200_ctx* ctx, double out[3]);
+
+/* Wall shear / heat flux at j=1 (wallprop(1:nx,1:nz,2:4) of visflx_reduced_ord2). */
+int streams_b200_get_wallprop(streams_b200_ctx* ctx, double* out /* nx*nz*3 */);
+
+/* Synchronise the context's stream and report any asynchronous error. */
+int streams_b200_synchronize(streams_b200_ctx* ctx);
+
+/* Number of kernel launches issued by this context since creation (instrumentation). */
+long long streams_b200_launch_count(const streams_b200_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STREAMS_B200_H */

@@ -1,0 +1,1037 @@
+// CPU oracle: restatement of the STREAmS-2 CPU backend time advance.  See oracle.hpp.
+// All line references are to code/src/singleideal/kernels_cpu.F90 unless stated otherwise.
+#include "oracle.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+
+#include "par_for.hpp"
+
+namespace streams_oracle {
+
+namespace {
+
+// wenorec_1d (kernels_cpu.F90:2526-2724).  vp, vm: [5][8] with Fortran index l = 1..8 at [m][l-1].
+void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], int iweno, int ord, int version,
+                double rho0, double u0) {
+  auto VP = [&](int m, int l) { return vp[m][l - 1]; };
+  auto VM = [&](int m, int l) { return vm[m][l - 1]; };
+  double u0_2 = u0 * u0;
+  double rho0_2u0_2 = rho0 * rho0 * u0_2;
+  double rho0_2u0_4 = rho0_2u0_2 * u0_2;
+  double betascale[5];
+  betascale[0] = 1.0 / rho0_2u0_2;
+  betascale[1] = betascale[0];
+  betascale[2] = 1.0 / rho0_2u0_4;
+  betascale[3] = betascale[2];
+  betascale[4] = betascale[0];
+  const int i = iweno;
+  if (ord == 1) {
+    for (int m = 0; m < 5; ++m) vhat[m] = VP(m, i) + VM(m, i + 1);
+  } else if (ord == 2) {
+    double dwe[2] = {1.0 / 3.0, 2.0 / 3.0};
+    for (int m = 0; m < 5; ++m) {
+      double bp[2], bm[2];
+      bp[0] = (VP(m, i) - VP(m, i - 1)) * (VP(m, i) - VP(m, i - 1));
+      bp[1] = (VP(m, i + 1) - VP(m, i)) * (VP(m, i + 1) - VP(m, i));
+      bp[1] = betascale[m] * bp[1];
+      bp[0] = betascale[m] * bp[0];
+      bm[0] = (VM(m, i + 2) - VM(m, i + 1)) * (VM(m, i + 2) - VM(m, i + 1));
+      bm[1] = (VM(m, i + 1) - VM(m, i)) * (VM(m, i + 1) - VM(m, i));
+      bm[1] = betascale[m] * bm[1];
+      bm[0] = betascale[m] * bm[0];
+      double sump = 0.0, summ = 0.0;
+      for (int l = 0; l < 2; ++l) {
+        double tp = 0.000001 + bp[l], tm = 0.000001 + bm[l];
+        bp[l] = dwe[l] / (tp * tp);
+        bm[l] = dwe[l] / (tm * tm);
+        sump = sump + bp[l];
+        summ = summ + bm[l];
+      }
+      for (int l = 0; l < 2; ++l) {
+        bp[l] = bp[l] / sump;
+        bm[l] = bm[l] / summ;
+      }
+      double vminus = bp[0] * (-VP(m, i - 1) + 3 * VP(m, i)) + bp[1] * (VP(m, i) + VP(m, i + 1));
+      double vplus = bm[0] * (-VM(m, i + 2) + 3 * VM(m, i + 1)) + bm[1] * (VM(m, i) + VM(m, i + 1));
+      vhat[m] = 0.5 * (vminus + vplus);
+    }
+  } else if (ord == 3) {
+    const double dwe[3] = {1.0 / 10.0, 6.0 / 10.0, 3.0 / 10.0};
+    const double d0 = 13.0 / 12.0, d1 = 1.0 / 4.0;
+    const double c0 = 1.0 / 3.0, c1 = 5.0 / 6.0, c2 = -1.0 / 6.0, c3 = -7.0 / 6.0, c4 = 11.0 / 6.0;
+    auto sq = [](double a) { return a * a; };
+    for (int m = 0; m < 5; ++m) {
+      double bp[3], bm[3];
+      bp[2] = d0 * sq(VP(m, i) - 2.0 * VP(m, i + 1) + VP(m, i + 2)) +
+              d1 * sq(3.0 * VP(m, i) - 4.0 * VP(m, i + 1) + VP(m, i + 2));
+      bp[1] = d0 * sq(VP(m, i - 1) - 2.0 * VP(m, i) + VP(m, i + 1)) + d1 * sq(VP(m, i - 1) - VP(m, i + 1));
+      bp[0] = d0 * sq(VP(m, i) - 2.0 * VP(m, i - 1) + VP(m, i - 2)) +
+              d1 * sq(3.0 * VP(m, i) - 4.0 * VP(m, i - 1) + VP(m, i - 2));
+      bp[2] = betascale[m] * bp[2];
+      bp[1] = betascale[m] * bp[1];
+      bp[0] = betascale[m] * bp[0];
+      bm[2] = d0 * sq(VM(m, i + 1) - 2.0 * VM(m, i) + VM(m, i - 1)) +
+              d1 * sq(3.0 * VM(m, i + 1) - 4.0 * VM(m, i) + VM(m, i - 1));
+      bm[1] = d0 * sq(VM(m, i + 2) - 2.0 * VM(m, i + 1) + VM(m, i)) + d1 * sq(VM(m, i + 2) - VM(m, i));
+      bm[0] = d0 * sq(VM(m, i + 1) - 2.0 * VM(m, i + 2) + VM(m, i + 3)) +
+              d1 * sq(3.0 * VM(m, i + 1) - 4.0 * VM(m, i + 2) + VM(m, i + 3));
+      bm[2] = betascale[m] * bm[2];
+      bm[1] = betascale[m] * bm[1];
+      bm[0] = betascale[m] * bm[0];
+      if (version == 0) {
+        double sump = 0.0, summ = 0.0;
+        for (int l = 0; l < 3; ++l) {
+          double tp = 0.000001 + bp[l], tm = 0.000001 + bm[l];
+          bp[l] = dwe[l] / (tp * tp);
+          bm[l] = dwe[l] / (tm * tm);
+          sump = sump + bp[l];
+          summ = summ + bm[l];
+        }
+        for (int l = 0; l < 3; ++l) {
+          bp[l] = bp[l] / sump;
+          bm[l] = bm[l] / summ;
+        }
+      } else {
+        // eps40 is a default-kind (single precision) literal in the reference
+        const double eps40 = static_cast<double>(1.e-35f);
+        double tau5p = std::fabs(bp[0] - bp[2]) + eps40;
+        double tau5m = std::fabs(bm[0] - bm[2]) + eps40;
+        for (int l = 0; l < 3; ++l) {
+          bp[l] = (bp[l] + eps40) / (bp[l] + tau5p);
+          bm[l] = (bm[l] + eps40) / (bm[l] + tau5m);
+        }
+        double sump = 0.0, summ = 0.0;
+        for (int l = 0; l < 3; ++l) {
+          bp[l] = dwe[l] / bp[l];
+          bm[l] = dwe[l] / bm[l];
+          sump = sump + bp[l];
+          summ = summ + bm[l];
+        }
+        for (int l = 0; l < 3; ++l) {
+          bp[l] = bp[l] / sump;
+          bm[l] = bm[l] / summ;
+        }
+      }
+      double vminus = bp[2] * (c0 * VP(m, i) + c1 * VP(m, i + 1) + c2 * VP(m, i + 2)) +
+                      bp[1] * (c2 * VP(m, i - 1) + c1 * VP(m, i) + c0 * VP(m, i + 1)) +
+                      bp[0] * (c0 * VP(m, i - 2) + c3 * VP(m, i - 1) + c4 * VP(m, i));
+      double vplus = bm[2] * (c0 * VM(m, i + 1) + c1 * VM(m, i) + c2 * VM(m, i - 1)) +
+                     bm[1] * (c2 * VM(m, i + 2) + c1 * VM(m, i + 1) + c0 * VM(m, i)) +
+                     bm[0] * (c0 * VM(m, i + 3) + c3 * VM(m, i + 2) + c4 * VM(m, i + 1));
+      vhat[m] = vminus + vplus;
+    }
+  } else if (ord == 4) {
+    const double dwe[4] = {1.0 / 35.0, 12.0 / 35.0, 18.0 / 35.0, 4.0 / 35.0};
+    const double d1 = 1.0 / 36.0, d2 = 13.0 / 12.0, d3 = 781.0 / 720.0;
+    auto sq = [](double a) { return a * a; };
+    for (int m = 0; m < 5; ++m) {
+      double bp[4], bm[4];
+      bp[3] = d1 * sq(-11 * VP(m, i) + 18 * VP(m, i + 1) - 9 * VP(m, i + 2) + 2 * VP(m, i + 3)) +
+              d2 * sq(2 * VP(m, i) - 5 * VP(m, i + 1) + 4 * VP(m, i + 2) - VP(m, i + 3)) +
+              d3 * sq(-VP(m, i) + 3 * VP(m, i + 1) - 3 * VP(m, i + 2) + VP(m, i + 3));
+      bp[2] = d1 * sq(-2 * VP(m, i - 1) - 3 * VP(m, i) + 6 * VP(m, i + 1) - VP(m, i + 2)) +
+              d2 * sq(VP(m, i - 1) - 2 * VP(m, i) + VP(m, i + 1)) +
+              d3 * sq(-VP(m, i - 1) + 3 * VP(m, i) - 3 * VP(m, i + 1) + VP(m, i + 2));
+      bp[1] = d1 * sq(VP(m, i - 2) - 6 * VP(m, i - 1) + 3 * VP(m, i) + 2 * VP(m, i + 1)) +
+              d2 * sq(VP(m, i - 1) - 2 * VP(m, i) + VP(m, i + 1)) +
+              d3 * sq(-VP(m, i - 2) + 3 * VP(m, i - 1) - 3 * VP(m, i) + VP(m, i + 1));
+      bp[0] = d1 * sq(-2 * VP(m, i - 3) + 9 * VP(m, i - 2) - 18 * VP(m, i - 1) + 11 * VP(m, i)) +
+              d2 * sq(-VP(m, i - 3) + 4 * VP(m, i - 2) - 5 * VP(m, i - 1) + 2 * VP(m, i)) +
+              d3 * sq(-VP(m, i - 3) + 3 * VP(m, i - 2) - 3 * VP(m, i - 1) + VP(m, i));
+      for (int l = 3; l >= 0; --l) bp[l] = betascale[m] * bp[l];
+      bm[3] = d1 * sq(-11 * VM(m, i + 1) + 18 * VM(m, i) - 9 * VM(m, i - 1) + 2 * VM(m, i - 2)) +
+              d2 * sq(2 * VM(m, i + 1) - 5 * VM(m, i) + 4 * VM(m, i - 1) - VM(m, i - 2)) +
+              d3 * sq(-VM(m, i + 1) + 3 * VM(m, i) - 3 * VM(m, i - 1) + VM(m, i - 2));
+      bm[2] = d1 * sq(-2 * VM(m, i + 2) - 3 * VM(m, i + 1) + 6 * VM(m, i) - VM(m, i - 1)) +
+              d2 * sq(VM(m, i + 2) - 2 * VM(m, i + 1) + VM(m, i)) +
+              d3 * sq(-VM(m, i + 2) + 3 * VM(m, i + 1) - 3 * VM(m, i) + VM(m, i - 1));
+      bm[1] = d1 * sq(VM(m, i + 3) - 6 * VM(m, i + 2) + 3 * VM(m, i + 1) + 2 * VM(m, i)) +
+              d2 * sq(VM(m, i + 2) - 2 * VM(m, i + 1) + VM(m, i)) +
+              d3 * sq(-VM(m, i + 3) + 3 * VM(m, i + 2) - 3 * VM(m, i + 1) + VM(m, i));
+      bm[0] = d1 * sq(-2 * VM(m, i + 4) + 9 * VM(m, i + 3) - 18 * VM(m, i + 2) + 11 * VM(m, i + 1)) +
+              d2 * sq(-VM(m, i + 4) + 4 * VM(m, i + 3) - 5 * VM(m, i + 2) + 2 * VM(m, i + 1)) +
+              d3 * sq(-VM(m, i + 4) + 3 * VM(m, i + 3) - 3 * VM(m, i + 2) + VM(m, i + 1));
+      for (int l = 3; l >= 0; --l) bm[l] = betascale[m] * bm[l];
+      double sump = 0.0, summ = 0.0;
+      for (int l = 0; l < 4; ++l) {
+        double tp = 0.000001 + bp[l], tm = 0.000001 + bm[l];
+        bp[l] = dwe[l] / (tp * tp);
+        bm[l] = dwe[l] / (tm * tm);
+        sump = sump + bp[l];
+        summ = summ + bm[l];
+      }
+      for (int l = 0; l < 4; ++l) {
+        bp[l] = bp[l] / sump;
+        bm[l] = bm[l] / summ;
+      }
+      double vminus = bp[3] * (6 * VP(m, i) + 26 * VP(m, i + 1) - 10 * VP(m, i + 2) + 2 * VP(m, i + 3)) +
+                      bp[2] * (-2 * VP(m, i - 1) + 14 * VP(m, i) + 14 * VP(m, i + 1) - 2 * VP(m, i + 2)) +
+                      bp[1] * (2 * VP(m, i - 2) - 10 * VP(m, i - 1) + 26 * VP(m, i) + 6 * VP(m, i + 1)) +
+                      bp[0] * (-6 * VP(m, i - 3) + 26 * VP(m, i - 2) - 46 * VP(m, i - 1) + 50 * VP(m, i));
+      double vplus = bm[3] * (6 * VM(m, i + 1) + 26 * VM(m, i) - 10 * VM(m, i - 1) + 2 * VM(m, i - 2)) +
+                     bm[2] * (-2 * VM(m, i + 2) + 14 * VM(m, i + 1) + 14 * VM(m, i) - 2 * VM(m, i - 1)) +
+                     bm[1] * (2 * VM(m, i + 3) - 10 * VM(m, i + 2) + 26 * VM(m, i + 1) + 6 * VM(m, i)) +
+                     bm[0] * (-6 * VM(m, i + 4) + 26 * VM(m, i + 3) - 46 * VM(m, i + 2) + 50 * VM(m, i + 1));
+      vhat[m] = (vminus + vplus) / 24.0;
+    }
+  }
+}
+
+// eigenvectors_x / _y / _z (kernels_cpu.F90:2728-2782, 2842-2896, 2956-3010).
+// el[r][c], er[r][c] hold the reference's el(r+1,c+1), er(r+1,c+1).
+void eigenvectors(int dir, double b1, double b2, double b3, double uu, double vv, double ww, double c, double ci,
+                  double h, double el[5][5], double er[5][5]) {
+  const double vel[3] = {uu, vv, ww};
+  const double vn = vel[dir];
+  // left eigenvectors: columns 1 and 5 (acoustic), 2 (entropy), 3 and 4 (tangential)
+  el[0][0] = 0.5 * (b1 + vn * ci);
+  el[1][0] = -0.5 * (dir == 0 ? b2 * uu + ci : b2 * uu);
+  el[2][0] = -0.5 * (dir == 1 ? b2 * vv + ci : b2 * vv);
+  el[3][0] = -0.5 * (dir == 2 ? b2 * ww + ci : b2 * ww);
+  el[4][0] = 0.5 * b2;
+  el[0][1] = 1.0 - b1;
+  el[1][1] = b2 * uu;
+  el[2][1] = b2 * vv;
+  el[3][1] = b2 * ww;
+  el[4][1] = -b2;
+  el[0][4] = 0.5 * (b1 - vn * ci);
+  el[1][4] = -0.5 * (dir == 0 ? b2 * uu - ci : b2 * uu);
+  el[2][4] = -0.5 * (dir == 1 ? b2 * vv - ci : b2 * vv);
+  el[3][4] = -0.5 * (dir == 2 ? b2 * ww - ci : b2 * ww);
+  el[4][4] = 0.5 * b2;
+  // tangential components: x -> (v, w), y -> (u, w), z -> (u, v)
+  const int t1 = (dir == 0) ? 1 : 0;
+  const int t2 = (dir == 2) ? 1 : 2;
+  for (int r = 0; r < 5; ++r) el[r][2] = el[r][3] = 0.0;
+  el[0][2] = -vel[t1];
+  el[1 + t1][2] = 1.0;
+  el[0][3] = -vel[t2];
+  el[1 + t2][3] = 1.0;
+  // right eigenvectors
+  for (int r = 0; r < 5; ++r)
+    for (int cc = 0; cc < 5; ++cc) er[r][cc] = 0.0;
+  er[0][0] = 1.0; er[1][0] = 1.0; er[4][0] = 1.0;
+  for (int d = 0; d < 3; ++d) {
+    if (d == dir) {
+      er[0][1 + d] = vel[d] - c;
+      er[1][1 + d] = vel[d];
+      er[4][1 + d] = vel[d] + c;
+    } else {
+      er[0][1 + d] = vel[d];
+      er[1][1 + d] = vel[d];
+      er[4][1 + d] = vel[d];
+    }
+  }
+  er[2][1 + t1] = 1.0;
+  er[3][1 + t2] = 1.0;
+  er[0][4] = h - vn * c;
+  er[1][4] = b3;
+  er[2][4] = vel[t1];
+  er[3][4] = vel[t2];
+  er[4][4] = h + vn * c;
+}
+
+}  // namespace
+
+Solver::Solver(const Setup& setup) : s(setup) {
+  nx = s.nxmax; ny = s.nymax; nz = s.nzmax; ng = s.ng;
+  sx = nx + 2 * ng; sy = ny + 2 * ng; sz = nz + 2 * ng;
+  w = s.w;
+  w_aux.assign(ncg() * 10, 0.0);
+  // initial_conditions: w_aux(:,:,:,6) = t0 (singleideal.F90:3032)
+  for (size_t q = 0; q < ncg(); ++q) w_aux[5 * ncg() + q] = s.t0;
+  fl.assign(nint_() * 5, 0.0);
+  fln.assign(nint_() * 5, 0.0);
+  fhat.assign(ncg() * 5, 0.0);
+  wallprop.assign(static_cast<size_t>(sx) * sz * 3, 0.0);
+  time = s.time0;
+  icyc = s.icyc0;
+}
+
+// base_cpu%bcswap (code/src/base_cpu.F90:1326-1435) on one block: face halos of periodic directions
+void Solver::bcswap() {
+  if (s.periodic[0])
+    par_for(1, nz, [&](int k) {
+      for (int j = 1; j <= ny; ++j)
+        for (int l = 1; l <= ng; ++l)
+          for (int m = 0; m < 5; ++m) {
+            W(nx + l, j, k, m) = W(l, j, k, m);
+            W(1 - l, j, k, m) = W(nx + 1 - l, j, k, m);
+          }
+    });
+  if (s.periodic[1])
+    par_for(1, nz, [&](int k) {
+      for (int l = 1; l <= ng; ++l)
+        for (int i = 1; i <= nx; ++i)
+          for (int m = 0; m < 5; ++m) {
+            W(i, ny + l, k, m) = W(i, l, k, m);
+            W(i, 1 - l, k, m) = W(i, ny + 1 - l, k, m);
+          }
+    });
+  if (s.periodic[2])
+    par_for(1, ng, [&](int l) {
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i)
+          for (int m = 0; m < 5; ++m) {
+            W(i, j, nz + l, m) = W(i, j, l, m);
+            W(i, j, 1 - l, m) = W(i, j, nz + 1 - l, m);
+          }
+    });
+}
+
+// base_cpu%bcswap_var (code/src/base_cpu.F90:1835-1912) for w_aux(:,:,:,m)
+void Solver::bcswap_var(int m) {
+  if (s.periodic[0])
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int l = 1; l <= ng; ++l) {
+          A(nx + l, j, k, m) = A(l, j, k, m);
+          A(1 - l, j, k, m) = A(nx + 1 - l, j, k, m);
+        }
+  if (s.periodic[1])
+    for (int k = 1; k <= nz; ++k)
+      for (int l = 1; l <= ng; ++l)
+        for (int i = 1; i <= nx; ++i) {
+          A(i, ny + l, k, m) = A(i, l, k, m);
+          A(i, 1 - l, k, m) = A(i, ny + 1 - l, k, m);
+        }
+  if (s.periodic[2])
+    for (int l = 1; l <= ng; ++l)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+          A(i, j, nz + l, m) = A(i, j, l, m);
+          A(i, j, 1 - l, m) = A(i, j, nz + 1 - l, m);
+        }
+}
+
+// update_ghost (singleideal_cpu.F90:1064-1138) with bcwall_staggered (kernels_cpu.F90:6612-6678)
+void Solver::update_ghost(int do_swap) {
+  const double twall = s.t_wall, t0 = s.t0, rgas0 = s.rgas0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
+  for (int ilat = 3; ilat <= 4; ++ilat) {
+    if (s.bctags[ilat - 1] != 6) continue;
+    par_for(1, nz, [&](int k) {
+      for (int l = 1; l <= ng; ++l)
+        for (int i = 1; i <= nx; ++i) {
+          const int js = (ilat == 3) ? l : ny + 1 - l;
+          const int jg = (ilat == 3) ? 1 - l : ny + l;
+          double rho = W(i, js, k, 0);
+          double uu = W(i, js, k, 1) / rho;
+          double vv = W(i, js, k, 2) / rho;
+          double ww = W(i, js, k, 3) / rho;
+          double rhoe = W(i, js, k, 4);
+          double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+          double ee = rhoe / rho - qq;
+          double tt = t0 + (ee - cvl * t0) / cv0;
+          double pp = rho * tt * rgas0;
+          tt = 2.0 * twall - tt;
+          ee = (cvl + cv0 * (tt / t0 - 1.0)) * t0;
+          rho = pp / tt / rgas0;
+          W(i, jg, k, 0) = rho;
+          W(i, jg, k, 1) = -rho * uu;
+          W(i, jg, k, 2) = -rho * vv;
+          W(i, jg, k, 3) = -rho * ww;
+          W(i, jg, k, 4) = rho * (ee + qq);
+        }
+    });
+  }
+  if (do_swap == 1) bcswap();
+}
+
+// eval_aux_subroutine (kernels_cpu.F90:6960-7011), calorically perfect gas
+void Solver::eval_aux(int i0, int i1, int j0, int j1, int k0, int k1) {
+  const double t0 = s.t0, rgas0 = s.rgas0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
+  const double mu0 = s.mu0, vtexp = s.powerlaw_vtexp, ss = s.sutherland_s, trd = s.t_ref_dim;
+  const int vm = s.visc_model;
+  par_for(k0, k1, [&](int k) {
+    for (int j = j0; j <= j1; ++j)
+      for (int i = i0; i <= i1; ++i) {
+        double rho = W(i, j, k, 0), rhou = W(i, j, k, 1), rhov = W(i, j, k, 2), rhow = W(i, j, k, 3),
+               rhoe = W(i, j, k, 4);
+        double ri = 1.0 / rho;
+        double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
+        double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        double ee = rhoe / rho - qq;
+        double tt = t0 + (ee - cvl * t0) / cv0;
+        double pp = rho * tt * rgas0;
+        A(i, j, k, 1) = rho;
+        A(i, j, k, 2) = uu;
+        A(i, j, k, 3) = vv;
+        A(i, j, k, 4) = ww;
+        A(i, j, k, 5) = (rhoe + pp) / rho;
+        A(i, j, k, 6) = tt;
+        double mu = 0.0;
+        if (vm == 1)
+          mu = mu0 * std::pow(tt / t0, vtexp);
+        else if (vm == 2)
+          mu = mu0 * std::pow(tt / t0, 1.5) * (1.0 + ss / trd) / (tt / t0 + ss / trd);
+        A(i, j, k, 7) = mu;
+      }
+  });
+}
+
+// compute_aux (singleideal_cpu.F90:281-330)
+void Solver::compute_aux(int central, int ghost) {
+  if (central == 1 && ghost == 1) {
+    eval_aux(1 - ng, nx + ng, 1 - ng, ny + ng, 1 - ng, nz + ng);
+  } else if (central == 1 && ghost == 0) {
+    eval_aux(1, nx, 1, ny, 1, nz);
+  } else if (central == 0 && ghost == 1) {
+    eval_aux(1 - ng, 0, 1 - ng, ny + ng, 1 - ng, nz + ng);
+    eval_aux(nx + 1, nx + ng, 1 - ng, ny + ng, 1 - ng, nz + ng);
+    eval_aux(1 - ng, nx + ng, 1 - ng, 0, 1 - ng, nz + ng);
+    eval_aux(1 - ng, nx + ng, ny + 1, ny + ng, 1 - ng, nz + ng);
+    eval_aux(1 - ng, nx + ng, 1 - ng, ny + ng, 1 - ng, 0);
+    eval_aux(1 - ng, nx + ng, 1 - ng, ny + ng, nz + 1, nz + ng);
+  }
+}
+
+// Hybrid convective flux at one face (euler_x_fluxes_hybrid_kernel kernels_cpu.F90:425-689,
+// euler_z_hybrid_kernel :1063-1325, euler_y_hybrid_kernel :1808-2071).  The face lies between
+// the point (i,j,k) and its neighbour +1 along dir.
+void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
+  const int ex = dir == 0, ey = dir == 1, ez = dir == 2;
+  auto at = [&](int o, int m) { return A(i + o * ex, j + o * ey, k + o * ez, m); };
+  const int pos = dir == 0 ? i : (dir == 1 ? j : k);
+  const int nd = dir == 0 ? nx : (dir == 1 ? ny : nz);
+  const int ws = s.weno_scheme;
+  const double rgas0 = s.rgas0;
+  int ishk = 0;
+  for (int o = -ws + 1; o <= ws; ++o)
+    if (at(o, 8) > s.sensor_threshold) ishk = 1;
+  const int epo = s.ep_ord[dir][pos];
+  if (ishk == 0) {
+    double ft1 = 0, ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
+    const int lmax = std::max(s.ep_order / 2 + epo, 1);
+    for (int l = 1; l <= lmax; ++l) {
+      double uvs1 = 0, uvs2 = 0, uvs3 = 0, uvs4 = 0, uvs5 = 0, uvs5_i = 0, uvs5_k = 0, uvs5_p = 0, uvs6 = 0;
+      for (int m = 0; m <= l - 1; ++m) {
+        double rhoi = at(-m, 1), uui = at(-m, 2), vvi = at(-m, 3), wwi = at(-m, 4), enti = at(-m, 5),
+               tti = at(-m, 6);
+        double ppi = tti * rhoi * rgas0;
+        double rhoip = at(-m + l, 1), uuip = at(-m + l, 2), vvip = at(-m + l, 3), wwip = at(-m + l, 4),
+               entip = at(-m + l, 5), ttip = at(-m + l, 6);
+        double ppip = ttip * rhoip * rgas0;
+        const double vni = dir == 0 ? uui : (dir == 1 ? vvi : wwi);
+        const double vnip = dir == 0 ? uuip : (dir == 1 ? vvip : wwip);
+        double rhom = rhoi + rhoip;
+        if (s.nkeep >= 0) {
+          double eei = enti - ppi / rhoi - 0.5 * (uui * uui + vvi * vvi + wwi * wwi);
+          double eeip = entip - ppip / rhoip - 0.5 * (uuip * uuip + vvip * vvip + wwip * wwip);
+          double eem = eei + eeip;
+          double drhof = 1.0, deef = 1.0;
+          if (s.nkeep != 0) {
+            double sumnumrho = 1.0;
+            double drho = 2.0 * (rhoip - rhoi) / rhom;
+            double dee = 2.0 * (eeip - eei) / eem;
+            double t_sumdenrho = (0.5 * drho) * (0.5 * drho);
+            double t_sumdenee = (0.5 * dee) * (0.5 * dee);
+            double t2_sumdenrho = t_sumdenrho, t2_sumdenee = t_sumdenee;
+            double sumdenrho = 1.0 + t_sumdenrho / 3.0;
+            double sumdenee = 1.0 + t_sumdenee;
+            double sumnumee = 1.0 + t_sumdenee / 3.0;
+            for (int n = 2; n <= s.nkeep; ++n) {
+              int n2 = 2 * n;
+              t_sumdenrho = t2_sumdenrho * t_sumdenrho;
+              t_sumdenee = t2_sumdenee * t_sumdenee;
+              sumdenrho = sumdenrho + t_sumdenrho / (1.0 + n2);
+              sumdenee = sumdenee + t_sumdenee;
+              sumnumee = sumnumee + t_sumdenee / (1.0 + n2);
+            }
+            drhof = sumnumrho / sumdenrho;
+            deef = sumnumee / sumdenee;
+          }
+          double uv_part = (vni + vnip) * rhom * drhof;
+          uvs1 = uvs1 + uv_part * 2.0;
+          uvs2 = uvs2 + uv_part * (uui + uuip);
+          uvs3 = uvs3 + uv_part * (vvi + vvip);
+          uvs4 = uvs4 + uv_part * (wwi + wwip);
+          uvs5_i = uvs5_i + uv_part * eem * deef;
+          uvs5_k = uvs5_k + uv_part * (uui * uuip + vvi * vvip + wwi * wwip);
+          uvs5_p = uvs5_p + 4.0 * (vni * ppip + vnip * ppi);
+          uvs6 = uvs6 + 2.0 * (ppi + ppip);
+        } else {
+          double uv_part = (vni + vnip) * rhom;
+          uvs1 = uvs1 + uv_part * 2.0;
+          uvs2 = uvs2 + uv_part * (uui + uuip);
+          uvs3 = uvs3 + uv_part * (vvi + vvip);
+          uvs4 = uvs4 + uv_part * (wwi + wwip);
+          uvs5 = uvs5 + uv_part * (enti + entip);
+          uvs6 = uvs6 + 2.0 * (ppi + ppip);
+        }
+      }
+      const double cl = s.coeff_deriv1[lmax - 1][l - 1];
+      ft1 = ft1 + cl * uvs1;
+      ft2 = ft2 + cl * uvs2;
+      ft3 = ft3 + cl * uvs3;
+      ft4 = ft4 + cl * uvs4;
+      if (s.nkeep >= 0)
+        ft5 = ft5 + cl * (uvs5_i + uvs5_k + uvs5_p);
+      else
+        ft5 = ft5 + cl * uvs5;
+      ft6 = ft6 + cl * uvs6;
+    }
+    fh[0] = 0.25 * ft1;
+    fh[1] = 0.25 * ft2;
+    fh[2] = 0.25 * ft3;
+    fh[3] = 0.25 * ft4;
+    fh[4] = 0.25 * ft5;
+    if ((pos == 0 && s.force_zero_flux[2 * dir] == 1) || (pos == nd && s.force_zero_flux[2 * dir + 1] == 1))
+      for (int m = 0; m < 5; ++m) fh[m] = 0.0;
+    fh[1 + dir] = fh[1 + dir] + 0.5 * ft6;
+  } else {
+    // compute_roe_average (kernels_cpu.F90:3013-3089), calorically perfect gas
+    double uu = at(0, 2), vv = at(0, 3), ww = at(0, 4);
+    double h = at(0, 5);
+    double up = at(1, 2), vp = at(1, 3), wp = at(1, 4);
+    double hp = at(1, 5);
+    double r = at(1, 1) / at(0, 1);
+    r = std::sqrt(r);
+    double rho = r * at(0, 1);
+    double rp1 = 1.0 / (r + 1.0);
+    uu = (r * up + uu) * rp1;
+    vv = (r * vp + vv) * rp1;
+    ww = (r * wp + ww) * rp1;
+    h = (r * hp + h) * rp1;
+    double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+    double hbar = h - qq - s.cp_coeff[1] * s.t0;
+    double tt = s.t0 + hbar / s.cp_coeff[0];
+    double gamloc = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
+    double cc = gamloc * tt * rgas0;
+    double gm1loc = gamloc - 1.0;
+    double c = std::sqrt(cc);
+    double ci = 1.0 / c;
+    double p_rho = tt * rgas0;
+    double p_e = rho * gm1loc;
+    double etot = h - tt * rgas0;
+    double b3 = etot - rho * p_rho / p_e;
+    double b2 = p_e / (rho * cc);
+    double b1 = p_rho / cc - b2 * (etot - 2.0 * qq);
+    double el[5][5], er[5][5];
+    eigenvectors(dir, b1, b2, b3, uu, vv, ww, c, ci, h, el, er);
+    double evmax[5];
+    for (int m = 0; m < 5; ++m) evmax[m] = -1.0;
+    const int wsz = 2 * ws;
+    for (int l = 1; l <= wsz; ++l) {
+      const int o = l - ws;
+      double vn = at(o, 2 + dir);
+      double t = at(o, 6);
+      double gl = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
+      double cs = std::sqrt(gl * rgas0 * t);
+      evmax[0] = std::max(std::fabs(vn - cs), evmax[0]);
+      evmax[1] = std::max(std::fabs(vn), evmax[1]);
+      evmax[2] = evmax[1];
+      evmax[3] = evmax[1];
+      evmax[4] = std::max(std::fabs(vn + cs), evmax[4]);
+    }
+    double gp[5][8], gm[5][8];
+    for (int l = 1; l <= wsz; ++l) {
+      const int o = l - ws;
+      double rr = at(o, 1), u1 = at(o, 2), v1 = at(o, 3), w1 = at(o, 4), h1 = at(o, 5);
+      double vn = dir == 0 ? u1 : (dir == 1 ? v1 : w1);
+      double rhovn = rr * vn;
+      double pp = rr * at(o, 6) * rgas0;
+      double fi[5];
+      fi[0] = rhovn;
+      fi[1] = u1 * rhovn;
+      fi[2] = v1 * rhovn;
+      fi[3] = w1 * rhovn;
+      fi[1 + dir] = fi[1 + dir] + pp;
+      fi[4] = h1 * rhovn;
+      for (int m = 0; m < 5; ++m) {
+        double wc = 0.0, gc = 0.0;
+        wc = wc + el[0][m] * rr;
+        gc = gc + el[0][m] * fi[0];
+        wc = wc + el[1][m] * rr * u1;
+        gc = gc + el[1][m] * fi[1];
+        wc = wc + el[2][m] * rr * v1;
+        gc = gc + el[2][m] * fi[2];
+        wc = wc + el[3][m] * rr * w1;
+        gc = gc + el[3][m] * fi[3];
+        wc = wc + el[4][m] * (rr * h1 - pp);
+        gc = gc + el[4][m] * fi[4];
+        double cm = 0.5 * (gc + evmax[m] * wc);
+        gp[m][l - 1] = cm;
+        gm[m][l - 1] = gc - cm;
+      }
+    }
+    const int ord = std::max(ws + epo, 1);
+    double fi[5];
+    wenorec_1d(gp, gm, fi, ws, ord, s.weno_version, s.rho0, s.u0);
+    for (int m = 0; m < 5; ++m) {
+      double acc = 0.0;
+      for (int mm = 0; mm < 5; ++mm) acc = acc + er[mm][m] * fi[mm];
+      fh[m] = acc;
+    }
+  }
+}
+
+// euler_x / euler_y / euler_z (singleideal_cpu.F90:674-843) = hybrid flux kernel + update
+// (euler_{x,y,z}_update_subroutine, kernels_cpu.F90:944-963, 991-1010, 1039-1058)
+void Solver::euler(int dir) {
+  int f0, f1;
+  if (dir == 0) { f0 = s.eul_imin - 1; f1 = s.eul_imax; }
+  else if (dir == 1) { f0 = s.eul_jmin - 1; f1 = s.eul_jmax; }
+  else { f0 = s.eul_kmin - 1; f1 = s.eul_kmax; }
+  if (f1 - (f0 + 1) < 0) return;
+  const int i0 = dir == 0 ? f0 : 1, i1 = dir == 0 ? f1 : nx;
+  const int j0 = dir == 1 ? f0 : 1, j1 = dir == 1 ? f1 : ny;
+  const int k0 = dir == 2 ? f0 : 1, k1 = dir == 2 ? f1 : nz;
+  par_for(k0, k1, [&](int k) {
+    for (int j = j0; j <= j1; ++j)
+      for (int i = i0; i <= i1; ++i) {
+        double fh[5];
+        face_flux(dir, i, j, k, fh);
+        for (int m = 0; m < 5; ++m) FH(i, j, k, m + 1) = fh[m];
+      }
+  });
+  const int ex = dir == 0, ey = dir == 1, ez = dir == 2;
+  const int u0i = dir == 0 ? f0 + 1 : 1, u1i = dir == 0 ? f1 : nx;
+  const int u0j = dir == 1 ? f0 + 1 : 1, u1j = dir == 1 ? f1 : ny;
+  const int u0k = dir == 2 ? f0 + 1 : 1, u1k = dir == 2 ? f1 : nz;
+  par_for(u0k, u1k, [&](int k) {
+    for (int j = u0j; j <= u1j; ++j)
+      for (int i = u0i; i <= u1i; ++i) {
+        const double met = dir == 0 ? s.dcsidx[i - 1] : (dir == 1 ? s.detady[j - 1] : s.dzitdz[k - 1]);
+        for (int iv = 1; iv <= 5; ++iv)
+          FL(i, j, k, iv) = FL(i, j, k, iv) + (FH(i, j, k, iv) - FH(i - ex, j - ey, k - ez, iv)) * met;
+      }
+  });
+}
+
+// visflx_reduced_ord2_subroutine (kernels_cpu.F90:4623-4721)
+void Solver::visflx_reduced_ord2(int update_sensor) {
+  const double prandtl = s.prandtl, u0 = s.u0, l0 = s.l0, cploc = s.cp_coeff[0];
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double uu = A(i, j, k, 2), vv = A(i, j, k, 3), ww = A(i, j, k, 4), mu = A(i, j, k, 7);
+        double dxl = 1.0 / (X(i + 1) - X(i - 1));
+        double dyl = 1.0 / (Y(j + 1) - Y(j - 1));
+        double dzl = 1.0 / (Z(k + 1) - Z(k - 1));
+        double ux = dxl * (A(i + 1, j, k, 2) - A(i - 1, j, k, 2));
+        double vx = dxl * (A(i + 1, j, k, 3) - A(i - 1, j, k, 3));
+        double wx = dxl * (A(i + 1, j, k, 4) - A(i - 1, j, k, 4));
+        double mux = dxl * (A(i + 1, j, k, 7) - A(i - 1, j, k, 7));
+        double uy = dyl * (A(i, j + 1, k, 2) - A(i, j - 1, k, 2));
+        double vy = dyl * (A(i, j + 1, k, 3) - A(i, j - 1, k, 3));
+        double wy = dyl * (A(i, j + 1, k, 4) - A(i, j - 1, k, 4));
+        double ty = dyl * (A(i, j + 1, k, 6) - A(i, j - 1, k, 6));
+        double muy = dyl * (A(i, j + 1, k, 7) - A(i, j - 1, k, 7));
+        double uz = dzl * (A(i, j, k + 1, 2) - A(i, j, k - 1, 2));
+        double vz = dzl * (A(i, j, k + 1, 3) - A(i, j, k - 1, 3));
+        double wz = dzl * (A(i, j, k + 1, 4) - A(i, j, k - 1, 4));
+        double muz = dzl * (A(i, j, k + 1, 7) - A(i, j, k - 1, 7));
+        if (j == 1) {
+          wallprop[(0 * sz + k + ng - 1) * sx + i + ng - 1] = mu * uy;
+          wallprop[(1 * sz + k + ng - 1) * sx + i + ng - 1] = mu * wy;
+          wallprop[(2 * sz + k + ng - 1) * sx + i + ng - 1] = mu * ty * cploc / prandtl;
+        }
+        double div = ux + vy + wz;
+        double div3l = div / 3.0;
+        A(i, j, k, 10) = div3l;
+        double omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
+        double omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
+        A(i, j, k, 9) = std::sqrt(omod2);
+        if (update_sensor == 1) {
+          double t = std::max(-div / std::sqrt(omod2 + div * div + (u0 / l0) * (u0 / l0)), 0.0);
+          A(i, j, k, 8) = t * t;
+        }
+        double sig11 = ux - 2.0 * div3l, sig12 = vx, sig13 = wx;
+        double sig21 = uy, sig22 = vy - 2.0 * div3l, sig23 = wy;
+        double sig31 = uz, sig32 = vz, sig33 = wz - 2.0 * div3l;
+        double sigx = mux * sig11 + muy * sig12 + muz * sig13;
+        double sigy = mux * sig21 + muy * sig22 + muz * sig23;
+        double sigz = mux * sig31 + muy * sig32 + muz * sig33;
+        double sigah = (sig11 * ux + sig12 * uy + sig13 * uz + sig21 * vx + sig22 * vy + sig23 * vz + sig31 * wx +
+                        sig32 * wy + sig33 * wz) *
+                       mu;
+        double sigq = sigx * uu + sigy * vv + sigz * ww + sigah;
+        FL(i, j, k, 2) = FL(i, j, k, 2) - sigx;
+        FL(i, j, k, 3) = FL(i, j, k, 3) - sigy;
+        FL(i, j, k, 4) = FL(i, j, k, 4) - sigz;
+        FL(i, j, k, 5) = FL(i, j, k, 5) - sigq;
+      }
+  });
+}
+
+// visflx_x / _y / _z_subroutine (kernels_cpu.F90:4779-4999): conservative face Laplacian
+void Solver::visflx_faces() {
+  const double prandtl = s.prandtl, cploc = s.cp_coeff[0];
+  // x: face fluxes into fhat(2:5), then the divergence
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 0; i <= nx; ++i) {
+        double uu = A(i, j, k, 2), uup = A(i + 1, j, k, 2), vv = A(i, j, k, 3), vvp = A(i + 1, j, k, 3);
+        double ww = A(i, j, k, 4), wwp = A(i + 1, j, k, 4), tt = A(i, j, k, 6), ttp = A(i + 1, j, k, 6);
+        double mu = A(i, j, k, 7), mup = A(i + 1, j, k, 7);
+        double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        double qqp = 0.5 * (uup * uup + vvp * vvp + wwp * wwp);
+        double sigx = uup - uu, sigy = vvp - vv, sigz = wwp - ww, sigq_tt = ttp - tt, sigq_qq = qqp - qq;
+        double muf = mu + mup;
+        muf = 0.5 * muf / (X(i + 1) - X(i));
+        sigx = sigx * muf;
+        sigy = sigy * muf;
+        sigz = sigz * muf;
+        double sigq = (sigq_tt * cploc / prandtl + sigq_qq) * muf;
+        FH(i, j, k, 2) = -sigx;
+        FH(i, j, k, 3) = -sigy;
+        FH(i, j, k, 4) = -sigz;
+        FH(i, j, k, 5) = -sigq;
+      }
+  });
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double dxhl = 2.0 / (X(i + 1) - X(i - 1));
+        for (int iv = 2; iv <= 5; ++iv) FL(i, j, k, iv) = FL(i, j, k, iv) + dxhl * (FH(i, j, k, iv) - FH(i - 1, j, k, iv));
+      }
+  });
+  // y: carried face flux along j
+  par_for(1, nz, [&](int k) {
+    for (int i = 1; i <= nx; ++i) {
+      double dyhl = 0, fl2o = 0, fl3o = 0, fl4o = 0, fl5o = 0;
+      for (int j = 0; j <= ny; ++j) {
+        double uu = A(i, j, k, 2), uup = A(i, j + 1, k, 2), vv = A(i, j, k, 3), vvp = A(i, j + 1, k, 3);
+        double ww = A(i, j, k, 4), wwp = A(i, j + 1, k, 4), tt = A(i, j, k, 6), ttp = A(i, j + 1, k, 6);
+        double mu = A(i, j, k, 7), mup = A(i, j + 1, k, 7);
+        double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        double qqp = 0.5 * (uup * uup + vvp * vvp + wwp * wwp);
+        double sigx = uup - uu, sigy = vvp - vv, sigz = wwp - ww, sigq_tt = ttp - tt, sigq_qq = qqp - qq;
+        double muf = mu + mup;
+        muf = 0.5 * muf / (Y(j + 1) - Y(j));
+        sigx = sigx * muf;
+        sigy = sigy * muf;
+        sigz = sigz * muf;
+        double sigq = (sigq_tt * cploc / prandtl + sigq_qq) * muf;
+        if (j > 0) {
+          FL(i, j, k, 2) = FL(i, j, k, 2) + fl2o - sigx * dyhl;
+          FL(i, j, k, 3) = FL(i, j, k, 3) + fl3o - sigy * dyhl;
+          FL(i, j, k, 4) = FL(i, j, k, 4) + fl4o - sigz * dyhl;
+          FL(i, j, k, 5) = FL(i, j, k, 5) + fl5o - sigq * dyhl;
+        }
+        if (j < ny) {
+          dyhl = 2.0 / (Y(j + 2) - Y(j));
+          fl2o = sigx * dyhl;
+          fl3o = sigy * dyhl;
+          fl4o = sigz * dyhl;
+          fl5o = sigq * dyhl;
+        }
+      }
+    }
+  });
+  // z: carried face flux along k
+  par_for(1, ny, [&](int j) {
+    for (int i = 1; i <= nx; ++i) {
+      double dzhl = 0, fl2o = 0, fl3o = 0, fl4o = 0, fl5o = 0;
+      for (int k = 0; k <= nz; ++k) {
+        double uu = A(i, j, k, 2), uup = A(i, j, k + 1, 2), vv = A(i, j, k, 3), vvp = A(i, j, k + 1, 3);
+        double ww = A(i, j, k, 4), wwp = A(i, j, k + 1, 4), tt = A(i, j, k, 6), ttp = A(i, j, k + 1, 6);
+        double mu = A(i, j, k, 7), mup = A(i, j, k + 1, 7);
+        double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        double qqp = 0.5 * (uup * uup + vvp * vvp + wwp * wwp);
+        double sigx = uup - uu, sigy = vvp - vv, sigz = wwp - ww, sigq_tt = ttp - tt, sigq_qq = qqp - qq;
+        double muf = mu + mup;
+        muf = 0.5 * muf / (Z(k + 1) - Z(k));
+        sigx = sigx * muf;
+        sigy = sigy * muf;
+        sigz = sigz * muf;
+        double sigq = (sigq_tt * cploc / prandtl + sigq_qq) * muf;
+        if (k > 0) {
+          FL(i, j, k, 2) = FL(i, j, k, 2) + fl2o - sigx * dzhl;
+          FL(i, j, k, 3) = FL(i, j, k, 3) + fl3o - sigy * dzhl;
+          FL(i, j, k, 4) = FL(i, j, k, 4) + fl4o - sigz * dzhl;
+          FL(i, j, k, 5) = FL(i, j, k, 5) + fl5o - sigq * dzhl;
+        }
+        if (k < nz) {
+          dzhl = 2.0 / (Z(k + 2) - Z(k));
+          fl2o = sigx * dzhl;
+          fl3o = sigy * dzhl;
+          fl4o = sigz * dzhl;
+          fl5o = sigq * dzhl;
+        }
+      }
+    }
+  });
+}
+
+// sensor_subroutine (kernels_cpu.F90:4726-4744)
+void Solver::sensor() {
+  const double u0 = s.u0, l0 = s.l0;
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double omod2 = A(i, j, k, 9) * A(i, j, k, 9);
+        double div = 3.0 * A(i, j, k, 10);
+        double t = std::max(-div / std::sqrt(omod2 + div * div + (u0 / l0) * (u0 / l0)), 0.0);
+        A(i, j, k, 8) = t * t;
+      }
+  });
+}
+
+// bcextr_var_subroutine (kernels_cpu.F90:6199-6254)
+void Solver::bcextr_var(int m) {
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int l = 1; l <= ng; ++l) A(1 - l, j, k, m) = A(1, j, k, m);
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int l = 1; l <= ng; ++l) A(nx + l, j, k, m) = A(nx, j, k, m);
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i)
+      for (int l = 1; l <= ng; ++l) A(i, 1 - l, k, m) = A(i, 1, k, m);
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i)
+      for (int l = 1; l <= ng; ++l) A(i, ny + l, k, m) = A(i, ny, k, m);
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i)
+      for (int l = 1; l <= ng; ++l) A(i, j, 1 - l, m) = A(i, j, 1, m);
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i)
+      for (int l = 1; l <= ng; ++l) A(i, j, nz + l, m) = A(i, j, nz, m);
+}
+
+// visflx_div_ord2_subroutine (kernels_cpu.F90:3446-3480)
+void Solver::visflx_div_ord2() {
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double uu = A(i, j, k, 2), vv = A(i, j, k, 3), ww = A(i, j, k, 4), mu = A(i, j, k, 7);
+        double dxl = mu / (X(i + 1) - X(i - 1));
+        double dyl = mu / (Y(j + 1) - Y(j - 1));
+        double dzl = mu / (Z(k + 1) - Z(k - 1));
+        double sigx = dxl * (A(i + 1, j, k, 10) - A(i - 1, j, k, 10));
+        double sigy = dyl * (A(i, j + 1, k, 10) - A(i, j - 1, k, 10));
+        double sigz = dzl * (A(i, j, k + 1, 10) - A(i, j, k - 1, 10));
+        double sigq = sigx * uu + sigy * vv + sigz * ww;
+        FL(i, j, k, 2) = FL(i, j, k, 2) - sigx;
+        FL(i, j, k, 3) = FL(i, j, k, 3) - sigy;
+        FL(i, j, k, 4) = FL(i, j, k, 4) - sigz;
+        FL(i, j, k, 5) = FL(i, j, k, 5) - sigq;
+      }
+  });
+}
+
+// force_rhs (singleideal_cpu.F90:845-889) with force_rhs_1/2 (kernels_cpu.F90:3157-3193, 3092-3116).
+// The oracle sums each k-plane sequentially and then the planes in k order.
+void Solver::force_rhs() {
+  std::vector<double> part(static_cast<size_t>(nz) * 5, 0.0);
+  par_for(1, nz, [&](int k) {
+    double b1 = 0, b2 = 0, b3 = 0, b4 = 0, b5 = 0;
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double dy = s.ynl[j] - s.ynl[j - 1];
+        b1 = b1 + FLN(i, j, k, 1) * dy;
+        b2 = b2 + FLN(i, j, k, 2) * dy;
+        b3 = b3 + W(i, j, k, 0) * dy;
+        b4 = b4 + W(i, j, k, 1) * dy;
+        b5 = b5 + W(i, j, k, 1) * dy * A(i, j, k, 6);
+      }
+    double* p = &part[(k - 1) * 5];
+    p[0] = b1; p[1] = b2; p[2] = b3; p[3] = b4; p[4] = b5;
+  });
+  double bulk[5] = {0, 0, 0, 0, 0};
+  for (int k = 0; k < nz; ++k)
+    for (int m = 0; m < 5; ++m) bulk[m] = bulk[m] + part[k * 5 + m];
+  for (int m = 0; m < 5; ++m) bulk[m] = bulk[m] / s.volchan;
+  dpdx = dpdx + bulk[1];
+  rhobulk = bulk[2];
+  ubulk = bulk[3] / rhobulk;
+  tbulk = bulk[4] / rhobulk / ubulk;
+  const double bulk_1 = bulk[0], bulk_2 = bulk[1];
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double uu = A(i, j, k, 2);
+        FLN(i, j, k, 1) = FLN(i, j, k, 1) - bulk_1;
+        FLN(i, j, k, 2) = FLN(i, j, k, 2) - bulk_2;
+        FLN(i, j, k, 5) = FLN(i, j, k, 5) - uu * bulk_2;
+      }
+  });
+}
+
+// force_var (singleideal_cpu.F90:890-933) with force_var_1/2 (kernels_cpu.F90:3241-3314)
+void Solver::force_var() {
+  if (!(s.theta_wall >= -1.0)) return;
+  const double t0 = s.t0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
+  std::vector<double> part(static_cast<size_t>(nz), 0.0);
+  par_for(1, nz, [&](int k) {
+    double b5 = 0;
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double dy = s.ynl[j] - s.ynl[j - 1];
+        double rho = W(i, j, k, 0), rhou = W(i, j, k, 1), rhov = W(i, j, k, 2), rhow = W(i, j, k, 3),
+               rhoe = W(i, j, k, 4);
+        double ri = 1.0 / rho;
+        double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
+        double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        double ee = rhoe / rho - qq;
+        double tt = t0 + (ee - cvl * t0) / cv0;
+        A(i, j, k, 6) = tt;
+        b5 = b5 + rhou * tt * dy;
+      }
+    part[k - 1] = b5;
+  });
+  double bulkt = 0;
+  for (int k = 0; k < nz; ++k) bulkt = bulkt + part[k];
+  double bulktg = bulkt / s.volchan;
+  bulktg = bulktg / rhobulk / ubulk;
+  double tbdiff = s.t_bulk_target - bulktg;
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double rho = W(i, j, k, 0), rhou = W(i, j, k, 1), rhov = W(i, j, k, 2), rhow = W(i, j, k, 3);
+        double tt = A(i, j, k, 6);
+        double ttnew = tt + tbdiff;
+        double ee = (cvl + cv0 * (ttnew / t0 - 1.0)) * t0;
+        W(i, j, k, 4) = rho * ee + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;
+      }
+  });
+}
+
+// rk_sync (singleideal_cpu.F90:332-409), conservative_viscous = 1, mode_async = 0
+void Solver::rk_sync() {
+  if (s.channel_case) dpdx = 0.0;
+  for (int istep = 1; istep <= s.nrk; ++istep) {
+    const double rhodt = s.rhork[istep - 1] * dt;
+    const double gamdt = s.gamrk[istep - 1] * dt;
+    // init_flux_subroutine (kernels_cpu.F90:29-47)
+    for (size_t q = 0; q < fl.size(); ++q) {
+      fln[q] = -rhodt * fl[q];
+      fl[q] = 0.0;
+    }
+    bcswap();
+    compute_aux(1, 1);
+    euler(0);
+    visflx_reduced_ord2(0);
+    visflx_faces();
+    bcextr_var(10);
+    bcswap_var(10);
+    euler(1);
+    euler(2);
+    if (istep == 3) {
+      sensor();
+      bcswap_var(8);
+    }
+    visflx_div_ord2();
+    // update_flux_subroutine (kernels_cpu.F90:3400-3418)
+    for (size_t q = 0; q < fl.size(); ++q) fln[q] = fln[q] - gamdt * fl[q];
+    if (s.channel_case) force_rhs();
+    // update_field_subroutine (kernels_cpu.F90:3422-3442)
+    par_for(1, nz, [&](int k) {
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i)
+          for (int m = 0; m < 5; ++m) W(i, j, k, m) = W(i, j, k, m) + FLN(i, j, k, m + 1);
+    });
+    if (s.channel_case) force_var();
+    update_ghost(0);
+  }
+}
+
+// compute_dt (singleideal_cpu.F90:1476-1517), compute_dt_subroutine (kernels_cpu.F90:6814-6880)
+void Solver::compute_dt() {
+  if (s.cfl < 0) {
+    dt = -s.cfl;
+    return;
+  }
+  std::vector<double> part(static_cast<size_t>(nz) * 9, 0.0);
+  const double rgas0 = s.rgas0, prandtl = s.prandtl;
+  const double gamloc = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
+  par_for(1, nz, [&](int k) {
+    double mx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double rho = W(i, j, k, 0);
+        double ri = 1.0 / rho;
+        double uu = A(i, j, k, 2), vv = A(i, j, k, 3), ww = A(i, j, k, 4), tt = A(i, j, k, 6), mu = A(i, j, k, 7);
+        double nu = ri * mu;
+        double k_over_rhocp = nu / prandtl;
+        double c = std::sqrt(gamloc * rgas0 * tt);
+        double v[9] = {(std::fabs(uu) + c) * s.dcsidx[i - 1], (std::fabs(vv) + c) * s.detady[j - 1],
+                       (std::fabs(ww) + c) * s.dzitdz[k - 1], nu * s.dcsidxs[i - 1],
+                       nu * s.detadys[j - 1], nu * s.dzitdzs[k - 1],
+                       k_over_rhocp * s.dcsidxs[i - 1], k_over_rhocp * s.detadys[j - 1],
+                       k_over_rhocp * s.dzitdzs[k - 1]};
+        for (int q = 0; q < 9; ++q) mx[q] = std::max(mx[q], v[q]);
+      }
+    for (int q = 0; q < 9; ++q) part[(k - 1) * 9 + q] = mx[q];
+  });
+  double dtinv_max = 0.0;
+  for (size_t q = 0; q < part.size(); ++q) dtinv_max = std::max(dtinv_max, part[q]);
+  double dt_min = 1.0 / dtinv_max;
+  dt = s.cfl * dt_min;
+}
+
+// compute_residual (singleideal_cpu.F90:1339-1364), kernels_cpu.F90:6682-6701, 6765-6810
+void Solver::compute_residual() {
+  std::vector<double> part(static_cast<size_t>(nz), 0.0);
+  par_for(1, nz, [&](int k) {
+    double r = 0;
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double q = FLN(i, j, k, 2) / dt;
+        r = r + q * q;
+      }
+    part[k - 1] = r;
+  });
+  double res = 0;
+  for (int k = 0; k < nz; ++k) res = res + part[k];
+  double restemp = static_cast<double>(nx) * static_cast<double>(ny) * static_cast<double>(nz);
+  residual_rhou = std::sqrt(res / restemp);
+  rhomin = std::numeric_limits<double>::max();
+  rhomax = -100.0;
+  tmin = rhomin; tmax = -100.0; pmin = rhomin; pmax = -100.0;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double rho = A(i, j, k, 1), tt = A(i, j, k, 6);
+        double pp = rho * tt * s.rgas0;
+        rhomin = std::min(rhomin, rho); rhomax = std::max(rhomax, rho);
+        tmin = std::min(tmin, tt); tmax = std::max(tmax, tt);
+        pmin = std::min(pmin, pp); pmax = std::max(pmax, pp);
+      }
+}
+
+void Solver::init_run() {
+  update_ghost(1);
+  compute_aux(1, 1);
+  visflx_reduced_ord2(1);
+  bcswap_var(8);
+  std::fill(fl.begin(), fl.end(), 0.0);
+  compute_dt();
+}
+
+void Solver::step() {
+  icyc = icyc + 1;
+  if (s.cfl > 0 && (icyc - s.icyc0) % s.iter_dt_recompute == 0) {
+    compute_aux(1, 0);
+    compute_dt();
+  }
+  rk_sync();
+  const bool print = ((icyc - s.icyc0) % s.print_control) == 0;
+  if (print) compute_residual();
+  time = time + dt;
+  if (print) rows.push_back(progress_row());
+}
+
+void Solver::run(int nsteps) {
+  for (int n = 0; n < nsteps; ++n) step();
+}
+
+// print_progress (singleideal_cpu.F90:1695-1732), channel row
+ProgressRow Solver::progress_row() const {
+  ProgressRow r;
+  r.icyc = icyc;
+  r.dt = dt;
+  r.time = time;
+  double res = residual_rhou / (s.u0 * s.u0) / s.rho0 * s.l0;
+  double dp = dpdx / (s.u0 * s.u0) / s.rho0 * s.l0;
+  r.residual_rhou = res;
+  r.dpdx_over_dt = -dp / dt;
+  r.rhobulk = rhobulk; r.ubulk = ubulk; r.tbulk = tbulk;
+  r.rhomin = rhomin; r.rhomax = rhomax; r.tmin = tmin; r.tmax = tmax; r.pmin = pmin; r.pmax = pmax;
+  return r;
+}
+
+}  // namespace streams_oracle

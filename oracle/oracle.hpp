@@ -1,0 +1,94 @@
+// CPU oracle (test infrastructure, not product code).
+//
+// A C++ restatement of STREAmS-2's pure-MPI CPU backend for the Cartesian per-Runge-Kutta-stage
+// right-hand side and update, on one block (the MPI halo exchange becomes a periodic copy):
+//   control flow : code/src/singleideal/singleideal_cpu.F90 (run, rk_sync, force_rhs, force_var,
+//                  update_ghost, compute_dt, compute_residual, print_progress, visflx, compute_aux)
+//   arithmetic   : code/src/singleideal/kernels_cpu.F90 (each routine below cites its lines)
+//   ghost fills  : code/src/base_cpu.F90 bcswap / bcswap_var (face halos only, no corners)
+// The case set-up (grid, parameters, initial field) comes from the package's host set-up code
+// (streams-2_b200/csrc/host/setup.cpp); the golden progress row of the reference's own
+// regression suite (tests/tests.ini, subsonic_channel) pins set-up and time advance together.
+//
+// Only tests/, the smoke check and bench.py's CPU-baseline leg use this code, as the checker.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "setup.hpp"
+
+namespace streams_oracle {
+
+using streams_b200::Setup;
+
+struct ProgressRow {
+  int icyc;
+  double dt, time, residual_rhou, dpdx_over_dt, rhobulk, ubulk, tbulk, rhomin, rhomax, tmin, tmax, pmin, pmax;
+};
+
+class Solver {
+ public:
+  explicit Solver(const Setup& s);
+
+  // run() preamble (singleideal_cpu.F90:1542-1557 and the first compute_dt)
+  void init_run();
+  // one iteration of the integration loop (singleideal_cpu.F90:1576-1637, cfl > 0 path)
+  void step();
+  // integration loop for n steps; appends a progress row at every print_control step
+  void run(int nsteps);
+
+  void compute_aux(int central, int ghost);
+  void compute_dt();
+  void rk_sync();
+  void compute_residual();
+  ProgressRow progress_row() const;
+
+  // state (Fortran layouts)
+  const Setup& s;
+  int nx, ny, nz, ng, sx, sy, sz;
+  std::vector<double> w;      // w(1-ng:nx+ng,1-ng:ny+ng,1-ng:nz+ng,5)
+  std::vector<double> w_aux;  // w_aux(...,10)
+  std::vector<double> fl, fln;  // (nx,ny,nz,5)
+  std::vector<double> fhat;   // (1-ng:..., 5)
+  std::vector<double> wallprop;  // (1-ng:nx+ng,1-ng:nz+ng,2:4)
+  double dt = 0, time = 0, dpdx = 0, rhobulk = 0, ubulk = 0, tbulk = 0;
+  double residual_rhou = 0, rhomin = 0, rhomax = 0, tmin = 0, tmax = 0, pmin = 0, pmax = 0;
+  int icyc = 0;
+  std::vector<ProgressRow> rows;
+
+  size_t gi(int i, int j, int k) const {
+    return (static_cast<size_t>(k + ng - 1) * sy + (j + ng - 1)) * sx + (i + ng - 1);
+  }
+  size_t ncg() const { return static_cast<size_t>(sx) * sy * sz; }
+  double& W(int i, int j, int k, int m) { return w[m * ncg() + gi(i, j, k)]; }
+  double& A(int i, int j, int k, int m) { return w_aux[(m - 1) * ncg() + gi(i, j, k)]; }
+  double A(int i, int j, int k, int m) const { return w_aux[(m - 1) * ncg() + gi(i, j, k)]; }
+  double& FH(int i, int j, int k, int m) { return fhat[(m - 1) * ncg() + gi(i, j, k)]; }
+  size_t ii(int i, int j, int k) const { return (static_cast<size_t>(k - 1) * ny + (j - 1)) * nx + (i - 1); }
+  size_t nint_() const { return static_cast<size_t>(nx) * ny * nz; }
+  double& FL(int i, int j, int k, int m) { return fl[(m - 1) * nint_() + ii(i, j, k)]; }
+  double& FLN(int i, int j, int k, int m) { return fln[(m - 1) * nint_() + ii(i, j, k)]; }
+
+  // grid accessors (1-based, ghosts included)
+  double X(int i) const { return s.x[i + ng - 1]; }
+  double Y(int j) const { return s.y[j + ng - 1]; }
+  double Z(int k) const { return s.z[k + ng - 1]; }
+
+ private:
+  void bcswap();
+  void bcswap_var(int m);
+  void update_ghost(int do_swap);
+  void eval_aux(int i0, int i1, int j0, int j1, int k0, int k1);
+  void euler(int dir);
+  void visflx_reduced_ord2(int update_sensor);
+  void visflx_faces();
+  void sensor();
+  void bcextr_var(int m);
+  void visflx_div_ord2();
+  void force_rhs();
+  void force_var();
+  void face_flux(int dir, int i, int j, int k, double fh[5]) const;
+};
+
+}  // namespace streams_oracle

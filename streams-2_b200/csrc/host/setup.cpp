@@ -1,0 +1,790 @@
+// Host-side case set-up; see setup.hpp.  Each function cites the reference routine it
+// restates (paths relative to the STREAmS-2 repository).
+#include "setup.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <sstream>
+
+namespace streams_b200 {
+
+namespace {
+
+constexpr int GRID_FROMFILE = 1, GRID_UNIFORM = 2, GRID_CHA = 3;
+constexpr double TOL_ITER = 0.000000001;  // parameters.F90:43 (REAL64 build)
+
+double pi() { return std::acos(-1.0); }
+
+// get_deriv_coeffs (code/src/grid.F90:143-190)
+void get_deriv_coeffs(double c1[4], double c2[5], int order1, int order2) {
+  for (int l = 0; l < 4; ++l) c1[l] = 0;
+  for (int l = 0; l < 5; ++l) c2[l] = 0;
+  switch (order1 / 2) {
+    case 1: c1[0] = 0.5; break;
+    case 2: c1[0] = 2.0 / 3.0; c1[1] = -1.0 / 12.0; break;
+    case 3: c1[0] = 0.75; c1[1] = -0.15; c1[2] = 1.0 / 60.0; break;
+    case 4: c1[0] = 4.0 / 5.0; c1[1] = -1.0 / 5.0; c1[2] = 4.0 / 105.0; c1[3] = -1.0 / 280.0; break;
+  }
+  switch (order2 / 2) {
+    case 1: c2[0] = -2.0; c2[1] = 1.0; break;
+    case 2: c2[0] = -2.5; c2[1] = 4.0 / 3.0; c2[2] = -1.0 / 12.0; break;
+    case 3: c2[0] = -245.0 / 90.0; c2[1] = 1.5; c2[2] = -0.15; c2[3] = 1.0 / 90.0; break;
+    case 4:
+      c2[0] = -205.0 / 72.0; c2[1] = 8.0 / 5.0; c2[2] = -1.0 / 5.0; c2[3] = 8.0 / 315.0; c2[4] = -1.0 / 560.0;
+      break;
+  }
+}
+
+// get_e_from_temperature (singleideal.F90:2661-2683), calorically perfect branch
+double e_from_t(const Setup& s, double tt) {
+  double ee = s.cv_coeff[1];
+  ee = ee + s.cv_coeff[0] * (tt / s.t0 - 1.0);
+  return ee * s.t0;
+}
+
+// get_gamloc (singleideal.F90:4752-4771), calorically perfect branch
+double gamloc_host(const Setup& s) {
+  double cploc = s.cp_coeff[0];
+  return cploc / (cploc - s.rgas0);
+}
+
+// velpiros_channel (singleideal.F90:3699-3724)
+double velpiros_channel(double yplus, double retau) {
+  double yp = yplus;
+  double eta = yp / retau;
+  eta = std::min(1.0, eta);
+  yp = eta * retau;
+  const double c = 5.3, vkc = 0.39, vkci = 1.0 / vkc;
+  const double c1 = -1.0 / vkc * std::log(vkc) + c;
+  const double etastar = 0.275, b_rich = 0.33, eta_rich = 11.0;
+  double uinn = vkci * std::log(1.0 + vkc * yp) +
+                c1 * (1.0 - std::exp(-yp / eta_rich) - yp / eta_rich * std::exp(-b_rich * yp));
+  double uout = c + vkci * std::log(retau) + vkci * std::log(etastar);
+  uout = uout + (1 - etastar) / (2 * vkc * etastar) * (1 - (1 - eta) * (1 - eta) / ((1 - etastar) * (1 - etastar)));
+  return (eta <= etastar) ? uinn : uout;
+}
+
+std::vector<double> read_column(const std::string& path, size_t n) {
+  std::ifstream f(path);
+  if (!f) throw InputError("cannot open grid file " + path);
+  std::vector<double> v;
+  std::string tok;
+  while (v.size() < n && (f >> tok)) {
+    for (char& c : tok)
+      if (c == 'd' || c == 'D') c = 'e';
+    v.push_back(std::strtod(tok.c_str(), nullptr));
+  }
+  if (v.size() < n) throw InputError("grid file " + path + " is too short");
+  return v;
+}
+
+// generate_grid_uniform_x / _y / _z (code/src/grid.F90:822-876)
+void uniform_grid(OffsetArray& g, int nmax, int ng, double size, bool periodic, int extra) {
+  double d = size / (nmax - 1);
+  if (periodic) d = size / nmax;
+  g.resize(1 - ng, nmax + ng + extra);
+  for (int i = 1 - ng; i <= nmax + ng + extra; ++i) g(i) = (i - 1) * d;
+}
+
+// generate_grid_cha (code/src/grid.F90:431-485)
+void generate_grid_cha(Setup& s, double jbgrid, double dyptarget, int nsmooy, double retaucha) {
+  const int nymax = s.nymax, ng = s.ng, nh = nymax / 2 + 1;
+  double alfc = 4.0 / 3.0 * std::pow(retaucha, 0.75) * 2.0 / nymax;
+  for (int j = 1; j <= nh; ++j) {
+    double rj = static_cast<double>(j - 1);
+    double q = rj / jbgrid;
+    s.yn(j) = 1.0 / (1.0 + q * q);
+    s.yn(j) = s.yn(j) * (rj * dyptarget + std::pow(0.75 * alfc * rj, 4.0 / 3.0) * (q * q));
+  }
+  double ynf = s.yn(nh);
+  for (int j = 1; j <= nh; ++j) s.yn(j) = s.yn(j) / ynf;
+  std::vector<double> ynold(nh + 1);
+  for (int l = 1; l <= nsmooy; ++l) {
+    for (int j = 1; j <= nh; ++j) ynold[j] = s.yn(j);
+    for (int j = 2; j <= nymax / 2; ++j) {
+      double fsm = 6.0 - 2.0 * (std::tanh((s.yn(j) - 0.75) / 0.15) + 1.0) * 0.5;
+      double fsl = 0.5 * (6.0 - fsm);
+      s.yn(j) = fsl * ynold[j - 1] + fsm * ynold[j] + fsl * ynold[j + 1];
+      s.yn(j) = s.yn(j) / 6.0;
+    }
+  }
+  for (int j = 1; j <= nh; ++j) s.yn(j) = s.yn(j) - 1.0;
+  for (int j = 1; j <= nymax / 2; ++j) s.yn(nymax + 2 - j) = -s.yn(j);
+  for (int j = 1; j <= nymax; ++j) s.yg(j) = 0.5 * (s.yn(j) + s.yn(j + 1));
+  for (int j = 1; j <= ng; ++j) {
+    s.yg(nymax + j) = 2.0 - s.yg(nymax + 1 - j);
+    s.yg(1 - j) = -2.0 - s.yg(j);
+  }
+}
+
+// Tanh-stretched staggered channel grid used by the synthetic channel cases:
+// yn(j) = tanh(b*(2(j-1)/ny-1))/tanh(b), cell centres midway, ghosts mirrored about the walls
+// exactly as generate_grid_cha mirrors them.
+void generate_grid_tanh(Setup& s, double b) {
+  const int nymax = s.nymax, ng = s.ng;
+  for (int j = 1; j <= nymax + 1; ++j)
+    s.yn(j) = std::tanh(b * (2.0 * (j - 1) / nymax - 1.0)) / std::tanh(b);
+  for (int j = 1; j <= nymax; ++j) s.yg(j) = 0.5 * (s.yn(j) + s.yn(j + 1));
+  for (int j = 1; j <= ng; ++j) {
+    s.yg(nymax + j) = 2.0 - s.yg(nymax + 1 - j);
+    s.yg(1 - j) = -2.0 - s.yg(j);
+  }
+}
+
+// read_grid (code/src/grid.F90:877-959)
+void read_grid(Setup& s, bool rebuild_ghost) {
+  const int ng = s.ng;
+  int i1 = 1 - ng, i2 = s.nxmax + ng + 1, j1 = 1 - ng, j2 = s.nymax + ng, k1 = 1 - ng, k2 = s.nzmax + ng;
+  if (rebuild_ghost) {
+    i1 = 1; i2 = s.nxmax; j1 = 1; j2 = s.nymax; k1 = 1; k2 = s.nzmax;
+  }
+  auto xv = read_column(s.dir + "/x.dat", i2 - i1 + 1);
+  for (int i = i1; i <= i2; ++i) s.xg(i) = xv[i - i1];
+  auto yv = read_column(s.dir + "/y.dat", j2 - j1 + 1);
+  for (int j = j1; j <= j2; ++j) s.yg(j) = yv[j - j1];
+  auto zv = read_column(s.dir + "/z.dat", k2 - k1 + 1);
+  for (int k = k1; k <= k2; ++k) s.zg(k) = zv[k - k1];
+  std::ifstream ds(s.dir + "/domain_size.dat");
+  if (ds) {
+    ds >> s.domain_size[0] >> s.domain_size[1] >> s.domain_size[2];
+  } else {
+    s.domain_size[0] = s.xg(s.nxmax) - s.xg(1);
+    s.domain_size[1] = s.yg(s.nymax) - s.yg(1);
+    s.domain_size[2] = s.zg(s.nzmax) - s.zg(1);
+  }
+  if (s.is_y_staggered) {
+    auto ynv = read_column(s.dir + "/yn.dat", s.nymax + 1);
+    for (int j = 1; j <= s.nymax + 1; ++j) s.yn(j) = ynv[j - 1];
+  }
+  if (rebuild_ghost) {
+    for (int i = 1; i <= ng; ++i) {
+      s.xg(1 - i) = 2.0 * s.xg(2 - i) - s.xg(3 - i);
+      s.xg(s.nxmax + i) = 2.0 * s.xg(s.nxmax + i - 1) - s.xg(s.nxmax + i - 2);
+    }
+    s.xg(s.nxmax + ng + 1) = 2.0 * s.xg(s.nxmax + ng) - s.xg(s.nxmax + ng - 1);
+    for (int j = 1; j <= ng; ++j) {
+      s.yg(1 - j) = 2.0 * s.yg(2 - j) - s.yg(3 - j);
+      s.yg(s.nymax + j) = 2.0 * s.yg(s.nymax + j - 1) - s.yg(s.nymax + j - 2);
+    }
+    for (int k = 1; k <= ng; ++k) {
+      s.zg(1 - k) = 2.0 * s.zg(2 - k) - s.zg(3 - k);
+      s.zg(s.nzmax + k) = 2.0 * s.zg(s.nzmax + k - 1) - s.zg(s.nzmax + k - 2);
+    }
+  }
+}
+
+// compute_metrics (code/src/grid.F90:71-141) for one direction
+void metrics_1d(const OffsetArray& g, int n, int mm, const double* c, const double* cc, OffsetArray& d,
+                OffsetArray& d2) {
+  d.resize(1, n);
+  d2.resize(1, n);
+  for (int i = 1; i <= n; ++i) {
+    double v = 0.0;
+    for (int l = 1; l <= mm; ++l) v = v + c[l - 1] * (g(i + l) - g(i - l));
+    d(i) = v;
+    double v2 = cc[0] * g(i);
+    for (int l = 1; l <= mm; ++l) v2 = v2 + cc[l] * (g(i + l) + g(i - l));
+    d2(i) = v2;
+  }
+}
+
+// set_fluid_prop (singleideal.F90:2685-2774), calorically perfect gas
+void set_fluid_prop(Setup& s) {
+  const IniFile& c = s.ini;
+  s.t_ref_dim = c.get_double("flow", "T_ref");
+  s.prandtl = c.get_double("fluid", "Prandtl");
+  s.gam = c.get_double("fluid", "gam");
+  s.visc_model = c.get_int("fluid", "visc_model");
+  s.sutherland_s = c.get_double("fluid", "s_suth");
+  s.powerlaw_vtexp = c.get_double("fluid", "vt_exp");
+  s.calorically_perfect = c.get_int("fluid", "calorically_perfect");
+  if (s.calorically_perfect != 1)
+    throw InputError("calorically_perfect = 0 (cp(T) polynomial) is not supported by the B200 backend");
+  s.indx_cp_l = 0;
+  s.indx_cp_r = 0;
+  s.rfac_type = c.get_int_or("fluid", "rfac_type", 0);
+  s.rfac = (s.rfac_type == 0) ? std::pow(s.prandtl, 1.0 / 3.0) : std::pow(s.prandtl, 1.0 / 2.0);
+  s.cp_coeff.assign(2, 0.0);
+  s.cv_coeff.assign(2, 0.0);
+  s.gm1 = s.gam - 1.0;
+  s.gm = 1.0 / s.gm1;
+  s.cv_coeff[0] = s.gm;
+  s.cp_coeff[0] = s.gm * s.gam;
+  double bcoeff = s.cv_coeff[0] + 1.0;
+  s.cp_coeff[1] = bcoeff;
+  s.cv_coeff[1] = bcoeff - 1.0;
+  for (auto& v : s.cv_coeff) v = v * s.rgas0;
+  for (auto& v : s.cp_coeff) v = v * s.rgas0;
+}
+
+struct ChanPre {
+  double rmb, tw_over_tr;
+};
+
+// first part of set_chan_prop (singleideal.F90:2894-2940)
+ChanPre chan_prop_pre(Setup& s) {
+  s.t_wall = s.t0;
+  double rmb, rmtw, trec_over_tb, tw_over_tb, tb_over_tw, tw_over_tr = 0;
+  if (s.theta_wall >= -1.0) {
+    double thtmp = s.theta_wall;
+    rmb = s.mach;
+    double gamloc = s.gam;
+    for (int l = 1; l <= 50; ++l) {
+      double gamlocold = gamloc;
+      double gamlocgm1 = gamloc - 1.0;
+      trec_over_tb = 1.0 + gamlocgm1 / 2.0 * s.rfac * (rmb * rmb);
+      tw_over_tb = 1.0 + thtmp * (trec_over_tb - 1.0);
+      tb_over_tw = 1.0 / tw_over_tb;
+      tw_over_tr = 1.0 / (trec_over_tb * tb_over_tw);
+      s.t_bulk_target = tb_over_tw * s.t_wall;
+      gamloc = gamloc_host(s);
+      if (std::fabs(gamloc - gamlocold) < 1.0e-9) break;
+    }
+    rmtw = rmb * std::sqrt(tb_over_tw);
+    s.mach = rmtw;
+  } else {
+    double thtmp = -1.0;
+    rmtw = s.mach;
+    rmb = std::sqrt(rmtw * rmtw / (1.0 - s.gm1 / 2.0 * s.rfac * thtmp * (rmtw * rmtw)));
+    trec_over_tb = 1.0 + s.gm1 / 2.0 * s.rfac * (rmb * rmb);
+    tw_over_tb = 1.0 + thtmp * (trec_over_tb - 1.0);
+    tb_over_tw = 1.0 / tw_over_tb;
+    tw_over_tr = 1.0 / (trec_over_tb * tb_over_tw);
+  }
+  return {rmb, tw_over_tr};
+}
+
+// set_flow_params (singleideal.F90:2776-2856) for the channel
+void set_flow_params(Setup& s, double reynolds_bulk_target) {
+  const IniFile& c = s.ini;
+  s.reynolds = c.get_double("flow", "Reynolds");
+  s.mach = c.get_double("flow", "Mach");
+  s.theta_wall = c.get_double("flow", "theta_wall");
+  if (s.bctags[3] == 7) throw InputError("oblique-shock top boundary (bc ymax = 7) is not supported yet");
+  double gm1h = 0.5 * s.gm1;
+  s.t_recovery = s.t0 * (1.0 + gm1h * s.rfac * (s.mach * s.mach));
+  s.t_wall = s.theta_wall * (s.t_recovery - s.t0) + s.t0;
+  if (s.flow_init == 0) {
+    ChanPre pre = chan_prop_pre(s);
+    bool visc_exp = (s.visc_model == 1);
+    double s2tinf = s.sutherland_s / s.t_ref_dim;
+    const int nh = s.nymax / 2;
+    std::vector<double> ynh(nh + 1);
+    for (int j = 1; j <= nh + 1; ++j) ynh[j - 1] = s.yn(j);
+    auto rebulk = [&](double retau) {
+      return get_reynolds_cha(retau, pre.rmb, pre.tw_over_tr, s2tinf, s.powerlaw_vtexp, visc_exp, s.gam, s.rfac, nh,
+                              ynh.data());
+    };
+    if (reynolds_bulk_target > 0) {
+      // choose the friction Reynolds number whose bulk Reynolds number is the target
+      double lo = 5.0, hi = 20000.0;
+      for (int it = 0; it < 200; ++it) {
+        double mid = 0.5 * (lo + hi);
+        if (rebulk(mid) < reynolds_bulk_target) lo = mid; else hi = mid;
+        if (hi - lo <= 1e-13 * hi) break;
+      }
+      s.reynolds = 0.5 * (lo + hi);
+    }
+    s.reynolds_friction = s.reynolds;
+    s.reynolds = rebulk(s.reynolds_friction);
+  } else {
+    throw InputError("flow_init other than 0 (channel) is not supported yet");
+  }
+  s.p0 = s.rho0 * s.rgas0 * s.t0;
+  s.c0 = std::sqrt(s.gam * s.rgas0 * s.t0);
+  s.u0 = s.mach * s.c0;
+  double e0 = e_from_t(s, s.t0);
+  double etot0 = e0 + 0.5 * (s.u0 * s.u0);
+  s.s0 = std::log(s.p0 / std::pow(s.rho0, s.gam));
+  s.ttot0 = s.t0 * (1.0 + gm1h * (s.mach * s.mach));
+  s.ptot0 = s.p0 * std::pow(1.0 + gm1h * (s.mach * s.mach), s.gam / s.gm1);
+  s.winf[0] = s.rho0;
+  s.winf[1] = s.rho0 * s.u0 * std::cos(s.aoa);
+  s.winf[2] = s.rho0 * s.u0 * std::sin(s.aoa);
+  s.winf[3] = 0.0;
+  s.winf[4] = s.rho0 * etot0;
+  if (std::fabs(s.u0) < TOL_ITER) {
+    s.mu0 = s.c0 * s.rho0 * s.l0 / s.reynolds;
+    s.u0 = s.c0;
+  } else {
+    s.mu0 = s.u0 * s.rho0 * s.l0 / s.reynolds;
+  }
+}
+
+// init_channel (singleideal.F90:4344-4419) with the per-rank seeding of an MPI run
+void init_channel(Setup& s) {
+  const int nxmax = s.nxmax, nymax = s.nymax, nzmax = s.nzmax;
+  const double lz = s.domain_size[2];
+  double u0_02 = 0.02 * s.u0;
+  if (s.rand_type == 0) u0_02 = 0.0;
+  double u0_05 = 0.05 * s.u0;
+  int nroll = static_cast<int>(lz / s.yn(nymax + 1));
+  const int nxl = nxmax / s.x_split, nyl = nymax / s.y_split, nzl = nzmax / s.z_split;
+  const int nprocs = s.x_split * s.y_split * s.z_split;
+  const double PI = pi();
+  for (int rank = 0; rank < nprocs; ++rank) {
+    // MPI_Cart_create(reorder=false) row-major rank order: the last dimension varies fastest
+    int cx = rank / (s.y_split * s.z_split);
+    int cy = (rank / s.z_split) % s.y_split;
+    int cz = rank % s.z_split;
+    // init_crandom_f(myrank+1) at initialize (singleideal.F90:315-325); rand_type 0 seeds 0 and rescales by 0
+    double rescale = 1.0;
+    if (s.rand_type == 0) {
+      std::srand(0);
+      rescale = 0.0;
+    } else {
+      std::srand(rank + 1);
+    }
+    for (int kl = 1; kl <= nzl; ++kl)
+      for (int jl = 1; jl <= nyl; ++jl)
+        for (int il = 1; il <= nxl; ++il) {
+          const int i = cx * nxl + il, j = cy * nyl + jl, k = cz * nzl + kl;
+          double rho = s.rho0;
+          double yj = s.yg(j);
+          double wm2 = 1.5 * s.rho0 * s.u0 * (1.0 - (yj / s.l0) * (yj / s.l0));
+          double uu = wm2 / rho, vv = 0.0 / rho, ww = 0.0 / rho;
+          double rr[3];
+          for (int l = 0; l < 3; ++l) {
+            int ir = std::rand();
+            rr[l] = rescale * static_cast<double>(ir) / RAND_MAX;
+            rr[l] = rr[l] - 0.5;
+          }
+          double ufluc = u0_02 * rr[0], vfluc = u0_02 * rr[1], wfluc = u0_02 * rr[2];
+          double zk = s.zg(k);
+          vfluc = vfluc + u0_05 * std::sin(0.5 * PI * yj / s.l0) * std::cos(2 * PI * zk / lz * nroll);
+          wfluc = wfluc + u0_05 * std::sin(0.5 * PI * yj / s.l0) * std::sin(2 * PI * zk / lz * nroll);
+          uu = uu + ufluc;
+          vv = vv + vfluc;
+          ww = ww + wfluc;
+          double rhouu = rho * uu, rhovv = rho * vv, rhoww = rho * ww;
+          s.w[s.widx(i, j, k, 0)] = rho;
+          s.w[s.widx(i, j, k, 1)] = rhouu;
+          s.w[s.widx(i, j, k, 2)] = rhovv;
+          s.w[s.widx(i, j, k, 3)] = rhoww;
+          double tt = s.p0 / s.rgas0 / rho;
+          double ee = e_from_t(s, tt);
+          s.w[s.widx(i, j, k, 4)] = rho * ee + 0.5 * (rhouu * rhouu + rhovv * rhovv + rhoww * rhoww) / rho;
+        }
+  }
+}
+
+// Synthetic channel field: Poiseuille u (peak 1.5 u0), v = w = 0, rho = rho0, T = T_wall,
+// plus uniform random perturbations of +-amp*u0 on u, v, w from glibc rand (seed), drawn in
+// k, j, i order, three per cell.
+void init_channel_synthetic(Setup& s, double amp, int seed) {
+  std::srand(seed);
+  for (int k = 1; k <= s.nzmax; ++k)
+    for (int j = 1; j <= s.nymax; ++j)
+      for (int i = 1; i <= s.nxmax; ++i) {
+        double rr[3];
+        for (int l = 0; l < 3; ++l) rr[l] = 2.0 * (static_cast<double>(std::rand()) / RAND_MAX) - 1.0;
+        double rho = s.rho0;
+        double yj = s.yg(j) / s.l0;
+        double uu = 1.5 * s.u0 * (1.0 - yj * yj) + amp * s.u0 * rr[0];
+        double vv = amp * s.u0 * rr[1];
+        double ww = amp * s.u0 * rr[2];
+        double rhouu = rho * uu, rhovv = rho * vv, rhoww = rho * ww;
+        double ee = e_from_t(s, s.t_wall);
+        s.w[s.widx(i, j, k, 0)] = rho;
+        s.w[s.widx(i, j, k, 1)] = rhouu;
+        s.w[s.widx(i, j, k, 2)] = rhovv;
+        s.w[s.widx(i, j, k, 3)] = rhoww;
+        s.w[s.widx(i, j, k, 4)] = rho * ee + 0.5 * (rhouu * rhouu + rhovv * rhovv + rhoww * rhoww) / rho;
+      }
+}
+
+// read_field (code/src/field.F90:1853-1905): rst.bin = nv global arrays, Fortran order, native REAL64
+void read_rst(Setup& s) {
+  const std::string path = s.dir + "/rst.bin";
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) throw InputError("cannot open " + path);
+  std::vector<double> plane(static_cast<size_t>(s.nxmax));
+  for (int m = 0; m < 5; ++m)
+    for (int k = 1; k <= s.nzmax; ++k)
+      for (int j = 1; j <= s.nymax; ++j) {
+        if (std::fread(plane.data(), sizeof(double), plane.size(), f) != plane.size()) {
+          std::fclose(f);
+          throw InputError("rst.bin is too short");
+        }
+        for (int i = 1; i <= s.nxmax; ++i) s.w[s.widx(i, j, k, m)] = plane[i - 1];
+      }
+  std::fclose(f);
+}
+
+void read_field_info(Setup& s) {
+  IniFile fi = IniFile::parse_file(s.dir + "/field_info0.dat");
+  s.icyc0 = fi.get_int("field_info", "icyc0");
+  s.time0 = fi.get_double("field_info", "time0");
+}
+
+}  // namespace
+
+// get_reynolds_cha (singleideal.F90:3052-3172), itransf = 0
+double get_reynolds_cha(double retau, double rm, double trat, double s2tinf, double vtexp, bool visc_exp, double gam,
+                        double rfac, int ny, const double* yn_in) {
+  const int N = ny + 1;
+  auto yn = [&](int j) { return yn_in[j - 1]; };
+  double gm1h = 0.5 * (gam - 1.0);
+  double tr = 1.0 + gm1h * rfac * (rm * rm);
+  double tw = trat * tr;
+  std::vector<double> yplus(N + 1, 0.0), uplus(N + 1, 0.0), ycplus(N + 1, 0.0), ucplus(N + 1, 0.0),
+      yplusold(N + 1, 0.0), ucplusold(N + 1, 0.0), density(N + 1, 0.0), viscosity(N + 1, 0.0),
+      temperature(N + 1, 0.0), uu(N + 1, 0.0);
+  for (int j = 2; j <= N; ++j) ycplus[j] = (yn(j) - yn(1)) / (yn(N) - yn(1)) * retau;
+  yplus = ycplus;
+  yplusold = yplus;
+  for (int outer = 0; outer < 100000; ++outer) {
+    for (int j = 1; j <= N; ++j) uplus[j] = 0.0;
+    for (int j = 2; j <= N; ++j) uplus[j] = velpiros_channel(yplus[j], retau);
+    ucplus = uplus;
+    for (int inner = 0; inner < 100000; ++inner) {
+      ucplusold = ucplus;
+      for (int j = 1; j <= N; ++j) {
+        uu[j] = ucplus[j] / ucplus[ny];
+        double fuu = uu[j];
+        temperature[j] = tw + (tr - tw) * fuu + (1.0 - tr) * (uu[j] * uu[j]);
+        density[j] = 1.0 / temperature[j];
+        if (visc_exp)
+          viscosity[j] = std::pow(temperature[j], vtexp);
+        else
+          viscosity[j] = std::pow(temperature[j], 1.5) * (1.0 + s2tinf) / (temperature[j] + s2tinf);
+      }
+      for (int j = 2; j <= N; ++j) {
+        double du = uplus[j] - uplus[j - 1];
+        double rhow_over_rho = density[1] / density[j];
+        double rhow_over_rhojm = density[1] / density[j - 1];
+        double rmu_over_rmuw = viscosity[j] / viscosity[1];
+        double rmu_over_rmuwjm = viscosity[j - 1] / viscosity[1];
+        double ucij = std::sqrt(rhow_over_rho) * std::sqrt(rmu_over_rmuw);
+        double ucijm = std::sqrt(rhow_over_rhojm) * std::sqrt(rmu_over_rmuwjm);
+        ucplus[j] = ucplus[j - 1] + 0.5 * (ucij + ucijm) * du;
+      }
+      double res = 0.0;
+      for (int j = 1; j <= N; ++j) res = res + std::fabs(ucplus[j] - ucplusold[j]);
+      res = res / N;
+      if (res < TOL_ITER) break;
+    }
+    for (int j = 1; j <= N; ++j) yplus[j] = 0.0;
+    for (int j = 2; j <= N; ++j) {
+      double dy = ycplus[j] - ycplus[j - 1];
+      double rhow_over_rho = density[1] / density[j];
+      double rhow_over_rhojm = density[1] / density[j - 1];
+      double rmu_over_rmuw = viscosity[j] / viscosity[1];
+      double rmu_over_rmuwjm = viscosity[j - 1] / viscosity[1];
+      double r3 = rmu_over_rmuw * rmu_over_rmuw * rmu_over_rmuw;
+      double r3m = rmu_over_rmuwjm * rmu_over_rmuwjm * rmu_over_rmuwjm;
+      double ycij = std::sqrt(rhow_over_rho) * std::sqrt(r3);
+      ycij = 1.0 / ycij;
+      double ycijm = std::sqrt(rhow_over_rhojm) * std::sqrt(r3m);
+      ycijm = 1.0 / ycijm;
+      yplus[j] = yplus[j - 1] + 0.5 * (ycij + ycijm) * dy;
+    }
+    // the reference overwrites (does not accumulate) res in this loop: only j = ny+1 counts
+    double res = 0.0;
+    for (int j = 1; j <= N; ++j) res = std::fabs(yplus[j] - yplusold[j]);
+    res = res / N;
+    if (res < TOL_ITER) break;
+    yplusold = yplus;
+  }
+  double rhosum = 0.0, rhousum = 0.0, ysum = 0.0;
+  for (int j = 1; j <= ny; ++j) {
+    double dy = yn(j + 1) - yn(j);
+    ysum = ysum + dy;
+    rhosum = rhosum + 0.5 * (density[j] + density[j + 1]) * dy;
+    rhousum = rhousum + 0.5 * (density[j] * ucplus[j] + density[j + 1] * ucplus[j + 1]) * dy;
+  }
+  rhosum = rhosum / ysum;
+  rhousum = rhousum / ysum;
+  double ubulk = rhousum / rhosum;
+  return retau * ubulk * rhosum / density[1];
+}
+
+Setup setup_from_dir(const std::string& dir) {
+  return setup_from_ini(IniFile::parse_file(dir + "/singleideal.ini"), dir);
+}
+
+Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
+  Setup s;
+  s.ini = ini;
+  s.dir = dir;
+  const IniFile& c = s.ini;
+
+  // equation initialize (singleideal.F90:284-864), Cartesian subset
+  s.rand_type = c.get_int("numerics", "rand_type");
+  s.l0 = c.get_double_or("ref_prop", "l0", 1.0);
+  s.t0 = c.get_double_or("ref_prop", "t0", 1.0);
+  s.rho0 = c.get_double_or("ref_prop", "rho0", 1.0);
+  s.rgas0 = c.get_double_or("ref_prop", "rgas0", 1.0);
+  int grid_dim = c.get_int_or("grid", "grid_dim", 1);
+  if (grid_dim != 1) throw InputError("grid_dim = 2 (curvilinear) is not supported by the B200 backend");
+  s.flow_init = c.get_int("flow", "flow_init");
+  s.channel_case = (s.flow_init == 0 || s.flow_init == 4);
+  s.aoa = c.get_double_or("flow", "aoa", 0.0) * pi() / 180.0;
+  const char* bcn[6] = {"xmin", "xmax", "ymin", "ymax", "zmin", "zmax"};
+  for (int l = 0; l < 6; ++l) s.bctags[l] = c.get_int("bc", bcn[l]);
+  for (int d = 0; d < 3; ++d) {
+    if (s.bctags[2 * d] == 0 || s.bctags[2 * d + 1] == 0) {
+      s.bctags[2 * d] = s.bctags[2 * d + 1] = 0;
+      s.periodic[d] = true;
+    }
+  }
+  for (int l = 0; l < 6; ++l) s.bctags_nr[l] = c.get_int("bc", std::string(bcn[l]) + "_nr");
+  s.restart_type = c.get_int("controls", "restart_type");
+  s.grid_type = c.get_int("grid", "grid_type");
+  bool rebuild_ghost = (s.grid_type == GRID_FROMFILE);
+  if (s.restart_type > 0) s.grid_type = GRID_FROMFILE;
+  s.nxmax = c.get_int("grid", "nxmax");
+  s.nymax = c.get_int("grid", "nymax");
+  s.nzmax = c.get_int("grid", "nzmax");
+  s.ng = c.get_int("grid", "ng");
+  s.domain_size[0] = c.get_double("grid", "domain_size_x");
+  s.domain_size[1] = c.get_double("grid", "domain_size_y");
+  s.domain_size[2] = c.get_double("grid", "domain_size_z");
+  s.metrics_order = c.get_int("grid", "metrics_order");
+  int ystag = c.get_int_or("grid", "ystag", 0);
+  s.is_y_staggered = (ystag > 0) || s.channel_case;
+  s.ep_order = c.get_int("numerics", "ep_order");
+  if (s.ep_order != s.metrics_order) throw InputError("ep_order must be equal to metrics_order");
+  if (s.nzmax == 1) throw InputError("2D runs (nzmax = 1) are not supported by the B200 backend");
+  s.ndim = 3;
+  if (s.ng < 3) throw InputError("the B200 backend needs ng >= 3");
+
+  const bool synthetic = c.has_section("synthetic");
+
+  // grid%initialize (code/src/grid.F90:192-308)
+  s.xg.resize(1 - s.ng, s.nxmax + s.ng + 1);
+  s.yg.resize(1 - s.ng, s.nymax + s.ng);
+  s.zg.resize(1 - s.ng, s.nzmax + s.ng);
+  s.yn.resize(1, s.nymax + 1 + s.ng);
+  if (s.grid_type == GRID_FROMFILE && !synthetic) {
+    read_grid(s, rebuild_ghost);
+  } else {
+    uniform_grid(s.xg, s.nxmax, s.ng, s.domain_size[0], s.periodic[0], 1);
+    OffsetArray zt;
+    uniform_grid(zt, s.nzmax, s.ng, s.domain_size[2], s.periodic[2], 0);
+    s.zg = zt;
+    if (synthetic && c.has_key("synthetic", "y_stretch")) {
+      generate_grid_tanh(s, c.get_double("synthetic", "y_stretch"));
+    } else if (s.grid_type == GRID_UNIFORM) {
+      OffsetArray yt;
+      uniform_grid(yt, s.nymax, s.ng, s.domain_size[1], s.periodic[1], 0);
+      for (int j = 1 - s.ng; j <= s.nymax + s.ng; ++j) s.yg(j) = yt(j);
+    } else if (s.grid_type == GRID_CHA) {
+      generate_grid_cha(s, c.get_double("grid", "jbgrid"), c.get_double("grid", "dyptarget"),
+                        static_cast<int>(std::lround(c.get_double("grid", "ysmoosteps"))),
+                        c.get_double("flow", "Reynolds"));
+    } else {
+      throw InputError("grid_type " + std::to_string(s.grid_type) + " is not supported by the B200 backend");
+    }
+  }
+  for (auto& v : s.xg.data) v *= s.l0;
+  for (auto& v : s.yg.data) v *= s.l0;
+  for (auto& v : s.zg.data) v *= s.l0;
+  for (auto& v : s.yn.data) v *= s.l0;
+  for (auto& v : s.domain_size) v *= s.l0;
+  {
+    double c1[4], c2[5];
+    get_deriv_coeffs(c1, c2, s.metrics_order, s.metrics_order);
+    const int mm = s.metrics_order / 2;
+    metrics_1d(s.xg, s.nxmax, mm, c1, c2, s.dxg, s.d2xg);
+    metrics_1d(s.yg, s.nymax, mm, c1, c2, s.dyg, s.d2yg);
+    metrics_1d(s.zg, s.nzmax, mm, c1, c2, s.dzg, s.d2zg);
+  }
+
+  // fluid and flow
+  set_fluid_prop(s);
+  double re_bulk_target = synthetic ? c.get_double_or("synthetic", "reynolds_bulk", -1.0) : -1.0;
+  set_flow_params(s, re_bulk_target);
+
+  s.nkeep = c.get_int_or("numerics", "nkeep", 0);
+  s.weno_scheme = c.get_int("numerics", "weno_scheme");
+  if (s.weno_scheme < 1 || s.weno_scheme > 4) throw InputError("weno_scheme must be 1, 2, 3 or 4");
+  s.weno_version = c.get_int("numerics", "weno_version");
+  if (s.weno_scheme != 3 && s.weno_version == 1) throw InputError("weno_version 1 supported only for weno_scheme = 3");
+  s.flux_splitting = c.get_int_or("numerics", "flux_splitting", 0);
+  if (s.flux_splitting != 0) throw InputError("flux_splitting = 1 (Rusanov) is not supported by the B200 backend");
+  s.visc_order = c.get_int("numerics", "visc_order");
+  if (s.visc_order != s.ep_order) throw InputError("viscous order must be equal to ep_order");
+  s.conservative_viscous = c.get_int("numerics", "conservative_viscous");
+  if (s.conservative_viscous != 1)
+    throw InputError("conservative_viscous = 0 is not supported by the B200 backend");
+  for (int i = 0; i < 4; ++i) get_deriv_coeffs(s.coeff_deriv1[i], s.coeff_deriv2[i], 2 * (i + 1), 2 * (i + 1));
+  s.sensor_threshold = c.get_double("numerics", "sensor_threshold");
+  s.x_split = c.get_int("mpi", "x_split");
+  s.y_split = c.get_int("mpi", "y_split");
+  s.z_split = c.get_int("mpi", "z_split");
+  if (s.nxmax % s.x_split || s.nzmax % s.z_split || s.y_split != 1)
+    throw InputError("inconsistent mpi split (nxmax/nzmax multiples of x/z split, y_split = 1)");
+
+  // bc_preproc (singleideal.F90:4703-4750)
+  s.eul_imin = 1; s.eul_imax = s.nxmax; s.eul_jmin = 1; s.eul_jmax = s.nymax; s.eul_kmin = 1; s.eul_kmax = s.nzmax;
+  for (int l = 0; l < 6; ++l) {
+    if (s.bctags[l] == 6 && s.is_y_staggered) {
+      s.force_zero_flux[l] = 1;
+      s.bctags_nr[l] = 0;
+    }
+    int offset = (s.bctags_nr[l] != 0) ? 1 : 0;
+    switch (l) {
+      case 0: s.eul_imin += offset; break;
+      case 1: s.eul_imax -= offset; break;
+      case 2: s.eul_jmin += offset; break;
+      case 3: s.eul_jmax -= offset; break;
+      case 4: s.eul_kmin += offset; break;
+      case 5: s.eul_kmax -= offset; break;
+    }
+  }
+  for (int l = 0; l < 6; ++l) {
+    if (s.bctags[l] != 0 && s.bctags[l] != 6)
+      throw InputError("boundary tag " + std::to_string(s.bctags[l]) + " is not supported by the B200 backend yet");
+    if (s.bctags_nr[l] != 0) throw InputError("non-reflecting boundary treatment is not supported yet");
+  }
+  if (s.bctags[0] == 6 || s.bctags[1] == 6 || s.bctags[4] == 6 || s.bctags[5] == 6)
+    throw InputError("viscous walls are supported on the y boundaries only");
+
+  // correct_bc_order (singleideal.F90:946-993)
+  const int n3[3] = {s.nxmax, s.nymax, s.nzmax};
+  for (int d = 0; d < 3; ++d) s.ep_ord[d].assign(n3[d] + 1, 0);
+  s.correct_bound_ord = c.get_int_or("bc", "correct_bound_ord", 0);
+  if (s.correct_bound_ord > 0) {
+    int st = std::max(s.ep_order / 2, s.weno_scheme);
+    for (int d = 0; d < 3; ++d) {
+      if (s.bctags[2 * d] == 0 && s.bctags[2 * d + 1] == 0) continue;
+      auto& e = s.ep_ord[d];
+      const int n = n3[d];
+      e[0] = -st + 1;
+      for (int i = 1; i <= st - 1; ++i) e[i] = -st + i;
+      e[n] = -st + 1;
+      for (int i = 1; i <= st - 1; ++i) e[n - i] = -st + i;
+    }
+  }
+
+  // runge_kutta_initialize (singleideal.F90:4773-4795)
+  s.rk_type = c.get_int("numerics", "rk_type");
+  if (s.rk_type != 1) throw InputError("only rk_type = 1 (Wray RK3) is supported");
+  s.nrk = 3;
+  s.rhork[0] = 0.0; s.rhork[1] = -17.0 / 60.0; s.rhork[2] = -5.0 / 12.0;
+  s.gamrk[0] = 8.0 / 15.0; s.gamrk[1] = 5.0 / 12.0; s.gamrk[2] = 3.0 / 4.0;
+  s.cfl = c.get_double("controls", "cfl");
+  s.num_iter = c.get_int("controls", "num_iter");
+  s.print_control = c.get_int("output", "print_control");
+  s.iter_dt_recompute = c.get_int("controls", "iter_dt_recompute");
+
+  // local grid of the single block (field.F90 set_local_grid)
+  const int ng = s.ng;
+  s.x.resize(s.nxmax + 2 * ng);
+  s.y.resize(s.nymax + 2 * ng);
+  s.z.resize(s.nzmax + 2 * ng);
+  for (int i = 1 - ng; i <= s.nxmax + ng; ++i) s.x[i + ng - 1] = s.xg(i);
+  for (int j = 1 - ng; j <= s.nymax + ng; ++j) s.y[j + ng - 1] = s.yg(j);
+  for (int k = 1 - ng; k <= s.nzmax + ng; ++k) s.z[k + ng - 1] = s.zg(k);
+  s.ynl.resize(s.nymax + 1);
+  for (int j = 1; j <= s.nymax + 1; ++j) s.ynl[j - 1] = s.yn(j);
+  auto loc = [](const OffsetArray& d, const OffsetArray& d2, int n, std::vector<double>& a, std::vector<double>& as,
+                std::vector<double>& a2) {
+    a.resize(n); as.resize(n); a2.resize(n);
+    for (int i = 1; i <= n; ++i) {
+      a[i - 1] = 1.0 / d(i);
+      as[i - 1] = a[i - 1] * a[i - 1];
+      a2[i - 1] = -d2(i) * as[i - 1];
+    }
+  };
+  loc(s.dxg, s.d2xg, s.nxmax, s.dcsidx, s.dcsidxs, s.dcsidx2);
+  loc(s.dyg, s.d2yg, s.nymax, s.detady, s.detadys, s.detady2);
+  loc(s.dzg, s.d2zg, s.nzmax, s.dzitdz, s.dzitdzs, s.dzitdz2);
+
+  // initial_conditions (singleideal.F90:3018-3051): winf everywhere, then the case initialiser
+  s.w.assign(s.ncells_ghost() * 5, 0.0);
+  for (int m = 0; m < 5; ++m) {
+    const size_t n = s.ncells_ghost();
+    for (size_t q = 0; q < n; ++q) s.w[m * n + q] = s.winf[m];
+  }
+  // volchan (init_channel, singleideal.F90:4364-4366)
+  s.volchan = s.yn(s.nymax + 1) - s.yn(1);
+  s.volchan = s.volchan * s.nxmax;
+  s.volchan = s.volchan * s.nzmax;
+  if (synthetic) {
+    std::string kind = "channel_poiseuille";
+    if (c.has_key("synthetic", "kind")) {
+      std::istringstream is(c.raw("synthetic", "kind"));
+      is >> kind;
+    }
+    if (kind != "channel_poiseuille") throw InputError("unknown synthetic initial field " + kind);
+    init_channel_synthetic(s, c.get_double_or("synthetic", "amp", 0.1), c.get_int_or("synthetic", "seed", 1));
+  } else {
+    init_channel(s);
+    if (s.restart_type == 1) {
+      read_rst(s);
+      read_field_info(s);
+    } else if (s.restart_type == 2) {
+      throw InputError("restart_type = 2 (statistics restart) is not supported by the B200 backend");
+    }
+  }
+  return s;
+}
+
+void Setup::fill_params(streams_b200_params* p, int precision) const {
+  *p = streams_b200_params{};
+  p->nx = nxmax; p->ny = nymax; p->nz = nzmax; p->ng = ng;
+  p->ep_order = ep_order; p->nkeep = nkeep; p->weno_scheme = weno_scheme; p->weno_version = weno_version;
+  p->flux_splitting = flux_splitting; p->conservative_viscous = conservative_viscous;
+  p->sensor_threshold = sensor_threshold;
+  for (int l = 0; l < 6; ++l) {
+    p->bctags[l] = bctags[l];
+    p->force_zero_flux[l] = force_zero_flux[l];
+  }
+  p->eul_imin = eul_imin; p->eul_imax = eul_imax; p->eul_jmin = eul_jmin;
+  p->eul_jmax = eul_jmax; p->eul_kmin = eul_kmin; p->eul_kmax = eul_kmax;
+  p->is_y_staggered = is_y_staggered ? 1 : 0;
+  p->visc_model = visc_model; p->calorically_perfect = calorically_perfect;
+  p->mu0 = mu0; p->t0 = t0; p->rgas0 = rgas0; p->rho0 = rho0; p->u0 = u0; p->l0 = l0;
+  p->sutherland_s = sutherland_s; p->t_ref_dim = t_ref_dim; p->powerlaw_vtexp = powerlaw_vtexp;
+  p->prandtl = prandtl;
+  p->cp0 = cp_coeff[0]; p->cv0 = cv_coeff[0]; p->cp_last = cp_coeff[1]; p->cv_last = cv_coeff[1];
+  p->channel_case = channel_case ? 1 : 0;
+  p->theta_wall = theta_wall; p->t_wall = t_wall; p->t_bulk_target = t_bulk_target; p->volchan = volchan;
+  p->nrk = nrk;
+  for (int l = 0; l < 3; ++l) {
+    p->rhork[l] = rhork[l];
+    p->gamrk[l] = gamrk[l];
+  }
+  p->cfl = cfl;
+  p->precision = precision;
+}
+
+void Setup::fill_grid(streams_b200_grid* g) const {
+  g->x = x.data(); g->y = y.data(); g->z = z.data(); g->yn = ynl.data();
+  g->dcsidx = dcsidx.data(); g->detady = detady.data(); g->dzitdz = dzitdz.data();
+  g->dcsidxs = dcsidxs.data(); g->detadys = detadys.data(); g->dzitdzs = dzitdzs.data();
+  g->coeff_deriv1 = &coeff_deriv1[0][0];
+  g->ep_ord_x = ep_ord[0].data(); g->ep_ord_y = ep_ord[1].data(); g->ep_ord_z = ep_ord[2].data();
+}
+
+void write_restart_inputs(const Setup& s, const std::string& dir) {
+  auto col = [&](const std::string& name, const OffsetArray& a, int lo, int hi) {
+    FILE* f = std::fopen((dir + "/" + name).c_str(), "w");
+    if (!f) throw InputError("cannot write " + dir + "/" + name);
+    for (int i = lo; i <= hi; ++i) std::fprintf(f, "%.17e\n", a(i));
+    std::fclose(f);
+  };
+  col("x.dat", s.xg, 1 - s.ng, s.nxmax + s.ng + 1);
+  col("y.dat", s.yg, 1 - s.ng, s.nymax + s.ng);
+  col("z.dat", s.zg, 1 - s.ng, s.nzmax + s.ng);
+  col("yn.dat", s.yn, 1, s.nymax + 1);
+  FILE* f = std::fopen((dir + "/rst.bin").c_str(), "wb");
+  if (!f) throw InputError("cannot write rst.bin");
+  std::vector<double> plane(static_cast<size_t>(s.nxmax));
+  for (int m = 0; m < 5; ++m)
+    for (int k = 1; k <= s.nzmax; ++k)
+      for (int j = 1; j <= s.nymax; ++j) {
+        for (int i = 1; i <= s.nxmax; ++i) plane[i - 1] = s.w[s.widx(i, j, k, m)];
+        std::fwrite(plane.data(), sizeof(double), plane.size(), f);
+      }
+  std::fclose(f);
+  FILE* fi = std::fopen((dir + "/field_info0.dat").c_str(), "w");
+  std::fprintf(fi, "[field_info]\nicyc0 = %d\ntime0 = %.17e\nitav = 0\nistore = 1\n", s.icyc0, s.time0);
+  std::fclose(fi);
+}
+
+}  // namespace streams_b200
