@@ -179,6 +179,16 @@ int streams_b200_synchronize(streams_b200_ctx* ctx);
 /* Number of kernel launches issued by this context since creation (instrumentation). */
 long long streams_b200_launch_count(const streams_b200_ctx* ctx);
 
+/*
+ * Diagnostics: copy an internal device array to the host (synchronous).  which =
+ *   0  aux fields rho, u, v, w, H, T, mu (7 ghosted arrays, w_aux(:,:,:,1:7))   7*nvol doubles
+ *   1  right-hand side fl of the last completed stage (5 interior arrays)        5*nint doubles
+ *   2  Ducros sensor used by the next stage's fluxes (w_aux(1:nx,1:ny,1:nz,8))    nint doubles
+ *   3  div/3 of the last stage (w_aux(1:nx,1:ny,1:nz,10))                        nint doubles
+ * n is the capacity of out in doubles.
+ */
+int streams_b200_debug_fetch(streams_b200_ctx* ctx, int which, double* out, long long n);
+
 #ifdef __cplusplus
 }
 #endif

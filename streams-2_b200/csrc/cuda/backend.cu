@@ -1,0 +1,463 @@
+// C ABI of the B200 backend: context life cycle, field transfer and the time-advance entry
+// points declared in include/streams_b200.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.hpp"
+#include "streams_b200.h"
+
+using namespace sb200;
+
+struct streams_b200_ctx {
+  streams_b200_params p{};
+  Geom g{};
+  DevState d{};
+  double* fl_a = nullptr;  // RK register written by stages 1 and 3
+  double* fl_b = nullptr;  // RK register written by stage 2
+  double* last_fl = nullptr;  // register written by the last completed stage
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  bool shift_pending = false;  // force_var energy shift not applied to w yet
+  bool aux_current = false;    // aux matches w (no update since the last aux pass)
+  bool have_stats = false;
+  long long launches = 0;
+  std::vector<void*> allocs;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_global_err;
+
+int set_err(streams_b200_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg; else g_global_err = msg;
+  return code;
+}
+
+int cuda_err(streams_b200_ctx* c, cudaError_t e, const char* what) {
+  return set_err(c, STREAMS_B200_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define SB_CHECK(ctx, call)                                   \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_err((ctx), e_, #call); \
+  } while (0)
+
+template <class T>
+cudaError_t dev_alloc(streams_b200_ctx* c, T** p, size_t count) {
+  void* v = nullptr;
+  cudaError_t e = cudaMalloc(&v, count * sizeof(T) > 0 ? count * sizeof(T) : 16);
+  if (e != cudaSuccess) return e;
+  c->allocs.push_back(v);
+  *p = static_cast<T*>(v);
+  return cudaSuccess;
+}
+
+long long footprint(const streams_b200_params* p) {
+  const long long sx = p->nx + 2LL * p->ng, sy = p->ny + 2LL * p->ng, sz = p->nz + 2LL * p->ng;
+  const long long nvol = sx * sy * sz, nint = (long long)p->nx * p->ny * p->nz;
+  long long b = 0;
+  b += nvol * 5 * 8;   // w
+  b += nvol * 7 * 8;   // aux
+  b += nint * 3 * 8;   // sensor, sensor_next, div3
+  b += nint * 10 * 8;  // two RK registers
+  b += (long long)p->nx * p->nz * 3 * 8;
+  b += ((nint + 255) / 256) * 9 * 8 + ((p->nx + 31) / 32) * ((p->nz + 7) / 8) * (long long)p->ny * 5 * 8;
+  return b + 4096;
+}
+
+std::string validate(const streams_b200_params* p) {
+  if (p->nx < 1 || p->ny < 1 || p->nz < 1) return "grid sizes must be positive";
+  if (p->ep_order < 2 || p->ep_order > 8 || p->ep_order % 2) return "ep_order must be 2, 4, 6 or 8";
+  const int lmax = p->ep_order / 2;
+  if (p->weno_scheme < 1 || p->weno_scheme > 4) return "weno_scheme must be 1..4";
+  if (!stage_supported(lmax, p->weno_scheme))
+    return "unsupported (ep_order, weno_scheme) pair for the device path";
+  if (p->ng < lmax || p->ng < p->weno_scheme || p->ng < 2) return "ng too small for the stencils";
+  if (p->nx < p->ng || p->ny < p->ng || p->nz < p->ng) return "every block dimension must be >= ng";
+  if (p->weno_version != 0 && p->weno_version != 1) return "weno_version must be 0 or 1";
+  if (p->weno_version == 1 && p->weno_scheme != 3) return "weno_version 1 requires weno_scheme 3";
+  if (p->flux_splitting != 0) return "flux_splitting = 1 (Rusanov) is not implemented on the device path";
+  if (p->conservative_viscous != 1) return "only conservative_viscous = 1 is implemented on the device path";
+  if (p->calorically_perfect != 1) return "only calorically perfect gas is implemented on the device path";
+  if (p->nrk != 3) return "only the Wray RK3 scheme (nrk = 3) is implemented";
+  if (p->precision != 0) return "precision must be 0 (FP64)";
+  if (p->visc_model < 0 || p->visc_model > 2) return "visc_model must be 0, 1 or 2";
+  for (int d = 0; d < 3; ++d) {
+    const int a = p->bctags[2 * d], b = p->bctags[2 * d + 1];
+    const bool per = (a == 0 && b == 0);
+    if (per) continue;
+    if (d == 1 && a == 6 && b == 6 && p->is_y_staggered) continue;
+    return "boundary tags: only periodic directions and staggered isothermal y walls (6) are implemented";
+  }
+  if (p->channel_case && !(p->volchan > 0)) return "channel forcing needs volchan > 0";
+  return "";
+}
+
+void fill_geom(streams_b200_ctx* c) {
+  const streams_b200_params& p = c->p;
+  Geom& g = c->g;
+  g.nx = p.nx; g.ny = p.ny; g.nz = p.nz; g.ng = p.ng;
+  g.sx = p.nx + 2 * p.ng; g.sy = p.ny + 2 * p.ng; g.sz = p.nz + 2 * p.ng;
+  g.nvol = (long long)g.sx * g.sy * g.sz;
+  g.nint = (long long)p.nx * p.ny * p.nz;
+  for (int d = 0; d < 3; ++d) g.periodic[d] = (p.bctags[2 * d] == 0 && p.bctags[2 * d + 1] == 0);
+  g.wall_ymin = p.bctags[2] == 6;
+  g.wall_ymax = p.bctags[3] == 6;
+  for (int l = 0; l < 6; ++l) g.fzf[l] = p.force_zero_flux[l];
+  g.eul_imin = p.eul_imin; g.eul_imax = p.eul_imax; g.eul_jmin = p.eul_jmin;
+  g.eul_jmax = p.eul_jmax; g.eul_kmin = p.eul_kmin; g.eul_kmax = p.eul_kmax;
+  g.lmax_base = p.ep_order / 2;
+  g.nkeep = p.nkeep;
+  g.weno_scheme = p.weno_scheme;
+  g.weno_version = p.weno_version;
+  g.sensor_threshold = p.sensor_threshold;
+  g.visc_model = p.visc_model;
+  g.mu0 = p.mu0; g.t0 = p.t0; g.rgas0 = p.rgas0; g.rho0 = p.rho0; g.u0 = p.u0; g.l0 = p.l0;
+  g.sutherland_s = p.sutherland_s; g.t_ref_dim = p.t_ref_dim; g.vtexp = p.powerlaw_vtexp; g.prandtl = p.prandtl;
+  g.cp0 = p.cp0; g.cv0 = p.cv0; g.cp_last = p.cp_last; g.cv_last = p.cv_last;
+  g.gamloc = p.cp0 / (p.cp0 - p.rgas0);
+  g.t_wall = p.t_wall;
+  g.channel_case = p.channel_case;
+  g.force_var = p.channel_case && p.theta_wall >= -1.0;
+  g.volchan = p.volchan;
+  g.t_bulk_target = p.t_bulk_target;
+}
+
+}  // namespace
+
+extern "C" {
+
+int streams_b200_abi_version(void) { return STREAMS_B200_ABI_VERSION; }
+const char* streams_b200_global_error(void) { return g_global_err.c_str(); }
+const char* streams_b200_last_error(const streams_b200_ctx* ctx) { return ctx ? ctx->err.c_str() : g_global_err.c_str(); }
+long long streams_b200_footprint_bytes(const streams_b200_params* p) { return p ? footprint(p) : -1; }
+long long streams_b200_launch_count(const streams_b200_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int streams_b200_destroy(streams_b200_ctx* ctx) {
+  if (!ctx) return STREAMS_B200_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void* a : ctx->allocs) cudaFree(a);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* gr, streams_b200_ctx** out) {
+  if (!p || !gr || !out) return set_err(nullptr, STREAMS_B200_EINVAL, "null argument");
+  *out = nullptr;
+  std::string why = validate(p);
+  if (!why.empty()) return set_err(nullptr, STREAMS_B200_EINVAL, why);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    cudaGetLastError();
+    return set_err(nullptr, STREAMS_B200_ENODEV, "no CUDA device available");
+  }
+  auto* c = new streams_b200_ctx();
+  c->p = *p;
+  cudaGetDevice(&c->device);
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, c->device);
+  if (prop.major < 10) {
+    delete c;
+    return set_err(nullptr, STREAMS_B200_ENODEV, "the backend is built for sm_100a (B200); device is sm_" +
+                                                     std::to_string(prop.major) + std::to_string(prop.minor));
+  }
+  fill_geom(c);
+  Geom& g = c->g;
+  auto fail = [&](cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    streams_b200_destroy(c);
+    return set_err(nullptr, e == cudaErrorMemoryAllocation ? STREAMS_B200_ENOMEM : STREAMS_B200_ECUDA, m);
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(e, "cudaStreamCreate");
+  // 1-D grid data
+  const int ng = p->ng;
+  double *dx, *dy, *dz, *dyn, *m1, *m2, *m3, *m4, *m5, *m6;
+  int *ex, *ey, *ez;
+  if ((e = dev_alloc(c, &dx, p->nx + 2 * ng)) || (e = dev_alloc(c, &dy, p->ny + 2 * ng)) ||
+      (e = dev_alloc(c, &dz, p->nz + 2 * ng)) || (e = dev_alloc(c, &dyn, p->ny + 1)) ||
+      (e = dev_alloc(c, &m1, p->nx)) || (e = dev_alloc(c, &m2, p->ny)) || (e = dev_alloc(c, &m3, p->nz)) ||
+      (e = dev_alloc(c, &m4, p->nx)) || (e = dev_alloc(c, &m5, p->ny)) || (e = dev_alloc(c, &m6, p->nz)) ||
+      (e = dev_alloc(c, &ex, p->nx + 1)) || (e = dev_alloc(c, &ey, p->ny + 1)) || (e = dev_alloc(c, &ez, p->nz + 1)))
+    return fail(e, "cudaMalloc(grid)");
+  const size_t nx = (size_t)p->nx, ny = (size_t)p->ny, nz = (size_t)p->nz, g2 = 2 * (size_t)ng;
+  struct Cp { void* d; const void* h; size_t b; } cps[] = {
+      {dx, gr->x, (nx + g2) * 8},      {dy, gr->y, (ny + g2) * 8},       {dz, gr->z, (nz + g2) * 8},
+      {dyn, gr->yn, (ny + 1) * 8},     {m1, gr->dcsidx, nx * 8},         {m2, gr->detady, ny * 8},
+      {m3, gr->dzitdz, nz * 8},        {m4, gr->dcsidxs, nx * 8},        {m5, gr->detadys, ny * 8},
+      {m6, gr->dzitdzs, nz * 8},       {ex, gr->ep_ord_x, (nx + 1) * 4}, {ey, gr->ep_ord_y, (ny + 1) * 4},
+      {ez, gr->ep_ord_z, (nz + 1) * 4}};
+  for (auto& cp : cps) {
+    if (!cp.h) {
+      streams_b200_destroy(c);
+      return set_err(nullptr, STREAMS_B200_EINVAL, "null grid array");
+    }
+    if ((e = cudaMemcpy(cp.d, cp.h, cp.b, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e, "cudaMemcpy(grid)");
+  }
+  g.x = dx + (ng - 1); g.y = dy + (ng - 1); g.z = dz + (ng - 1);
+  g.yn = dyn - 1;
+  g.dcsidx = m1 - 1; g.detady = m2 - 1; g.dzitdz = m3 - 1;
+  g.dcsidxs = m4 - 1; g.detadys = m5 - 1; g.dzitdzs = m6 - 1;
+  g.epx = ex; g.epy = ey; g.epz = ez;
+  for (int lm = 0; lm < 4; ++lm)
+    for (int l = 0; l < 4; ++l) g.coeff[lm][l] = gr->coeff_deriv1 ? gr->coeff_deriv1[lm * 4 + l] : 0.0;
+  // state
+  DevState& d = c->d;
+  if ((e = dev_alloc(c, &d.w, g.nvol * 5)) || (e = dev_alloc(c, &d.aux, g.nvol * 7)) ||
+      (e = dev_alloc(c, &d.sensor, g.nint)) || (e = dev_alloc(c, &d.sensor_next, g.nint)) ||
+      (e = dev_alloc(c, &d.div3, g.nint)) || (e = dev_alloc(c, &c->fl_a, g.nint * 5)) ||
+      (e = dev_alloc(c, &c->fl_b, g.nint * 5)) || (e = dev_alloc(c, &d.wallprop, (size_t)p->nx * p->nz * 3)) ||
+      (e = dev_alloc(c, &d.sc, 1)))
+    return fail(e, "cudaMalloc(state)");
+  d.red_capacity = reduction_slots(g);
+  if ((e = dev_alloc(c, &d.red, d.red_capacity))) return fail(e, "cudaMalloc(reductions)");
+  d.fl_a = c->fl_a;
+  d.fl_b = c->fl_b;
+  if ((e = cudaMemsetAsync(d.w, 0, g.nvol * 5 * 8, c->stream)) || (e = cudaMemsetAsync(d.aux, 0, g.nvol * 7 * 8, c->stream)) ||
+      (e = cudaMemsetAsync(d.sensor, 0, g.nint * 8, c->stream)) ||
+      (e = cudaMemsetAsync(d.sensor_next, 0, g.nint * 8, c->stream)) ||
+      (e = cudaMemsetAsync(d.div3, 0, g.nint * 8, c->stream)) || (e = cudaMemsetAsync(c->fl_a, 0, g.nint * 40, c->stream)) ||
+      (e = cudaMemsetAsync(c->fl_b, 0, g.nint * 40, c->stream)) || (e = cudaMemsetAsync(d.sc, 0, sizeof(Scalars), c->stream)) ||
+      (e = cudaStreamSynchronize(c->stream)))
+    return fail(e, "initialise state");
+  *out = c;
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_copy_from_field(streams_b200_ctx* c, const double* w) {
+  if (!c || !w) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  SB_CHECK(c, cudaMemcpyAsync(c->d.w, w, c->g.nvol * 5 * 8, cudaMemcpyHostToDevice, c->stream));
+  c->shift_pending = false;
+  c->aux_current = false;
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_copy_from_device(streams_b200_ctx* c, const double* w) {
+  if (!c || !w) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  SB_CHECK(c, cudaMemcpyAsync(c->d.w, w, c->g.nvol * 5 * 8, cudaMemcpyDeviceToDevice, c->stream));
+  c->shift_pending = false;
+  c->aux_current = false;
+  return STREAMS_B200_OK;
+}
+
+static int finalize_w(streams_b200_ctx* c) {
+  // apply a pending force_var shift and rebuild the ghost layers (update_ghost + bcswap)
+  if (c->shift_pending) {
+    SB_CHECK(c, launch_apply_shift(c->g, c->d, c->stream, &c->launches));
+    c->shift_pending = false;
+  }
+  SB_CHECK(c, launch_fill_ghosts(c->g, c->d, c->stream, &c->launches));
+  c->aux_current = true;
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_copy_to_field(streams_b200_ctx* c, double* w) {
+  if (!c || !w) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  int rc = finalize_w(c);
+  if (rc) return rc;
+  SB_CHECK(c, cudaMemcpyAsync(w, c->d.w, c->g.nvol * 5 * 8, cudaMemcpyDeviceToHost, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_copy_to_device(streams_b200_ctx* c, double* w) {
+  if (!c || !w) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  int rc = finalize_w(c);
+  if (rc) return rc;
+  SB_CHECK(c, cudaMemcpyAsync(w, c->d.w, c->g.nvol * 5 * 8, cudaMemcpyDeviceToDevice, c->stream));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_init_run(streams_b200_ctx* c) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  SB_CHECK(c, launch_aux(c->g, c->d, c->shift_pending ? 1 : 0, c->stream, &c->launches));
+  c->shift_pending = false;
+  c->aux_current = true;
+  SB_CHECK(c, launch_init_sensor(c->g, c->d, c->stream, &c->launches));
+  SB_CHECK(c, cudaMemsetAsync(c->fl_a, 0, c->g.nint * 40, c->stream));
+  SB_CHECK(c, cudaMemsetAsync(c->fl_b, 0, c->g.nint * 40, c->stream));
+  return STREAMS_B200_OK;
+}
+
+static int do_compute_dt(streams_b200_ctx* c) {
+  if (c->p.cfl < 0) {
+    double dt = -c->p.cfl;
+    SB_CHECK(c, cudaMemcpyAsync(&c->d.sc->dt, &dt, 8, cudaMemcpyHostToDevice, c->stream));
+    SB_CHECK(c, cudaStreamSynchronize(c->stream));
+    return STREAMS_B200_OK;
+  }
+  if (!c->aux_current || c->shift_pending) {
+    SB_CHECK(c, launch_aux(c->g, c->d, c->shift_pending ? 1 : 0, c->stream, &c->launches));
+    c->shift_pending = false;
+    c->aux_current = true;
+  }
+  SB_CHECK(c, launch_dt(c->g, c->d, c->p.cfl, c->stream, &c->launches));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_compute_dt(streams_b200_ctx* c, double* dt) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  int rc = do_compute_dt(c);
+  if (rc) return rc;
+  if (dt) {
+    SB_CHECK(c, cudaMemcpyAsync(dt, &c->d.sc->dt, 8, cudaMemcpyDeviceToHost, c->stream));
+    SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  }
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_set_dt(streams_b200_ctx* c, double dt) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  SB_CHECK(c, cudaMemcpyAsync(&c->d.sc->dt, &dt, 8, cudaMemcpyHostToDevice, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_set_time(streams_b200_ctx* c, double t) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  SB_CHECK(c, cudaMemcpyAsync(&c->d.sc->time, &t, 8, cudaMemcpyHostToDevice, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  return STREAMS_B200_OK;
+}
+
+static int do_rk_sync(streams_b200_ctx* c, bool add_time) {
+  const bool fv = c->g.force_var != 0;
+  for (int istep = 1; istep <= 3; ++istep) {
+    StageArgs a{};
+    a.istep = istep;
+    a.rhork = c->p.rhork[istep - 1];
+    a.gamrk = c->p.gamrk[istep - 1];
+    a.apply_shift = c->shift_pending ? 1 : 0;
+    a.run_aux = (c->aux_current && !c->shift_pending) ? 0 : 1;
+    a.want_stats = istep == 3;
+    a.add_time = add_time && istep == 3;
+    // fixed register roles: stage 1 writes A, stage 2 reads A writes B, stage 3 reads B writes A
+    double* prev = istep == 2 ? c->fl_a : c->fl_b;
+    double* next = istep == 2 ? c->fl_b : c->fl_a;
+    SB_CHECK(c, launch_stage(c->g, c->d, a, prev, next, c->stream, &c->launches));
+    c->last_fl = next;
+    c->shift_pending = fv;
+    c->aux_current = false;
+  }
+  c->have_stats = true;
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_rk_sync(streams_b200_ctx* c) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  return do_rk_sync(c, false);
+}
+
+int streams_b200_advance(streams_b200_ctx* c, int nsteps, int iter_dt_recompute, int icyc_start, int icyc0) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  if (nsteps < 0 || iter_dt_recompute < 1) return set_err(c, STREAMS_B200_EINVAL, "bad step counts");
+  cudaSetDevice(c->device);
+  int icyc = icyc_start;
+  for (int n = 0; n < nsteps; ++n) {
+    icyc = icyc + 1;
+    if (c->p.cfl > 0 && (icyc - icyc0) % iter_dt_recompute == 0) {
+      int rc = do_compute_dt(c);
+      if (rc) return rc;
+    }
+    int rc = do_rk_sync(c, true);
+    if (rc) return rc;
+  }
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_get_scalars(streams_b200_ctx* c, double out[7]) {
+  if (!c || !out) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  Scalars s{};
+  SB_CHECK(c, cudaMemcpyAsync(&s, c->d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  out[0] = s.dt; out[1] = s.time; out[2] = s.dpdx; out[3] = s.rhobulk; out[4] = s.ubulk; out[5] = s.tbulk;
+  out[6] = s.tbdiff;
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_compute_residual(streams_b200_ctx* c, double out[7]) {
+  if (!c || !out) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  if (!c->have_stats) return set_err(c, STREAMS_B200_EINVAL, "compute_residual needs a completed rk_sync");
+  cudaSetDevice(c->device);
+  Scalars s{};
+  SB_CHECK(c, cudaMemcpyAsync(&s, c->d.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  const double restemp = (double)c->p.nx * (double)c->p.ny * (double)c->p.nz;
+  out[0] = std::sqrt(s.residual_sum / restemp);
+  out[1] = s.rhomin; out[2] = s.rhomax; out[3] = s.tmin; out[4] = s.tmax; out[5] = s.pmin; out[6] = s.pmax;
+  if (std::isnan(out[0])) return set_err(c, STREAMS_B200_ENAN, "NaN residual");
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_count_weno(streams_b200_ctx* c, double out[3]) {
+  if (!c || !out) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  SB_CHECK(c, launch_count_weno(c->g, c->d, c->stream, &c->launches));
+  const long long nb = (c->g.nint + 255) / 256;
+  std::vector<double> h((size_t)nb * 3);
+  SB_CHECK(c, cudaMemcpyAsync(h.data(), c->d.red, h.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  double s[3] = {0, 0, 0};
+  for (long long b = 0; b < nb; ++b)
+    for (int r = 0; r < 3; ++r) s[r] += h[b * 3 + r];
+  const streams_b200_params& p = c->p;
+  out[0] = s[0] / ((double)(p.eul_imax - p.eul_imin + 1) * p.ny * p.nz);
+  out[1] = s[1] / ((double)p.nx * (p.eul_jmax - p.eul_jmin + 1) * p.nz);
+  out[2] = s[2] / ((double)p.nx * p.ny * (p.eul_kmax - p.eul_kmin + 1));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_get_wallprop(streams_b200_ctx* c, double* out) {
+  if (!c || !out) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  SB_CHECK(c, cudaMemcpyAsync(out, c->d.wallprop, (size_t)c->p.nx * c->p.nz * 3 * 8, cudaMemcpyDeviceToHost, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_debug_fetch(streams_b200_ctx* c, int which, double* out, long long n) {
+  if (!c || !out) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  const double* src = nullptr;
+  long long cnt = 0;
+  switch (which) {
+    case 0: src = c->d.aux; cnt = 7 * c->g.nvol; break;
+    case 1: src = c->last_fl ? c->last_fl : c->fl_a; cnt = 5 * c->g.nint; break;
+    case 2: src = c->d.sensor; cnt = c->g.nint; break;
+    case 3: src = c->d.div3; cnt = c->g.nint; break;
+    default: return set_err(c, STREAMS_B200_EINVAL, "unknown diagnostic array");
+  }
+  if (n < cnt) return set_err(c, STREAMS_B200_EINVAL, "output buffer too small");
+  SB_CHECK(c, cudaMemcpyAsync(out, src, cnt * 8, cudaMemcpyDeviceToHost, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_synchronize(streams_b200_ctx* c) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  SB_CHECK(c, cudaGetLastError());
+  return STREAMS_B200_OK;
+}
+
+}  // extern "C"

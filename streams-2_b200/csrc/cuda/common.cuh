@@ -1,0 +1,132 @@
+// Shared device-side definitions of the B200 backend: the per-context geometry and parameter
+// block (passed by value to every kernel), array indexing, thermodynamics of the calorically
+// perfect gas, and deterministic block reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sb200 {
+
+constexpr int NV = 5;
+
+// Number of FP64 reduction slots produced per block by the stage kernels.
+constexpr int NRED_RHS = 5;   // force_rhs: sum fln1*dy, fln2*dy, rho*dy, rhou*dy, rhou*T*dy
+constexpr int NRED_UPD = 8;   // force_var sum rhou*T*dy, residual sum, rho/T/p min and max
+
+struct Geom {
+  // block sizes and padded strides (ghosted arrays: index (i,j,k), i in 1-ng..nx+ng)
+  int nx, ny, nz, ng;
+  int sx, sy, sz;
+  long long nvol;  // sx*sy*sz: stride between variables of a ghosted array
+  long long nint;  // nx*ny*nz: stride between variables of an interior array
+  // one-dimensional grid (device pointers, already offset so that x[i] is x(i) of the reference)
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* yn;       // yn[j], j = 1..ny+1
+  const double* dcsidx;   // [i], i = 1..nx
+  const double* detady;
+  const double* dzitdz;
+  const double* dcsidxs;
+  const double* detadys;
+  const double* dzitdzs;
+  const int* epx;         // ep_ord_change along x, [i] for faces i = 0..nx
+  const int* epy;
+  const int* epz;
+  double coeff[4][4];     // coeff_deriv1(l, lmax) at [lmax-1][l-1]
+  // boundary handling
+  int periodic[3];
+  int wall_ymin, wall_ymax;  // staggered isothermal walls
+  int fzf[6];                // force_zero_flux
+  int eul_imin, eul_imax, eul_jmin, eul_jmax, eul_kmin, eul_kmax;
+  // numerics
+  int lmax_base, nkeep, weno_scheme, weno_version;
+  double sensor_threshold;
+  // fluid
+  int visc_model;
+  double mu0, t0, rgas0, rho0, u0, l0, sutherland_s, t_ref_dim, vtexp, prandtl;
+  double cp0, cv0, cp_last, cv_last, gamloc;
+  double t_wall;
+  // channel forcing
+  int channel_case, force_var;
+  double volchan, t_bulk_target;
+};
+
+__host__ __device__ __forceinline__ long long gidx(const Geom& g, int i, int j, int k) {
+  return ((long long)(k + g.ng - 1) * g.sy + (j + g.ng - 1)) * g.sx + (i + g.ng - 1);
+}
+__host__ __device__ __forceinline__ long long iidx(const Geom& g, int i, int j, int k) {
+  return ((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1);
+}
+
+// Device-resident scalars of a context (one cache line group).
+struct Scalars {
+  double dt;
+  double time;
+  double dpdx;
+  double rhobulk, ubulk, tbulk;
+  double tbdiff;       // pending force_var energy shift (applied by the next aux pass)
+  double bulk[5];      // last force_rhs bulk values (divided by volchan)
+  double residual_sum; // sum of (fln_2/dt)^2 of the last stage 3
+  double rhomin, rhomax, tmin, tmax, pmin, pmax;
+  int pending_shift;   // 1 when tbdiff has not been applied to w yet
+  int nan_flag;
+  int err_flag;
+  int pad;
+};
+
+// get_temperature_from_e_dev / get_e_from_temperature_dev (kernels_cpu.F90:7116-7176),
+// calorically perfect branch
+__device__ __forceinline__ double t_from_e(const Geom& g, double ee) {
+  double ebar = ee - g.cv_last * g.t0;
+  return g.t0 + ebar / g.cv0;
+}
+__device__ __forceinline__ double e_from_t(const Geom& g, double tt) {
+  double ee = g.cv_last;
+  ee = ee + g.cv0 * (tt / g.t0 - 1.0);
+  return ee * g.t0;
+}
+
+// viscosity law of eval_aux_subroutine (kernels_cpu.F90:6995-7002)
+__device__ __forceinline__ double viscosity(const Geom& g, double tt) {
+  if (g.visc_model == 1) return g.mu0 * pow(tt / g.t0, g.vtexp);
+  if (g.visc_model == 2) {
+    double tr = tt / g.t0;
+    double st = g.sutherland_s / g.t_ref_dim;
+    return g.mu0 * pow(tr, 1.5) * (1.0 + st) / (tr + st);
+  }
+  return 0.0;
+}
+
+// Index of a stencil point along one axis of the sensor / div arrays (stored interior only):
+// periodic directions wrap; otherwise the caller decides (sensor: 0, div: clamp).
+__device__ __forceinline__ int wrap(int i, int n) { return i < 1 ? i + n : (i > n ? i - n : i); }
+
+// Deterministic block reduction of NR values per thread (sum), fixed tree order.  Every thread
+// of the block must call it; thread 0 of the block receives the totals.
+template <int NR, int NT>
+__device__ __forceinline__ void block_reduce_sum(double (&v)[NR], double* smem /* NR * NT/32 */) {
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[r] += __shfl_down_sync(0xffffffffu, v[r], o);
+  // linear thread index: the helper is also called from 2-D blocks
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int lane = tid & 31, warp = tid >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) smem[r * (NT / 32) + warp] = v[r];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      double a = lane < NT / 32 ? smem[r * (NT / 32) + lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+      v[r] = a;
+    }
+  }
+}
+
+}  // namespace sb200

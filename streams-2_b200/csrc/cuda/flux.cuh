@@ -1,0 +1,403 @@
+// Device functions of the hybrid convective flux at one cell face: energy-preserving split-form
+// central flux (KEEP variants) and characteristic WENO where the Ducros sensor fires.
+// Restates euler_{x,y,z}_*hybrid_kernel, compute_roe_average, eigenvectors_{x,y,z} and
+// wenorec_1d of code/src/singleideal/kernels_cpu.F90 (lines cited per function).
+#pragma once
+
+#include "common.cuh"
+
+namespace sb200 {
+
+// Stencil of a face: NP = 2*S points at offsets o = -(S-1) .. S from the face's lower point.
+template <class R, int S>
+struct Stencil {
+  R rho[2 * S], u[2 * S], v[2 * S], w[2 * S], h[2 * S], t[2 * S];
+};
+
+// wenorec_1d (kernels_cpu.F90:2526-2724) for one characteristic variable.
+// vp[l-1], vm[l-1] hold the reference's vp(m,l), vm(m,l), l = 1..2*WS; i = iweno = WS.
+template <class R, int WS>
+__device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS], int ord, int version,
+                                     R betascale) {
+  auto VP = [&](int l) -> R { return vp[l - 1]; };
+  auto VM = [&](int l) -> R { return vm[l - 1]; };
+  constexpr int i = WS;
+  const R eps6 = R(0.000001);
+  if (ord == 1) {
+    return VP(i) + VM(i + 1);
+  }
+  if constexpr (WS >= 2) {
+    if (ord == 2) {
+      const R dwe0 = R(1.0) / R(3.0), dwe1 = R(2.0) / R(3.0);
+      R a = VP(i) - VP(i - 1), b = VP(i + 1) - VP(i);
+      R bp0 = betascale * (a * a), bp1 = betascale * (b * b);
+      R c = VM(i + 2) - VM(i + 1), d = VM(i + 1) - VM(i);
+      R bm0 = betascale * (c * c), bm1 = betascale * (d * d);
+      R tp0 = eps6 + bp0, tp1 = eps6 + bp1, tm0 = eps6 + bm0, tm1 = eps6 + bm1;
+      bp0 = dwe0 / (tp0 * tp0);
+      bm0 = dwe0 / (tm0 * tm0);
+      bp1 = dwe1 / (tp1 * tp1);
+      bm1 = dwe1 / (tm1 * tm1);
+      R sump = (R(0) + bp0) + bp1, summ = (R(0) + bm0) + bm1;
+      bp0 = bp0 / sump; bp1 = bp1 / sump; bm0 = bm0 / summ; bm1 = bm1 / summ;
+      R vminus = bp0 * (-VP(i - 1) + R(3) * VP(i)) + bp1 * (VP(i) + VP(i + 1));
+      R vplus = bm0 * (-VM(i + 2) + R(3) * VM(i + 1)) + bm1 * (VM(i) + VM(i + 1));
+      return R(0.5) * (vminus + vplus);
+    }
+  }
+  if constexpr (WS >= 3) {
+    if (ord == 3) {
+      const R dwe[3] = {R(1.0) / R(10.0), R(6.0) / R(10.0), R(3.0) / R(10.0)};
+      const R d0 = R(13.0) / R(12.0), d1 = R(1.0) / R(4.0);
+      const R c0 = R(1.0) / R(3.0), c1 = R(5.0) / R(6.0), c2 = R(-1.0) / R(6.0), c3 = R(-7.0) / R(6.0),
+              c4 = R(11.0) / R(6.0);
+      R bp[3], bm[3];
+      {
+        R a = VP(i) - R(2) * VP(i + 1) + VP(i + 2), b = R(3) * VP(i) - R(4) * VP(i + 1) + VP(i + 2);
+        bp[2] = d0 * (a * a) + d1 * (b * b);
+        a = VP(i - 1) - R(2) * VP(i) + VP(i + 1);
+        b = VP(i - 1) - VP(i + 1);
+        bp[1] = d0 * (a * a) + d1 * (b * b);
+        a = VP(i) - R(2) * VP(i - 1) + VP(i - 2);
+        b = R(3) * VP(i) - R(4) * VP(i - 1) + VP(i - 2);
+        bp[0] = d0 * (a * a) + d1 * (b * b);
+        a = VM(i + 1) - R(2) * VM(i) + VM(i - 1);
+        b = R(3) * VM(i + 1) - R(4) * VM(i) + VM(i - 1);
+        bm[2] = d0 * (a * a) + d1 * (b * b);
+        a = VM(i + 2) - R(2) * VM(i + 1) + VM(i);
+        b = VM(i + 2) - VM(i);
+        bm[1] = d0 * (a * a) + d1 * (b * b);
+        a = VM(i + 1) - R(2) * VM(i + 2) + VM(i + 3);
+        b = R(3) * VM(i + 1) - R(4) * VM(i + 2) + VM(i + 3);
+        bm[0] = d0 * (a * a) + d1 * (b * b);
+      }
+#pragma unroll
+      for (int l = 2; l >= 0; --l) {
+        bp[l] = betascale * bp[l];
+        bm[l] = betascale * bm[l];
+      }
+      if (version == 0) {
+        R sump = R(0), summ = R(0);
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+          R tp = eps6 + bp[l], tm = eps6 + bm[l];
+          bp[l] = dwe[l] / (tp * tp);
+          bm[l] = dwe[l] / (tm * tm);
+          sump = sump + bp[l];
+          summ = summ + bm[l];
+        }
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+          bp[l] = bp[l] / sump;
+          bm[l] = bm[l] / summ;
+        }
+      } else {
+        // eps40 is a single-precision literal in the reference
+        const R eps40 = R(static_cast<double>(1.e-35f));
+        R tau5p = fabs(bp[0] - bp[2]) + eps40;
+        R tau5m = fabs(bm[0] - bm[2]) + eps40;
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+          bp[l] = (bp[l] + eps40) / (bp[l] + tau5p);
+          bm[l] = (bm[l] + eps40) / (bm[l] + tau5m);
+        }
+        R sump = R(0), summ = R(0);
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+          bp[l] = dwe[l] / bp[l];
+          bm[l] = dwe[l] / bm[l];
+          sump = sump + bp[l];
+          summ = summ + bm[l];
+        }
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+          bp[l] = bp[l] / sump;
+          bm[l] = bm[l] / summ;
+        }
+      }
+      R vminus = bp[2] * (c0 * VP(i) + c1 * VP(i + 1) + c2 * VP(i + 2)) +
+                 bp[1] * (c2 * VP(i - 1) + c1 * VP(i) + c0 * VP(i + 1)) +
+                 bp[0] * (c0 * VP(i - 2) + c3 * VP(i - 1) + c4 * VP(i));
+      R vplus = bm[2] * (c0 * VM(i + 1) + c1 * VM(i) + c2 * VM(i - 1)) +
+                bm[1] * (c2 * VM(i + 2) + c1 * VM(i + 1) + c0 * VM(i)) +
+                bm[0] * (c0 * VM(i + 3) + c3 * VM(i + 2) + c4 * VM(i + 1));
+      return vminus + vplus;
+    }
+  }
+  if constexpr (WS >= 4) {
+    if (ord == 4) {
+      const R dwe[4] = {R(1.0) / R(35.0), R(12.0) / R(35.0), R(18.0) / R(35.0), R(4.0) / R(35.0)};
+      const R d1 = R(1.0) / R(36.0), d2 = R(13.0) / R(12.0), d3 = R(781.0) / R(720.0);
+      auto sq = [](R a) { return a * a; };
+      R bp[4], bm[4];
+      bp[3] = d1 * sq(-11 * VP(i) + 18 * VP(i + 1) - 9 * VP(i + 2) + 2 * VP(i + 3)) +
+              d2 * sq(2 * VP(i) - 5 * VP(i + 1) + 4 * VP(i + 2) - VP(i + 3)) +
+              d3 * sq(-VP(i) + 3 * VP(i + 1) - 3 * VP(i + 2) + VP(i + 3));
+      bp[2] = d1 * sq(-2 * VP(i - 1) - 3 * VP(i) + 6 * VP(i + 1) - VP(i + 2)) +
+              d2 * sq(VP(i - 1) - 2 * VP(i) + VP(i + 1)) + d3 * sq(-VP(i - 1) + 3 * VP(i) - 3 * VP(i + 1) + VP(i + 2));
+      bp[1] = d1 * sq(VP(i - 2) - 6 * VP(i - 1) + 3 * VP(i) + 2 * VP(i + 1)) +
+              d2 * sq(VP(i - 1) - 2 * VP(i) + VP(i + 1)) + d3 * sq(-VP(i - 2) + 3 * VP(i - 1) - 3 * VP(i) + VP(i + 1));
+      bp[0] = d1 * sq(-2 * VP(i - 3) + 9 * VP(i - 2) - 18 * VP(i - 1) + 11 * VP(i)) +
+              d2 * sq(-VP(i - 3) + 4 * VP(i - 2) - 5 * VP(i - 1) + 2 * VP(i)) +
+              d3 * sq(-VP(i - 3) + 3 * VP(i - 2) - 3 * VP(i - 1) + VP(i));
+      bm[3] = d1 * sq(-11 * VM(i + 1) + 18 * VM(i) - 9 * VM(i - 1) + 2 * VM(i - 2)) +
+              d2 * sq(2 * VM(i + 1) - 5 * VM(i) + 4 * VM(i - 1) - VM(i - 2)) +
+              d3 * sq(-VM(i + 1) + 3 * VM(i) - 3 * VM(i - 1) + VM(i - 2));
+      bm[2] = d1 * sq(-2 * VM(i + 2) - 3 * VM(i + 1) + 6 * VM(i) - VM(i - 1)) +
+              d2 * sq(VM(i + 2) - 2 * VM(i + 1) + VM(i)) + d3 * sq(-VM(i + 2) + 3 * VM(i + 1) - 3 * VM(i) + VM(i - 1));
+      bm[1] = d1 * sq(VM(i + 3) - 6 * VM(i + 2) + 3 * VM(i + 1) + 2 * VM(i)) +
+              d2 * sq(VM(i + 2) - 2 * VM(i + 1) + VM(i)) + d3 * sq(-VM(i + 3) + 3 * VM(i + 2) - 3 * VM(i + 1) + VM(i));
+      bm[0] = d1 * sq(-2 * VM(i + 4) + 9 * VM(i + 3) - 18 * VM(i + 2) + 11 * VM(i + 1)) +
+              d2 * sq(-VM(i + 4) + 4 * VM(i + 3) - 5 * VM(i + 2) + 2 * VM(i + 1)) +
+              d3 * sq(-VM(i + 4) + 3 * VM(i + 3) - 3 * VM(i + 2) + VM(i + 1));
+      R sump = R(0), summ = R(0);
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        bp[l] = betascale * bp[l];
+        bm[l] = betascale * bm[l];
+      }
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        R tp = eps6 + bp[l], tm = eps6 + bm[l];
+        bp[l] = dwe[l] / (tp * tp);
+        bm[l] = dwe[l] / (tm * tm);
+        sump = sump + bp[l];
+        summ = summ + bm[l];
+      }
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        bp[l] = bp[l] / sump;
+        bm[l] = bm[l] / summ;
+      }
+      R vminus = bp[3] * (6 * VP(i) + 26 * VP(i + 1) - 10 * VP(i + 2) + 2 * VP(i + 3)) +
+                 bp[2] * (-2 * VP(i - 1) + 14 * VP(i) + 14 * VP(i + 1) - 2 * VP(i + 2)) +
+                 bp[1] * (2 * VP(i - 2) - 10 * VP(i - 1) + 26 * VP(i) + 6 * VP(i + 1)) +
+                 bp[0] * (-6 * VP(i - 3) + 26 * VP(i - 2) - 46 * VP(i - 1) + 50 * VP(i));
+      R vplus = bm[3] * (6 * VM(i + 1) + 26 * VM(i) - 10 * VM(i - 1) + 2 * VM(i - 2)) +
+                bm[2] * (-2 * VM(i + 2) + 14 * VM(i + 1) + 14 * VM(i) - 2 * VM(i - 1)) +
+                bm[1] * (2 * VM(i + 3) - 10 * VM(i + 2) + 26 * VM(i + 1) + 6 * VM(i)) +
+                bm[0] * (-6 * VM(i + 4) + 26 * VM(i + 3) - 46 * VM(i + 2) + 50 * VM(i + 1));
+      return (vminus + vplus) / R(24);
+    }
+  }
+  return R(0);
+}
+
+// Central energy-preserving split-form flux (kernels_cpu.F90:462-612 for x; same in y, z).
+// DIR: 0 x, 1 y, 2 z.  Points of st are at offsets -(S-1)..S (index o + S - 1).
+template <class R, int DIR, int LB, int S>
+__device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>& st, int lmax, int nkeep,
+                                             bool zero_flux, R (&fh)[5]) {
+  const R rgas0 = R(g.rgas0);
+  R pp[2 * S], ee[2 * S];
+#pragma unroll
+  for (int q = 0; q < 2 * S; ++q) {
+    pp[q] = st.t[q] * st.rho[q] * rgas0;
+    ee[q] = st.h[q] - pp[q] / st.rho[q] - R(0.5) * (st.u[q] * st.u[q] + st.v[q] * st.v[q] + st.w[q] * st.w[q]);
+  }
+  R ft1 = 0, ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
+#pragma unroll
+  for (int l = 1; l <= LB; ++l) {
+    if (l <= lmax) {
+      R uvs1 = 0, uvs2 = 0, uvs3 = 0, uvs4 = 0, uvs5 = 0, uvs5_i = 0, uvs5_k = 0, uvs5_p = 0, uvs6 = 0;
+#pragma unroll
+      for (int m = 0; m < LB; ++m) {
+        if (m <= l - 1) {
+          const int a = -m + S - 1, b = -m + l + S - 1;
+          const R vna = DIR == 0 ? st.u[a] : (DIR == 1 ? st.v[a] : st.w[a]);
+          const R vnb = DIR == 0 ? st.u[b] : (DIR == 1 ? st.v[b] : st.w[b]);
+          R rhom = st.rho[a] + st.rho[b];
+          if (nkeep >= 0) {
+            R eem = ee[a] + ee[b];
+            R drhof = R(1), deef = R(1);
+            if (nkeep != 0) {
+              R drho = R(2) * (st.rho[b] - st.rho[a]) / rhom;
+              R dee = R(2) * (ee[b] - ee[a]) / eem;
+              R t_sumdenrho = (R(0.5) * drho) * (R(0.5) * drho);
+              R t_sumdenee = (R(0.5) * dee) * (R(0.5) * dee);
+              R t2r = t_sumdenrho, t2e = t_sumdenee;
+              R sumdenrho = R(1) + t_sumdenrho / R(3);
+              R sumdenee = R(1) + t_sumdenee;
+              R sumnumee = R(1) + t_sumdenee / R(3);
+              for (int n = 2; n <= nkeep; ++n) {
+                R n21 = R(1) + R(2 * n);
+                t_sumdenrho = t2r * t_sumdenrho;
+                t_sumdenee = t2e * t_sumdenee;
+                sumdenrho = sumdenrho + t_sumdenrho / n21;
+                sumdenee = sumdenee + t_sumdenee;
+                sumnumee = sumnumee + t_sumdenee / n21;
+              }
+              drhof = R(1) / sumdenrho;
+              deef = sumnumee / sumdenee;
+            }
+            R uv_part = (vna + vnb) * rhom * drhof;
+            uvs1 = uvs1 + uv_part * R(2);
+            uvs2 = uvs2 + uv_part * (st.u[a] + st.u[b]);
+            uvs3 = uvs3 + uv_part * (st.v[a] + st.v[b]);
+            uvs4 = uvs4 + uv_part * (st.w[a] + st.w[b]);
+            uvs5_i = uvs5_i + uv_part * eem * deef;
+            uvs5_k = uvs5_k + uv_part * (st.u[a] * st.u[b] + st.v[a] * st.v[b] + st.w[a] * st.w[b]);
+            uvs5_p = uvs5_p + R(4) * (vna * pp[b] + vnb * pp[a]);
+            uvs6 = uvs6 + R(2) * (pp[a] + pp[b]);
+          } else {
+            R uv_part = (vna + vnb) * rhom;
+            uvs1 = uvs1 + uv_part * R(2);
+            uvs2 = uvs2 + uv_part * (st.u[a] + st.u[b]);
+            uvs3 = uvs3 + uv_part * (st.v[a] + st.v[b]);
+            uvs4 = uvs4 + uv_part * (st.w[a] + st.w[b]);
+            uvs5 = uvs5 + uv_part * (st.h[a] + st.h[b]);
+            uvs6 = uvs6 + R(2) * (pp[a] + pp[b]);
+          }
+        }
+      }
+      const R cl = R(g.coeff[lmax - 1][l - 1]);
+      ft1 = ft1 + cl * uvs1;
+      ft2 = ft2 + cl * uvs2;
+      ft3 = ft3 + cl * uvs3;
+      ft4 = ft4 + cl * uvs4;
+      ft5 = ft5 + cl * (nkeep >= 0 ? (uvs5_i + uvs5_k + uvs5_p) : uvs5);
+      ft6 = ft6 + cl * uvs6;
+    }
+  }
+  fh[0] = R(0.25) * ft1;
+  fh[1] = R(0.25) * ft2;
+  fh[2] = R(0.25) * ft3;
+  fh[3] = R(0.25) * ft4;
+  fh[4] = R(0.25) * ft5;
+  if (zero_flux) {
+#pragma unroll
+    for (int m = 0; m < 5; ++m) fh[m] = R(0);
+  }
+  fh[1 + DIR] = fh[1 + DIR] + R(0.5) * ft6;
+}
+
+// Characteristic WENO flux: compute_roe_average (kernels_cpu.F90:3013-3089), eigenvectors_{x,y,z}
+// (:2728-2782, :2842-2896, :2956-3010), local Lax-Friedrichs splitting with the stencil maximum
+// of |u_n -+ c| (:614-675) and wenorec_1d; back-projection with the right eigenvectors (:677-683).
+template <class R, int DIR, int WS, int S>
+__device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5]) {
+  const R rgas0 = R(g.rgas0);
+  const int o0 = S - 1, o1 = S;  // the two points adjacent to the face
+  // Roe average
+  R uu = st.u[o0], vv = st.v[o0], ww = st.w[o0], h = st.h[o0];
+  R r = st.rho[o1] / st.rho[o0];
+  r = sqrt(r);
+  R rho = r * st.rho[o0];
+  R rp1 = R(1) / (r + R(1));
+  uu = (r * st.u[o1] + uu) * rp1;
+  vv = (r * st.v[o1] + vv) * rp1;
+  ww = (r * st.w[o1] + ww) * rp1;
+  h = (r * st.h[o1] + h) * rp1;
+  R qq = R(0.5) * (uu * uu + vv * vv + ww * ww);
+  R hbar = h - qq - R(g.cp_last) * R(g.t0);
+  R tt = R(g.t0) + hbar / R(g.cp0);
+  R gamloc = R(g.gamloc);
+  R cc = gamloc * tt * rgas0;
+  R gm1loc = gamloc - R(1);
+  R c = sqrt(cc);
+  R ci = R(1) / c;
+  R p_rho = tt * rgas0;
+  R p_e = rho * gm1loc;
+  R etot = h - tt * rgas0;
+  R b3 = etot - rho * p_rho / p_e;
+  R b2 = p_e / (rho * cc);
+  R b1 = p_rho / cc - b2 * (etot - R(2) * qq);
+  const R vel[3] = {uu, vv, ww};
+  const R vn = vel[DIR];
+  constexpr int t1 = DIR == 0 ? 1 : 0;
+  constexpr int t2 = DIR == 2 ? 1 : 2;
+  // stencil maximum of the characteristic speeds (offsets -WS+1 .. WS)
+  R ev0 = R(-1), ev1 = R(-1), ev4 = R(-1);
+#pragma unroll
+  for (int l = 0; l < 2 * WS; ++l) {
+    const int q = l + S - WS;
+    const R vnq = DIR == 0 ? st.u[q] : (DIR == 1 ? st.v[q] : st.w[q]);
+    R cs = sqrt(gamloc * rgas0 * st.t[q]);
+    ev0 = fmax(fabs(vnq - cs), ev0);
+    ev1 = fmax(fabs(vnq), ev1);
+    ev4 = fmax(fabs(vnq + cs), ev4);
+  }
+  const R betascale_a = R(1) / (R(g.rho0) * R(g.rho0) * (R(g.u0) * R(g.u0)));
+  const R betascale_b = R(1) / (R(g.rho0) * R(g.rho0) * (R(g.u0) * R(g.u0)) * (R(g.u0) * R(g.u0)));
+#pragma unroll
+  for (int m = 0; m < 5; ++m) fh[m] = R(0);
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    // column m of the left eigenvector matrix el(1:5, m)
+    R e0, e1, e2, e3, e4;
+    if (m == 0 || m == 4) {
+      const R sgn = m == 0 ? R(1) : R(-1);
+      e0 = R(0.5) * (b1 + sgn * (vn * ci));
+      e1 = R(-0.5) * (DIR == 0 ? b2 * uu + sgn * ci : b2 * uu);
+      e2 = R(-0.5) * (DIR == 1 ? b2 * vv + sgn * ci : b2 * vv);
+      e3 = R(-0.5) * (DIR == 2 ? b2 * ww + sgn * ci : b2 * ww);
+      e4 = R(0.5) * b2;
+    } else if (m == 1) {
+      e0 = R(1) - b1; e1 = b2 * uu; e2 = b2 * vv; e3 = b2 * ww; e4 = -b2;
+    } else {
+      const int tt_ = m == 2 ? t1 : t2;
+      e0 = -vel[tt_];
+      e1 = tt_ == 0 ? R(1) : R(0);
+      e2 = tt_ == 1 ? R(1) : R(0);
+      e3 = tt_ == 2 ? R(1) : R(0);
+      e4 = R(0);
+    }
+    const R evm = m == 0 ? ev0 : (m == 4 ? ev4 : ev1);
+    R gp[2 * WS], gm[2 * WS];
+#pragma unroll
+    for (int l = 0; l < 2 * WS; ++l) {
+      const int q = l + S - WS;
+      const R rr = st.rho[q], u1 = st.u[q], v1 = st.v[q], w1 = st.w[q], h1 = st.h[q];
+      const R vnq = DIR == 0 ? u1 : (DIR == 1 ? v1 : w1);
+      const R rhovn = rr * vnq;
+      const R pp = rr * st.t[q] * rgas0;
+      R f1 = u1 * rhovn, f2 = v1 * rhovn, f3 = w1 * rhovn;
+      if (DIR == 0) f1 = f1 + pp;
+      if (DIR == 1) f2 = f2 + pp;
+      if (DIR == 2) f3 = f3 + pp;
+      const R f4 = h1 * rhovn;
+      R wc = R(0), gc = R(0);
+      wc = wc + e0 * rr;
+      gc = gc + e0 * rhovn;
+      wc = wc + e1 * rr * u1;
+      gc = gc + e1 * f1;
+      wc = wc + e2 * rr * v1;
+      gc = gc + e2 * f2;
+      wc = wc + e3 * rr * w1;
+      gc = gc + e3 * f3;
+      wc = wc + e4 * (rr * h1 - pp);
+      gc = gc + e4 * f4;
+      R cm = R(0.5) * (gc + evm * wc);
+      gp[l] = cm;
+      gm[l] = gc - cm;
+    }
+    const R bs = (m == 2 || m == 3) ? betascale_b : betascale_a;
+    const R fi = wenorec<R, WS>(gp, gm, ord, g.weno_version, bs);
+    // row m of the right eigenvector matrix er(m, 1:5)
+    R r0, r1, r2, r3, r4;
+    if (m == 0 || m == 4) {
+      const R sc = m == 0 ? -c : c;
+      r0 = R(1);
+      r1 = DIR == 0 ? uu + sc : uu;
+      r2 = DIR == 1 ? vv + sc : vv;
+      r3 = DIR == 2 ? ww + sc : ww;
+      r4 = m == 0 ? h - vn * c : h + vn * c;
+    } else if (m == 1) {
+      r0 = R(1); r1 = uu; r2 = vv; r3 = ww; r4 = b3;
+    } else {
+      const int tt_ = m == 2 ? t1 : t2;
+      r0 = R(0);
+      r1 = tt_ == 0 ? R(1) : R(0);
+      r2 = tt_ == 1 ? R(1) : R(0);
+      r3 = tt_ == 2 ? R(1) : R(0);
+      r4 = vel[tt_];
+    }
+    fh[0] = fh[0] + r0 * fi;
+    fh[1] = fh[1] + r1 * fi;
+    fh[2] = fh[2] + r2 * fi;
+    fh[3] = fh[3] + r3 * fi;
+    fh[4] = fh[4] + r4 * fi;
+  }
+}
+
+}  // namespace sb200

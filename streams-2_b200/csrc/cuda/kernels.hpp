@@ -1,0 +1,51 @@
+// Host-side launchers of the stage kernels (implemented in stage_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace sb200 {
+
+// Device buffers of one context (single block).
+struct DevState {
+  double* w = nullptr;        // ghosted, 5 variables
+  double* aux = nullptr;      // ghosted, 7 variables: rho, u, v, w, H, T, mu
+  double* sensor = nullptr;   // interior: Ducros theta used by the fluxes
+  double* sensor_next = nullptr;
+  double* div3 = nullptr;     // interior: div/3
+  double* fl_a = nullptr;     // interior, 5 variables (two RK registers, ping-pong)
+  double* fl_b = nullptr;
+  double* wallprop = nullptr; // nx*nz*3
+  double* red = nullptr;      // block partials of the reductions
+  Scalars* sc = nullptr;      // device scalars
+  long long red_capacity = 0; // doubles in red
+};
+
+struct StageArgs {
+  int istep;           // 1..nrk
+  double rhork, gamrk; // RK coefficients of the stage
+  int apply_shift;     // aux pass applies the pending force_var energy shift
+  int want_stats;      // update pass accumulates residual and min/max (stage 3)
+  int run_aux;         // recompute aux (skipped when it is already current)
+  int add_time;        // accumulate time += dt on the device after the stage
+};
+
+// Launch-count instrumentation is kept by the caller.
+cudaError_t launch_aux(const Geom& g, DevState& d, int apply_shift, cudaStream_t s, long long* nl);
+cudaError_t launch_init_sensor(const Geom& g, DevState& d, cudaStream_t s, long long* nl);
+cudaError_t launch_dt(const Geom& g, DevState& d, double cfl, cudaStream_t s, long long* nl);
+// One RK stage.  fl_prev holds the previous stage's right-hand side (unused at stage 1),
+// fl_new receives this stage's.  At stage 3 the next Ducros sensor becomes current.
+cudaError_t launch_stage(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
+                         cudaStream_t s, long long* nl);
+bool stage_supported(int lmax_base, int weno_scheme);
+cudaError_t launch_apply_shift(const Geom& g, DevState& d, cudaStream_t s, long long* nl);
+cudaError_t launch_fill_ghosts(const Geom& g, DevState& d, cudaStream_t s, long long* nl);
+cudaError_t launch_count_weno(const Geom& g, DevState& d, cudaStream_t s, long long* nl);
+cudaError_t launch_add_time(DevState& d, cudaStream_t s, long long* nl);
+
+// partial-sum slots needed for a geometry
+long long reduction_slots(const Geom& g);
+
+}  // namespace sb200

@@ -1,0 +1,303 @@
+"""Python binding of the B200 backend C ABI (ctypes).
+
+This is a thin host-side mirror of the solver-object interface of STREAmS-2
+(``equation_singleideal_<backend>_object``, code/src/singleideal/singleideal_cpu.F90:99-135):
+``Solver`` wraps one device context and exposes ``init_run``, ``compute_dt``, ``rk_sync``,
+``compute_residual``, ``copy_from_field``/``copy_to_field`` and a no-sync ``advance`` loop;
+``Case`` wraps the host set-up of a ``singleideal.ini`` case.  All compute happens in the
+compiled library ``lib/libstreams_b200.so``; importing this module fails loudly when the
+library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE.parent / "lib" / "libstreams_b200.so"
+
+OK, EINVAL, ECUDA, ENOMEM, ENAN, ETIMEOUT, ENODEV = 0, -1, -2, -3, -4, -5, -6
+
+
+class Params(C.Structure):
+    """Mirror of ``streams_b200_params`` (include/streams_b200.h)."""
+
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("ng", C.c_int),
+        ("ep_order", C.c_int), ("nkeep", C.c_int), ("weno_scheme", C.c_int), ("weno_version", C.c_int),
+        ("flux_splitting", C.c_int), ("conservative_viscous", C.c_int),
+        ("sensor_threshold", C.c_double),
+        ("bctags", C.c_int * 6), ("force_zero_flux", C.c_int * 6),
+        ("eul_imin", C.c_int), ("eul_imax", C.c_int), ("eul_jmin", C.c_int),
+        ("eul_jmax", C.c_int), ("eul_kmin", C.c_int), ("eul_kmax", C.c_int),
+        ("is_y_staggered", C.c_int),
+        ("visc_model", C.c_int), ("calorically_perfect", C.c_int),
+        ("mu0", C.c_double), ("t0", C.c_double), ("rgas0", C.c_double), ("rho0", C.c_double),
+        ("u0", C.c_double), ("l0", C.c_double),
+        ("sutherland_s", C.c_double), ("t_ref_dim", C.c_double), ("powerlaw_vtexp", C.c_double),
+        ("prandtl", C.c_double),
+        ("cp0", C.c_double), ("cv0", C.c_double), ("cp_last", C.c_double), ("cv_last", C.c_double),
+        ("channel_case", C.c_int),
+        ("theta_wall", C.c_double), ("t_wall", C.c_double), ("t_bulk_target", C.c_double),
+        ("volchan", C.c_double),
+        ("nrk", C.c_int),
+        ("rhork", C.c_double * 4), ("gamrk", C.c_double * 4),
+        ("cfl", C.c_double),
+        ("precision", C.c_int),
+    ]
+
+
+class Grid(C.Structure):
+    """Mirror of ``streams_b200_grid``."""
+
+    _fields_ = [(n, C.POINTER(C.c_double)) for n in
+                ("x", "y", "z", "yn", "dcsidx", "detady", "dzitdz", "dcsidxs", "detadys", "dzitdzs",
+                 "coeff_deriv1")] + [(n, C.POINTER(C.c_int)) for n in ("ep_ord_x", "ep_ord_y", "ep_ord_z")]
+
+
+class BackendError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"streams_b200 error {code}: {msg}")
+        self.code = code
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C streams-2_b200` "
+                          "(or __graft_entry__.build()); there is no CPU fallback")
+    lib = C.CDLL(str(LIB_PATH))
+    P, V, D, I, LL = C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_longlong
+    sig = {
+        "streams_b200_abi_version": (I, []),
+        "streams_b200_global_error": (C.c_char_p, []),
+        "streams_b200_create": (I, [C.POINTER(Params), C.POINTER(Grid), C.POINTER(P)]),
+        "streams_b200_destroy": (I, [P]),
+        "streams_b200_last_error": (C.c_char_p, [P]),
+        "streams_b200_footprint_bytes": (LL, [C.POINTER(Params)]),
+        "streams_b200_copy_from_field": (I, [P, D]),
+        "streams_b200_copy_to_field": (I, [P, D]),
+        "streams_b200_copy_from_device": (I, [P, V]),
+        "streams_b200_copy_to_device": (I, [P, V]),
+        "streams_b200_init_run": (I, [P]),
+        "streams_b200_compute_dt": (I, [P, D]),
+        "streams_b200_set_dt": (I, [P, C.c_double]),
+        "streams_b200_set_time": (I, [P, C.c_double]),
+        "streams_b200_rk_sync": (I, [P]),
+        "streams_b200_advance": (I, [P, I, I, I, I]),
+        "streams_b200_get_scalars": (I, [P, D]),
+        "streams_b200_compute_residual": (I, [P, D]),
+        "streams_b200_count_weno": (I, [P, D]),
+        "streams_b200_get_wallprop": (I, [P, D]),
+        "streams_b200_synchronize": (I, [P]),
+        "streams_b200_launch_count": (LL, [P]),
+        "streams_b200_debug_fetch": (I, [P, I, D, LL]),
+        "streams_b200_case_load": (I, [C.c_char_p, C.c_char_p, C.POINTER(P)]),
+        "streams_b200_case_free": (I, [P]),
+        "streams_b200_case_error": (C.c_char_p, []),
+        "streams_b200_case_params": (I, [P, I, C.POINTER(Params)]),
+        "streams_b200_case_grid": (I, [P, C.POINTER(Grid)]),
+        "streams_b200_case_field": (D, [P]),
+        "streams_b200_case_info": (I, [P, D]),
+        "streams_b200_case_write_restart": (I, [P, C.c_char_p]),
+        "streams_b200_run_case": (I, [P, I, I, C.c_char_p, D, D]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+# Every symbol the C headers declare (checked by the CPU test suite).
+EXPORTED = [
+    "streams_b200_abi_version", "streams_b200_global_error", "streams_b200_create", "streams_b200_destroy",
+    "streams_b200_last_error", "streams_b200_footprint_bytes", "streams_b200_copy_from_field",
+    "streams_b200_copy_to_field", "streams_b200_copy_from_device", "streams_b200_copy_to_device",
+    "streams_b200_init_run", "streams_b200_compute_dt", "streams_b200_set_dt", "streams_b200_rk_sync",
+    "streams_b200_advance", "streams_b200_get_scalars", "streams_b200_set_time", "streams_b200_compute_residual",
+    "streams_b200_count_weno", "streams_b200_get_wallprop", "streams_b200_synchronize",
+    "streams_b200_launch_count", "streams_b200_debug_fetch", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
+    "streams_b200_case_params", "streams_b200_case_grid", "streams_b200_case_field", "streams_b200_case_info",
+    "streams_b200_case_write_restart", "streams_b200_run_case",
+]
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Case:
+    """Host set-up of a case (``singleideal.ini`` in ``directory`` or ``ini_text``)."""
+
+    def __init__(self, directory: str | os.PathLike = ".", ini_text: str | None = None):
+        h = C.c_void_p()
+        rc = lib.streams_b200_case_load(str(directory).encode(), (ini_text or "").encode(), C.byref(h))
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_case_error().decode())
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.streams_b200_case_free(h)
+            self._h = None
+
+    def params(self, precision: int = 0) -> Params:
+        p = Params()
+        lib.streams_b200_case_params(self._h, precision, C.byref(p))
+        return p
+
+    def grid(self) -> Grid:
+        g = Grid()
+        lib.streams_b200_case_grid(self._h, C.byref(g))
+        return g
+
+    @property
+    def shape(self):
+        p = self.params()
+        return p.nx, p.ny, p.nz, p.ng
+
+    def field(self) -> np.ndarray:
+        """Initial conserved field as an array w[m, k, j, i] (ghosts included; a copy)."""
+        nx, ny, nz, ng = self.shape
+        n = (nx + 2 * ng) * (ny + 2 * ng) * (nz + 2 * ng) * 5
+        ptr = lib.streams_b200_case_field(self._h)
+        a = np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+        return a.reshape(5, nz + 2 * ng, ny + 2 * ng, nx + 2 * ng)
+
+    def info(self) -> dict:
+        out = np.zeros(12)
+        lib.streams_b200_case_info(self._h, _dptr(out))
+        keys = ["u0", "rho0", "l0", "mu0", "num_iter", "print_control", "iter_dt_recompute", "icyc0", "time0",
+                "cfl", "volchan", "t_bulk_target"]
+        return dict(zip(keys, out.tolist()))
+
+    def write_restart(self, directory: str | os.PathLike) -> None:
+        rc = lib.streams_b200_case_write_restart(self._h, str(directory).encode())
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_case_error().decode())
+
+    def run(self, nsteps: int = -1, precision: int = 0, progress_path: str | None = None,
+            return_field: bool = False):
+        """The solver's run() loop on the device; returns (last progress row, final field or None)."""
+        row = np.zeros(14)
+        w = None
+        if return_field:
+            nx, ny, nz, ng = self.shape
+            w = np.zeros((5, nz + 2 * ng, ny + 2 * ng, nx + 2 * ng))
+        rc = lib.streams_b200_run_case(self._h, nsteps, precision,
+                                       progress_path.encode() if progress_path else None,
+                                       _dptr(row), _dptr(w) if w is not None else None)
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_case_error().decode())
+        return row, w
+
+
+class Solver:
+    """One device context: the B200 counterpart of the backend solver object."""
+
+    def __init__(self, params: Params, grid: Grid, keepalive=None):
+        self._keep = keepalive
+        h = C.c_void_p()
+        rc = lib.streams_b200_create(C.byref(params), C.byref(grid), C.byref(h))
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_global_error().decode())
+        self._h = h
+        self.params = params
+        self.shape = (params.nx, params.ny, params.nz, params.ng)
+
+    @classmethod
+    def from_case(cls, case: Case, precision: int = 0) -> "Solver":
+        s = cls(case.params(precision), case.grid(), keepalive=case)
+        s.copy_from_field(case.field())
+        return s
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.streams_b200_destroy(h)
+            self._h = None
+
+    __del__ = close
+
+    def _check(self, rc: int):
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_last_error(self._h).decode())
+
+    def copy_from_field(self, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        self._check(lib.streams_b200_copy_from_field(self._h, _dptr(w)))
+        self._sync_keep = w  # the copy is asynchronous: keep the host buffer alive
+        self.synchronize()
+
+    def copy_to_field(self) -> np.ndarray:
+        nx, ny, nz, ng = self.shape
+        w = np.zeros((5, nz + 2 * ng, ny + 2 * ng, nx + 2 * ng))
+        self._check(lib.streams_b200_copy_to_field(self._h, _dptr(w)))
+        return w
+
+    def init_run(self):
+        self._check(lib.streams_b200_init_run(self._h))
+
+    def compute_dt(self) -> float:
+        dt = C.c_double()
+        self._check(lib.streams_b200_compute_dt(self._h, C.byref(dt)))
+        return dt.value
+
+    def set_dt(self, dt: float):
+        self._check(lib.streams_b200_set_dt(self._h, dt))
+
+    def set_time(self, t: float):
+        self._check(lib.streams_b200_set_time(self._h, t))
+
+    def rk_sync(self):
+        self._check(lib.streams_b200_rk_sync(self._h))
+
+    def advance(self, nsteps: int, iter_dt_recompute: int = 1, icyc_start: int = 0, icyc0: int = 0):
+        self._check(lib.streams_b200_advance(self._h, nsteps, iter_dt_recompute, icyc_start, icyc0))
+
+    def scalars(self) -> dict:
+        out = np.zeros(7)
+        self._check(lib.streams_b200_get_scalars(self._h, _dptr(out)))
+        return dict(zip(["dt", "time", "dpdx", "rhobulk", "ubulk", "tbulk", "tbdiff"], out.tolist()))
+
+    def compute_residual(self) -> dict:
+        out = np.zeros(7)
+        rc = lib.streams_b200_compute_residual(self._h, _dptr(out))
+        if rc not in (OK, ENAN):
+            self._check(rc)
+        d = dict(zip(["residual_rhou", "rhomin", "rhomax", "tmin", "tmax", "pmin", "pmax"], out.tolist()))
+        d["nan"] = rc == ENAN
+        return d
+
+    def count_weno(self):
+        out = np.zeros(3)
+        self._check(lib.streams_b200_count_weno(self._h, _dptr(out)))
+        return out
+
+    def wallprop(self) -> np.ndarray:
+        nx, ny, nz, ng = self.shape
+        out = np.zeros(3 * nx * nz)
+        self._check(lib.streams_b200_get_wallprop(self._h, _dptr(out)))
+        return out.reshape(3, nz, nx)
+
+    def synchronize(self):
+        self._check(lib.streams_b200_synchronize(self._h))
+
+    def debug_fetch(self, which: int) -> np.ndarray:
+        """Internal arrays: 0 aux (7 ghosted), 1 last stage RHS fl (5), 2 sensor, 3 div/3."""
+        nx, ny, nz, ng = self.shape
+        gs = (nz + 2 * ng, ny + 2 * ng, nx + 2 * ng)
+        shapes = {0: (7,) + gs, 1: (5, nz, ny, nx), 2: (nz, ny, nx), 3: (nz, ny, nx)}
+        out = np.zeros(shapes[which])
+        self._check(lib.streams_b200_debug_fetch(self._h, which, _dptr(out), out.size))
+        return out
+
+    @property
+    def launches(self) -> int:
+        return int(lib.streams_b200_launch_count(self._h))
