@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 backend: throughput of the per-RK-stage RHS + update of the Cartesian
+channel in Mcell-steps/s (1 cell-step = one interior cell advanced one full RK3 step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size NXxNYxNZ]
+
+Default workload: the supersonic turbulent channel of the benchmark suite at its largest
+single-GPU size, 512x256x256 (the enlarged channel), in FP64: domain 2pi x 2 x pi, tanh-stretched
+staggered y (factor 1.5), isothermal walls, gamma 1.4, Pr 0.72, power-law viscosity 0.76, bulk
+Mach 1.5, bulk Reynolds 3000 with bulk-flow and bulk-temperature forcing, hybrid 6th-order central /
+WENO5 with Ducros threshold 0.05, CFL 0.8.  Seeded synthetic initial field: Poiseuille u (peak
+1.5 u_b), v = w = 0, uniform density and wall temperature, +-10% uniform random velocity noise.
+
+The b200 arm prints one JSON line with: device-timed throughput (value, CUDA events on the
+context's stream, max over ranks), the end-to-end throughput through the C ABI with pinned host
+buffers (e2e), the roofline of the dominant kernel from live per-kernel CUDA events, the CPU
+oracle timed on the host cores (cpu_baseline), and the SM clocks sampled during the timed region.
+With --gpus N > 1 each rank advances an independent replica (the path has no exchange step).
+--impl reference times the CPU restatement of the reference's CPU backend (oracle/) on the host.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for p in (ROOT / "streams-2_b200", ROOT / "oracle", ROOT / "tests"):
+    sys.path.insert(0, str(p))
+
+# Algorithmic (compulsory) bytes per interior cell of one launch of each kernel: the fields the
+# kernel must read and write once; stencil re-reads of neighbours are excluded.
+ALG_BYTES_PER_CELL = {
+    "k_aux": 40 + 56,                          # read w (5), write rho,u,v,w,H,T,mu
+    "k_euler_x": 6 * 8 + 8 + 40,               # read rho,u,v,w,H,T + sensor, write fl (5)
+    "k_visc": 5 * 8 + 32 + 32 + 8,             # read u,v,w,T,mu + fl(2:5), write fl(2:5) + div/3
+    "k_euler_y": 6 * 8 + 8 + 40 + 40,          # + read-modify-write fl
+    "k_euler_z": 7 * 8 + 8 + 8 + 40 + 40 + 32,  # + div/3, fl_prev(1:2), w(1:2)
+    "k_update": 40 + 40 + 40 + 8 + 40,         # read w, fl_prev, fl_new, u; write w
+    "k_dt": 8 + 5 * 8,
+}
+# Compulsory traffic of a whole RK3 step per cell (state read/written once per stage, RK register).
+STEP_BYTES_PER_CELL = 440
+
+
+def parse_size(s):
+    a = [int(v) for v in s.lower().split("x")]
+    assert len(a) == 3
+    return a
+
+
+def peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.out:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.out.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def channel_case_ini(nx, ny, nz, steps):
+    from conftest import channel_ini
+    return channel_ini(nx, ny, nz, num_iter=steps, print_control=max(1, steps))
+
+
+def cpu_oracle_rate(nx, ny, nz, nsteps, budget_s=20.0):
+    """Oracle (restated CPU backend) throughput on a slab of the workload: all host threads."""
+    from oracle_py import Oracle
+    ini = channel_case_ini(nx, ny, nz, nsteps)
+    with tempfile.TemporaryDirectory() as d:
+        o = Oracle(d, ini)
+        o.init_run()
+        o.step()  # warm-up step (first-touch of the arrays)
+        t0 = time.perf_counter()
+        n = 0
+        while n < nsteps:
+            o.step()
+            n += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+        dt = time.perf_counter() - t0
+    return nx * ny * nz * n / dt / 1e6, n, dt
+
+
+def sample_dims(nx, ny, nz, target_cells=2_200_000):
+    """Slab of the workload with the same x-y plane and fewer z planes (at least 8)."""
+    kz = max(8, min(nz, target_cells // (nx * ny)))
+    return nx, ny, kz
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nx, ny, nz = parse_size(args.size)
+    sx, sy, sz = sample_dims(nx, ny, nz)
+    from oracle_py import Oracle
+    threads = os.environ.get("ORACLE_THREADS") or str(os.cpu_count() or 1)
+    ini = channel_case_ini(sx, sy, sz, args.steps)
+    with tempfile.TemporaryDirectory() as d:
+        o = Oracle(d, ini)
+        o.init_run()
+        for _ in range(args.warmup):
+            o.step()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            o.step()
+        dt = time.perf_counter() - t0
+    value = sx * sy * sz * args.steps / dt / 1e6
+    line = {
+        "impl": "reference", "metric": "Mcell-steps/s", "value": value, "unit": "Mcell-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(nx, ny, nz),
+        "cpu_baseline": {"value": value, "unit": "Mcell-steps/s", "cores": int(threads), "kind": "port",
+                         "sample": f"{sx}x{sy}x{sz} slab of the {nx}x{ny}x{nz} channel, {args.steps} RK3 steps"},
+        "e2e": {"value": value, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's Fortran/MPI CPU backend cannot be built on this image (no Fortran compiler, "
+                "no MPI); this arm times the C++ restatement of that backend (oracle/), pinned to the "
+                "reference's golden row",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(nx, ny, nz):
+    return {"workload": f"supersonic channel {nx}x{ny}x{nz} FP64, hybrid central-6/WENO5 (Ducros 0.05), "
+                        "Mach_b 1.5, Re_b 3000, power-law mu, CFL 0.8",
+            "grid": [nx, ny, nz], "cells": nx * ny * nz, "precision": "fp64",
+            "l2_policy": "inputs larger than L2 (state ~12 x 8 B per cell)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", default="512x256x256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from streams_b200 import Case, Solver
+
+    nx, ny, nz = parse_size(args.size)
+    ncell = nx * ny * nz
+    with tempfile.TemporaryDirectory() as d:
+        case = Case(d, channel_case_ini(nx, ny, nz, args.steps))
+    info = case.info()
+    s = Solver.from_case(case)
+    s.init_run()
+    stream = torch.cuda.ExternalStream(s.stream_handle)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    s.advance(args.warmup, 1, 0, 0)
+    s.synchronize()
+    icyc = args.warmup
+
+    # timed region: device-resident state, CUDA events on the context's stream
+    barrier()
+    l0 = s.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        s.advance(args.steps, 1, icyc, 0)
+        ev1.record(stream)
+        s.synchronize()
+        barrier()
+    icyc += args.steps
+    launches = s.launches - l0
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = ncell * args.steps * world / (ms / 1e3) / 1e6
+
+    # per-kernel device time (separate pass with the event profiler on)
+    s.profile(-1)
+    s.profile(1)
+    s.advance(args.steps, 1, icyc, 0)
+    icyc += args.steps
+    s.synchronize()
+    s.profile(0)
+    prof = s.profile_report()
+    total_prof = sum(v[0] for v in prof.values())
+    dom = max((k for k in prof if k in ALG_BYTES_PER_CELL), key=lambda k: prof[k][0])
+    dom_ms = prof[dom][0] / prof[dom][1]
+    dom_bytes = ALG_BYTES_PER_CELL[dom] * ncell
+    peak, peak_kind = peaks()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "dram_traffic.json"
+    if tf.exists():
+        t = json.loads(tf.read_text()).get(dom)
+        if t:
+            traffic = t["bytes_per_cell"] * ncell
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                "alg_bytes_per_cell": ALG_BYTES_PER_CELL[dom], "launch_ms": dom_ms,
+                "share": prof[dom][0] / total_prof}
+    step_gbs = STEP_BYTES_PER_CELL * ncell * args.steps / (ms / 1e3) / 1e9
+    step_roofline = {"bytes_per_cell_step": STEP_BYTES_PER_CELL, "achieved": step_gbs, "peak": peak,
+                     "frac": step_gbs / peak, "unit": "GB/s", "peak_kind": peak_kind}
+    kernels = {k: {"ms_per_launch": v[0] / v[1], "launches": v[1], "share": v[0] / total_prof}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
+
+    # end to end through the C ABI with pinned host buffers: upload the field, run, read the
+    # progress scalars after every step (the step's metric), download the final field
+    nbytes = 5 * (nx + 6) * (ny + 6) * (nz + 6) * 8
+    hin = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    hout = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    hin.numpy()[:] = case.field().reshape(-1)
+    s2 = Solver(case.params(0), case.grid(), keepalive=case)
+    st2 = torch.cuda.ExternalStream(s2.stream_handle)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    t0 = time.perf_counter()
+    e0.record(st2)
+    s2.copy_from_host_ptr(hin.data_ptr())
+    s2.init_run()
+    for n in range(args.steps):
+        s2.advance(1, 1, n, 0)
+        s2.scalars()
+    s2.copy_to_host_ptr(hout.data_ptr())
+    e1.record(st2)
+    s2.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_val = ncell * args.steps * world / (e2e_ms / 1e3) / 1e6
+    s2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            sx, sy, sz = sample_dims(nx, ny, nz)
+            rate, nst, sec = cpu_oracle_rate(sx, sy, sz, 5)
+            cpu = {"value": rate, "unit": "Mcell-steps/s", "cores": int(os.environ.get("ORACLE_THREADS") or
+                                                                       (os.cpu_count() or 1)),
+                   "kind": "port", "sample": f"{sx}x{sy}x{sz} slab of the {nx}x{ny}x{nz} channel, {nst} RK3 steps "
+                                             f"in {sec:.1f} s"}
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": "Mcell-steps/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+
+    res = s.compute_residual()
+    sc = s.scalars()
+    if rank == 0:
+        line = {
+            "metric": "Mcell-steps/s", "value": value, "unit": "Mcell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(nx, ny, nz),
+            "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": nbytes / args.steps,
+                    "d2h_bytes_per_step": (nbytes + 56 * args.steps) / args.steps, "wall_s": wall,
+                    "what": "copy_from_field (pinned) + init_run + K x (rk step + scalar read) + copy_to_field"},
+            "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
+            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu,
+            "state": {"dt": sc["dt"], "rhobulk": sc["rhobulk"], "ubulk": sc["ubulk"], "tbulk": sc["tbulk"],
+                      "residual_rhou": res["residual_rhou"], "nan": res["nan"]},
+            "u0": info["u0"],
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -179,6 +179,20 @@ int streams_b200_synchronize(streams_b200_ctx* ctx);
 /* Number of kernel launches issued by this context since creation (instrumentation). */
 long long streams_b200_launch_count(const streams_b200_ctx* ctx);
 
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own work after it. */
+int streams_b200_get_stream(streams_b200_ctx* ctx, void** stream);
+
+/*
+ * Per-kernel CUDA-event timing.  profile_enable(ctx, 1) records an event pair around every
+ * launch of the context from then on (0 stops and keeps the totals; -1 clears them);
+ * profile_read resolves the recorded events and returns the accumulated device time and launch
+ * count of kernel kid (0 <= kid < streams_b200_kernel_count()).
+ */
+int streams_b200_profile_enable(streams_b200_ctx* ctx, int on);
+int streams_b200_profile_read(streams_b200_ctx* ctx, int kid, double* total_ms, long long* count);
+int streams_b200_kernel_count(void);
+const char* streams_b200_kernel_name(int kid);
+
 /*
  * Diagnostics: copy an internal device array to the host (synchronous).  which =
  *   0  aux fields rho, u, v, w, H, T, mu (7 ghosted arrays, w_aux(:,:,:,1:7))   7*nvol doubles

@@ -26,6 +26,7 @@ struct streams_b200_ctx {
   bool aux_current = false;    // aux matches w (no update since the last aux pass)
   bool have_stats = false;
   long long launches = 0;
+  Prof prof;
   std::vector<void*> allocs;
   std::string err;
 };
@@ -144,6 +145,7 @@ int streams_b200_destroy(streams_b200_ctx* ctx) {
   if (!ctx) return STREAMS_B200_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->prof.resolve();
   for (void* a : ctx->allocs) cudaFree(a);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -222,6 +224,7 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
   if ((e = dev_alloc(c, &d.red, d.red_capacity))) return fail(e, "cudaMalloc(reductions)");
   d.fl_a = c->fl_a;
   d.fl_b = c->fl_b;
+  d.prof = &c->prof;
   if ((e = cudaMemsetAsync(d.w, 0, g.nvol * 5 * 8, c->stream)) || (e = cudaMemsetAsync(d.aux, 0, g.nvol * 7 * 8, c->stream)) ||
       (e = cudaMemsetAsync(d.sensor, 0, g.nint * 8, c->stream)) ||
       (e = cudaMemsetAsync(d.sensor_next, 0, g.nint * 8, c->stream)) ||
@@ -433,6 +436,36 @@ int streams_b200_get_wallprop(streams_b200_ctx* c, double* out) {
   SB_CHECK(c, cudaStreamSynchronize(c->stream));
   return STREAMS_B200_OK;
 }
+
+int streams_b200_get_stream(streams_b200_ctx* c, void** stream) {
+  if (!c || !stream) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  *stream = (void*)c->stream;
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_profile_enable(streams_b200_ctx* c, int on) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  if (on < 0) {
+    c->prof.reset();
+    c->prof.on = false;
+  } else {
+    c->prof.on = on != 0;
+  }
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_profile_read(streams_b200_ctx* c, int kid, double* total_ms, long long* count) {
+  if (!c || kid < 0 || kid >= K_NUM) return set_err(c, STREAMS_B200_EINVAL, "bad kernel id");
+  cudaSetDevice(c->device);
+  SB_CHECK(c, c->prof.resolve());
+  if (total_ms) *total_ms = c->prof.total_ms[kid];
+  if (count) *count = c->prof.count[kid];
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_kernel_count(void) { return K_NUM; }
+const char* streams_b200_kernel_name(int kid) { return kernel_name(kid); }
 
 int streams_b200_debug_fetch(streams_b200_ctx* c, int which, double* out, long long n) {
   if (!c || !out) return set_err(c, STREAMS_B200_EINVAL, "null argument");

@@ -3,9 +3,31 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace sb200 {
+
+// Kernel identifiers of the optional per-kernel event profiler.
+enum KernelId {
+  K_AUX = 0, K_EULER_X, K_VISC, K_EULER_Y, K_EULER_Z, K_FINISH_RHS, K_UPDATE, K_FINISH_UPD, K_DT, K_DT_FINISH,
+  K_INIT_SENSOR, K_APPLY_SHIFT, K_FILL_GHOSTS, K_COUNT_WENO, K_ADD_TIME, K_NUM
+};
+const char* kernel_name(int kid);
+
+// Per-kernel CUDA-event timing (off unless enabled on the context).
+struct Prof {
+  bool on = false;
+  struct Rec { int kid; cudaEvent_t a, b; };
+  std::vector<Rec> pending;
+  double total_ms[K_NUM] = {};
+  long long count[K_NUM] = {};
+  void begin(int kid, cudaStream_t s);
+  void end(cudaStream_t s);
+  cudaError_t resolve();  // synchronises on the recorded events and accumulates
+  void reset();
+};
 
 // Device buffers of one context (single block).
 struct DevState {
@@ -20,6 +42,7 @@ struct DevState {
   double* red = nullptr;      // block partials of the reductions
   Scalars* sc = nullptr;      // device scalars
   long long red_capacity = 0; // doubles in red
+  Prof* prof = nullptr;       // optional per-kernel timing
 };
 
 struct StageArgs {

@@ -703,7 +703,56 @@ __global__ void __launch_bounds__(256) k_count_weno(Geom g, const double* __rest
 
 inline unsigned nblocks(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
+// Wrap one launch with profiler events when profiling is on.
+#define SB_LAUNCH(dst, kid, s, ...)                  \
+  do {                                               \
+    if ((dst).prof && (dst).prof->on) (dst).prof->begin((kid), (s)); \
+    __VA_ARGS__;                                     \
+    if ((dst).prof && (dst).prof->on) (dst).prof->end((s));          \
+  } while (0)
+
 }  // namespace
+
+const char* kernel_name(int kid) {
+  static const char* names[K_NUM] = {"k_aux", "k_euler_x", "k_visc", "k_euler_y", "k_euler_z", "k_finish_rhs",
+                                     "k_update", "k_finish_upd", "k_dt", "k_dt_finish", "k_init_sensor",
+                                     "k_apply_shift", "k_fill_ghosts", "k_count_weno", "k_add_time"};
+  return (kid >= 0 && kid < K_NUM) ? names[kid] : "?";
+}
+
+void Prof::begin(int kid, cudaStream_t s) {
+  Rec r{kid, nullptr, nullptr};
+  cudaEventCreate(&r.a);
+  cudaEventCreate(&r.b);
+  cudaEventRecord(r.a, s);
+  pending.push_back(r);
+}
+
+void Prof::end(cudaStream_t s) { cudaEventRecord(pending.back().b, s); }
+
+cudaError_t Prof::resolve() {
+  cudaError_t err = cudaSuccess;
+  for (auto& r : pending) {
+    cudaError_t e = cudaEventSynchronize(r.b);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, r.a, r.b);
+    if (e == cudaSuccess) {
+      total_ms[r.kid] += ms;
+      count[r.kid] += 1;
+    } else {
+      err = e;
+    }
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  pending.clear();
+  return err;
+}
+
+void Prof::reset() {
+  resolve();
+  for (int k = 0; k < K_NUM; ++k) { total_ms[k] = 0; count[k] = 0; }
+}
 
 long long reduction_slots(const Geom& g) {
   long long a = (long long)nblocks(g.nint, 256) * (NRED_UPD > 9 ? NRED_UPD : 9);
@@ -712,46 +761,46 @@ long long reduction_slots(const Geom& g) {
 }
 
 cudaError_t launch_aux(const Geom& g, DevState& d, int apply_shift, cudaStream_t s, long long* nl) {
-  k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, apply_shift, 0);
+  SB_LAUNCH(d, K_AUX, s, k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, apply_shift, 0));
   ++*nl;
   return cudaGetLastError();
 }
 
 cudaError_t launch_fill_ghosts(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
-  k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, 0, 1);
+  SB_LAUNCH(d, K_FILL_GHOSTS, s, k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, 0, 1));
   ++*nl;
   return cudaGetLastError();
 }
 
 cudaError_t launch_apply_shift(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
-  k_apply_shift<<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.sc);
+  SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.sc));
   ++*nl;
   return cudaGetLastError();
 }
 
 cudaError_t launch_init_sensor(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
-  k_init_sensor<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.aux, d.sensor);
+  SB_LAUNCH(d, K_INIT_SENSOR, s, k_init_sensor<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.aux, d.sensor));
   ++*nl;
   return cudaGetLastError();
 }
 
 cudaError_t launch_dt(const Geom& g, DevState& d, double cfl, cudaStream_t s, long long* nl) {
   const unsigned nb = nblocks(g.nint, 256);
-  k_dt<<<nb, 256, 0, s>>>(g, d.w, d.aux, d.red);
-  k_dt_finish<<<1, FIN_NT, 0, s>>>(d.red, nb, cfl, d.sc);
+  SB_LAUNCH(d, K_DT, s, k_dt<<<nb, 256, 0, s>>>(g, d.w, d.aux, d.red));
+  SB_LAUNCH(d, K_DT_FINISH, s, k_dt_finish<<<1, FIN_NT, 0, s>>>(d.red, nb, cfl, d.sc));
   *nl += 2;
   return cudaGetLastError();
 }
 
 cudaError_t launch_add_time(DevState& d, cudaStream_t s, long long* nl) {
-  k_add_time<<<1, 1, 0, s>>>(d.sc);
+  SB_LAUNCH(d, K_ADD_TIME, s, k_add_time<<<1, 1, 0, s>>>(d.sc));
   ++*nl;
   return cudaGetLastError();
 }
 
 cudaError_t launch_count_weno(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
   const unsigned nb = nblocks(g.nint, 256);
-  k_count_weno<<<nb, 256, 0, s>>>(g, d.sensor, d.red);
+  SB_LAUNCH(d, K_COUNT_WENO, s, k_count_weno<<<nb, 256, 0, s>>>(g, d.sensor, d.red));
   ++*nl;
   return cudaGetLastError();
 }
@@ -764,25 +813,32 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   const dim3 gy((g.nx + EU_TX - 1) / EU_TX, (g.ny + EU_TY - 1) / EU_TY, g.nz);
   const dim3 gz((g.nx + EU_TX - 1) / EU_TX, (g.nz + EU_TY - 1) / EU_TY, g.ny);
   if (a.run_aux) {
-    k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, a.apply_shift, 0);
+    SB_LAUNCH(d, K_AUX, s, k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, a.apply_shift, 0));
     ++*nl;
   }
-  k_euler<0, LB, WS><<<gx, blk, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc, a.rhork, a.gamrk,
-                                        a.istep, d.red);
-  k_visc<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.aux, fl_new, d.div3, d.sensor_next, d.wallprop, a.istep == 3);
-  k_euler<1, LB, WS><<<gy, blk, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc, a.rhork, a.gamrk,
-                                        a.istep, d.red);
-  k_euler<2, LB, WS><<<gz, blk, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc, a.rhork, a.gamrk,
-                                        a.istep, d.red);
+  SB_LAUNCH(d, K_EULER_X, s,
+            k_euler<0, LB, WS><<<gx, blk, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc, a.rhork,
+                                                  a.gamrk, a.istep, d.red));
+  SB_LAUNCH(d, K_VISC, s,
+            k_visc<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.aux, fl_new, d.div3, d.sensor_next, d.wallprop,
+                                                        a.istep == 3));
+  SB_LAUNCH(d, K_EULER_Y, s,
+            k_euler<1, LB, WS><<<gy, blk, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc, a.rhork,
+                                                  a.gamrk, a.istep, d.red));
+  SB_LAUNCH(d, K_EULER_Z, s,
+            k_euler<2, LB, WS><<<gz, blk, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc, a.rhork,
+                                                  a.gamrk, a.istep, d.red));
   *nl += 4;
   if (g.channel_case) {
-    k_finish_rhs<<<1, FIN_NT, 0, s>>>(g, d.red, (long long)gz.x * gz.y * gz.z, a.istep == 1, d.sc);
+    SB_LAUNCH(d, K_FINISH_RHS, s,
+              k_finish_rhs<<<1, FIN_NT, 0, s>>>(g, d.red, (long long)gz.x * gz.y * gz.z, a.istep == 1, d.sc));
     ++*nl;
   }
   const unsigned nbu = nblocks(g.nint, 256);
-  k_update<<<nbu, 256, 0, s>>>(g, d.w, d.aux, fl_prev, fl_new, d.sc, a.rhork, a.gamrk, a.istep, a.want_stats, d.red,
-                               d.sensor_next, d.sensor);
-  k_finish_upd<<<1, FIN_NT, 0, s>>>(g, d.red, nbu, a.want_stats, a.add_time, d.sc);
+  SB_LAUNCH(d, K_UPDATE, s,
+            k_update<<<nbu, 256, 0, s>>>(g, d.w, d.aux, fl_prev, fl_new, d.sc, a.rhork, a.gamrk, a.istep,
+                                         a.want_stats, d.red, d.sensor_next, d.sensor));
+  SB_LAUNCH(d, K_FINISH_UPD, s, k_finish_upd<<<1, FIN_NT, 0, s>>>(g, d.red, nbu, a.want_stats, a.add_time, d.sc));
   *nl += 2;
   return cudaGetLastError();
 }

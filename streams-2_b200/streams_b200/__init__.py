@@ -94,6 +94,11 @@ def _load() -> C.CDLL:
         "streams_b200_synchronize": (I, [P]),
         "streams_b200_launch_count": (LL, [P]),
         "streams_b200_debug_fetch": (I, [P, I, D, LL]),
+        "streams_b200_get_stream": (I, [P, C.POINTER(P)]),
+        "streams_b200_profile_enable": (I, [P, I]),
+        "streams_b200_profile_read": (I, [P, I, D, C.POINTER(LL)]),
+        "streams_b200_kernel_count": (I, []),
+        "streams_b200_kernel_name": (C.c_char_p, [I]),
         "streams_b200_case_load": (I, [C.c_char_p, C.c_char_p, C.POINTER(P)]),
         "streams_b200_case_free": (I, [P]),
         "streams_b200_case_error": (C.c_char_p, []),
@@ -121,7 +126,9 @@ EXPORTED = [
     "streams_b200_init_run", "streams_b200_compute_dt", "streams_b200_set_dt", "streams_b200_rk_sync",
     "streams_b200_advance", "streams_b200_get_scalars", "streams_b200_set_time", "streams_b200_compute_residual",
     "streams_b200_count_weno", "streams_b200_get_wallprop", "streams_b200_synchronize",
-    "streams_b200_launch_count", "streams_b200_debug_fetch", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
+    "streams_b200_launch_count", "streams_b200_debug_fetch", "streams_b200_get_stream",
+    "streams_b200_profile_enable", "streams_b200_profile_read", "streams_b200_kernel_count",
+    "streams_b200_kernel_name", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
     "streams_b200_case_params", "streams_b200_case_grid", "streams_b200_case_field", "streams_b200_case_info",
     "streams_b200_case_write_restart", "streams_b200_run_case",
 ]
@@ -214,8 +221,18 @@ class Solver:
     @classmethod
     def from_case(cls, case: Case, precision: int = 0) -> "Solver":
         s = cls(case.params(precision), case.grid(), keepalive=case)
-        s.copy_from_field(case.field())
+        # upload the case's initial field straight from the set-up's own buffer
+        s._check(lib.streams_b200_copy_from_field(s._h, lib.streams_b200_case_field(case._h)))
+        s.synchronize()
         return s
+
+    def copy_from_host_ptr(self, ptr: int) -> None:
+        """Upload w from a host address (e.g. a pinned buffer); asynchronous on the context stream."""
+        self._check(lib.streams_b200_copy_from_field(self._h, C.cast(C.c_void_p(ptr), C.POINTER(C.c_double))))
+
+    def copy_to_host_ptr(self, ptr: int) -> None:
+        """Download w (ghosts rebuilt) to a host address; returns after the copy completed."""
+        self._check(lib.streams_b200_copy_to_field(self._h, C.cast(C.c_void_p(ptr), C.POINTER(C.c_double))))
 
     def close(self):
         h = getattr(self, "_h", None)
@@ -296,6 +313,26 @@ class Solver:
         shapes = {0: (7,) + gs, 1: (5, nz, ny, nx), 2: (nz, ny, nx), 3: (nz, ny, nx)}
         out = np.zeros(shapes[which])
         self._check(lib.streams_b200_debug_fetch(self._h, which, _dptr(out), out.size))
+        return out
+
+    @property
+    def stream_handle(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        h = C.c_void_p()
+        self._check(lib.streams_b200_get_stream(self._h, C.byref(h)))
+        return int(h.value or 0)
+
+    def profile(self, on: int):
+        self._check(lib.streams_b200_profile_enable(self._h, on))
+
+    def profile_report(self) -> dict:
+        """{kernel name: (total device ms, launches)} from the event profiler."""
+        out = {}
+        for kid in range(lib.streams_b200_kernel_count()):
+            ms, n = C.c_double(), C.c_longlong()
+            self._check(lib.streams_b200_profile_read(self._h, kid, C.byref(ms), C.byref(n)))
+            if n.value:
+                out[lib.streams_b200_kernel_name(kid).decode()] = (ms.value, int(n.value))
         return out
 
     @property
