@@ -203,6 +203,39 @@ const char* streams_b200_kernel_name(int kid);
  */
 int streams_b200_debug_fetch(streams_b200_ctx* ctx, int which, double* out, long long n);
 
+/*
+ * CFL time step over caller-owned device arrays, allocating nothing.
+ *
+ * No counterpart in the reference: STREAmS-2's compute_dt always runs on the solver's own
+ * arrays.  This entry point is for callers that cannot let a library call cudaMalloc, such as
+ * a host code that owns every byte of device memory through its own pool or mapping (a Fortran
+ * solver that keeps its arrays under OpenACC or CUDA Fortran), or one that runs under a fixed
+ * memory budget in which an allocation inside the time loop may fail or fragment the pool.
+ * It needs no context: the caller passes its own device arrays and a device word for dt.
+ *
+ *   w        device w(1-ng:nx+ng,1-ng:ny+ng,1-ng:nz+ng,5)   (only the density is read)
+ *   aux      device aux fields rho,u,v,w,H,T,mu, 7 arrays of the same ghosted shape
+ *            (the layout of streams_b200_debug_fetch(ctx, 0, ...)), current for w
+ *   dcsidx.. device metric arrays of nx, ny, nz entries (set_local_grid, field.F90:456-516)
+ *   gamma    cp/(cp - rgas0) of the calorically perfect gas
+ *   dt       device address that receives cfl / max(inverse time scales)
+ *   stream   cudaStream_t on which both kernels run (asynchronous; NULL = default stream)
+ *
+ * The block partial maxima live in a static device array compiled into the library, so every
+ * GPU that loads the library holds 1.125 MiB for it until the process exits.  At most
+ * STREAMS_B200_DT_NOALLOC_MAX_CELLS interior cells per call; larger sizes return
+ * STREAMS_B200_EINVAL with the reason in streams_b200_global_error().  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array: calls whose kernels overlap on the
+ * GPU (other streams, other host threads) race on it and must be serialised by the caller.
+ */
+#define STREAMS_B200_DT_NOALLOC_MAX_CELLS 4194304LL
+int streams_b200_compute_dt_noalloc(int nx, int ny, int nz, int ng, const double* w, const double* aux,
+                                    const double* dcsidx, const double* detady, const double* dzitdz,
+                                    const double* dcsidxs, const double* detadys, const double* dzitdzs,
+                                    double rgas0, double prandtl, double gamma, double cfl, double* dt,
+                                    void* stream);
+
 #ifdef __cplusplus
 }
 #endif

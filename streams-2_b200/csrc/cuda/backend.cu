@@ -133,6 +133,10 @@ void fill_geom(streams_b200_ctx* c) {
 
 }  // namespace
 
+namespace sb200 {
+void set_global_error(const std::string& msg) { g_global_err = msg; }
+}  // namespace sb200
+
 extern "C" {
 
 int streams_b200_abi_version(void) { return STREAMS_B200_ABI_VERSION; }

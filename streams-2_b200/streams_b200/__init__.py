@@ -99,6 +99,7 @@ def _load() -> C.CDLL:
         "streams_b200_profile_read": (I, [P, I, D, C.POINTER(LL)]),
         "streams_b200_kernel_count": (I, []),
         "streams_b200_kernel_name": (C.c_char_p, [I]),
+        "streams_b200_compute_dt_noalloc": (I, [I, I, I, I] + [V] * 8 + [C.c_double] * 4 + [V, V]),
         "streams_b200_case_load": (I, [C.c_char_p, C.c_char_p, C.POINTER(P)]),
         "streams_b200_case_free": (I, [P]),
         "streams_b200_case_error": (C.c_char_p, []),
@@ -128,7 +129,7 @@ EXPORTED = [
     "streams_b200_count_weno", "streams_b200_get_wallprop", "streams_b200_synchronize",
     "streams_b200_launch_count", "streams_b200_debug_fetch", "streams_b200_get_stream",
     "streams_b200_profile_enable", "streams_b200_profile_read", "streams_b200_kernel_count",
-    "streams_b200_kernel_name", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
+    "streams_b200_kernel_name", "streams_b200_compute_dt_noalloc", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
     "streams_b200_case_params", "streams_b200_case_grid", "streams_b200_case_field", "streams_b200_case_info",
     "streams_b200_case_write_restart", "streams_b200_run_case",
 ]
