@@ -25,7 +25,8 @@ namespace sb200 {
 namespace {
 
 constexpr int AUX_NT = 256;
-constexpr int EU_TX = 32, EU_TY = 8, EU_NT = EU_TX * EU_TY;
+constexpr int XF_TX = 32, XF_TY = 4, XF_NT = XF_TX * XF_TY;  // x faces: 4 row-warps per block
+constexpr int MT_NT = 128;                                     // march kernels
 constexpr int FIN_NT = 1024;
 
 // Apply force_var_2 (kernels_cpu.F90:3285-3314) to the conserved values of one interior point:
@@ -177,133 +178,193 @@ __device__ __forceinline__ void face_flux(const Geom& g, const double* __restric
   }
 }
 
-// Face-flux + divergence pass for one direction.  Block: 32 cells along x times 8 cells along
-// the second axis (y for DIR 0 and 1, z for DIR 2); blockIdx.z is the third axis.
-// Mode: DIR 0 writes fl, DIR 1 adds, DIR 2 adds, applies the grad(mu div/3) term of
-// visflx_div_ord2_subroutine (kernels_cpu.F90:3446-3480) and emits force_rhs partials.
+// Flux at a face from a loaded stencil window (points p-(S-1) .. p+S of face p).
+template <int DIR, int LB, int WS, int S>
+__device__ __forceinline__ void window_flux(const Geom& g, const Stencil<double, S>& st, bool ishk, int p,
+                                            double (&fh)[5]) {
+  const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
+  const int ep = face_ep<DIR>(g, p);
+  if (!ishk) {
+    const int lmax = max(g.lmax_base + ep, 1);
+    const bool zf = (p == 0 && g.fzf[2 * DIR] == 1) || (p == nd && g.fzf[2 * DIR + 1] == 1);
+    central_flux<double, DIR, LB, S>(g, st, lmax, g.nkeep, zf, fh);
+  } else {
+    const int ord = max(WS + ep, 1);
+    weno_flux<double, DIR, WS, S>(g, st, ord, fh);
+  }
+}
+
+template <int S>
+__device__ __forceinline__ void load_point(Stencil<double, S>& st, int q, const double* __restrict__ aux, long long n,
+                                           long long a) {
+  st.rho[q] = __ldg(aux + a);
+  st.u[q] = __ldg(aux + n + a);
+  st.v[q] = __ldg(aux + 2 * n + a);
+  st.w[q] = __ldg(aux + 3 * n + a);
+  st.h[q] = __ldg(aux + 4 * n + a);
+  st.t[q] = __ldg(aux + 5 * n + a);
+}
+
+// x faces: each warp owns one (j,k) row segment of 32 faces (i0-1 .. i0+30) and updates the 31
+// cells between them; the upper face of a cell comes from the neighbouring lane by a shuffle,
+// so no shared memory and no block barrier are needed.  fl is written (first contribution of the
+// stage, euler_x after init_flux).
+template <int LB, int WS>
+__global__ void __launch_bounds__(XF_NT) k_xflux(Geom g, const double* __restrict__ aux,
+                                                 const double* __restrict__ sensor, double* __restrict__ fl) {
+  constexpr int S = LB > WS ? LB : WS;
+  const int lane = threadIdx.x;
+  const int j = blockIdx.y * XF_TY + threadIdx.y + 1, k = blockIdx.z + 1;
+  const int i0 = blockIdx.x * (XF_TX - 1) + 1;  // first cell of the segment
+  const int p = i0 - 1 + lane;                  // this lane's face (between p and p+1)
+  if (j > g.ny) return;                         // whole warp leaves together
+  const bool face_ok = p >= g.eul_imin - 1 && p <= g.eul_imax;
+  double fh[5] = {0, 0, 0, 0, 0};
+  if (face_ok) {
+    bool ishk = false;
+#pragma unroll
+    for (int o = -WS + 1; o <= WS; ++o) ishk = ishk || sensor_at(g, sensor, p + o, j, k) > g.sensor_threshold;
+    Stencil<double, S> st;
+    const long long base = gidx(g, p, j, k);
+#pragma unroll
+    for (int q = 0; q < 2 * S; ++q) load_point<S>(st, q, aux, g.nvol, base + (q - (S - 1)));
+    window_flux<0, LB, WS, S>(g, st, ishk, p, fh);
+  }
+  double hi[5];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) hi[m] = __shfl_down_sync(0xffffffffu, fh[m], 1);
+  const int i = i0 + lane;  // cell between faces p and p+1
+  if (lane < XF_TX - 1 && i <= g.nx) {
+    const bool upd = i >= g.eul_imin && i <= g.eul_imax;
+    const double met = g.dcsidx[i];
+    const long long ic = iidx(g, i, j, k);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) fl[m * g.nint + ic] = upd ? (hi[m] - fh[m]) * met : 0.0;
+  }
+}
+
+// y or z faces by marching: each thread owns one line (fixed i and the other transverse index)
+// over a segment of cells, keeps the stencil window of the current face in registers (one new
+// point loaded per face), computes every face of the segment once and adds the divergence to fl.
+// The z pass also applies the grad(mu div/3) term of visflx_div_ord2_subroutine
+// (kernels_cpu.F90:3446-3480) and emits the force_rhs block partials (:3157-3193).
 template <int DIR, int LB, int WS>
-__global__ void __launch_bounds__(EU_NT) k_euler(Geom g, const double* __restrict__ aux,
+__global__ void __launch_bounds__(MT_NT) k_march(Geom g, const double* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl,
                                                  const double* __restrict__ div3, const double* __restrict__ w,
                                                  const double* __restrict__ fl_prev, const Scalars* __restrict__ sc,
-                                                 double rhork, double gamrk, int istep,
+                                                 double rhork, double gamrk, int istep, int seglen, int nseg,
                                                  double* __restrict__ red) {
-  __shared__ double fsh[5][EU_TY + 1][EU_TX + 1];
-  __shared__ double rsh[5 * (EU_NT / 32)];
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * EU_TX + tx;
-  const int i0 = blockIdx.x * EU_TX;  // cells i0+1 .. i0+32
-  int i, j, k;
-  if (DIR == 2) { i = i0 + tx + 1; k = blockIdx.y * EU_TY + ty + 1; j = blockIdx.z + 1; }
-  else { i = i0 + tx + 1; j = blockIdx.y * EU_TY + ty + 1; k = blockIdx.z + 1; }
-  const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
-  const int emin = DIR == 0 ? g.eul_imin : (DIR == 1 ? g.eul_jmin : g.eul_kmin);
-  const int emax = DIR == 0 ? g.eul_imax : (DIR == 1 ? g.eul_jmax : g.eul_kmax);
-  const int cpos = DIR == 0 ? i : (DIR == 1 ? j : k);
-  const bool cell_ok = i <= g.nx && j <= g.ny && k <= g.nz;
-
-  // face phase: lower face of every cell, plus the upper face of the last cell row
-  {
-    // lower face of this thread's cell: between cpos-1 and cpos.  A thread whose cell lies one
-    // past the end of the block's direction still owns that face (the upper face of cell nd).
-    int fi = i - (DIR == 0), fj = j - (DIR == 1), fk = k - (DIR == 2);
-    const int p = cpos - 1;
-    const bool others_ok = (DIR == 0 || i <= g.nx) && (DIR == 1 || j <= g.ny) && (DIR == 2 || k <= g.nz);
-    if (others_ok && p >= emin - 1 && p <= emax) {
-      double fh[5];
-      face_flux<DIR, LB, WS>(g, aux, sensor, fi, fj, fk, fh);
-#pragma unroll
-      for (int m = 0; m < 5; ++m) fsh[m][ty][tx] = fh[m];
-    }
-    // extra faces: warp 0
-    if (ty == 0) {
-      int xi, xj, xk, slot_r, slot_c;
-      bool ok;
-      if (DIR == 0) {
-        // upper face of the last cell of row `tx` (tx < 8)
-        xi = i0 + EU_TX;  // face between i0+32 and i0+33
-        xj = blockIdx.y * EU_TY + tx + 1;
-        xk = blockIdx.z + 1;
-        ok = tx < EU_TY && xj <= g.ny && xi <= g.nx;
-        slot_r = tx; slot_c = EU_TX;
-      } else {
-        xi = i0 + tx + 1;
-        if (DIR == 1) { xj = blockIdx.y * EU_TY + EU_TY; xk = blockIdx.z + 1; }
-        else { xk = blockIdx.y * EU_TY + EU_TY; xj = blockIdx.z + 1; }
-        ok = xi <= g.nx && (DIR == 1 ? xj <= g.ny : xk <= g.nz);
-        slot_r = EU_TY; slot_c = tx;
-      }
-      const int p = DIR == 0 ? xi : (DIR == 1 ? xj : xk);
-      // the face p exists only if the cell p (last row) lies inside the block range
-      if (ok && p >= emin - 1 && p <= emax) {
-        double fh[5];
-        face_flux<DIR, LB, WS>(g, aux, sensor, xi, xj, xk, fh);
-#pragma unroll
-        for (int m = 0; m < 5; ++m) fsh[m][slot_r][slot_c] = fh[m];
-      }
-    }
-  }
-  __syncthreads();
-
-  // cell phase
+  static_assert(DIR == 1 || DIR == 2, "march kernel handles y and z");
+  constexpr int S = LB > WS ? LB : WS;
+  constexpr int NP = 2 * S;
+  __shared__ double rsh[5 * (MT_NT / 32)];
+  const int n1 = g.nx;
+  const int n2 = DIR == 1 ? g.nz : g.ny;
+  const int nd = DIR == 1 ? g.ny : g.nz;
+  const int emin = DIR == 1 ? g.eul_jmin : g.eul_kmin;
+  const int emax = DIR == 1 ? g.eul_jmax : g.eul_kmax;
+  const long long nlines = (long long)n1 * n2;
+  const long long t = (long long)blockIdx.x * MT_NT + threadIdx.x;
   double part[5] = {0, 0, 0, 0, 0};
-  if (cell_ok) {
-    const long long ic = iidx(g, i, j, k);
-    const long long nI = g.nint;
-    const bool upd = cpos >= emin && cpos <= emax;
-    double met = DIR == 0 ? g.dcsidx[i] : (DIR == 1 ? g.detady[j] : g.dzitdz[k]);
-    double f[5];
-#pragma unroll
-    for (int m = 0; m < 5; ++m) {
-      double lo, hi;
-      if (DIR == 0) { lo = fsh[m][ty][tx]; hi = fsh[m][ty][tx + 1]; }
-      else { lo = fsh[m][ty][tx]; hi = fsh[m][ty + 1][tx]; }
-      double d = upd ? (hi - lo) * met : 0.0;
-      if (DIR == 0) f[m] = d;
-      else f[m] = upd ? fl[m * nI + ic] + d : fl[m * nI + ic];
-    }
-    if (DIR == 2) {
-      // visflx_div_ord2: -grad(mu * div/3) and its work
-      const long long a = gidx(g, i, j, k);
-      const long long n = g.nvol;
-      double uu = aux[n + a], vv = aux[2 * n + a], ww = aux[3 * n + a], mu = aux[6 * n + a];
-      double dxl = mu / (g.x[i + 1] - g.x[i - 1]);
-      double dyl = mu / (g.y[j + 1] - g.y[j - 1]);
-      double dzl = mu / (g.z[k + 1] - g.z[k - 1]);
-      double sigx = dxl * (div3_at(g, div3, i + 1, j, k) - div3_at(g, div3, i - 1, j, k));
-      double sigy = dyl * (div3_at(g, div3, i, j + 1, k) - div3_at(g, div3, i, j - 1, k));
-      double sigz = dzl * (div3_at(g, div3, i, j, k + 1) - div3_at(g, div3, i, j, k - 1));
-      double sigq = sigx * uu + sigy * vv + sigz * ww;
-      f[1] = f[1] - sigx;
-      f[2] = f[2] - sigy;
-      f[3] = f[3] - sigz;
-      f[4] = f[4] - sigq;
-      if (g.channel_case) {
-        // force_rhs_1_subroutine (kernels_cpu.F90:3157-3193) on fln = -rhodt*fl_prev - gamdt*fl
-        const double dt = sc->dt;
-        const double rhodt = rhork * dt, gamdt = gamrk * dt;
-        double fln1 = (istep > 1 ? -(rhodt * fl_prev[ic]) : 0.0) - gamdt * f[0];
-        double fln2 = (istep > 1 ? -(rhodt * fl_prev[nI + ic]) : 0.0) - gamdt * f[1];
-        double dy = g.yn[j + 1] - g.yn[j];
-        double rho = w[a], rhou = w[n + a], tt = aux[5 * n + a];
-        part[0] = fln1 * dy;
-        part[1] = fln2 * dy;
-        part[2] = rho * dy;
-        part[3] = rhou * dy;
-        part[4] = rhou * dy * tt;
+  if (t < nlines * nseg) {
+    const int i = (int)(t % n1) + 1;
+    const int b = (int)((t / n1) % n2) + 1;  // k for y lines, j for z lines
+    const int sgi = (int)(t / nlines);
+    const int c0 = emin + sgi * seglen;
+    const int c1 = min(c0 + seglen - 1, emax);
+    const long long n = g.nvol, nI = g.nint;
+    const long long sd = DIR == 1 ? (long long)g.sx : (long long)g.sx * g.sy;
+    const long long base0 = DIR == 1 ? gidx(g, i, 0, b) : gidx(g, i, b, 0);  // address of c = 0
+    const long long sI = DIR == 1 ? (long long)g.nx : (long long)g.nx * g.ny;  // interior stride
+    // sensor bits of the face p: points p-WS+1 .. p+WS at bits 0 .. 2WS-1
+    auto sensor_bit = [&](int c) -> unsigned {
+      double th;
+      if (c < 1 || c > nd) {
+        if (!g.periodic[DIR]) return 0u;
+        c = wrap(c, nd);
       }
-    }
+      th = DIR == 1 ? sensor[iidx(g, i, c, b)] : sensor[iidx(g, i, b, c)];
+      return th > g.sensor_threshold ? 1u : 0u;
+    };
+    // preload the window and sensor bits of the face c0-2; the loop starts at the face c0-1
+    Stencil<double, S> st;
+    const int p = c0 - 2;
 #pragma unroll
-    for (int m = 0; m < 5; ++m) fl[m * nI + ic] = f[m];
+    for (int q = 1; q < NP; ++q) load_point<S>(st, q, aux, n, base0 + (long long)(p - (S - 1) + q) * sd);
+    unsigned mask = 0;
+#pragma unroll
+    for (int bq = 1; bq < 2 * WS; ++bq) mask |= sensor_bit(p - WS + 1 + bq) << bq;
+    double flo[5] = {0, 0, 0, 0, 0};
+    for (int c = c0 - 1; c <= c1; ++c) {
+      // slide the window to the face c
+#pragma unroll
+      for (int q = 0; q < NP - 1; ++q) {
+        st.rho[q] = st.rho[q + 1]; st.u[q] = st.u[q + 1]; st.v[q] = st.v[q + 1];
+        st.w[q] = st.w[q + 1]; st.h[q] = st.h[q + 1]; st.t[q] = st.t[q + 1];
+      }
+      load_point<S>(st, NP - 1, aux, n, base0 + (long long)(c + S) * sd);
+      mask = (mask >> 1) | (sensor_bit(c + WS) << (2 * WS - 1));
+      double fhi[5];
+      window_flux<DIR, LB, WS, S>(g, st, mask != 0u, c, fhi);
+      if (c < c0) {
+#pragma unroll
+        for (int m = 0; m < 5; ++m) flo[m] = fhi[m];
+        continue;
+      }
+      // cell c lies between the faces c-1 (flo) and c (fhi)
+      const long long ic = DIR == 1 ? iidx(g, i, c, b) : iidx(g, i, b, c);
+      const double met = DIR == 1 ? g.detady[c] : g.dzitdz[c];
+      double f[5];
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        f[m] = fl[m * nI + ic] + (fhi[m] - flo[m]) * met;
+        flo[m] = fhi[m];
+      }
+      if (DIR == 2) {
+        const int j = b, k = c;
+        const long long a = gidx(g, i, j, k);
+        double uu = aux[n + a], vv = aux[2 * n + a], ww = aux[3 * n + a], mu = aux[6 * n + a];
+        double dxl = mu / (g.x[i + 1] - g.x[i - 1]);
+        double dyl = mu / (g.y[j + 1] - g.y[j - 1]);
+        double dzl = mu / (g.z[k + 1] - g.z[k - 1]);
+        double sigx = dxl * (div3_at(g, div3, i + 1, j, k) - div3_at(g, div3, i - 1, j, k));
+        double sigy = dyl * (div3_at(g, div3, i, j + 1, k) - div3_at(g, div3, i, j - 1, k));
+        double sigz = dzl * (div3_at(g, div3, i, j, k + 1) - div3_at(g, div3, i, j, k - 1));
+        double sigq = sigx * uu + sigy * vv + sigz * ww;
+        f[1] = f[1] - sigx;
+        f[2] = f[2] - sigy;
+        f[3] = f[3] - sigz;
+        f[4] = f[4] - sigq;
+        if (g.channel_case) {
+          const double dt = sc->dt;
+          const double rhodt = rhork * dt, gamdt = gamrk * dt;
+          double fln1 = (istep > 1 ? -(rhodt * fl_prev[ic]) : 0.0) - gamdt * f[0];
+          double fln2 = (istep > 1 ? -(rhodt * fl_prev[nI + ic]) : 0.0) - gamdt * f[1];
+          double dy = g.yn[j + 1] - g.yn[j];
+          double rho = w[a], rhou = w[n + a], tt = aux[5 * n + a];
+          part[0] += fln1 * dy;
+          part[1] += fln2 * dy;
+          part[2] += rho * dy;
+          part[3] += rhou * dy;
+          part[4] += rhou * dy * tt;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < 5; ++m) fl[m * nI + ic] = f[m];
+      (void)sI;
+    }
   }
   if (DIR == 2 && g.channel_case) {
-    block_reduce_sum<5, EU_NT>(part, rsh);
-    if (tid == 0) {
-      const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    block_reduce_sum<5, MT_NT>(part, rsh);
+    if (threadIdx.x == 0)
 #pragma unroll
-      for (int r = 0; r < 5; ++r) red[b * 5 + r] = part[r];
-    }
+      for (int r = 0; r < 5; ++r) red[(long long)blockIdx.x * 5 + r] = part[r];
   }
 }
+
+// Cells of the flux passes without a face update (outside eul_[jk]min..max) keep fl unchanged;
+// with the channel's staggered walls every cell is inside.
 
 // visflx_reduced_ord2_subroutine (kernels_cpu.F90:4623-4721, update_sensor = 0) followed by
 // visflx_x/y/z_subroutine (:4779-4999), in the reference's accumulation order; at stage 3 also
@@ -754,9 +815,29 @@ void Prof::reset() {
   for (int k = 0; k < K_NUM; ++k) { total_ms[k] = 0; count[k] = 0; }
 }
 
+// Segments of a march pass: enough threads to fill the device, segments of at least 16 cells
+// (one redundant face per segment).
+static void march_split(const Geom& g, int dir, int* seglen, int* nseg, long long* nthreads) {
+  const int emin = dir == 1 ? g.eul_jmin : g.eul_kmin, emax = dir == 1 ? g.eul_jmax : g.eul_kmax;
+  const int ncell = emax - emin + 1;
+  const long long lines = (long long)g.nx * (dir == 1 ? g.nz : g.ny);
+  const long long target = 148LL * 1024;
+  long long ns = (target + lines - 1) / lines;
+  int sl = (int)((ncell + ns - 1) / ns);
+  if (sl < 16) sl = 16;
+  if (sl > ncell) sl = ncell;
+  if (sl < 1) sl = 1;
+  *seglen = sl;
+  *nseg = ncell > 0 ? (ncell + sl - 1) / sl : 0;
+  *nthreads = lines * *nseg;
+}
+
 long long reduction_slots(const Geom& g) {
   long long a = (long long)nblocks(g.nint, 256) * (NRED_UPD > 9 ? NRED_UPD : 9);
-  long long b = (long long)((g.nx + EU_TX - 1) / EU_TX) * ((g.nz + EU_TY - 1) / EU_TY) * g.ny * 5;
+  int sl, ns;
+  long long nt;
+  march_split(g, 2, &sl, &ns, &nt);
+  long long b = (long long)nblocks(nt, MT_NT) * 5;
   return a > b ? a : b;
 }
 
@@ -808,30 +889,31 @@ cudaError_t launch_count_weno(const Geom& g, DevState& d, cudaStream_t s, long l
 template <int LB, int WS>
 static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
                               cudaStream_t s, long long* nl) {
-  const dim3 blk(EU_TX, EU_TY);
-  const dim3 gx((g.nx + EU_TX - 1) / EU_TX, (g.ny + EU_TY - 1) / EU_TY, g.nz);
-  const dim3 gy((g.nx + EU_TX - 1) / EU_TX, (g.ny + EU_TY - 1) / EU_TY, g.nz);
-  const dim3 gz((g.nx + EU_TX - 1) / EU_TX, (g.nz + EU_TY - 1) / EU_TY, g.ny);
+  const dim3 xb(XF_TX, XF_TY);
+  const dim3 xg((g.nx + XF_TX - 2) / (XF_TX - 1), (g.ny + XF_TY - 1) / XF_TY, g.nz);
+  int sly, nsy, slz, nsz;
+  long long nty, ntz;
+  march_split(g, 1, &sly, &nsy, &nty);
+  march_split(g, 2, &slz, &nsz, &ntz);
+  const unsigned gyb = nblocks(nty, MT_NT), gzb = nblocks(ntz, MT_NT);
   if (a.run_aux) {
     SB_LAUNCH(d, K_AUX, s, k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, a.apply_shift, 0));
     ++*nl;
   }
-  SB_LAUNCH(d, K_EULER_X, s,
-            k_euler<0, LB, WS><<<gx, blk, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc, a.rhork,
-                                                  a.gamrk, a.istep, d.red));
+  SB_LAUNCH(d, K_EULER_X, s, k_xflux<LB, WS><<<xg, xb, 0, s>>>(g, d.aux, d.sensor, fl_new));
   SB_LAUNCH(d, K_VISC, s,
             k_visc<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.aux, fl_new, d.div3, d.sensor_next, d.wallprop,
                                                         a.istep == 3));
-  SB_LAUNCH(d, K_EULER_Y, s,
-            k_euler<1, LB, WS><<<gy, blk, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc, a.rhork,
-                                                  a.gamrk, a.istep, d.red));
+  if (gyb > 0)
+    SB_LAUNCH(d, K_EULER_Y, s,
+              k_march<1, LB, WS><<<gyb, MT_NT, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc,
+                                                       a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
   SB_LAUNCH(d, K_EULER_Z, s,
-            k_euler<2, LB, WS><<<gz, blk, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc, a.rhork,
-                                                  a.gamrk, a.istep, d.red));
+            k_march<2, LB, WS><<<gzb, MT_NT, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc,
+                                                     a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
   *nl += 4;
   if (g.channel_case) {
-    SB_LAUNCH(d, K_FINISH_RHS, s,
-              k_finish_rhs<<<1, FIN_NT, 0, s>>>(g, d.red, (long long)gz.x * gz.y * gz.z, a.istep == 1, d.sc));
+    SB_LAUNCH(d, K_FINISH_RHS, s, k_finish_rhs<<<1, FIN_NT, 0, s>>>(g, d.red, (long long)gzb, a.istep == 1, d.sc));
     ++*nl;
   }
   const unsigned nbu = nblocks(g.nint, 256);
