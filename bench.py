@@ -196,6 +196,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", default="512x256x256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -313,6 +314,37 @@ def main():
     e2e_val = ncell * args.steps * world / (e2e_ms / 1e3) / 1e6
     s2.close()
 
+    # mixed form (FP32 fluxes, FP64 state): throughput on the same workload, and its error against
+    # the FP64 form after 100 steps of the 128x96x64 channel (relative L2 per conserved variable)
+    mixed = None
+    if not args.no_mixed:
+        sm = Solver.from_case(case, precision=1)
+        sm.init_run()
+        sm.advance(args.warmup, 1, 0, 0)
+        stm = torch.cuda.ExternalStream(sm.stream_handle)
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        m0.record(stm)
+        sm.advance(args.steps, 1, args.warmup, 0)
+        m1.record(stm)
+        sm.synchronize()
+        mms = max_over_ranks(m0.elapsed_time(m1))
+        mval = ncell * args.steps * world / (mms / 1e3) / 1e6
+        sm.close()
+        with tempfile.TemporaryDirectory() as d:
+            c0 = Case(d, channel_case_ini(128, 96, 64, 100))
+        fields = []
+        for prec in (0, 1):
+            sv = Solver.from_case(c0, precision=prec)
+            sv.init_run()
+            sv.advance(100, 1, 0, 0)
+            fields.append(sv.copy_to_field()[:, 3:-3, 3:-3, 3:-3])
+            sv.close()
+        errs = [float(np.linalg.norm(fields[1][m] - fields[0][m]) / np.linalg.norm(fields[0][m])) for m in range(5)]
+        mixed = {"value": mval, "unit": "Mcell-steps/s", "ms_per_step": mms / args.steps, "speedup_vs_fp64": mval / value,
+                 "rel_l2_vs_fp64_100_steps_128x96x64": errs, "max_rel_l2": max(errs),
+                 "precision": "FP32 flux/viscous arithmetic, FP64 state, RK register, T recovery, dt, reductions"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -337,7 +369,7 @@ def main():
                     "d2h_bytes_per_step": (nbytes + 56 * args.steps) / args.steps, "wall_s": wall,
                     "what": "copy_from_field (pinned) + init_run + K x (rk step + scalar read) + copy_to_field"},
             "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
-            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu,
+            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "mixed": mixed,
             "state": {"dt": sc["dt"], "rhobulk": sc["rhobulk"], "ubulk": sc["ubulk"], "tbulk": sc["tbulk"],
                       "residual_rhou": res["residual_rhou"], "nan": res["nan"]},
             "u0": info["u0"],

@@ -63,10 +63,12 @@ cudaError_t dev_alloc(streams_b200_ctx* c, T** p, size_t count) {
 long long footprint(const streams_b200_params* p) {
   const long long sx = p->nx + 2LL * p->ng, sy = p->ny + 2LL * p->ng, sz = p->nz + 2LL * p->ng;
   const long long nvol = sx * sy * sz, nint = (long long)p->nx * p->ny * p->nz;
+  const long long fb = p->precision == 1 ? 4 : 8;  // bytes of the flux-input fields
   long long b = 0;
   b += nvol * 5 * 8;   // w
-  b += nvol * 7 * 8;   // aux
-  b += nint * 3 * 8;   // sensor, sensor_next, div3
+  b += nvol * 7 * fb;  // aux
+  b += nint * fb;      // div3
+  b += nint * 2 * 8;   // sensor, sensor_next
   b += nint * 10 * 8;  // two RK registers
   b += (long long)p->nx * p->nz * 3 * 8;
   b += ((nint + 255) / 256) * 9 * 8 + ((p->nx + 31) / 32) * ((p->nz + 7) / 8) * (long long)p->ny * 5 * 8;
@@ -88,7 +90,7 @@ std::string validate(const streams_b200_params* p) {
   if (p->conservative_viscous != 1) return "only conservative_viscous = 1 is implemented on the device path";
   if (p->calorically_perfect != 1) return "only calorically perfect gas is implemented on the device path";
   if (p->nrk != 3) return "only the Wray RK3 scheme (nrk = 3) is implemented";
-  if (p->precision != 0) return "precision must be 0 (FP64)";
+  if (p->precision != 0 && p->precision != 1) return "precision must be 0 (FP64) or 1 (mixed)";
   if (p->visc_model < 0 || p->visc_model > 2) return "visc_model must be 0, 1 or 2";
   for (int d = 0; d < 3; ++d) {
     const int a = p->bctags[2 * d], b = p->bctags[2 * d + 1];
@@ -129,6 +131,7 @@ void fill_geom(streams_b200_ctx* c) {
   g.force_var = p.channel_case && p.theta_wall >= -1.0;
   g.volchan = p.volchan;
   g.t_bulk_target = p.t_bulk_target;
+  g.precision = p.precision;
 }
 
 }  // namespace
@@ -218,9 +221,17 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
     for (int l = 0; l < 4; ++l) g.coeff[lm][l] = gr->coeff_deriv1 ? gr->coeff_deriv1[lm * 4 + l] : 0.0;
   // state
   DevState& d = c->d;
-  if ((e = dev_alloc(c, &d.w, g.nvol * 5)) || (e = dev_alloc(c, &d.aux, g.nvol * 7)) ||
-      (e = dev_alloc(c, &d.sensor, g.nint)) || (e = dev_alloc(c, &d.sensor_next, g.nint)) ||
-      (e = dev_alloc(c, &d.div3, g.nint)) || (e = dev_alloc(c, &c->fl_a, g.nint * 5)) ||
+  const bool mixed = p->precision == 1;
+  if (mixed) {
+    if ((e = dev_alloc(c, &d.auxf, g.nvol * 7)) || (e = dev_alloc(c, &d.div3f, g.nint)))
+      return fail(e, "cudaMalloc(state)");
+  } else {
+    if ((e = dev_alloc(c, &d.aux, g.nvol * 7)) || (e = dev_alloc(c, &d.div3, g.nint)))
+      return fail(e, "cudaMalloc(state)");
+  }
+  if ((e = dev_alloc(c, &d.sensor, g.nint)) || (e = dev_alloc(c, &d.sensor_next, g.nint)))
+    return fail(e, "cudaMalloc(state)");
+  if ((e = dev_alloc(c, &d.w, g.nvol * 5)) || (e = dev_alloc(c, &c->fl_a, g.nint * 5)) ||
       (e = dev_alloc(c, &c->fl_b, g.nint * 5)) || (e = dev_alloc(c, &d.wallprop, (size_t)p->nx * p->nz * 3)) ||
       (e = dev_alloc(c, &d.sc, 1)))
     return fail(e, "cudaMalloc(state)");
@@ -229,10 +240,13 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
   d.fl_a = c->fl_a;
   d.fl_b = c->fl_b;
   d.prof = &c->prof;
-  if ((e = cudaMemsetAsync(d.w, 0, g.nvol * 5 * 8, c->stream)) || (e = cudaMemsetAsync(d.aux, 0, g.nvol * 7 * 8, c->stream)) ||
+  const size_t fb = mixed ? 4 : 8;
+  void* auxp = mixed ? (void*)d.auxf : (void*)d.aux;
+  void* dv = mixed ? (void*)d.div3f : (void*)d.div3;
+  if ((e = cudaMemsetAsync(d.w, 0, g.nvol * 5 * 8, c->stream)) || (e = cudaMemsetAsync(auxp, 0, g.nvol * 7 * fb, c->stream)) ||
       (e = cudaMemsetAsync(d.sensor, 0, g.nint * 8, c->stream)) ||
       (e = cudaMemsetAsync(d.sensor_next, 0, g.nint * 8, c->stream)) ||
-      (e = cudaMemsetAsync(d.div3, 0, g.nint * 8, c->stream)) || (e = cudaMemsetAsync(c->fl_a, 0, g.nint * 40, c->stream)) ||
+      (e = cudaMemsetAsync(dv, 0, g.nint * fb, c->stream)) || (e = cudaMemsetAsync(c->fl_a, 0, g.nint * 40, c->stream)) ||
       (e = cudaMemsetAsync(c->fl_b, 0, g.nint * 40, c->stream)) || (e = cudaMemsetAsync(d.sc, 0, sizeof(Scalars), c->stream)) ||
       (e = cudaStreamSynchronize(c->stream)))
     return fail(e, "initialise state");
@@ -474,18 +488,27 @@ const char* streams_b200_kernel_name(int kid) { return kernel_name(kid); }
 int streams_b200_debug_fetch(streams_b200_ctx* c, int which, double* out, long long n) {
   if (!c || !out) return set_err(c, STREAMS_B200_EINVAL, "null argument");
   cudaSetDevice(c->device);
-  const double* src = nullptr;
+  const bool mixed = c->p.precision == 1;
+  const void* src = nullptr;
   long long cnt = 0;
+  bool is_float = false;
   switch (which) {
-    case 0: src = c->d.aux; cnt = 7 * c->g.nvol; break;
+    case 0: src = mixed ? (const void*)c->d.auxf : (const void*)c->d.aux; cnt = 7 * c->g.nvol; is_float = mixed; break;
     case 1: src = c->last_fl ? c->last_fl : c->fl_a; cnt = 5 * c->g.nint; break;
     case 2: src = c->d.sensor; cnt = c->g.nint; break;
-    case 3: src = c->d.div3; cnt = c->g.nint; break;
+    case 3: src = mixed ? (const void*)c->d.div3f : (const void*)c->d.div3; cnt = c->g.nint; is_float = mixed; break;
     default: return set_err(c, STREAMS_B200_EINVAL, "unknown diagnostic array");
   }
   if (n < cnt) return set_err(c, STREAMS_B200_EINVAL, "output buffer too small");
-  SB_CHECK(c, cudaMemcpyAsync(out, src, cnt * 8, cudaMemcpyDeviceToHost, c->stream));
-  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  if (is_float) {
+    std::vector<float> tmp((size_t)cnt);
+    SB_CHECK(c, cudaMemcpyAsync(tmp.data(), src, cnt * 4, cudaMemcpyDeviceToHost, c->stream));
+    SB_CHECK(c, cudaStreamSynchronize(c->stream));
+    for (long long q = 0; q < cnt; ++q) out[q] = tmp[(size_t)q];
+  } else {
+    SB_CHECK(c, cudaMemcpyAsync(out, src, cnt * 8, cudaMemcpyDeviceToHost, c->stream));
+    SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  }
   return STREAMS_B200_OK;
 }
 

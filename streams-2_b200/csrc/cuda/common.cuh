@@ -51,6 +51,8 @@ struct Geom {
   // channel forcing
   int channel_case, force_var;
   double volchan, t_bulk_target;
+  // arithmetic of the flux and viscous passes: 0 FP64, 1 mixed (FP32 fluxes, FP64 state)
+  int precision;
 };
 
 __host__ __device__ __forceinline__ long long gidx(const Geom& g, int i, int j, int k) {

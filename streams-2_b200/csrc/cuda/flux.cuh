@@ -8,13 +8,49 @@
 
 namespace sb200 {
 
+// Error-free transformations for the mixed form: the face fluxes are accumulated as float-float
+// pairs (hi + lo) so that the flux differences of neighbouring faces can be formed in FP64
+// without the cancellation of the FP32 rounding of their final sums.  Explicit rounding
+// intrinsics keep the compiler from contracting them.
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = __fadd_rn(a, b);
+  const float bb = __fsub_rn(s, a);
+  e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+// acc (hi, lo) += a * b
+__device__ __forceinline__ void acc_prod(float& hi, float& lo, float a, float b) {
+  const float p = __fmul_rn(a, b);
+  const float ep = __fmaf_rn(a, b, -p);
+  float s, es;
+  two_sum(hi, p, s, es);
+  hi = s;
+  lo = lo + (es + ep);
+}
+__device__ __forceinline__ void acc_prod(double& hi, double& lo, double a, double b) {
+  hi = hi + a * b;
+  (void)lo;
+}
+__device__ __forceinline__ void acc_add(float& hi, float& lo, float b) {
+  float s, es;
+  two_sum(hi, b, s, es);
+  hi = s;
+  lo = lo + es;
+}
+__device__ __forceinline__ void acc_add(double& hi, double& lo, double b) {
+  hi = hi + b;
+  (void)lo;
+}
+
 // Stencil of a face: NP = 2*S points at offsets o = -(S-1) .. S from the face's lower point.
 template <class R, int S>
 struct Stencil {
   R rho[2 * S], u[2 * S], v[2 * S], w[2 * S], h[2 * S], t[2 * S];
+  R c[2 * S];  // sound speed sqrt(gamma R T) of each point, computed once when the point is loaded
 };
 
-// wenorec_1d (kernels_cpu.F90:2526-2724) for one characteristic variable.
+// wenorec_1d (kernels_cpu.F90:2526-2724) for one characteristic variable.  The nonlinear weights
+// are normalised by one reciprocal of their sum (the reference divides each weight by the sum;
+// the results differ in the last bit only).
 // vp[l-1], vm[l-1] hold the reference's vp(m,l), vm(m,l), l = 1..2*WS; i = iweno = WS.
 template <class R, int WS>
 __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS], int ord, int version,
@@ -38,8 +74,8 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
       bm0 = dwe0 / (tm0 * tm0);
       bp1 = dwe1 / (tp1 * tp1);
       bm1 = dwe1 / (tm1 * tm1);
-      R sump = (R(0) + bp0) + bp1, summ = (R(0) + bm0) + bm1;
-      bp0 = bp0 / sump; bp1 = bp1 / sump; bm0 = bm0 / summ; bm1 = bm1 / summ;
+      const R rsp = R(1) / ((R(0) + bp0) + bp1), rsm = R(1) / ((R(0) + bm0) + bm1);
+      bp0 = bp0 * rsp; bp1 = bp1 * rsp; bm0 = bm0 * rsm; bm1 = bm1 * rsm;
       R vminus = bp0 * (-VP(i - 1) + R(3) * VP(i)) + bp1 * (VP(i) + VP(i + 1));
       R vplus = bm0 * (-VM(i + 2) + R(3) * VM(i + 1)) + bm1 * (VM(i) + VM(i + 1));
       return R(0.5) * (vminus + vplus);
@@ -86,10 +122,11 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
           sump = sump + bp[l];
           summ = summ + bm[l];
         }
+        const R rsp = R(1) / sump, rsm = R(1) / summ;
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
-          bp[l] = bp[l] / sump;
-          bm[l] = bm[l] / summ;
+          bp[l] = bp[l] * rsp;
+          bm[l] = bm[l] * rsm;
         }
       } else {
         // eps40 is a single-precision literal in the reference
@@ -109,10 +146,11 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
           sump = sump + bp[l];
           summ = summ + bm[l];
         }
+        const R rsp = R(1) / sump, rsm = R(1) / summ;
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
-          bp[l] = bp[l] / sump;
-          bm[l] = bm[l] / summ;
+          bp[l] = bp[l] * rsp;
+          bm[l] = bm[l] * rsm;
         }
       }
       R vminus = bp[2] * (c0 * VP(i) + c1 * VP(i + 1) + c2 * VP(i + 2)) +
@@ -164,10 +202,11 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
         sump = sump + bp[l];
         summ = summ + bm[l];
       }
+      const R rsp = R(1) / sump, rsm = R(1) / summ;
 #pragma unroll
       for (int l = 0; l < 4; ++l) {
-        bp[l] = bp[l] / sump;
-        bm[l] = bm[l] / summ;
+        bp[l] = bp[l] * rsp;
+        bm[l] = bm[l] * rsm;
       }
       R vminus = bp[3] * (6 * VP(i) + 26 * VP(i + 1) - 10 * VP(i + 2) + 2 * VP(i + 3)) +
                  bp[2] * (-2 * VP(i - 1) + 14 * VP(i) + 14 * VP(i + 1) - 2 * VP(i + 2)) +
@@ -187,7 +226,7 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
 // DIR: 0 x, 1 y, 2 z.  Points of st are at offsets -(S-1)..S (index o + S - 1).
 template <class R, int DIR, int LB, int S>
 __device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>& st, int lmax, int nkeep,
-                                             bool zero_flux, R (&fh)[5]) {
+                                             bool zero_flux, R (&fh)[5], R (&fl)[5]) {
   const R rgas0 = R(g.rgas0);
   R pp[2 * S], ee[2 * S];
 #pragma unroll
@@ -196,6 +235,7 @@ __device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>&
     ee[q] = st.h[q] - pp[q] / st.rho[q] - R(0.5) * (st.u[q] * st.u[q] + st.v[q] * st.v[q] + st.w[q] * st.w[q]);
   }
   R ft1 = 0, ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
+  R lt1 = 0, lt2 = 0, lt3 = 0, lt4 = 0, lt5 = 0, lt6 = 0;  // compensation (mixed form)
 #pragma unroll
   for (int l = 1; l <= LB; ++l) {
     if (l <= lmax) {
@@ -251,31 +291,34 @@ __device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>&
         }
       }
       const R cl = R(g.coeff[lmax - 1][l - 1]);
-      ft1 = ft1 + cl * uvs1;
-      ft2 = ft2 + cl * uvs2;
-      ft3 = ft3 + cl * uvs3;
-      ft4 = ft4 + cl * uvs4;
-      ft5 = ft5 + cl * (nkeep >= 0 ? (uvs5_i + uvs5_k + uvs5_p) : uvs5);
-      ft6 = ft6 + cl * uvs6;
+      acc_prod(ft1, lt1, cl, uvs1);
+      acc_prod(ft2, lt2, cl, uvs2);
+      acc_prod(ft3, lt3, cl, uvs3);
+      acc_prod(ft4, lt4, cl, uvs4);
+      acc_prod(ft5, lt5, cl, (nkeep >= 0 ? (uvs5_i + uvs5_k + uvs5_p) : uvs5));
+      acc_prod(ft6, lt6, cl, uvs6);
     }
   }
-  fh[0] = R(0.25) * ft1;
-  fh[1] = R(0.25) * ft2;
-  fh[2] = R(0.25) * ft3;
-  fh[3] = R(0.25) * ft4;
-  fh[4] = R(0.25) * ft5;
+  // scaling by 1/4 and 1/2 is exact, so the compensation terms scale with their sums
+  fh[0] = R(0.25) * ft1; fl[0] = R(0.25) * lt1;
+  fh[1] = R(0.25) * ft2; fl[1] = R(0.25) * lt2;
+  fh[2] = R(0.25) * ft3; fl[2] = R(0.25) * lt3;
+  fh[3] = R(0.25) * ft4; fl[3] = R(0.25) * lt4;
+  fh[4] = R(0.25) * ft5; fl[4] = R(0.25) * lt5;
   if (zero_flux) {
 #pragma unroll
-    for (int m = 0; m < 5; ++m) fh[m] = R(0);
+    for (int m = 0; m < 5; ++m) fh[m] = fl[m] = R(0);
   }
-  fh[1 + DIR] = fh[1 + DIR] + R(0.5) * ft6;
+  acc_add(fh[1 + DIR], fl[1 + DIR], R(0.5) * ft6);
+  fl[1 + DIR] = fl[1 + DIR] + R(0.5) * lt6;
 }
 
 // Characteristic WENO flux: compute_roe_average (kernels_cpu.F90:3013-3089), eigenvectors_{x,y,z}
 // (:2728-2782, :2842-2896, :2956-3010), local Lax-Friedrichs splitting with the stencil maximum
 // of |u_n -+ c| (:614-675) and wenorec_1d; back-projection with the right eigenvectors (:677-683).
 template <class R, int DIR, int WS, int S>
-__device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5]) {
+__device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5],
+                                          R (&fl)[5]) {
   const R rgas0 = R(g.rgas0);
   const int o0 = S - 1, o1 = S;  // the two points adjacent to the face
   // Roe average
@@ -312,7 +355,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   for (int l = 0; l < 2 * WS; ++l) {
     const int q = l + S - WS;
     const R vnq = DIR == 0 ? st.u[q] : (DIR == 1 ? st.v[q] : st.w[q]);
-    R cs = sqrt(gamloc * rgas0 * st.t[q]);
+    const R cs = st.c[q];
     ev0 = fmax(fabs(vnq - cs), ev0);
     ev1 = fmax(fabs(vnq), ev1);
     ev4 = fmax(fabs(vnq + cs), ev4);
@@ -320,7 +363,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   const R betascale_a = R(1) / (R(g.rho0) * R(g.rho0) * (R(g.u0) * R(g.u0)));
   const R betascale_b = R(1) / (R(g.rho0) * R(g.rho0) * (R(g.u0) * R(g.u0)) * (R(g.u0) * R(g.u0)));
 #pragma unroll
-  for (int m = 0; m < 5; ++m) fh[m] = R(0);
+  for (int m = 0; m < 5; ++m) fh[m] = fl[m] = R(0);
 #pragma unroll
   for (int m = 0; m < 5; ++m) {
     // column m of the left eigenvector matrix el(1:5, m)
@@ -392,11 +435,11 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
       r3 = tt_ == 2 ? R(1) : R(0);
       r4 = vel[tt_];
     }
-    fh[0] = fh[0] + r0 * fi;
-    fh[1] = fh[1] + r1 * fi;
-    fh[2] = fh[2] + r2 * fi;
-    fh[3] = fh[3] + r3 * fi;
-    fh[4] = fh[4] + r4 * fi;
+    acc_prod(fh[0], fl[0], r0, fi);
+    acc_prod(fh[1], fl[1], r1, fi);
+    acc_prod(fh[2], fl[2], r2, fi);
+    acc_prod(fh[3], fl[3], r3, fi);
+    acc_prod(fh[4], fl[4], r4, fi);
   }
 }
 

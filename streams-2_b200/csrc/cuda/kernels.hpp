@@ -32,10 +32,14 @@ struct Prof {
 // Device buffers of one context (single block).
 struct DevState {
   double* w = nullptr;        // ghosted, 5 variables
+  // FP64 form
   double* aux = nullptr;      // ghosted, 7 variables: rho, u, v, w, H, T, mu
-  double* sensor = nullptr;   // interior: Ducros theta used by the fluxes
+  double* sensor = nullptr;   // interior: Ducros theta used by the fluxes (both forms)
   double* sensor_next = nullptr;
   double* div3 = nullptr;     // interior: div/3
+  // mixed form: primitive fields and div/3 in FP32 (the sensor stays FP64 in both forms)
+  float* auxf = nullptr;
+  float* div3f = nullptr;
   double* fl_a = nullptr;     // interior, 5 variables (two RK registers, ping-pong)
   double* fl_b = nullptr;
   double* wallprop = nullptr; // nx*nz*3
@@ -48,7 +52,7 @@ struct DevState {
 struct StageArgs {
   int istep;           // 1..nrk
   double rhork, gamrk; // RK coefficients of the stage
-  int apply_shift;     // aux pass applies the pending force_var energy shift
+  int apply_shift;     // apply the pending force_var energy shift before the aux pass
   int want_stats;      // update pass accumulates residual and min/max (stage 3)
   int run_aux;         // recompute aux (skipped when it is already current)
   int add_time;        // accumulate time += dt on the device after the stage

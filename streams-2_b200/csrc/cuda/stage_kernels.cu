@@ -1,20 +1,25 @@
-// Stage kernels of the B200 backend (FP64 form).
+// Stage kernels of the B200 backend (FP64 and mixed forms).
 //
 // One Runge-Kutta stage (rk_sync, code/src/singleideal/singleideal_cpu.F90:332-409) runs as:
+//   k_apply_shift  the pending force_var energy shift of the previous stage, on interior w
 //   k_aux      w -> primitive/thermo fields at interior and face-ghost points; ghost values are
-//              produced on the fly (periodic wrap, staggered isothermal wall mirror), and the
-//              pending force_var energy shift of the previous stage is applied to w first
-//   k_euler<0> x-face hybrid fluxes + divergence (fl = ...)
+//              produced on the fly (periodic wrap, staggered isothermal wall mirror)
+//   k_xflux    x-face hybrid fluxes + divergence (fl = ...); one warp per row, shuffles between lanes
 //   k_visc     reduced 2nd-order viscous terms, conservative face Laplacian in x, y, z,
 //              div/3, stage-3 Ducros sensor, wall shear
-//   k_euler<1> y-face fluxes + divergence (fl += ...)
-//   k_euler<2> z-face fluxes + divergence + grad(mu div/3) term; block partials of force_rhs
+//   k_march<1> y-face fluxes + divergence (fl += ...); register-window march along y lines
+//   k_march<2> z-face fluxes + divergence + grad(mu div/3) term; block partials of force_rhs
 //   k_finish_rhs  bulk quantities and the forcing correction (deterministic order)
 //   k_update   RK register fln, forcing correction, w += fln, force_var / residual partials
 //   k_finish_upd  bulk temperature -> pending energy shift; residual and min/max
-// No face flux array is stored: face fluxes live in shared memory between the face and the
-// cell phases of each k_euler block.  All reductions are block partials summed in a fixed
-// order, so results do not depend on scheduling.
+// No face flux array is stored.  All reductions are block partials summed in a fixed order, so
+// results do not depend on scheduling.
+//
+// Precision: template parameter R is the arithmetic type of the fluxes and viscous terms and the
+// storage type of the primitive fields (aux) and div/3.  R = double is the FP64 form; R = float
+// the mixed form, where w, the RK registers fl, the temperature recovery from the total energy,
+// the Ducros sensor, the time step and all reductions stay FP64 and the face fluxes are carried
+// as float-float pairs whose differences are formed in FP64.
 #include <cfloat>
 
 #include "flux.cuh"
@@ -43,21 +48,31 @@ __device__ __forceinline__ double shifted_rhoe(const Geom& g, double rho, double
   return rho * en + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;
 }
 
-// w -> aux at all interior and face-ghost points (eval_aux_subroutine, kernels_cpu.F90:6960-7011).
-// Ghost states: bcswap periodic copy (code/src/base_cpu.F90:1326-1435) and
-// bcwall_staggered_subroutine (kernels_cpu.F90:6612-6678).
-__global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, double* __restrict__ aux,
-                                                const Scalars* __restrict__ sc, int apply_shift,
-                                                int write_ghost_w) {
+// Primitive state of an interior point recomputed from w in FP64, with the operations of
+// eval_aux_subroutine (kernels_cpu.F90:6960-7011).
+struct Prim {
+  double rho, uu, vv, ww, tt;
+};
+__device__ __forceinline__ Prim prim_from_w(const Geom& g, const double* __restrict__ w, long long c) {
   const long long n = g.nvol;
-  const long long q = (long long)blockIdx.x * AUX_NT + threadIdx.x;
-  if (q >= n) return;
-  const int ii = (int)(q % g.sx);
-  const int jj = (int)((q / g.sx) % g.sy);
-  const int kk = (int)(q / ((long long)g.sx * g.sy));
-  const int i = ii - g.ng + 1, j = jj - g.ng + 1, k = kk - g.ng + 1;
+  Prim p;
+  p.rho = w[c];
+  const double ri = 1.0 / p.rho;
+  p.uu = w[n + c] * ri;
+  p.vv = w[2 * n + c] * ri;
+  p.ww = w[3 * n + c] * ri;
+  const double qq = 0.5 * (p.uu * p.uu + p.vv * p.vv + p.ww * p.ww);
+  p.tt = t_from_e(g, w[4 * n + c] / p.rho - qq);
+  return p;
+}
+
+// Conserved state at an interior or face-ghost point (i,j,k): the stored value, a periodic copy
+// (bcswap, code/src/base_cpu.F90:1326-1435) or the staggered-wall mirror of
+// bcwall_staggered_subroutine (kernels_cpu.F90:6612-6678).
+__device__ __forceinline__ void point_state(const Geom& g, const double* __restrict__ w, int i, int j, int k,
+                                            double (&st)[5]) {
+  const long long n = g.nvol;
   const int ox = (i < 1 || i > g.nx), oy = (j < 1 || j > g.ny), oz = (k < 1 || k > g.nz);
-  if (ox + oy + oz > 1) return;  // halo edges and corners are never read
   int si = i, sj = j, sk = k;
   int wall = 0;
   if (ox) si = wrap(i, g.nx);
@@ -71,12 +86,8 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   }
   const long long src = gidx(g, si, sj, sk);
   double rho = w[src], rhou = w[n + src], rhov = w[2 * n + src], rhow = w[3 * n + src], rhoe = w[4 * n + src];
-  if (apply_shift) {
-    rhoe = shifted_rhoe(g, rho, rhou, rhov, rhow, rhoe, sc->tbdiff);
-    if (!(ox | oy | oz)) w[4 * n + src] = rhoe;
-  }
   if (wall) {
-    // bcwall_staggered: mirror about the wall, T_g = 2 T_w - T, p_g = p, velocity reversed
+    // mirror about the wall, T_g = 2 T_w - T, p_g = p, velocity reversed
     double uu = rhou / rho, vv = rhov / rho, ww = rhow / rho;
     double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
     double ee = rhoe / rho - qq;
@@ -90,6 +101,26 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
     rhow = -rho * ww;
     rhoe = rho * (ee + qq);
   }
+  st[0] = rho; st[1] = rhou; st[2] = rhov; st[3] = rhow; st[4] = rhoe;
+}
+
+// w -> aux at all interior and face-ghost points (eval_aux_subroutine, kernels_cpu.F90:6960-7011),
+// computed in FP64 and stored as A; with write_ghost_w the ghost states are also stored into w.
+template <class A>
+__global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, A* __restrict__ aux,
+                                                int write_ghost_w) {
+  const long long n = g.nvol;
+  const long long q = (long long)blockIdx.x * AUX_NT + threadIdx.x;
+  if (q >= n) return;
+  const int ii = (int)(q % g.sx);
+  const int jj = (int)((q / g.sx) % g.sy);
+  const int kk = (int)(q / ((long long)g.sx * g.sy));
+  const int i = ii - g.ng + 1, j = jj - g.ng + 1, k = kk - g.ng + 1;
+  const int ox = (i < 1 || i > g.nx), oy = (j < 1 || j > g.ny), oz = (k < 1 || k > g.nz);
+  if (ox + oy + oz > 1) return;  // halo edges and corners are never read
+  double st[5];
+  point_state(g, w, i, j, k, st);
+  double rho = st[0], rhou = st[1], rhov = st[2], rhow = st[3], rhoe = st[4];
   const long long dst = gidx(g, i, j, k);
   if (write_ghost_w && (ox | oy | oz)) {
     w[dst] = rho; w[n + dst] = rhou; w[2 * n + dst] = rhov; w[3 * n + dst] = rhow; w[4 * n + dst] = rhoe;
@@ -100,15 +131,53 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   double ee = rhoe / rho - qq;
   double tt = t_from_e(g, ee);
   double pp = rho * tt * g.rgas0;
-  aux[dst] = rho;
-  aux[n + dst] = uu;
-  aux[2 * n + dst] = vv;
-  aux[3 * n + dst] = ww;
-  aux[4 * n + dst] = (rhoe + pp) / rho;
-  aux[5 * n + dst] = tt;
-  aux[6 * n + dst] = viscosity(g, tt);
+  aux[dst] = A(rho);
+  aux[n + dst] = A(uu);
+  aux[2 * n + dst] = A(vv);
+  aux[3 * n + dst] = A(ww);
+  aux[4 * n + dst] = A((rhoe + pp) / rho);
+  aux[5 * n + dst] = A(tt);
+  aux[6 * n + dst] = A(viscosity(g, tt));
 }
 
+// Ducros sensor in FP64 from w for the mixed form, so that the central/WENO switch is taken
+// on the same values as in the FP64 form.  mode 0: initial sensor of run() (visflx(mode=2),
+// kernels_cpu.F90:4680-4682); mode 1: sensor_subroutine of stage 3 (:4726-4744), which works
+// from the stored |omega| and div/3.
+__global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restrict__ w, double* __restrict__ out,
+                                                  int mode) {
+  const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (q >= g.nint) return;
+  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+  auto vel = [&](int a, int b, int c, double (&v)[3]) {
+    double st[5];
+    point_state(g, w, a, b, c, st);
+    const double ri = 1.0 / st[0];
+    v[0] = st[1] * ri; v[1] = st[2] * ri; v[2] = st[3] * ri;
+  };
+  double xp[3], xm[3], yp[3], ym[3], zp[3], zm[3];
+  vel(i + 1, j, k, xp); vel(i - 1, j, k, xm);
+  vel(i, j + 1, k, yp); vel(i, j - 1, k, ym);
+  vel(i, j, k + 1, zp); vel(i, j, k - 1, zm);
+  double dxl = 1.0 / (g.x[i + 1] - g.x[i - 1]);
+  double dyl = 1.0 / (g.y[j + 1] - g.y[j - 1]);
+  double dzl = 1.0 / (g.z[k + 1] - g.z[k - 1]);
+  double ux = dxl * (xp[0] - xm[0]), vx = dxl * (xp[1] - xm[1]), wx = dxl * (xp[2] - xm[2]);
+  double uy = dyl * (yp[0] - ym[0]), vy = dyl * (yp[1] - ym[1]), wy = dyl * (yp[2] - ym[2]);
+  double uz = dzl * (zp[0] - zm[0]), vz = dzl * (zp[1] - zm[1]), wz = dzl * (zp[2] - zm[2]);
+  double div = ux + vy + wz;
+  double omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
+  double omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
+  double u0l0 = g.u0 / g.l0;
+  if (mode == 1) {
+    double div3l = div / 3.0;
+    double om = sqrt(omod2);
+    omod2 = om * om;
+    div = 3.0 * div3l;
+  }
+  double t = fmax(-div / sqrt(omod2 + div * div + u0l0 * u0l0), 0.0);
+  out[q] = t * t;
+}
 // Pending energy shift on interior points only (before a download).
 __global__ void __launch_bounds__(AUX_NT) k_apply_shift(Geom g, double* __restrict__ w,
                                                         const Scalars* __restrict__ sc) {
@@ -120,14 +189,16 @@ __global__ void __launch_bounds__(AUX_NT) k_apply_shift(Geom g, double* __restri
 }
 
 // Readers of the interior-only sensor and div/3 arrays at a stencil point that may be a ghost.
-__device__ __forceinline__ double sensor_at(const Geom& g, const double* __restrict__ s, int i, int j, int k) {
-  if (i < 1 || i > g.nx) { if (!g.periodic[0]) return 0.0; i = wrap(i, g.nx); }
-  if (j < 1 || j > g.ny) { if (!g.periodic[1]) return 0.0; j = wrap(j, g.ny); }
-  if (k < 1 || k > g.nz) { if (!g.periodic[2]) return 0.0; k = wrap(k, g.nz); }
+template <class R>
+__device__ __forceinline__ R sensor_at(const Geom& g, const R* __restrict__ s, int i, int j, int k) {
+  if (i < 1 || i > g.nx) { if (!g.periodic[0]) return R(0); i = wrap(i, g.nx); }
+  if (j < 1 || j > g.ny) { if (!g.periodic[1]) return R(0); j = wrap(j, g.ny); }
+  if (k < 1 || k > g.nz) { if (!g.periodic[2]) return R(0); k = wrap(k, g.nz); }
   return s[iidx(g, i, j, k)];
 }
 // bcextr_var (kernels_cpu.F90:6199-6254) then bcswap_var: periodic wrap, otherwise nearest interior
-__device__ __forceinline__ double div3_at(const Geom& g, const double* __restrict__ d, int i, int j, int k) {
+template <class R>
+__device__ __forceinline__ R div3_at(const Geom& g, const R* __restrict__ d, int i, int j, int k) {
   if (i < 1 || i > g.nx) i = g.periodic[0] ? wrap(i, g.nx) : (i < 1 ? 1 : g.nx);
   if (j < 1 || j > g.ny) j = g.periodic[1] ? wrap(j, g.ny) : (j < 1 ? 1 : g.ny);
   if (k < 1 || k > g.nz) k = g.periodic[2] ? wrap(k, g.nz) : (k < 1 ? 1 : g.nz);
@@ -139,78 +210,51 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
   return DIR == 0 ? g.epx[p] : (DIR == 1 ? g.epy[p] : g.epz[p]);
 }
 
-// Flux at the face between (i,j,k) and its +1 neighbour along DIR.
-template <int DIR, int LB, int WS>
-__device__ __forceinline__ void face_flux(const Geom& g, const double* __restrict__ aux,
-                                          const double* __restrict__ sensor, int i, int j, int k,
-                                          double (&fh)[5]) {
-  constexpr int S = LB > WS ? LB : WS;
-  const int p = DIR == 0 ? i : (DIR == 1 ? j : k);
-  const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
-  bool ishk = false;
-#pragma unroll
-  for (int o = -WS + 1; o <= WS; ++o) {
-    const double th = sensor_at(g, sensor, i + (DIR == 0) * o, j + (DIR == 1) * o, k + (DIR == 2) * o);
-    ishk = ishk || (th > g.sensor_threshold);
-  }
-  const long long n = g.nvol;
-  const long long base = gidx(g, i, j, k);
-  const long long stride = DIR == 0 ? 1 : (DIR == 1 ? (long long)g.sx : (long long)g.sx * g.sy);
-  Stencil<double, S> st;
-#pragma unroll
-  for (int q = 0; q < 2 * S; ++q) {
-    const long long a = base + (q - (S - 1)) * stride;
-    st.rho[q] = __ldg(aux + a);
-    st.u[q] = __ldg(aux + n + a);
-    st.v[q] = __ldg(aux + 2 * n + a);
-    st.w[q] = __ldg(aux + 3 * n + a);
-    st.h[q] = __ldg(aux + 4 * n + a);
-    st.t[q] = __ldg(aux + 5 * n + a);
-  }
-  const int ep = face_ep<DIR>(g, p);
-  if (!ishk) {
-    const int lmax = max(g.lmax_base + ep, 1);
-    const bool zf = (p == 0 && g.fzf[2 * DIR] == 1) || (p == nd && g.fzf[2 * DIR + 1] == 1);
-    central_flux<double, DIR, LB, S>(g, st, lmax, g.nkeep, zf, fh);
-  } else {
-    const int ord = max(WS + ep, 1);
-    weno_flux<double, DIR, WS, S>(g, st, ord, fh);
-  }
-}
-
-// Flux at a face from a loaded stencil window (points p-(S-1) .. p+S of face p).
-template <int DIR, int LB, int WS, int S>
-__device__ __forceinline__ void window_flux(const Geom& g, const Stencil<double, S>& st, bool ishk, int p,
-                                            double (&fh)[5]) {
+// Flux at a face from a loaded stencil window (points p-(S-1) .. p+S of face p):
+// hi + lo is the face flux (lo = 0 in the FP64 form).
+template <class R, int DIR, int LB, int WS, int S>
+__device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& st, bool ishk, int p,
+                                            R (&hi)[5], R (&lo)[5]) {
   const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
   const int ep = face_ep<DIR>(g, p);
   if (!ishk) {
     const int lmax = max(g.lmax_base + ep, 1);
     const bool zf = (p == 0 && g.fzf[2 * DIR] == 1) || (p == nd && g.fzf[2 * DIR + 1] == 1);
-    central_flux<double, DIR, LB, S>(g, st, lmax, g.nkeep, zf, fh);
+    central_flux<R, DIR, LB, S>(g, st, lmax, g.nkeep, zf, hi, lo);
   } else {
     const int ord = max(WS + ep, 1);
-    weno_flux<double, DIR, WS, S>(g, st, ord, fh);
+    weno_flux<R, DIR, WS, S>(g, st, ord, hi, lo);
   }
 }
 
-template <int S>
-__device__ __forceinline__ void load_point(Stencil<double, S>& st, int q, const double* __restrict__ aux, long long n,
-                                           long long a) {
+template <class R, int S>
+__device__ __forceinline__ void load_point(const Geom& g, Stencil<R, S>& st, int q, const R* __restrict__ aux,
+                                           long long n, long long a) {
   st.rho[q] = __ldg(aux + a);
   st.u[q] = __ldg(aux + n + a);
   st.v[q] = __ldg(aux + 2 * n + a);
   st.w[q] = __ldg(aux + 3 * n + a);
   st.h[q] = __ldg(aux + 4 * n + a);
   st.t[q] = __ldg(aux + 5 * n + a);
+  st.c[q] = sqrt(R(g.gamloc) * R(g.rgas0) * st.t[q]);
+}
+
+// Divergence of one variable between a face pair, in FP64: (hi_up - hi_lo) + (lo_up - lo_lo).
+template <class R>
+__device__ __forceinline__ double face_diff(R hup, R lup, R hlo, R llo) {
+  if constexpr (sizeof(R) == sizeof(double)) {
+    return double(hup) - double(hlo);
+  } else {
+    return (double(hup) - double(hlo)) + (double(lup) - double(llo));
+  }
 }
 
 // x faces: each warp owns one (j,k) row segment of 32 faces (i0-1 .. i0+30) and updates the 31
 // cells between them; the upper face of a cell comes from the neighbouring lane by a shuffle,
 // so no shared memory and no block barrier are needed.  fl is written (first contribution of the
 // stage, euler_x after init_flux).
-template <int LB, int WS>
-__global__ void __launch_bounds__(XF_NT) k_xflux(Geom g, const double* __restrict__ aux,
+template <class R, int LB, int WS>
+__global__ void __launch_bounds__(XF_NT) k_xflux(Geom g, const R* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl) {
   constexpr int S = LB > WS ? LB : WS;
   const int lane = threadIdx.x;
@@ -219,27 +263,31 @@ __global__ void __launch_bounds__(XF_NT) k_xflux(Geom g, const double* __restric
   const int p = i0 - 1 + lane;                  // this lane's face (between p and p+1)
   if (j > g.ny) return;                         // whole warp leaves together
   const bool face_ok = p >= g.eul_imin - 1 && p <= g.eul_imax;
-  double fh[5] = {0, 0, 0, 0, 0};
+  R fh[5] = {0, 0, 0, 0, 0}, fo[5] = {0, 0, 0, 0, 0};
   if (face_ok) {
     bool ishk = false;
 #pragma unroll
     for (int o = -WS + 1; o <= WS; ++o) ishk = ishk || sensor_at(g, sensor, p + o, j, k) > g.sensor_threshold;
-    Stencil<double, S> st;
+    Stencil<R, S> st;
     const long long base = gidx(g, p, j, k);
 #pragma unroll
-    for (int q = 0; q < 2 * S; ++q) load_point<S>(st, q, aux, g.nvol, base + (q - (S - 1)));
-    window_flux<0, LB, WS, S>(g, st, ishk, p, fh);
+    for (int q = 0; q < 2 * S; ++q) load_point<R, S>(g, st, q, aux, g.nvol, base + (q - (S - 1)));
+    window_flux<R, 0, LB, WS, S>(g, st, ishk, p, fh, fo);
   }
-  double hi[5];
+  R hu[5], lu[5];
 #pragma unroll
-  for (int m = 0; m < 5; ++m) hi[m] = __shfl_down_sync(0xffffffffu, fh[m], 1);
+  for (int m = 0; m < 5; ++m) {
+    hu[m] = __shfl_down_sync(0xffffffffu, fh[m], 1);
+    if constexpr (sizeof(R) != sizeof(double)) lu[m] = __shfl_down_sync(0xffffffffu, fo[m], 1);
+    else lu[m] = R(0);
+  }
   const int i = i0 + lane;  // cell between faces p and p+1
   if (lane < XF_TX - 1 && i <= g.nx) {
     const bool upd = i >= g.eul_imin && i <= g.eul_imax;
     const double met = g.dcsidx[i];
     const long long ic = iidx(g, i, j, k);
 #pragma unroll
-    for (int m = 0; m < 5; ++m) fl[m * g.nint + ic] = upd ? (hi[m] - fh[m]) * met : 0.0;
+    for (int m = 0; m < 5; ++m) fl[m * g.nint + ic] = upd ? face_diff<R>(hu[m], lu[m], fh[m], fo[m]) * met : 0.0;
   }
 }
 
@@ -248,13 +296,13 @@ __global__ void __launch_bounds__(XF_NT) k_xflux(Geom g, const double* __restric
 // point loaded per face), computes every face of the segment once and adds the divergence to fl.
 // The z pass also applies the grad(mu div/3) term of visflx_div_ord2_subroutine
 // (kernels_cpu.F90:3446-3480) and emits the force_rhs block partials (:3157-3193).
-template <int DIR, int LB, int WS>
-__global__ void __launch_bounds__(MT_NT) k_march(Geom g, const double* __restrict__ aux,
+template <class R, int DIR, int LB, int WS>
+__global__ void __launch_bounds__(MT_NT) k_march(Geom g, const R* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl,
-                                                 const double* __restrict__ div3, const double* __restrict__ w,
-                                                 const double* __restrict__ fl_prev, const Scalars* __restrict__ sc,
-                                                 double rhork, double gamrk, int istep, int seglen, int nseg,
-                                                 double* __restrict__ red) {
+                                                 const R* __restrict__ div3,
+                                                 const double* __restrict__ w, const double* __restrict__ fl_prev,
+                                                 const Scalars* __restrict__ sc, double rhork, double gamrk,
+                                                 int istep, int seglen, int nseg, double* __restrict__ red) {
   static_assert(DIR == 1 || DIR == 2, "march kernel handles y and z");
   constexpr int S = LB > WS ? LB : WS;
   constexpr int NP = 2 * S;
@@ -276,83 +324,80 @@ __global__ void __launch_bounds__(MT_NT) k_march(Geom g, const double* __restric
     const long long n = g.nvol, nI = g.nint;
     const long long sd = DIR == 1 ? (long long)g.sx : (long long)g.sx * g.sy;
     const long long base0 = DIR == 1 ? gidx(g, i, 0, b) : gidx(g, i, b, 0);  // address of c = 0
-    const long long sI = DIR == 1 ? (long long)g.nx : (long long)g.nx * g.ny;  // interior stride
     // sensor bits of the face p: points p-WS+1 .. p+WS at bits 0 .. 2WS-1
     auto sensor_bit = [&](int c) -> unsigned {
-      double th;
       if (c < 1 || c > nd) {
         if (!g.periodic[DIR]) return 0u;
         c = wrap(c, nd);
       }
-      th = DIR == 1 ? sensor[iidx(g, i, c, b)] : sensor[iidx(g, i, b, c)];
+      const double th = DIR == 1 ? sensor[iidx(g, i, c, b)] : sensor[iidx(g, i, b, c)];
       return th > g.sensor_threshold ? 1u : 0u;
     };
     // preload the window and sensor bits of the face c0-2; the loop starts at the face c0-1
-    Stencil<double, S> st;
+    Stencil<R, S> st;
     const int p = c0 - 2;
 #pragma unroll
-    for (int q = 1; q < NP; ++q) load_point<S>(st, q, aux, n, base0 + (long long)(p - (S - 1) + q) * sd);
+    for (int q = 1; q < NP; ++q) load_point<R, S>(g, st, q, aux, n, base0 + (long long)(p - (S - 1) + q) * sd);
     unsigned mask = 0;
 #pragma unroll
     for (int bq = 1; bq < 2 * WS; ++bq) mask |= sensor_bit(p - WS + 1 + bq) << bq;
-    double flo[5] = {0, 0, 0, 0, 0};
+    R hlo[5] = {0, 0, 0, 0, 0}, llo[5] = {0, 0, 0, 0, 0};
     for (int c = c0 - 1; c <= c1; ++c) {
       // slide the window to the face c
 #pragma unroll
       for (int q = 0; q < NP - 1; ++q) {
         st.rho[q] = st.rho[q + 1]; st.u[q] = st.u[q + 1]; st.v[q] = st.v[q + 1];
-        st.w[q] = st.w[q + 1]; st.h[q] = st.h[q + 1]; st.t[q] = st.t[q + 1];
+        st.w[q] = st.w[q + 1]; st.h[q] = st.h[q + 1]; st.t[q] = st.t[q + 1]; st.c[q] = st.c[q + 1];
       }
-      load_point<S>(st, NP - 1, aux, n, base0 + (long long)(c + S) * sd);
+      load_point<R, S>(g, st, NP - 1, aux, n, base0 + (long long)(c + S) * sd);
       mask = (mask >> 1) | (sensor_bit(c + WS) << (2 * WS - 1));
-      double fhi[5];
-      window_flux<DIR, LB, WS, S>(g, st, mask != 0u, c, fhi);
-      if (c < c0) {
+      R hhi[5], lhi[5];
+      window_flux<R, DIR, LB, WS, S>(g, st, mask != 0u, c, hhi, lhi);
+      if (c >= c0) {
+        // cell c lies between the faces c-1 (lo) and c (hi)
+        const long long ic = DIR == 1 ? iidx(g, i, c, b) : iidx(g, i, b, c);
+        const double met = DIR == 1 ? g.detady[c] : g.dzitdz[c];
+        double f[5];
 #pragma unroll
-        for (int m = 0; m < 5; ++m) flo[m] = fhi[m];
-        continue;
+        for (int m = 0; m < 5; ++m) f[m] = fl[m * nI + ic] + face_diff<R>(hhi[m], lhi[m], hlo[m], llo[m]) * met;
+        if (DIR == 2) {
+          const int j = b, k = c;
+          const long long a = gidx(g, i, j, k);
+          const R uu = aux[n + a], vv = aux[2 * n + a], ww = aux[3 * n + a], mu = aux[6 * n + a];
+          const R dxl = mu / R(g.x[i + 1] - g.x[i - 1]);
+          const R dyl = mu / R(g.y[j + 1] - g.y[j - 1]);
+          const R dzl = mu / R(g.z[k + 1] - g.z[k - 1]);
+          const R sigx = dxl * (div3_at(g, div3, i + 1, j, k) - div3_at(g, div3, i - 1, j, k));
+          const R sigy = dyl * (div3_at(g, div3, i, j + 1, k) - div3_at(g, div3, i, j - 1, k));
+          const R sigz = dzl * (div3_at(g, div3, i, j, k + 1) - div3_at(g, div3, i, j, k - 1));
+          const R sigq = sigx * uu + sigy * vv + sigz * ww;
+          f[1] = f[1] - double(sigx);
+          f[2] = f[2] - double(sigy);
+          f[3] = f[3] - double(sigz);
+          f[4] = f[4] - double(sigq);
+          if (g.channel_case) {
+            const double dt = sc->dt;
+            const double rhodt = rhork * dt, gamdt = gamrk * dt;
+            double fln1 = (istep > 1 ? -(rhodt * fl_prev[ic]) : 0.0) - gamdt * f[0];
+            double fln2 = (istep > 1 ? -(rhodt * fl_prev[nI + ic]) : 0.0) - gamdt * f[1];
+            double dy = g.yn[j + 1] - g.yn[j];
+            const Prim pr = prim_from_w(g, w, a);
+            double rhou = w[n + a];
+            part[0] += fln1 * dy;
+            part[1] += fln2 * dy;
+            part[2] += pr.rho * dy;
+            part[3] += rhou * dy;
+            part[4] += rhou * dy * pr.tt;
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < 5; ++m) fl[m * nI + ic] = f[m];
       }
-      // cell c lies between the faces c-1 (flo) and c (fhi)
-      const long long ic = DIR == 1 ? iidx(g, i, c, b) : iidx(g, i, b, c);
-      const double met = DIR == 1 ? g.detady[c] : g.dzitdz[c];
-      double f[5];
 #pragma unroll
       for (int m = 0; m < 5; ++m) {
-        f[m] = fl[m * nI + ic] + (fhi[m] - flo[m]) * met;
-        flo[m] = fhi[m];
+        hlo[m] = hhi[m];
+        llo[m] = lhi[m];
       }
-      if (DIR == 2) {
-        const int j = b, k = c;
-        const long long a = gidx(g, i, j, k);
-        double uu = aux[n + a], vv = aux[2 * n + a], ww = aux[3 * n + a], mu = aux[6 * n + a];
-        double dxl = mu / (g.x[i + 1] - g.x[i - 1]);
-        double dyl = mu / (g.y[j + 1] - g.y[j - 1]);
-        double dzl = mu / (g.z[k + 1] - g.z[k - 1]);
-        double sigx = dxl * (div3_at(g, div3, i + 1, j, k) - div3_at(g, div3, i - 1, j, k));
-        double sigy = dyl * (div3_at(g, div3, i, j + 1, k) - div3_at(g, div3, i, j - 1, k));
-        double sigz = dzl * (div3_at(g, div3, i, j, k + 1) - div3_at(g, div3, i, j, k - 1));
-        double sigq = sigx * uu + sigy * vv + sigz * ww;
-        f[1] = f[1] - sigx;
-        f[2] = f[2] - sigy;
-        f[3] = f[3] - sigz;
-        f[4] = f[4] - sigq;
-        if (g.channel_case) {
-          const double dt = sc->dt;
-          const double rhodt = rhork * dt, gamdt = gamrk * dt;
-          double fln1 = (istep > 1 ? -(rhodt * fl_prev[ic]) : 0.0) - gamdt * f[0];
-          double fln2 = (istep > 1 ? -(rhodt * fl_prev[nI + ic]) : 0.0) - gamdt * f[1];
-          double dy = g.yn[j + 1] - g.yn[j];
-          double rho = w[a], rhou = w[n + a], tt = aux[5 * n + a];
-          part[0] += fln1 * dy;
-          part[1] += fln2 * dy;
-          part[2] += rho * dy;
-          part[3] += rhou * dy;
-          part[4] += rhou * dy * tt;
-        }
-      }
-#pragma unroll
-      for (int m = 0; m < 5; ++m) fl[m * nI + ic] = f[m];
-      (void)sI;
     }
   }
   if (DIR == 2 && g.channel_case) {
@@ -363,14 +408,13 @@ __global__ void __launch_bounds__(MT_NT) k_march(Geom g, const double* __restric
   }
 }
 
-// Cells of the flux passes without a face update (outside eul_[jk]min..max) keep fl unchanged;
-// with the channel's staggered walls every cell is inside.
-
 // visflx_reduced_ord2_subroutine (kernels_cpu.F90:4623-4721, update_sensor = 0) followed by
 // visflx_x/y/z_subroutine (:4779-4999), in the reference's accumulation order; at stage 3 also
-// sensor_subroutine (:4726-4744) into the next sensor buffer.
-__global__ void __launch_bounds__(256) k_visc(Geom g, const double* __restrict__ aux, double* __restrict__ fl,
-                                              double* __restrict__ div3, double* __restrict__ sensor_next,
+// sensor_subroutine (:4726-4744) into the next sensor buffer.  Arithmetic in R, accumulation
+// into the FP64 register.
+template <class R>
+__global__ void __launch_bounds__(256) k_visc(Geom g, const R* __restrict__ aux, double* __restrict__ fl,
+                                              R* __restrict__ div3, double* __restrict__ sensor_next,
                                               double* __restrict__ wallprop, int do_sensor) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
   if (q >= g.nint) return;
@@ -378,72 +422,72 @@ __global__ void __launch_bounds__(256) k_visc(Geom g, const double* __restrict__
   const long long n = g.nvol, nI = g.nint;
   const long long c = gidx(g, i, j, k);
   const long long sX = 1, sY = g.sx, sZ = (long long)g.sx * g.sy;
-  auto A = [&](long long a, int m) { return __ldg(aux + (m - 1) * n + a); };
-  const double uu = A(c, 2), vv = A(c, 3), ww = A(c, 4), tt = A(c, 6), mu = A(c, 7);
-  const double cploc = g.cp0, prandtl = g.prandtl;
-  double dxl = 1.0 / (g.x[i + 1] - g.x[i - 1]);
-  double dyl = 1.0 / (g.y[j + 1] - g.y[j - 1]);
-  double dzl = 1.0 / (g.z[k + 1] - g.z[k - 1]);
-  double ux = dxl * (A(c + sX, 2) - A(c - sX, 2));
-  double vx = dxl * (A(c + sX, 3) - A(c - sX, 3));
-  double wx = dxl * (A(c + sX, 4) - A(c - sX, 4));
-  double mux = dxl * (A(c + sX, 7) - A(c - sX, 7));
-  double uy = dyl * (A(c + sY, 2) - A(c - sY, 2));
-  double vy = dyl * (A(c + sY, 3) - A(c - sY, 3));
-  double wy = dyl * (A(c + sY, 4) - A(c - sY, 4));
-  double ty = dyl * (A(c + sY, 6) - A(c - sY, 6));
-  double muy = dyl * (A(c + sY, 7) - A(c - sY, 7));
-  double uz = dzl * (A(c + sZ, 2) - A(c - sZ, 2));
-  double vz = dzl * (A(c + sZ, 3) - A(c - sZ, 3));
-  double wz = dzl * (A(c + sZ, 4) - A(c - sZ, 4));
-  double muz = dzl * (A(c + sZ, 7) - A(c - sZ, 7));
+  auto A = [&](long long a, int m) -> R { return __ldg(aux + (m - 1) * n + a); };
+  const R uu = A(c, 2), vv = A(c, 3), ww = A(c, 4), mu = A(c, 7);
+  const R cploc = R(g.cp0), prandtl = R(g.prandtl);
+  R dxl = R(1) / R(g.x[i + 1] - g.x[i - 1]);
+  R dyl = R(1) / R(g.y[j + 1] - g.y[j - 1]);
+  R dzl = R(1) / R(g.z[k + 1] - g.z[k - 1]);
+  R ux = dxl * (A(c + sX, 2) - A(c - sX, 2));
+  R vx = dxl * (A(c + sX, 3) - A(c - sX, 3));
+  R wx = dxl * (A(c + sX, 4) - A(c - sX, 4));
+  R mux = dxl * (A(c + sX, 7) - A(c - sX, 7));
+  R uy = dyl * (A(c + sY, 2) - A(c - sY, 2));
+  R vy = dyl * (A(c + sY, 3) - A(c - sY, 3));
+  R wy = dyl * (A(c + sY, 4) - A(c - sY, 4));
+  R ty = dyl * (A(c + sY, 6) - A(c - sY, 6));
+  R muy = dyl * (A(c + sY, 7) - A(c - sY, 7));
+  R uz = dzl * (A(c + sZ, 2) - A(c - sZ, 2));
+  R vz = dzl * (A(c + sZ, 3) - A(c - sZ, 3));
+  R wz = dzl * (A(c + sZ, 4) - A(c - sZ, 4));
+  R muz = dzl * (A(c + sZ, 7) - A(c - sZ, 7));
   if (j == 1) {
     const long long wp = (long long)(k - 1) * g.nx + (i - 1);
     const long long nw = (long long)g.nx * g.nz;
-    wallprop[wp] = mu * uy;
-    wallprop[nw + wp] = mu * wy;
-    wallprop[2 * nw + wp] = mu * ty * cploc / prandtl;
+    wallprop[wp] = double(mu * uy);
+    wallprop[nw + wp] = double(mu * wy);
+    wallprop[2 * nw + wp] = double(mu * ty * cploc / prandtl);
   }
-  double div = ux + vy + wz;
-  double div3l = div / 3.0;
+  R div = ux + vy + wz;
+  R div3l = div / R(3);
   div3[q] = div3l;
-  double omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
-  double omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
+  R omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
+  R omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
   if (do_sensor) {
     // sensor_subroutine works from the stored |omega| and div/3
-    double om = sqrt(omod2);
-    double om2 = om * om;
-    double dv = 3.0 * div3l;
-    double u0l0 = g.u0 / g.l0;
-    double t = fmax(-dv / sqrt(om2 + dv * dv + u0l0 * u0l0), 0.0);
-    sensor_next[q] = t * t;
+    R om = sqrt(omod2);
+    R om2 = om * om;
+    R dv = R(3) * div3l;
+    R u0l0 = R(g.u0 / g.l0);
+    R t = fmax(-dv / sqrt(om2 + dv * dv + u0l0 * u0l0), R(0));
+    sensor_next[q] = double(t * t);
   }
-  double sig11 = ux - 2.0 * div3l, sig12 = vx, sig13 = wx;
-  double sig21 = uy, sig22 = vy - 2.0 * div3l, sig23 = wy;
-  double sig31 = uz, sig32 = vz, sig33 = wz - 2.0 * div3l;
-  double sigx = mux * sig11 + muy * sig12 + muz * sig13;
-  double sigy = mux * sig21 + muy * sig22 + muz * sig23;
-  double sigz = mux * sig31 + muy * sig32 + muz * sig33;
-  double sigah = (sig11 * ux + sig12 * uy + sig13 * uz + sig21 * vx + sig22 * vy + sig23 * vz + sig31 * wx +
-                  sig32 * wy + sig33 * wz) * mu;
-  double sigq = sigx * uu + sigy * vv + sigz * ww + sigah;
+  R sig11 = ux - R(2) * div3l, sig12 = vx, sig13 = wx;
+  R sig21 = uy, sig22 = vy - R(2) * div3l, sig23 = wy;
+  R sig31 = uz, sig32 = vz, sig33 = wz - R(2) * div3l;
+  R sigx = mux * sig11 + muy * sig12 + muz * sig13;
+  R sigy = mux * sig21 + muy * sig22 + muz * sig23;
+  R sigz = mux * sig31 + muy * sig32 + muz * sig33;
+  R sigah = (sig11 * ux + sig12 * uy + sig13 * uz + sig21 * vx + sig22 * vy + sig23 * vz + sig31 * wx +
+             sig32 * wy + sig33 * wz) * mu;
+  R sigq = sigx * uu + sigy * vv + sigz * ww + sigah;
   double f2 = fl[nI + q], f3 = fl[2 * nI + q], f4 = fl[3 * nI + q], f5 = fl[4 * nI + q];
-  f2 = f2 - sigx;
-  f3 = f3 - sigy;
-  f4 = f4 - sigz;
-  f5 = f5 - sigq;
+  f2 = f2 - double(sigx);
+  f3 = f3 - double(sigy);
+  f4 = f4 - double(sigz);
+  f5 = f5 - double(sigq);
   // conservative face Laplacian: face sigma between points a (lower) and b (upper)
   auto face = [&](long long a, long long b, double d, double (&s)[4]) {
-    double u1 = A(a, 2), u2 = A(b, 2), v1 = A(a, 3), v2 = A(b, 3), w1 = A(a, 4), w2 = A(b, 4);
-    double t1 = A(a, 6), t2 = A(b, 6), m1 = A(a, 7), m2 = A(b, 7);
-    double qq1 = 0.5 * (u1 * u1 + v1 * v1 + w1 * w1);
-    double qq2 = 0.5 * (u2 * u2 + v2 * v2 + w2 * w2);
-    double muf = m1 + m2;
-    muf = 0.5 * muf / d;
-    s[0] = (u2 - u1) * muf;
-    s[1] = (v2 - v1) * muf;
-    s[2] = (w2 - w1) * muf;
-    s[3] = ((t2 - t1) * cploc / prandtl + (qq2 - qq1)) * muf;
+    R u1 = A(a, 2), u2 = A(b, 2), v1 = A(a, 3), v2 = A(b, 3), w1 = A(a, 4), w2 = A(b, 4);
+    R t1 = A(a, 6), t2 = A(b, 6), m1 = A(a, 7), m2 = A(b, 7);
+    R qq1 = R(0.5) * (u1 * u1 + v1 * v1 + w1 * w1);
+    R qq2 = R(0.5) * (u2 * u2 + v2 * v2 + w2 * w2);
+    R muf = m1 + m2;
+    muf = R(0.5) * muf / R(d);
+    s[0] = double((u2 - u1) * muf);
+    s[1] = double((v2 - v1) * muf);
+    s[2] = double((w2 - w1) * muf);
+    s[3] = double(((t2 - t1) * cploc / prandtl + (qq2 - qq1)) * muf);
   };
   double lo[4], hi[4];
   // x: fl += dxhl*(fhat(i) - fhat(i-1)), fhat = -sigma
@@ -477,35 +521,38 @@ __global__ void __launch_bounds__(256) k_visc(Geom g, const double* __restrict__
 
 // Initial Ducros sensor of run() (visflx(mode=2), singleideal_cpu.F90:1550-1555):
 // visflx_reduced_ord2 with update_sensor = 1 (kernels_cpu.F90:4680-4682)
-__global__ void __launch_bounds__(256) k_init_sensor(Geom g, const double* __restrict__ aux,
+template <class R>
+__global__ void __launch_bounds__(256) k_init_sensor(Geom g, const R* __restrict__ aux,
                                                      double* __restrict__ sensor) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
   if (q >= g.nint) return;
   const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
   const long long n = g.nvol, c = gidx(g, i, j, k), sY = g.sx, sZ = (long long)g.sx * g.sy;
-  auto A = [&](long long a, int m) { return aux[(m - 1) * n + a]; };
-  double dxl = 1.0 / (g.x[i + 1] - g.x[i - 1]);
-  double dyl = 1.0 / (g.y[j + 1] - g.y[j - 1]);
-  double dzl = 1.0 / (g.z[k + 1] - g.z[k - 1]);
-  double ux = dxl * (A(c + 1, 2) - A(c - 1, 2));
-  double vx = dxl * (A(c + 1, 3) - A(c - 1, 3));
-  double wx = dxl * (A(c + 1, 4) - A(c - 1, 4));
-  double uy = dyl * (A(c + sY, 2) - A(c - sY, 2));
-  double vy = dyl * (A(c + sY, 3) - A(c - sY, 3));
-  double wy = dyl * (A(c + sY, 4) - A(c - sY, 4));
-  double uz = dzl * (A(c + sZ, 2) - A(c - sZ, 2));
-  double vz = dzl * (A(c + sZ, 3) - A(c - sZ, 3));
-  double wz = dzl * (A(c + sZ, 4) - A(c - sZ, 4));
-  double div = ux + vy + wz;
-  double omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
-  double omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
-  double u0l0 = g.u0 / g.l0;
-  double t = fmax(-div / sqrt(omod2 + div * div + u0l0 * u0l0), 0.0);
-  sensor[q] = t * t;
+  auto A = [&](long long a, int m) -> R { return aux[(m - 1) * n + a]; };
+  R dxl = R(1) / R(g.x[i + 1] - g.x[i - 1]);
+  R dyl = R(1) / R(g.y[j + 1] - g.y[j - 1]);
+  R dzl = R(1) / R(g.z[k + 1] - g.z[k - 1]);
+  R ux = dxl * (A(c + 1, 2) - A(c - 1, 2));
+  R vx = dxl * (A(c + 1, 3) - A(c - 1, 3));
+  R wx = dxl * (A(c + 1, 4) - A(c - 1, 4));
+  R uy = dyl * (A(c + sY, 2) - A(c - sY, 2));
+  R vy = dyl * (A(c + sY, 3) - A(c - sY, 3));
+  R wy = dyl * (A(c + sY, 4) - A(c - sY, 4));
+  R uz = dzl * (A(c + sZ, 2) - A(c - sZ, 2));
+  R vz = dzl * (A(c + sZ, 3) - A(c - sZ, 3));
+  R wz = dzl * (A(c + sZ, 4) - A(c - sZ, 4));
+  R div = ux + vy + wz;
+  R omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
+  R omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
+  R u0l0 = R(g.u0 / g.l0);
+  R t = fmax(-div / sqrt(omod2 + div * div + u0l0 * u0l0), R(0));
+  sensor[q] = double(t * t);
 }
 
-// compute_dt_subroutine (kernels_cpu.F90:6814-6880): block maxima of the 9 inverse time scales
-__global__ void __launch_bounds__(256) k_dt(Geom g, const double* __restrict__ w, const double* __restrict__ aux,
+// compute_dt_subroutine (kernels_cpu.F90:6814-6880): block maxima of the 9 inverse time scales.
+// The FP64 form reads the primitive fields; the mixed form recomputes them from w in FP64.
+template <class R>
+__global__ void __launch_bounds__(256) k_dt(Geom g, const double* __restrict__ w, const R* __restrict__ aux,
                                             double* __restrict__ red) {
   __shared__ double sm[9 * 8];
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
@@ -515,7 +562,13 @@ __global__ void __launch_bounds__(256) k_dt(Geom g, const double* __restrict__ w
     const long long n = g.nvol, c = gidx(g, i, j, k);
     double rho = w[c];
     double ri = 1.0 / rho;
-    double uu = aux[n + c], vv = aux[2 * n + c], ww = aux[3 * n + c], tt = aux[5 * n + c], mu = aux[6 * n + c];
+    double uu, vv, ww, tt, mu;
+    if constexpr (sizeof(R) == sizeof(double)) {
+      uu = aux[n + c]; vv = aux[2 * n + c]; ww = aux[3 * n + c]; tt = aux[5 * n + c]; mu = aux[6 * n + c];
+    } else {
+      const Prim p = prim_from_w(g, w, c);
+      uu = p.uu; vv = p.vv; ww = p.ww; tt = p.tt; mu = viscosity(g, tt);
+    }
     double nu = ri * mu;
     double kr = nu / g.prandtl;
     double cs = sqrt(g.gamloc * g.rgas0 * tt);
@@ -595,12 +648,14 @@ __global__ void __launch_bounds__(FIN_NT) k_finish_rhs(Geom g, const double* __r
 }
 
 // update_flux + force_rhs_2 + update_field (kernels_cpu.F90:3400-3442, 3092-3116) and the
-// partials of force_var_1 (:3241-3282) and of compute_residual / minmax (:6682-6810).
-__global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, const double* __restrict__ aux,
-                                                const double* __restrict__ fl_prev, const double* __restrict__ fl_new,
-                                                const Scalars* __restrict__ sc, double rhork, double gamrk, int istep,
-                                                int stats, double* __restrict__ red,
-                                                const double* __restrict__ sensor_next, double* __restrict__ sensor) {
+// partials of force_var_1 (:3241-3282) and of compute_residual / minmax (:6682-6810).  All FP64;
+// the primitive values of the stage's starting state are recomputed from w as eval_aux does.
+template <class R>
+__global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, const double* __restrict__ fl_prev,
+                                                const double* __restrict__ fl_new, const Scalars* __restrict__ sc,
+                                                double rhork, double gamrk, int istep, int stats,
+                                                double* __restrict__ red, const double* __restrict__ sensor_next,
+                                                double* __restrict__ sensor) {
   __shared__ double sm[2 * 8];
   __shared__ double smn[3 * 8];
   __shared__ double smx[3 * 8];
@@ -613,6 +668,7 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
     const long long n = g.nvol, nI = g.nint, c = gidx(g, i, j, k);
     const double dt = sc->dt;
     const double rhodt = rhork * dt, gamdt = gamrk * dt;
+    const Prim old = prim_from_w(g, w, c);
     double fln[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
@@ -621,10 +677,9 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
     }
     if (g.channel_case) {
       const double b1 = sc->bulk[0], b2 = sc->bulk[1];
-      double uu = aux[n + c];
       fln[0] = fln[0] - b1;
       fln[1] = fln[1] - b2;
-      fln[4] = fln[4] - uu * b2;
+      fln[4] = fln[4] - old.uu * b2;
     }
     double wn[5];
 #pragma unroll
@@ -634,7 +689,7 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
     }
     // the stage-3 sensor becomes current once every flux of the stage has used the old one
     if (istep == 3) sensor[q] = sensor_next[q];
-    double tstat = aux[5 * n + c];
+    double tstat = old.tt;
     if (g.force_var) {
       double dy = g.yn[j + 1] - g.yn[j];
       double ri = 1.0 / wn[0];
@@ -648,7 +703,7 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
     if (stats) {
       double r = fln[1] / dt;
       s2[1] = r * r;
-      double rho = aux[c];
+      double rho = old.rho;
       double pp = rho * tstat * g.rgas0;
       mn[0] = rho; mn[1] = tstat; mn[2] = pp;
       mx[0] = rho; mx[1] = tstat; mx[2] = pp;
@@ -741,19 +796,20 @@ __global__ void __launch_bounds__(256) k_count_weno(Geom g, const double* __rest
   if (q < g.nint) {
     const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
     const int ws = g.weno_scheme;
+    const double thr = g.sensor_threshold;
     if (i >= g.eul_imin && i <= g.eul_imax) {
       bool s = false;
-      for (int o = -ws + 1; o <= ws; ++o) s = s || sensor_at(g, sensor, i + o, j, k) > g.sensor_threshold;
+      for (int o = -ws + 1; o <= ws; ++o) s = s || sensor_at(g, sensor, i + o, j, k) > thr;
       v[0] = s ? 1.0 : 0.0;
     }
     if (j >= g.eul_jmin && j <= g.eul_jmax) {
       bool s = false;
-      for (int o = -ws + 1; o <= ws; ++o) s = s || sensor_at(g, sensor, i, j + o, k) > g.sensor_threshold;
+      for (int o = -ws + 1; o <= ws; ++o) s = s || sensor_at(g, sensor, i, j + o, k) > thr;
       v[1] = s ? 1.0 : 0.0;
     }
     if (k >= g.eul_kmin && k <= g.eul_kmax) {
       bool s = false;
-      for (int o = -ws + 1; o <= ws; ++o) s = s || sensor_at(g, sensor, i, j, k + o) > g.sensor_threshold;
+      for (int o = -ws + 1; o <= ws; ++o) s = s || sensor_at(g, sensor, i, j, k + o) > thr;
       v[2] = s ? 1.0 : 0.0;
     }
   }
@@ -765,10 +821,10 @@ __global__ void __launch_bounds__(256) k_count_weno(Geom g, const double* __rest
 inline unsigned nblocks(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
 // Wrap one launch with profiler events when profiling is on.
-#define SB_LAUNCH(dst, kid, s, ...)                  \
-  do {                                               \
+#define SB_LAUNCH(dst, kid, s, ...)                                  \
+  do {                                                               \
     if ((dst).prof && (dst).prof->on) (dst).prof->begin((kid), (s)); \
-    __VA_ARGS__;                                     \
+    __VA_ARGS__;                                                     \
     if ((dst).prof && (dst).prof->on) (dst).prof->end((s));          \
   } while (0)
 
@@ -841,15 +897,36 @@ long long reduction_slots(const Geom& g) {
   return a > b ? a : b;
 }
 
-cudaError_t launch_aux(const Geom& g, DevState& d, int apply_shift, cudaStream_t s, long long* nl) {
-  SB_LAUNCH(d, K_AUX, s, k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, apply_shift, 0));
+// typed views of the precision-dependent buffers
+template <class R> static R* aux_of(DevState& d);
+template <> double* aux_of<double>(DevState& d) { return d.aux; }
+template <> float* aux_of<float>(DevState& d) { return d.auxf; }
+template <class R> static R* div3_of(DevState& d);
+template <> double* div3_of<double>(DevState& d) { return d.div3; }
+template <> float* div3_of<float>(DevState& d) { return d.div3f; }
+
+// A pending energy shift is applied to the interior in its own pass first: the aux pass reads
+// interior points as the sources of ghost states, so it must not rewrite them itself.
+template <class R>
+static void aux_launch(const Geom& g, DevState& d, int apply_shift, int write_ghost, int kid, cudaStream_t s,
+                       long long* nl) {
+  if (apply_shift) {
+    SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.sc));
+    ++*nl;
+  }
+  SB_LAUNCH(d, kid, s, k_aux<R><<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), write_ghost));
   ++*nl;
+}
+
+cudaError_t launch_aux(const Geom& g, DevState& d, int apply_shift, cudaStream_t s, long long* nl) {
+  if (g.precision == 1) aux_launch<float>(g, d, apply_shift, 0, K_AUX, s, nl);
+  else aux_launch<double>(g, d, apply_shift, 0, K_AUX, s, nl);
   return cudaGetLastError();
 }
 
 cudaError_t launch_fill_ghosts(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
-  SB_LAUNCH(d, K_FILL_GHOSTS, s, k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, 0, 1));
-  ++*nl;
+  if (g.precision == 1) aux_launch<float>(g, d, 0, 1, K_FILL_GHOSTS, s, nl);
+  else aux_launch<double>(g, d, 0, 1, K_FILL_GHOSTS, s, nl);
   return cudaGetLastError();
 }
 
@@ -860,14 +937,20 @@ cudaError_t launch_apply_shift(const Geom& g, DevState& d, cudaStream_t s, long 
 }
 
 cudaError_t launch_init_sensor(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
-  SB_LAUNCH(d, K_INIT_SENSOR, s, k_init_sensor<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.aux, d.sensor));
+  if (g.precision == 1)
+    SB_LAUNCH(d, K_INIT_SENSOR, s, k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, d.sensor, 0));
+  else
+    SB_LAUNCH(d, K_INIT_SENSOR, s, k_init_sensor<double><<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.aux, d.sensor));
   ++*nl;
   return cudaGetLastError();
 }
 
 cudaError_t launch_dt(const Geom& g, DevState& d, double cfl, cudaStream_t s, long long* nl) {
   const unsigned nb = nblocks(g.nint, 256);
-  SB_LAUNCH(d, K_DT, s, k_dt<<<nb, 256, 0, s>>>(g, d.w, d.aux, d.red));
+  if (g.precision == 1)
+    SB_LAUNCH(d, K_DT, s, k_dt<float><<<nb, 256, 0, s>>>(g, d.w, d.auxf, d.red));
+  else
+    SB_LAUNCH(d, K_DT, s, k_dt<double><<<nb, 256, 0, s>>>(g, d.w, d.aux, d.red));
   SB_LAUNCH(d, K_DT_FINISH, s, k_dt_finish<<<1, FIN_NT, 0, s>>>(d.red, nb, cfl, d.sc));
   *nl += 2;
   return cudaGetLastError();
@@ -886,7 +969,7 @@ cudaError_t launch_count_weno(const Geom& g, DevState& d, cudaStream_t s, long l
   return cudaGetLastError();
 }
 
-template <int LB, int WS>
+template <class R, int LB, int WS>
 static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
                               cudaStream_t s, long long* nl) {
   const dim3 xb(XF_TX, XF_TY);
@@ -896,21 +979,28 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   march_split(g, 1, &sly, &nsy, &nty);
   march_split(g, 2, &slz, &nsz, &ntz);
   const unsigned gyb = nblocks(nty, MT_NT), gzb = nblocks(ntz, MT_NT);
-  if (a.run_aux) {
-    SB_LAUNCH(d, K_AUX, s, k_aux<<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc, a.apply_shift, 0));
+  R* aux = aux_of<R>(d);
+  double* sensor = d.sensor;
+  double* sensor_next = d.sensor_next;
+  R* div3 = div3_of<R>(d);
+  const bool fp64 = sizeof(R) == sizeof(double);
+  if (a.run_aux) aux_launch<R>(g, d, a.apply_shift, 0, K_AUX, s, nl);
+  SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS><<<xg, xb, 0, s>>>(g, aux, sensor, fl_new));
+  SB_LAUNCH(d, K_VISC, s,
+            k_visc<R><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
+                                                           fp64 && a.istep == 3));
+  if (!fp64 && a.istep == 3) {
+    // the mixed form takes the stage-3 sensor in FP64 from the stage's starting state
+    SB_LAUNCH(d, K_INIT_SENSOR, s, k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, sensor_next, 1));
     ++*nl;
   }
-  SB_LAUNCH(d, K_EULER_X, s, k_xflux<LB, WS><<<xg, xb, 0, s>>>(g, d.aux, d.sensor, fl_new));
-  SB_LAUNCH(d, K_VISC, s,
-            k_visc<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.aux, fl_new, d.div3, d.sensor_next, d.wallprop,
-                                                        a.istep == 3));
   if (gyb > 0)
     SB_LAUNCH(d, K_EULER_Y, s,
-              k_march<1, LB, WS><<<gyb, MT_NT, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc,
-                                                       a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
+              k_march<R, 1, LB, WS><<<gyb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
+                                                          a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
   SB_LAUNCH(d, K_EULER_Z, s,
-            k_march<2, LB, WS><<<gzb, MT_NT, 0, s>>>(g, d.aux, d.sensor, fl_new, d.div3, d.w, fl_prev, d.sc,
-                                                     a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
+            k_march<R, 2, LB, WS><<<gzb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
+                                                        a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
   *nl += 4;
   if (g.channel_case) {
     SB_LAUNCH(d, K_FINISH_RHS, s, k_finish_rhs<<<1, FIN_NT, 0, s>>>(g, d.red, (long long)gzb, a.istep == 1, d.sc));
@@ -918,20 +1008,27 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   }
   const unsigned nbu = nblocks(g.nint, 256);
   SB_LAUNCH(d, K_UPDATE, s,
-            k_update<<<nbu, 256, 0, s>>>(g, d.w, d.aux, fl_prev, fl_new, d.sc, a.rhork, a.gamrk, a.istep,
-                                         a.want_stats, d.red, d.sensor_next, d.sensor));
+            k_update<R><<<nbu, 256, 0, s>>>(g, d.w, fl_prev, fl_new, d.sc, a.rhork, a.gamrk, a.istep,
+                                            a.want_stats, d.red, sensor_next, sensor));
   SB_LAUNCH(d, K_FINISH_UPD, s, k_finish_upd<<<1, FIN_NT, 0, s>>>(g, d.red, nbu, a.want_stats, a.add_time, d.sc));
   *nl += 2;
   return cudaGetLastError();
 }
 
+template <class R>
+static cudaError_t stage_dispatch(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
+                                  cudaStream_t s, long long* nl) {
+  if (g.lmax_base == 3 && g.weno_scheme == 3) return stage_impl<R, 3, 3>(g, d, a, fl_prev, fl_new, s, nl);
+  if (g.lmax_base == 2 && g.weno_scheme == 2) return stage_impl<R, 2, 2>(g, d, a, fl_prev, fl_new, s, nl);
+  if (g.lmax_base == 4 && g.weno_scheme == 4) return stage_impl<R, 4, 4>(g, d, a, fl_prev, fl_new, s, nl);
+  if (g.lmax_base == 3 && g.weno_scheme == 2) return stage_impl<R, 3, 2>(g, d, a, fl_prev, fl_new, s, nl);
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_stage(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
                          cudaStream_t s, long long* nl) {
-  if (g.lmax_base == 3 && g.weno_scheme == 3) return stage_impl<3, 3>(g, d, a, fl_prev, fl_new, s, nl);
-  if (g.lmax_base == 2 && g.weno_scheme == 2) return stage_impl<2, 2>(g, d, a, fl_prev, fl_new, s, nl);
-  if (g.lmax_base == 4 && g.weno_scheme == 4) return stage_impl<4, 4>(g, d, a, fl_prev, fl_new, s, nl);
-  if (g.lmax_base == 3 && g.weno_scheme == 2) return stage_impl<3, 2>(g, d, a, fl_prev, fl_new, s, nl);
-  return cudaErrorInvalidValue;
+  if (g.precision == 1) return stage_dispatch<float>(g, d, a, fl_prev, fl_new, s, nl);
+  return stage_dispatch<double>(g, d, a, fl_prev, fl_new, s, nl);
 }
 
 bool stage_supported(int lmax_base, int weno_scheme) {
