@@ -345,8 +345,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   R b3 = etot - rho * p_rho / p_e;
   R b2 = p_e / (rho * cc);
   R b1 = p_rho / cc - b2 * (etot - R(2) * qq);
-  const R vel[3] = {uu, vv, ww};
-  const R vn = vel[DIR];
+  const R vn = DIR == 0 ? uu : (DIR == 1 ? vv : ww);
   constexpr int t1 = DIR == 0 ? 1 : 0;
   constexpr int t2 = DIR == 2 ? 1 : 2;
   // stencil maximum of the characteristic speeds (offsets -WS+1 .. WS)
@@ -364,7 +363,9 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   const R betascale_b = R(1) / (R(g.rho0) * R(g.rho0) * (R(g.u0) * R(g.u0)) * (R(g.u0) * R(g.u0)));
 #pragma unroll
   for (int m = 0; m < 5; ++m) fh[m] = fl[m] = R(0);
-#pragma unroll
+  // one characteristic field per iteration; the loop is kept rolled so that the reconstruction
+  // is emitted once (the unrolled form overflows the instruction cache)
+#pragma unroll 1
   for (int m = 0; m < 5; ++m) {
     // column m of the left eigenvector matrix el(1:5, m)
     R e0, e1, e2, e3, e4;
@@ -379,7 +380,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
       e0 = R(1) - b1; e1 = b2 * uu; e2 = b2 * vv; e3 = b2 * ww; e4 = -b2;
     } else {
       const int tt_ = m == 2 ? t1 : t2;
-      e0 = -vel[tt_];
+      e0 = -(tt_ == 0 ? uu : (tt_ == 1 ? vv : ww));
       e1 = tt_ == 0 ? R(1) : R(0);
       e2 = tt_ == 1 ? R(1) : R(0);
       e3 = tt_ == 2 ? R(1) : R(0);
@@ -433,7 +434,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
       r1 = tt_ == 0 ? R(1) : R(0);
       r2 = tt_ == 1 ? R(1) : R(0);
       r3 = tt_ == 2 ? R(1) : R(0);
-      r4 = vel[tt_];
+      r4 = tt_ == 0 ? uu : (tt_ == 1 ? vv : ww);
     }
     acc_prod(fh[0], fl[0], r0, fi);
     acc_prod(fh[1], fl[1], r1, fi);

@@ -32,6 +32,21 @@ namespace {
 constexpr int AUX_NT = 256;
 constexpr int XF_TX = 32, XF_TY = 4, XF_NT = XF_TX * XF_TY;  // x faces: 4 row-warps per block
 constexpr int MT_NT = 128;                                     // march kernels
+// Resident blocks per SM asked of the register allocator for the FP64 and FP32 instantiations
+// of the flux kernels (measured: 3 and 4 blocks of 128 threads beat the unconstrained
+// 2 blocks, although the FP64 march kernels then spill a little; the kernels are latency bound).
+#ifndef XF_MINB_D
+#define XF_MINB_D 3
+#endif
+#ifndef XF_MINB_F
+#define XF_MINB_F 4
+#endif
+#ifndef MT_MINB_D
+#define MT_MINB_D 3
+#endif
+#ifndef MT_MINB_F
+#define MT_MINB_F 4
+#endif
 constexpr int FIN_NT = 1024;
 
 // Apply force_var_2 (kernels_cpu.F90:3285-3314) to the conserved values of one interior point:
@@ -254,7 +269,7 @@ __device__ __forceinline__ double face_diff(R hup, R lup, R hlo, R llo) {
 // so no shared memory and no block barrier are needed.  fl is written (first contribution of the
 // stage, euler_x after init_flux).
 template <class R, int LB, int WS>
-__global__ void __launch_bounds__(XF_NT) k_xflux(Geom g, const R* __restrict__ aux,
+__global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F) k_xflux(Geom g, const R* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl) {
   constexpr int S = LB > WS ? LB : WS;
   const int lane = threadIdx.x;
@@ -297,7 +312,7 @@ __global__ void __launch_bounds__(XF_NT) k_xflux(Geom g, const R* __restrict__ a
 // The z pass also applies the grad(mu div/3) term of visflx_div_ord2_subroutine
 // (kernels_cpu.F90:3446-3480) and emits the force_rhs block partials (:3157-3193).
 template <class R, int DIR, int LB, int WS>
-__global__ void __launch_bounds__(MT_NT) k_march(Geom g, const R* __restrict__ aux,
+__global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F) k_march(Geom g, const R* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl,
                                                  const R* __restrict__ div3,
                                                  const double* __restrict__ w, const double* __restrict__ fl_prev,

@@ -17,7 +17,10 @@ from pathlib import Path
 import numpy as np
 
 _HERE = Path(__file__).resolve().parent
-LIB_PATH = _HERE.parent / "lib" / "libstreams_b200.so"
+_DEFAULT_LIB = _HERE.parent / "lib" / "libstreams_b200.so"
+# STREAMS_B200_LIB selects another build of the same library (for example one compiled with
+# different launch bounds); the default is the in-tree build.
+LIB_PATH = Path(os.environ.get("STREAMS_B200_LIB", str(_DEFAULT_LIB)))
 
 OK, EINVAL, ECUDA, ENOMEM, ENAN, ETIMEOUT, ENODEV = 0, -1, -2, -3, -4, -5, -6
 

@@ -16,8 +16,19 @@ for p in (ROOT / "streams-2_b200", ROOT / "oracle", ROOT):
         sys.path.insert(0, str(p))
 
 
+def _ensure_built():
+    """Build the oracle and the CUDA library when a fresh checkout lacks them (both build on a
+    CPU-only machine: nvcc cross-compiles for sm_100a)."""
+    import subprocess
+    for target, d in ((ROOT / "oracle" / "_build" / "liboracle.so", ROOT / "oracle"),
+                      (ROOT / "streams-2_b200" / "lib" / "libstreams_b200.so", ROOT / "streams-2_b200")):
+        if not target.exists():
+            subprocess.run(["make", "-s", "-C", str(d), "-j8"], check=True)
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+    _ensure_built()
 
 
 def gpu_available() -> bool:
