@@ -31,7 +31,7 @@ import time
 from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
-for p in (ROOT / "streams-2_b200", ROOT / "oracle", ROOT / "tests"):
+for p in (ROOT / "streams-2_b200", ROOT / "oracle"):
     sys.path.insert(0, str(p))
 
 # Algorithmic (compulsory) bytes per interior cell of one launch of each kernel: the fields the
@@ -116,9 +116,79 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def channel_case_ini(nx, ny, nz, steps):
-    from conftest import channel_ini
-    return channel_ini(nx, ny, nz, num_iter=steps, print_control=max(1, steps))
+def channel_case_ini(nx, ny, nz, steps, **kw):
+    from streams_b200.cases import channel_ini
+    return channel_ini(nx, ny, nz, num_iter=steps, print_control=max(1, steps), **kw)
+
+
+def run_batched(torch, precision, steps, warmup, tune_cache):
+    """The batched form: 48 channel boxes of uneven grids and flow parameters (seeded mix),
+    autotuned launch shapes, one CUDA graph per 10 steps of all boxes.  Device time from CUDA
+    events recorded on every box's stream (start on the first box, max over the ends)."""
+    from streams_b200 import Batch, Case, Solver
+    from streams_b200.cases import batch_mix
+    from streams_b200.tune import autotune
+    boxes = batch_mix()
+    solvers, cells = [], 0
+    with tempfile.TemporaryDirectory() as d:
+        for i, b in enumerate(boxes):
+            kw = dict(b)
+            nx, ny, nz = kw.pop("nx"), kw.pop("ny"), kw.pop("nz")
+            bd = os.path.join(d, f"b{i}")
+            os.makedirs(bd)
+            case = Case(bd, channel_case_ini(nx, ny, nz, steps, **kw))
+            t = autotune(case, precision=precision, cache=tune_cache)
+            sv = Solver.from_case(case, precision=precision)
+            sv.set_tuning(*t)
+            sv.init_run()
+            solvers.append(sv)
+            cells += nx * ny * nz
+    batch = Batch(solvers, steps_per_graph=10)
+    batch.advance(1 + warmup)
+    batch.synchronize()
+    streams = [torch.cuda.ExternalStream(sv.stream_handle) for sv in solvers]
+    e0 = torch.cuda.Event(enable_timing=True)
+    ends = [torch.cuda.Event(enable_timing=True) for _ in solvers]
+    torch.cuda.synchronize()
+    l0 = sum(sv.launches for sv in solvers)
+    e0.record(streams[0])
+    batch.advance(steps)
+    for e, st in zip(ends, streams):
+        e.record(st)
+    batch.synchronize()
+    ms = max(e0.elapsed_time(e) for e in ends)
+    replays, per = batch.stats()
+    launches = sum(sv.launches for sv in solvers) - l0
+    batch.close()
+    for sv in solvers:
+        sv.close()
+    return {"value": cells * steps / (ms / 1e3) / 1e6, "unit": "Mcell-steps/s", "boxes": len(boxes),
+            "cells": cells, "steps": steps, "ms": ms, "graph_replays": replays, "launches_per_replay": per,
+            "gpu_launches": launches}
+
+
+def run_serving(torch, duration_s, step_scale, single_rate, tune_cache):
+    """The served form: a Poisson stream of channel solves (grids log-uniform between 48^3 and
+    384x192x128 cells, Mach 0.5-2.5, FP64 or mixed), arrivals over duration_s seconds at a rate
+    that saturates the GPU (from the single-box throughput), step counts 200-2000 scaled by
+    step_scale so the run stays short; HBM budget 150 GB (or what is free)."""
+    import numpy as np
+    from streams_b200.cases import serve_mix
+    from streams_b200.serve import Server
+    lo, hi = max(2, int(200 * step_scale)), max(3, int(2000 * step_scale))
+    mean_cells = (384 * 192 * 128 - 48 ** 3) / np.log((384 * 192 * 128) / 48 ** 3)
+    mean_work = mean_cells * (lo + hi) / 2
+    rate = 1.1 * single_rate * 1e6 / mean_work
+    reqs = [r for r in serve_mix(int(rate * duration_s * 1.5) + 4, rate, steps=(lo, hi)) if r["arrival"] <= duration_s]
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(150e9, free - 8e9))
+    srv = Server(budget_bytes=budget, tick_steps=10, tune_cache=tune_cache)
+    out = srv.run(reqs)
+    return {"requests": len(reqs), "completed": out["completed"], "rejected": len(out["rejected"]),
+            "rate_per_s": rate, "arrival_window_s": duration_s, "steps_range": [lo, hi],
+            "p50_s": out["p50_s"], "p99_s": out["p99_s"], "mean_s": out["mean_s"],
+            "mcell_steps_per_s": out["mcell_steps_per_s"], "mcell_steps_per_busy_s": out["mcell_steps_per_busy_s"],
+            "max_resident": out["max_resident"], "ticks": out["ticks"], "budget_gb": budget / 1e9}
 
 
 def cpu_oracle_rate(nx, ny, nz, nsteps, budget_s=20.0):
@@ -197,6 +267,11 @@ def main():
     ap.add_argument("--size", default="512x256x256")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
+    ap.add_argument("--batched-steps", type=int, default=200)
+    ap.add_argument("--serve-seconds", type=float, default=30.0)
+    ap.add_argument("--serve-step-scale", type=float, default=0.1)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -345,6 +420,22 @@ def main():
                  "rel_l2_vs_fp64_100_steps_128x96x64": errs, "max_rel_l2": max(errs),
                  "precision": "FP32 flux/viscous arithmetic, FP64 state, RK register, T recovery, dt, reductions"}
 
+    # batched and served forms (rank 0 of a replica run measures them on its own GPU)
+    tune_cache = {}
+    batched = None
+    if not args.no_batched:
+        batched = {"fp64": run_batched(torch, 0, args.batched_steps, args.warmup, tune_cache),
+                   "mixed": run_batched(torch, 1, args.batched_steps, args.warmup, tune_cache)}
+        batched["fp64"]["vs_single_box"] = batched["fp64"]["value"] / value
+        if mixed:
+            batched["mixed"]["vs_single_box"] = batched["mixed"]["value"] / mixed["value"]
+        batched["workload"] = ("48 channel boxes, grids from {64,96,128}x{64,96}x{32,64,96}, Mach U[0.3,2], "
+                               "Re_b U[2000,6000], seeded; one CUDA graph per 10 steps of all boxes")
+    serving = None
+    if not args.no_serve:
+        serving = run_serving(torch, args.serve_seconds, args.serve_step_scale, value, tune_cache)
+        serving["vs_single_box"] = (serving["mcell_steps_per_s"] or 0.0) / value
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -370,6 +461,7 @@ def main():
                     "what": "copy_from_field (pinned) + init_run + K x (rk step + scalar read) + copy_to_field"},
             "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
             "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "mixed": mixed,
+            "batched": batched, "serving": serving,
             "state": {"dt": sc["dt"], "rhobulk": sc["rhobulk"], "ubulk": sc["ubulk"], "tbulk": sc["tbulk"],
                       "residual_rhou": res["residual_rhou"], "nan": res["nan"]},
             "u0": info["u0"],

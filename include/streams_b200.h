@@ -204,6 +204,49 @@ const char* streams_b200_kernel_name(int kid);
 int streams_b200_debug_fetch(streams_b200_ctx* ctx, int which, double* out, long long n);
 
 /*
+ * Launch shape of the y and z flux passes (no counterpart in the reference, whose GPU kernels
+ * use fixed thread blocks).  Each (x, y-or-z) line is cut into segments of at least
+ * march_minseg cells so that about march_threads threads run.  Defaults: 151552 (148 SMs x
+ * 1024) and 16.  Limits: march_minseg >= 4, 1024 <= march_threads <= 2^26.  A tuning changes
+ * only the thread partition; results are bit-identical for equal tunings and otherwise differ
+ * in the summation order of the force_rhs block partials.  get_tuning reads the current values.
+ */
+int streams_b200_set_tuning(streams_b200_ctx* ctx, long long march_threads, int march_minseg);
+int streams_b200_get_tuning(streams_b200_ctx* ctx, long long* march_threads, int* march_minseg);
+
+/*
+ * Batched form: many independent contexts (boxes of any size and flow parameters, one device,
+ * one precision each) advanced together.  The per-box step sequences (compute_dt + rk_sync)
+ * are captured once into one CUDA graph whose branches, one per box, run concurrently on the
+ * GPU; each streams_b200_batch_advance replays it.  No counterpart in the reference (one box
+ * per MPI rank there).
+ *
+ *   steps_per_graph  time steps per graph replay (>= 1)
+ *   dt_every         dt is recomputed at batch steps s with s % dt_every == 0 (contexts with
+ *                    cfl < 0 keep their fixed dt); must divide steps_per_graph
+ *
+ * batch_advance(b, nsteps) advances every box by exactly nsteps steps: a box that has not
+ * completed a step since its last upload/init_run first takes one ordinary step (the graph
+ * holds the steady step sequence), then whole graph replays, then the remainder as ordinary
+ * steps.  It is asynchronous; streams_b200_batch_synchronize waits for all boxes.  Results
+ * are bit-identical to advancing each context alone with streams_b200_advance(ctx, n, dt_every,
+ * s0, 0) under the same tuning.  Contexts must outlive the batch and must not be profiled
+ * (profile_enable) while in a batch.  Work issued on a box's own stream between batch calls
+ * (uploads, direct advance, downloads) is ordered with the replays; a re-tuned box makes the
+ * next advance capture the graph again, and streams_b200_batch_invalidate forces that.
+ */
+typedef struct streams_b200_batch streams_b200_batch;
+int streams_b200_batch_create(streams_b200_ctx** ctxs, int n, int steps_per_graph, int dt_every,
+                              streams_b200_batch** out);
+int streams_b200_batch_advance(streams_b200_batch* b, int nsteps);
+int streams_b200_batch_synchronize(streams_b200_batch* b);
+int streams_b200_batch_invalidate(streams_b200_batch* b);
+/* Graph replays issued and kernel launches they contain (instrumentation). */
+int streams_b200_batch_stats(streams_b200_batch* b, long long* replays, long long* launches_per_replay);
+const char* streams_b200_batch_last_error(streams_b200_batch* b);
+int streams_b200_batch_destroy(streams_b200_batch* b);
+
+/*
  * CFL time step over caller-owned device arrays, allocating nothing.
  *
  * No counterpart in the reference: STREAmS-2's compute_dt always runs on the solver's own

@@ -132,6 +132,8 @@ void fill_geom(streams_b200_ctx* c) {
   g.volchan = p.volchan;
   g.t_bulk_target = p.t_bulk_target;
   g.precision = p.precision;
+  g.march_threads = 148LL * 1024;
+  g.march_minseg = 16;
 }
 
 }  // namespace
@@ -517,6 +519,252 @@ int streams_b200_synchronize(streams_b200_ctx* c) {
   cudaSetDevice(c->device);
   SB_CHECK(c, cudaStreamSynchronize(c->stream));
   SB_CHECK(c, cudaGetLastError());
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_set_tuning(streams_b200_ctx* c, long long march_threads, int march_minseg) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  if (march_minseg < MARCH_MINSEG_MIN || march_minseg > (1 << 20))
+    return set_err(c, STREAMS_B200_EINVAL, "march_minseg must be in [4, 2^20]");
+  if (march_threads < 1024 || march_threads > (1LL << 26))
+    return set_err(c, STREAMS_B200_EINVAL, "march_threads must be in [1024, 2^26]");
+  c->g.march_threads = march_threads;
+  c->g.march_minseg = march_minseg;
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_get_tuning(streams_b200_ctx* c, long long* march_threads, int* march_minseg) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  if (march_threads) *march_threads = c->g.march_threads;
+  if (march_minseg) *march_minseg = c->g.march_minseg;
+  return STREAMS_B200_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Batched form: one CUDA graph holding every box's step sequence as a parallel branch.
+
+struct streams_b200_batch {
+  std::vector<streams_b200_ctx*> ctxs;
+  std::vector<long long> launches_per_replay;  // per box
+  std::vector<long long> tuned_threads;        // per box tuning the graph was captured with
+  std::vector<int> tuned_minseg;
+  int steps_per_graph = 1, dt_every = 1;
+  long long step = 0;  // batch steps taken (drives the dt recompute pattern)
+  long long replays = 0;
+  int device = 0;
+  cudaStream_t master = nullptr;
+  cudaEvent_t ev_master = nullptr;
+  std::vector<cudaEvent_t> ev_box;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int batch_err(streams_b200_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg; else g_global_err = msg;
+  return code;
+}
+
+#define SB_BCHECK(b, call)                                                                                   \
+  do {                                                                                                       \
+    cudaError_t e_ = (call);                                                                                 \
+    if (e_ != cudaSuccess) return batch_err((b), STREAMS_B200_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// A context is in the steady state when its host flags are those that every completed step
+// leaves behind; the captured step sequence is valid from (and returns to) that state.
+bool steady(const streams_b200_ctx* c) {
+  return c->have_stats && !c->aux_current && c->shift_pending == (c->g.force_var != 0);
+}
+
+// One step of one box, as streams_b200_advance issues it, with the batch's dt pattern.
+int box_step(streams_b200_ctx* c, long long step, int dt_every) {
+  if (c->p.cfl > 0 && step % dt_every == 0) {
+    int rc = do_compute_dt(c);
+    if (rc) return rc;
+  }
+  return do_rk_sync(c, true);
+}
+
+void drop_graph(streams_b200_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+int capture(streams_b200_batch* b) {
+  drop_graph(b);
+  SB_BCHECK(b, cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+  int rc = STREAMS_B200_OK;
+  std::string why;
+  cudaError_t e = cudaEventRecord(b->ev_master, b->master);
+  for (size_t i = 0; i < b->ctxs.size() && e == cudaSuccess && rc == STREAMS_B200_OK; ++i) {
+    streams_b200_ctx* c = b->ctxs[i];
+    const long long l0 = c->launches;
+    e = cudaStreamWaitEvent(c->stream, b->ev_master, 0);
+    for (int s = 0; s < b->steps_per_graph && e == cudaSuccess && rc == STREAMS_B200_OK; ++s) {
+      rc = box_step(c, s, b->dt_every);
+      if (rc) why = "box " + std::to_string(i) + ": " + c->err;
+    }
+    if (e == cudaSuccess && rc == STREAMS_B200_OK) e = cudaEventRecord(b->ev_box[i], c->stream);
+    if (e == cudaSuccess && rc == STREAMS_B200_OK) e = cudaStreamWaitEvent(b->master, b->ev_box[i], 0);
+    b->launches_per_replay[i] = c->launches - l0;
+    c->launches = l0;
+    b->tuned_threads[i] = c->g.march_threads;
+    b->tuned_minseg[i] = c->g.march_minseg;
+  }
+  cudaGraph_t gr = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(b->master, &gr);
+  if (e != cudaSuccess || rc != STREAMS_B200_OK || e2 != cudaSuccess) {
+    if (gr) cudaGraphDestroy(gr);
+    cudaGetLastError();
+    if (rc) return batch_err(b, rc, "capture: " + why);
+    return batch_err(b, STREAMS_B200_ECUDA,
+                     std::string("capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  b->graph = gr;
+  SB_BCHECK(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return STREAMS_B200_OK;
+}
+
+// eager steps of every box on its own stream
+int eager_steps(streams_b200_batch* b, int n) {
+  for (int s = 0; s < n; ++s) {
+    for (size_t i = 0; i < b->ctxs.size(); ++i) {
+      int rc = box_step(b->ctxs[i], b->step, b->dt_every);
+      if (rc) return batch_err(b, rc, "box " + std::to_string(i) + ": " + b->ctxs[i]->err);
+    }
+    ++b->step;
+  }
+  return STREAMS_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int streams_b200_batch_create(streams_b200_ctx** ctxs, int n, int steps_per_graph, int dt_every,
+                              streams_b200_batch** out) {
+  if (!ctxs || !out || n < 1) return batch_err(nullptr, STREAMS_B200_EINVAL, "batch needs at least one context");
+  *out = nullptr;
+  if (steps_per_graph < 1 || dt_every < 1 || steps_per_graph % dt_every != 0)
+    return batch_err(nullptr, STREAMS_B200_EINVAL, "steps_per_graph must be a positive multiple of dt_every");
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i]) return batch_err(nullptr, STREAMS_B200_EINVAL, "null context in batch");
+    if (ctxs[i]->device != ctxs[0]->device)
+      return batch_err(nullptr, STREAMS_B200_EINVAL, "all contexts of a batch must be on one device");
+    for (int k = 0; k < i; ++k)
+      if (ctxs[k] == ctxs[i]) return batch_err(nullptr, STREAMS_B200_EINVAL, "context listed twice in batch");
+  }
+  auto* b = new streams_b200_batch();
+  b->ctxs.assign(ctxs, ctxs + n);
+  b->launches_per_replay.assign(n, 0);
+  b->tuned_threads.assign(n, 0);
+  b->tuned_minseg.assign(n, 0);
+  b->ev_box.assign(n, nullptr);
+  b->steps_per_graph = steps_per_graph;
+  b->dt_every = dt_every;
+  b->device = ctxs[0]->device;
+  cudaSetDevice(b->device);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_master, cudaEventDisableTiming);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&b->ev_box[i], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    std::string m = std::string("batch set-up: ") + cudaGetErrorString(e);
+    streams_b200_batch_destroy(b);
+    return batch_err(nullptr, STREAMS_B200_ECUDA, m);
+  }
+  *out = b;
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_batch_advance(streams_b200_batch* b, int nsteps) {
+  if (!b) return batch_err(b, STREAMS_B200_EINVAL, "null batch");
+  if (nsteps < 0) return batch_err(b, STREAMS_B200_EINVAL, "negative step count");
+  cudaSetDevice(b->device);
+  for (auto* c : b->ctxs)
+    if (c->prof.on) return batch_err(b, STREAMS_B200_EINVAL, "a profiled context cannot run in a batch");
+  bool all_steady = true;
+  for (auto* c : b->ctxs) all_steady = all_steady && steady(c);
+  if (!all_steady && nsteps > 0) {
+    drop_graph(b);
+    int rc = eager_steps(b, 1);
+    if (rc) return rc;
+    --nsteps;
+  }
+  // graph replays start on a step of the dt pattern's period (steps_per_graph is a multiple)
+  int lead = 0;
+  if (b->step % b->dt_every != 0) lead = (int)(b->dt_every - b->step % b->dt_every);
+  if (lead > nsteps) lead = nsteps;
+  int rc = eager_steps(b, lead);
+  if (rc) return rc;
+  nsteps -= lead;
+  const int nrep = nsteps / b->steps_per_graph;
+  if (nrep > 0) {
+    for (size_t i = 0; i < b->ctxs.size() && b->exec; ++i)
+      if (b->ctxs[i]->g.march_threads != b->tuned_threads[i] || b->ctxs[i]->g.march_minseg != b->tuned_minseg[i])
+        drop_graph(b);  // a box was re-tuned since the capture
+    if (!b->exec) {
+      rc = capture(b);
+      if (rc) return rc;
+    }
+    for (size_t i = 0; i < b->ctxs.size(); ++i) {
+      SB_BCHECK(b, cudaEventRecord(b->ev_box[i], b->ctxs[i]->stream));
+      SB_BCHECK(b, cudaStreamWaitEvent(b->master, b->ev_box[i], 0));
+    }
+    for (int r = 0; r < nrep; ++r) SB_BCHECK(b, cudaGraphLaunch(b->exec, b->master));
+    SB_BCHECK(b, cudaEventRecord(b->ev_master, b->master));
+    for (size_t i = 0; i < b->ctxs.size(); ++i) {
+      SB_BCHECK(b, cudaStreamWaitEvent(b->ctxs[i]->stream, b->ev_master, 0));
+      b->ctxs[i]->launches += b->launches_per_replay[i] * nrep;
+    }
+    b->replays += nrep;
+    b->step += (long long)nrep * b->steps_per_graph;
+  }
+  return eager_steps(b, nsteps - nrep * b->steps_per_graph);
+}
+
+int streams_b200_batch_synchronize(streams_b200_batch* b) {
+  if (!b) return batch_err(b, STREAMS_B200_EINVAL, "null batch");
+  cudaSetDevice(b->device);
+  SB_BCHECK(b, cudaStreamSynchronize(b->master));
+  for (auto* c : b->ctxs) SB_BCHECK(b, cudaStreamSynchronize(c->stream));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_batch_invalidate(streams_b200_batch* b) {
+  if (!b) return batch_err(b, STREAMS_B200_EINVAL, "null batch");
+  cudaSetDevice(b->device);
+  drop_graph(b);
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_batch_stats(streams_b200_batch* b, long long* replays, long long* launches_per_replay) {
+  if (!b) return batch_err(b, STREAMS_B200_EINVAL, "null batch");
+  long long t = 0;
+  for (long long v : b->launches_per_replay) t += v;
+  if (replays) *replays = b->replays;
+  if (launches_per_replay) *launches_per_replay = t;
+  return STREAMS_B200_OK;
+}
+
+const char* streams_b200_batch_last_error(streams_b200_batch* b) { return b ? b->err.c_str() : ""; }
+
+int streams_b200_batch_destroy(streams_b200_batch* b) {
+  if (!b) return STREAMS_B200_OK;
+  cudaSetDevice(b->device);
+  if (b->master) cudaStreamSynchronize(b->master);
+  drop_graph(b);
+  for (auto ev : b->ev_box)
+    if (ev) cudaEventDestroy(ev);
+  if (b->ev_master) cudaEventDestroy(b->ev_master);
+  if (b->master) cudaStreamDestroy(b->master);
+  delete b;
   return STREAMS_B200_OK;
 }
 

@@ -53,7 +53,13 @@ struct Geom {
   double volchan, t_bulk_target;
   // arithmetic of the flux and viscous passes: 0 FP64, 1 mixed (FP32 fluxes, FP64 state)
   int precision;
+  // launch shape of the y/z march passes (host side only): the lines are cut into segments so
+  // that about march_threads threads run, each segment at least march_minseg cells long
+  long long march_threads;
+  int march_minseg;
 };
+// smallest march segment length a context may be tuned to (sizes the reduction scratch)
+constexpr int MARCH_MINSEG_MIN = 4;
 
 __host__ __device__ __forceinline__ long long gidx(const Geom& g, int i, int j, int k) {
   return ((long long)(k + g.ng - 1) * g.sy + (j + g.ng - 1)) * g.sx + (i + g.ng - 1);

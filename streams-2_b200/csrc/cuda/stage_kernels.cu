@@ -888,14 +888,14 @@ void Prof::reset() {
 
 // Segments of a march pass: enough threads to fill the device, segments of at least 16 cells
 // (one redundant face per segment).
-static void march_split(const Geom& g, int dir, int* seglen, int* nseg, long long* nthreads) {
+static void march_split_with(const Geom& g, int dir, long long target, int minseg, int* seglen, int* nseg,
+                             long long* nthreads) {
   const int emin = dir == 1 ? g.eul_jmin : g.eul_kmin, emax = dir == 1 ? g.eul_jmax : g.eul_kmax;
   const int ncell = emax - emin + 1;
   const long long lines = (long long)g.nx * (dir == 1 ? g.nz : g.ny);
-  const long long target = 148LL * 1024;
   long long ns = (target + lines - 1) / lines;
   int sl = (int)((ncell + ns - 1) / ns);
-  if (sl < 16) sl = 16;
+  if (sl < minseg) sl = minseg;
   if (sl > ncell) sl = ncell;
   if (sl < 1) sl = 1;
   *seglen = sl;
@@ -903,11 +903,16 @@ static void march_split(const Geom& g, int dir, int* seglen, int* nseg, long lon
   *nthreads = lines * *nseg;
 }
 
+static void march_split(const Geom& g, int dir, int* seglen, int* nseg, long long* nthreads) {
+  march_split_with(g, dir, g.march_threads, g.march_minseg, seglen, nseg, nthreads);
+}
+
 long long reduction_slots(const Geom& g) {
   long long a = (long long)nblocks(g.nint, 256) * (NRED_UPD > 9 ? NRED_UPD : 9);
   int sl, ns;
   long long nt;
-  march_split(g, 2, &sl, &ns, &nt);
+  // the largest segment count any tuning can reach: segments of MARCH_MINSEG_MIN cells
+  march_split_with(g, 2, 1LL << 40, MARCH_MINSEG_MIN, &sl, &ns, &nt);
   long long b = (long long)nblocks(nt, MT_NT) * 5;
   return a > b ? a : b;
 }

@@ -3,6 +3,7 @@
 #include "setup.hpp"
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -313,6 +314,41 @@ void set_flow_params(Setup& s, double reynolds_bulk_target) {
   }
 }
 
+// glibc's rand() (the additive feedback generator behind random(), TYPE_3: degree 31,
+// separation 3), restated as a per-call object so that case set-ups running in several threads
+// do not share one global sequence.  Seeding: r0 = seed (1 if 0), r_i = 16807 r_{i-1} mod
+// (2^31 - 1) for i < 31, r_i = r_{i-31} for i = 31..33; then r_i = r_{i-31} + r_{i-3} (mod 2^32)
+// and output k is r_{k+344} >> 1.  crandom.c (code/third-party/crandom/crandom.c:12-29) calls
+// srand/rand, so the draws are those of the reference.
+class GlibcRand {
+ public:
+  explicit GlibcRand(unsigned seed) {
+    int32_t r[34];
+    r[0] = seed == 0 ? 1 : static_cast<int32_t>(seed);
+    for (int i = 1; i < 31; ++i) {
+      const int32_t hi = r[i - 1] / 127773, lo = r[i - 1] % 127773;
+      int32_t word = 16807 * lo - 2836 * hi;
+      if (word < 0) word += 2147483647;
+      r[i] = word;
+    }
+    for (int i = 31; i < 34; ++i) r[i] = r[i - 31];
+    for (int i = 0; i < 34; ++i) ring_[i] = static_cast<uint32_t>(r[i]);
+    pos_ = 34;
+    for (int i = 34; i < 344; ++i) next_raw();
+  }
+  int operator()() { return static_cast<int>(next_raw() >> 1); }
+
+ private:
+  uint32_t next_raw() {
+    const uint32_t v = ring_[(pos_ - 31) % 34] + ring_[(pos_ - 3) % 34];
+    ring_[pos_ % 34] = v;
+    ++pos_;
+    return v;
+  }
+  uint32_t ring_[34];
+  long long pos_;
+};
+
 // init_channel (singleideal.F90:4344-4419) with the per-rank seeding of an MPI run
 void init_channel(Setup& s) {
   const int nxmax = s.nxmax, nymax = s.nymax, nzmax = s.nzmax;
@@ -331,12 +367,12 @@ void init_channel(Setup& s) {
     int cz = rank % s.z_split;
     // init_crandom_f(myrank+1) at initialize (singleideal.F90:315-325); rand_type 0 seeds 0 and rescales by 0
     double rescale = 1.0;
+    unsigned seed = static_cast<unsigned>(rank + 1);
     if (s.rand_type == 0) {
-      std::srand(0);
+      seed = 0;
       rescale = 0.0;
-    } else {
-      std::srand(rank + 1);
     }
+    GlibcRand rnd(seed);
     for (int kl = 1; kl <= nzl; ++kl)
       for (int jl = 1; jl <= nyl; ++jl)
         for (int il = 1; il <= nxl; ++il) {
@@ -347,7 +383,7 @@ void init_channel(Setup& s) {
           double uu = wm2 / rho, vv = 0.0 / rho, ww = 0.0 / rho;
           double rr[3];
           for (int l = 0; l < 3; ++l) {
-            int ir = std::rand();
+            int ir = rnd();
             rr[l] = rescale * static_cast<double>(ir) / RAND_MAX;
             rr[l] = rr[l] - 0.5;
           }
@@ -374,12 +410,12 @@ void init_channel(Setup& s) {
 // plus uniform random perturbations of +-amp*u0 on u, v, w from glibc rand (seed), drawn in
 // k, j, i order, three per cell.
 void init_channel_synthetic(Setup& s, double amp, int seed) {
-  std::srand(seed);
+  GlibcRand rnd(static_cast<unsigned>(seed));
   for (int k = 1; k <= s.nzmax; ++k)
     for (int j = 1; j <= s.nymax; ++j)
       for (int i = 1; i <= s.nxmax; ++i) {
         double rr[3];
-        for (int l = 0; l < 3; ++l) rr[l] = 2.0 * (static_cast<double>(std::rand()) / RAND_MAX) - 1.0;
+        for (int l = 0; l < 3; ++l) rr[l] = 2.0 * (static_cast<double>(rnd()) / RAND_MAX) - 1.0;
         double rho = s.rho0;
         double yj = s.yg(j) / s.l0;
         double uu = 1.5 * s.u0 * (1.0 - yj * yj) + amp * s.u0 * rr[0];

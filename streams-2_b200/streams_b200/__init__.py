@@ -112,6 +112,15 @@ def _load() -> C.CDLL:
         "streams_b200_case_info": (I, [P, D]),
         "streams_b200_case_write_restart": (I, [P, C.c_char_p]),
         "streams_b200_run_case": (I, [P, I, I, C.c_char_p, D, D]),
+        "streams_b200_set_tuning": (I, [P, LL, I]),
+        "streams_b200_get_tuning": (I, [P, C.POINTER(LL), C.POINTER(I)]),
+        "streams_b200_batch_create": (I, [C.POINTER(P), I, I, I, C.POINTER(P)]),
+        "streams_b200_batch_advance": (I, [P, I]),
+        "streams_b200_batch_synchronize": (I, [P]),
+        "streams_b200_batch_invalidate": (I, [P]),
+        "streams_b200_batch_stats": (I, [P, C.POINTER(LL), C.POINTER(LL)]),
+        "streams_b200_batch_last_error": (C.c_char_p, [P]),
+        "streams_b200_batch_destroy": (I, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -134,7 +143,10 @@ EXPORTED = [
     "streams_b200_profile_enable", "streams_b200_profile_read", "streams_b200_kernel_count",
     "streams_b200_kernel_name", "streams_b200_compute_dt_noalloc", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
     "streams_b200_case_params", "streams_b200_case_grid", "streams_b200_case_field", "streams_b200_case_info",
-    "streams_b200_case_write_restart", "streams_b200_run_case",
+    "streams_b200_case_write_restart", "streams_b200_run_case", "streams_b200_set_tuning",
+    "streams_b200_get_tuning", "streams_b200_batch_create", "streams_b200_batch_advance",
+    "streams_b200_batch_synchronize", "streams_b200_batch_invalidate", "streams_b200_batch_stats",
+    "streams_b200_batch_last_error", "streams_b200_batch_destroy",
 ]
 
 
@@ -342,3 +354,59 @@ class Solver:
     @property
     def launches(self) -> int:
         return int(lib.streams_b200_launch_count(self._h))
+
+    def set_tuning(self, march_threads: int, march_minseg: int) -> None:
+        """Launch shape of the y/z flux passes (see streams_b200_set_tuning)."""
+        self._check(lib.streams_b200_set_tuning(self._h, int(march_threads), int(march_minseg)))
+
+    def get_tuning(self) -> tuple[int, int]:
+        t, m = C.c_longlong(), C.c_int()
+        self._check(lib.streams_b200_get_tuning(self._h, C.byref(t), C.byref(m)))
+        return int(t.value), int(m.value)
+
+
+class Batch:
+    """Many independent solvers advanced together through one CUDA graph per replay.
+
+    Every solver keeps its own fields, stream and flow parameters; the graph holds each box's
+    step sequence as a parallel branch, so small boxes share the GPU instead of running one
+    after another.  Results equal advancing each solver alone with the same tuning.
+    """
+
+    def __init__(self, solvers, steps_per_graph: int = 10, dt_every: int = 1):
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s._h for s in self.solvers])
+        h = C.c_void_p()
+        rc = lib.streams_b200_batch_create(arr, len(self.solvers), steps_per_graph, dt_every, C.byref(h))
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_global_error().decode())
+        self._h = h
+        self.steps_per_graph = steps_per_graph
+
+    def _check(self, rc: int):
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_batch_last_error(self._h).decode())
+
+    def advance(self, nsteps: int) -> None:
+        """Advance every box by nsteps (asynchronous)."""
+        self._check(lib.streams_b200_batch_advance(self._h, int(nsteps)))
+
+    def synchronize(self) -> None:
+        self._check(lib.streams_b200_batch_synchronize(self._h))
+
+    def invalidate(self) -> None:
+        self._check(lib.streams_b200_batch_invalidate(self._h))
+
+    def stats(self) -> tuple[int, int]:
+        """(graph replays so far, kernel launches per replay)."""
+        r, n = C.c_longlong(), C.c_longlong()
+        self._check(lib.streams_b200_batch_stats(self._h, C.byref(r), C.byref(n)))
+        return int(r.value), int(n.value)
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib.streams_b200_batch_destroy(h)
+            self._h = None
+
+    __del__ = close

@@ -1,0 +1,151 @@
+"""Seeded synthetic channel cases in the solver's own input-file syntax.
+
+The same builder serves the tests, the benchmark and the batched / served forms: a channel of
+any size and flow parameters, with the seeded Poiseuille + uniform-noise initial field of the
+benchmark channel, and the random case mixes of the batched and served workloads.
+"""
+from __future__ import annotations
+
+import math
+import random
+
+
+def channel_ini(nx=32, ny=24, nz=16, *, lx=6.283185307179586, ly=2.0, lz=3.141592653589793, mach=1.5,
+                re_bulk=3000.0, theta_wall=0.0, visc_model=1, vt_exp=0.76, sensor=0.05, ep_order=6,
+                weno_scheme=3, weno_version=0, nkeep=0, amp=0.1, seed=1, y_stretch=1.5, cfl=0.8,
+                num_iter=100, print_control=1, correct_bound_ord=1, reynolds_tau=None) -> str:
+    """Input file of a seeded synthetic channel case (the shape of the benchmark channel).
+
+    A [synthetic] section selects the seeded Poiseuille + uniform-noise initial field and the
+    tanh-stretched staggered y grid; the rest is the solver's own singleideal.ini syntax.
+    """
+    syn = [f"kind = channel_poiseuille", f"amp = {amp!r}", f"seed = {seed}", f"y_stretch = {y_stretch!r}"]
+    if reynolds_tau is None:
+        syn.append(f"reynolds_bulk = {re_bulk!r}")
+    return f"""[grid]
+grid_dim = 1
+domain_size_x = {lx!r}
+domain_size_y = {ly!r}
+domain_size_z = {lz!r}
+nxmax = {nx}
+nymax = {ny}
+nzmax = {nz}
+ng = 3
+metrics_order = {ep_order}
+grid_type = 3
+dyptarget = 0.7
+jbgrid = 32
+ysmoosteps = 50
+
+[bc]
+xmin = 0
+xmax = 0
+ymin = 6
+ymax = 6
+zmin = 0
+zmax = 0
+xmin_nr = 0
+xmax_nr = 0
+ymin_nr = 0
+ymax_nr = 0
+zmin_nr = 0
+zmax_nr = 0
+correct_bound_ord = {correct_bound_ord}
+
+[mpi]
+x_split = 1
+y_split = 1
+z_split = 1
+
+[controls]
+restart_type = 0
+cfl = {cfl!r}
+iter_dt_recompute = 1
+num_iter = {num_iter}
+
+[numerics]
+ep_order = {ep_order}
+nkeep = {nkeep}
+visc_order = {ep_order}
+conservative_viscous = 1
+weno_scheme = {weno_scheme}
+weno_version = {weno_version}
+flux_splitting = 0
+sensor_threshold = {sensor!r}
+rk_type = 1
+rand_type = 1
+
+[flow]
+flow_init = 0
+Mach = {mach!r}
+Reynolds = {reynolds_tau if reynolds_tau is not None else 150.0!r}
+theta_wall = {theta_wall!r}
+xshock_imp = 0.
+shock_angle = 0.
+T_ref = 220.
+aoa = 0.
+
+[fluid]
+gam = 1.4
+Prandtl = 0.72
+visc_model = {visc_model}
+vt_exp = {vt_exp!r}
+s_suth = 110.4
+calorically_perfect = 1
+
+[output]
+print_control = {print_control}
+dtsave_restart = 50.
+dtsave = 50.
+dtstat = 50.
+dtslice = 50.
+igslice = 0
+jgslice = 0
+kgslice = 0
+enable_plot3d = 0
+enable_vtk = 0
+
+[synthetic]
+{chr(10).join(syn)}
+"""
+
+
+# grid choices of the batched workload (48 boxes)
+BATCH_NX = (64, 96, 128)
+BATCH_NY = (64, 96)
+BATCH_NZ = (32, 64, 96)
+
+
+def batch_mix(nboxes: int = 48, seed: int = 2024) -> list[dict]:
+    """The batched workload: per box a grid drawn from {64,96,128} x {64,96} x {32,64,96},
+    bulk Mach uniform in [0.3, 2.0], bulk Reynolds uniform in [2000, 6000], and the benchmark
+    channel's initial field (its own noise seed)."""
+    rng = random.Random(seed)
+    out = []
+    for b in range(nboxes):
+        out.append(dict(nx=rng.choice(BATCH_NX), ny=rng.choice(BATCH_NY), nz=rng.choice(BATCH_NZ),
+                        mach=round(rng.uniform(0.3, 2.0), 6), re_bulk=round(rng.uniform(2000.0, 6000.0), 3),
+                        seed=b + 1))
+    return out
+
+
+def serve_mix(nreq: int, rate_per_s: float, seed: int = 7, cells_min: int = 48 ** 3,
+              cells_max: int = 384 * 192 * 128, steps=(200, 2000), mixed_fraction: float = 0.5) -> list[dict]:
+    """A Poisson stream of channel solve requests: arrival offsets with exponential gaps at
+    rate_per_s, grids log-uniform in cell count between cells_min and cells_max (aspect
+    2:1:1 rounded to multiples of 16), bulk Mach uniform in [0.5, 2.5], step counts uniform in
+    `steps`, and FP64 or mixed precision."""
+    rng = random.Random(seed)
+    t = 0.0
+    out = []
+    for r in range(nreq):
+        t += rng.expovariate(rate_per_s)
+        cells = math.exp(rng.uniform(math.log(cells_min), math.log(cells_max)))
+        base = (cells / 4.0) ** (1.0 / 3.0)
+        nx = max(32, int(round(2 * base / 16)) * 16)
+        ny = max(32, int(round(base / 16)) * 16)
+        nz = max(32, int(round(base / 16)) * 16)
+        out.append(dict(rid=r, arrival=t, nx=nx, ny=ny, nz=nz, mach=round(rng.uniform(0.5, 2.5), 6),
+                        nsteps=rng.randint(*steps), precision=1 if rng.random() < mixed_fraction else 0,
+                        seed=r + 1))
+    return out
