@@ -177,9 +177,18 @@ def run_serving(torch, duration_s, step_scale, single_rate, tune_cache):
     from streams_b200.serve import Server
     lo, hi = max(2, int(200 * step_scale)), max(3, int(2000 * step_scale))
     mean_cells = (384 * 192 * 128 - 48 ** 3) / np.log((384 * 192 * 128) / 48 ** 3)
-    mean_work = mean_cells * (lo + hi) / 2
-    rate = 1.1 * single_rate * 1e6 / mean_work
-    reqs = [r for r in serve_mix(int(rate * duration_s * 1.5) + 4, rate, steps=(lo, hi)) if r["arrival"] <= duration_s]
+    # offered load: 1.25x what one large box sustains, from the drawn requests' own work
+    rate = 1.25 * single_rate * 1e6 / (mean_cells * (lo + hi) / 2)
+    reqs = serve_mix(int(rate * duration_s * 2) + 8, 1.0, steps=(lo, hi))
+    work, k = 0.0, 0
+    while k < len(reqs) and work < 1.25 * single_rate * 1e6 * duration_s:
+        work += reqs[k]["nx"] * reqs[k]["ny"] * reqs[k]["nz"] * reqs[k]["nsteps"]
+        k += 1
+    reqs = reqs[:k]
+    scale = duration_s / reqs[-1]["arrival"]
+    for r in reqs:
+        r["arrival"] *= scale
+    rate = len(reqs) / duration_s
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(150e9, free - 8e9))
     srv = Server(budget_bytes=budget, tick_steps=10, tune_cache=tune_cache)
@@ -188,7 +197,9 @@ def run_serving(torch, duration_s, step_scale, single_rate, tune_cache):
             "rate_per_s": rate, "arrival_window_s": duration_s, "steps_range": [lo, hi],
             "p50_s": out["p50_s"], "p99_s": out["p99_s"], "mean_s": out["mean_s"],
             "mcell_steps_per_s": out["mcell_steps_per_s"], "mcell_steps_per_busy_s": out["mcell_steps_per_busy_s"],
-            "max_resident": out["max_resident"], "ticks": out["ticks"], "budget_gb": budget / 1e9}
+            "max_resident": out["max_resident"], "ticks": out["ticks"], "budget_gb": budget / 1e9,
+            "offered_mcell_steps_per_s": work / duration_s / 1e6, "host_admit_s": out["admit_s"],
+            "host_batch_build_s": out["batch_build_s"]}
 
 
 def cpu_oracle_rate(nx, ny, nz, nsteps, budget_s=20.0):

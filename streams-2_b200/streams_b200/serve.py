@@ -6,10 +6,10 @@ threads, so that set-up overlaps the GPU work), then admitted in arrival order a
 device footprint fits the HBM budget next to the solves already resident.  A resident solve
 keeps its fields in HBM from admission to completion.  The loop advances all resident solves
 together in ticks: one ``Batch`` (one CUDA graph with a branch per solve) runs a few steps of
-every solve, so the stages of different solves share launches and overlap on the GPU; solves
-join at the next tick after admission and leave (freeing their memory) at the tick in which
-they complete.  Completion latency is measured from a request's arrival to the end of the tick
-that completes it.
+every solve, so the stages of different solves share launches and overlap on the GPU.  Solves
+are admitted while a tick runs (their first step overlaps it), join the next tick, and leave,
+freeing their memory, at the end of the tick in which they complete.  Completion latency is
+measured from a request's arrival to the end of the tick that completes it.
 
 A solve's arithmetic does not depend on what else is resident: with the same launch tuning its
 result is bit-identical alone and in any mix.
@@ -97,6 +97,7 @@ class Server:
         nxt = 0
         batch, members = None, ()
         busy = 0.0
+        host = {"admit_s": 0.0, "batch_build_s": 0.0}
         try:
             while nxt < len(reqs) or futures or waiting or active:
                 # arrivals: start host set-up of every request whose arrival time has come
@@ -118,7 +119,25 @@ class Server:
                         else:
                             waiting.append(s)
                 waiting.sort(key=lambda s: s.arrival)
-                # admission by footprint, first come first served
+                # issue one tick of every resident solve through one shared graph (asynchronous)
+                n = 0
+                if active:
+                    key = tuple(s.rid for s in active)
+                    if key != members:
+                        tc = now()
+                        if batch is not None:
+                            batch.close()
+                        batch = Batch([s.solver for s in active], steps_per_graph=self.tick_steps, dt_every=1)
+                        members = key
+                        host["batch_build_s"] += now() - tc
+                    n = tick_length([s.remaining for s in active], self.tick_steps)
+                    ta = now()
+                    batch.advance(n)
+                # admission by footprint, first come first served, while the tick runs; the
+                # solves admitted now take their first step on their own streams and join the
+                # next tick (memory of solves finishing in this tick is released after it)
+                tadm = now()
+                joining = []
                 for _ in range(admit_fifo([w.footprint for w in waiting], used, self.budget)):
                     s = waiting.pop(0)
                     if self.tune:
@@ -132,44 +151,37 @@ class Server:
                     s.remaining = s.nsteps - 1
                     s.admitted = now()
                     used += s.footprint
-                    active.append(s)
+                    joining.append(s)
+                host["admit_s"] += now() - tadm
+                if n:
+                    batch.synchronize()
+                    tb = now()
+                    busy += tb - ta
+                    self.log.append((ta, tb, len(active), n))
+                    still = []
+                    for s in active:
+                        s.remaining -= n
+                        if s.remaining > 0:
+                            still.append(s)
+                        else:
+                            used -= self._finish(s, tb, done)
+                    if len(still) != len(active):
+                        batch.close()
+                        batch, members = None, ()
+                    active = still
                 # a one-step solve is complete after its first step
-                for s in [s for s in active if s.remaining <= 0]:
-                    s.solver.synchronize()
-                    used -= self._finish(s, now(), done)
-                    active.remove(s)
-                if not active:
+                for s in joining:
+                    if s.remaining <= 0:
+                        s.solver.synchronize()
+                        used -= self._finish(s, now(), done)
+                    else:
+                        active.append(s)
+                if not active and not joining:
                     # idle until the next arrival or finished set-up
                     if futures:
                         cf.wait(list(futures.values()), timeout=0.05, return_when=cf.FIRST_COMPLETED)
                     elif nxt < len(reqs):
                         time.sleep(max(0.0, min(0.05, reqs[nxt]["arrival"] * time_scale - now())))
-                    continue
-                # one tick of every resident solve through one shared graph
-                key = tuple(s.rid for s in active)
-                if key != members:
-                    if batch is not None:
-                        batch.close()
-                    batch = Batch([s.solver for s in active], steps_per_graph=self.tick_steps, dt_every=1)
-                    members = key
-                n = tick_length([s.remaining for s in active], self.tick_steps)
-                ta = now()
-                batch.advance(n)
-                batch.synchronize()
-                tb = now()
-                busy += tb - ta
-                self.log.append((ta, tb, len(active), n))
-                still = []
-                for s in active:
-                    s.remaining -= n
-                    if s.remaining > 0:
-                        still.append(s)
-                    else:
-                        used -= self._finish(s, tb, done)
-                if len(still) != len(active):
-                    batch.close()
-                    batch, members = None, ()
-                active = still
         finally:
             if batch is not None:
                 batch.close()
@@ -177,7 +189,9 @@ class Server:
                 if s.solver is not None:
                     s.solver.close()
             pool.shutdown(wait=True)
-        return summarize(done, rejected, busy, self.log)
+        out = summarize(done, rejected, busy, self.log)
+        out.update(host)
+        return out
 
 
     def _finish(self, s: Solve, t: float, done: list) -> int:

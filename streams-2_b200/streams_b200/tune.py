@@ -8,9 +8,12 @@ each candidate on a scratch copy of the box (its own context, so the solve being
 advanced) with the library's CUDA-event profiler and keeps the fastest; results are cached
 per (grid, precision, scheme).  A tuning changes only the thread partition: boxes with equal
 tunings give bit-identical results, different tunings differ in the summation order of the
-bulk-forcing block partials.
+bulk-forcing block partials.  Boxes of one tuning class (sizes within a factor sqrt(2) of the
+same powers of two) share a tuning.
 """
 from __future__ import annotations
+
+import math
 
 from . import Solver
 
@@ -22,7 +25,10 @@ _cache: dict[tuple, tuple[int, int]] = {}
 
 
 def key_of(params) -> tuple:
-    return (params.nx, params.ny, params.nz, params.precision, params.ep_order, params.weno_scheme,
+    """Tuning class of a box: grid sizes rounded to the nearest power of two (the launch shape
+    depends on the line counts and lengths, not on their exact values), precision and scheme."""
+    b = lambda n: int(round(math.log2(max(n, 1))))
+    return (b(params.nx), b(params.ny), b(params.nz), params.precision, params.ep_order, params.weno_scheme,
             params.nkeep, params.weno_version)
 
 
