@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define STREAMS_B200_ABI_VERSION 1
+#define STREAMS_B200_ABI_VERSION 2
 
 /* error codes */
 #define STREAMS_B200_OK 0
@@ -96,6 +96,12 @@ typedef struct streams_b200_grid {
   const int* ep_ord_x;      /* ep_ord_change(i,*,*,1), i = 0..nx */
   const int* ep_ord_y;      /* ep_ord_change(*,j,*,2), j = 0..ny */
   const int* ep_ord_z;      /* ep_ord_change(*,*,k,3), k = 0..nz */
+  /* second-derivative data of the non-conservative viscous form (conservative_viscous = 0;
+   * may be NULL otherwise): compute_metrics (code/src/grid.F90:71-141) and get_deriv_coeffs */
+  const double* dcsidx2;    /* dcsidx2(1:nx) */
+  const double* detady2;    /* detady2(1:ny) */
+  const double* dzitdz2;    /* dzitdz2(1:nz) */
+  const double* coeff_deriv2; /* coeff_deriv2(0:4,1:4), Fortran order (l fastest) */
 } streams_b200_grid;
 
 typedef struct streams_b200_ctx streams_b200_ctx;

@@ -813,6 +813,131 @@ void Solver::visflx_div_ord2() {
   });
 }
 
+// visflx_nosensor_subroutine (kernels_cpu.F90:3996-4180): non-conservative viscous form
+// (conservative_viscous = 0, calorically perfect gas)
+void Solver::visflx_nosensor() {
+  const int lmax = s.visc_order / 2;
+  const double prandtl = s.prandtl, cploc = s.cp_coeff[0];
+  const double* c1 = s.coeff_deriv1[lmax - 1];
+  const double* c2 = s.coeff_deriv2[lmax - 1];
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const double uu = A(i, j, k, 2), vv = A(i, j, k, 3), ww = A(i, j, k, 4), tt = A(i, j, k, 6),
+                     mu = A(i, j, k, 7);
+        double ux = 0, vx = 0, wx = 0, tx = 0, mux = 0;
+        double uy = 0, vy = 0, wy = 0, ty = 0, muy = 0;
+        double uz = 0, vz = 0, wz = 0, tz = 0, muz = 0;
+        double ulapx = c2[0] * uu, ulapy = ulapx, ulapz = ulapx;
+        double vlapx = c2[0] * vv, vlapy = vlapx, vlapz = vlapx;
+        double wlapx = c2[0] * ww, wlapy = wlapx, wlapz = wlapx;
+        double tlapx = c2[0] * tt, tlapy = tlapx, tlapz = tlapx;
+        for (int l = 1; l <= lmax; ++l) {
+          const double ccl = c1[l - 1], clapl = c2[l];
+          ux = ux + ccl * (A(i + l, j, k, 2) - A(i - l, j, k, 2));
+          ulapx = ulapx + clapl * (A(i + l, j, k, 2) + A(i - l, j, k, 2));
+          vx = vx + ccl * (A(i + l, j, k, 3) - A(i - l, j, k, 3));
+          vlapx = vlapx + clapl * (A(i + l, j, k, 3) + A(i - l, j, k, 3));
+          wx = wx + ccl * (A(i + l, j, k, 4) - A(i - l, j, k, 4));
+          wlapx = wlapx + clapl * (A(i + l, j, k, 4) + A(i - l, j, k, 4));
+          tx = tx + ccl * (A(i + l, j, k, 6) - A(i - l, j, k, 6));
+          tlapx = tlapx + clapl * (A(i + l, j, k, 6) + A(i - l, j, k, 6));
+          mux = mux + ccl * (A(i + l, j, k, 7) - A(i - l, j, k, 7));
+        }
+        for (int l = 1; l <= lmax; ++l) {
+          const double ccl = c1[l - 1], clapl = c2[l];
+          uy = uy + ccl * (A(i, j + l, k, 2) - A(i, j - l, k, 2));
+          ulapy = ulapy + clapl * (A(i, j + l, k, 2) + A(i, j - l, k, 2));
+          vy = vy + ccl * (A(i, j + l, k, 3) - A(i, j - l, k, 3));
+          vlapy = vlapy + clapl * (A(i, j + l, k, 3) + A(i, j - l, k, 3));
+          wy = wy + ccl * (A(i, j + l, k, 4) - A(i, j - l, k, 4));
+          wlapy = wlapy + clapl * (A(i, j + l, k, 4) + A(i, j - l, k, 4));
+          ty = ty + ccl * (A(i, j + l, k, 6) - A(i, j - l, k, 6));
+          tlapy = tlapy + clapl * (A(i, j + l, k, 6) + A(i, j - l, k, 6));
+          muy = muy + ccl * (A(i, j + l, k, 7) - A(i, j - l, k, 7));
+        }
+        for (int l = 1; l <= lmax; ++l) {
+          const double ccl = c1[l - 1], clapl = c2[l];
+          uz = uz + ccl * (A(i, j, k + l, 2) - A(i, j, k - l, 2));
+          ulapz = ulapz + clapl * (A(i, j, k + l, 2) + A(i, j, k - l, 2));
+          vz = vz + ccl * (A(i, j, k + l, 3) - A(i, j, k - l, 3));
+          vlapz = vlapz + clapl * (A(i, j, k + l, 3) + A(i, j, k - l, 3));
+          wz = wz + ccl * (A(i, j, k + l, 4) - A(i, j, k - l, 4));
+          wlapz = wlapz + clapl * (A(i, j, k + l, 4) + A(i, j, k - l, 4));
+          tz = tz + ccl * (A(i, j, k + l, 6) - A(i, j, k - l, 6));
+          tlapz = tlapz + clapl * (A(i, j, k + l, 6) + A(i, j, k - l, 6));
+          muz = muz + ccl * (A(i, j, k + l, 7) - A(i, j, k - l, 7));
+        }
+        const double dx = s.dcsidx[i - 1], dy = s.detady[j - 1], dz = s.dzitdz[k - 1];
+        ux = ux * dx; vx = vx * dx; wx = wx * dx; tx = tx * dx; mux = mux * dx;
+        uy = uy * dy; vy = vy * dy; wy = wy * dy; ty = ty * dy; muy = muy * dy;
+        uz = uz * dz; vz = vz * dz; wz = wz * dz; tz = tz * dz; muz = muz * dz;
+        const double sx2 = s.dcsidxs[i - 1], sy2 = s.detadys[j - 1], sz2 = s.dzitdzs[k - 1];
+        const double x2 = s.dcsidx2[i - 1], y2 = s.detady2[j - 1], z2 = s.dzitdz2[k - 1];
+        ulapx = ulapx * sx2 + ux * x2; vlapx = vlapx * sx2 + vx * x2;
+        wlapx = wlapx * sx2 + wx * x2; tlapx = tlapx * sx2 + tx * x2;
+        ulapy = ulapy * sy2 + uy * y2; vlapy = vlapy * sy2 + vy * y2;
+        wlapy = wlapy * sy2 + wy * y2; tlapy = tlapy * sy2 + ty * y2;
+        ulapz = ulapz * sz2 + uz * z2; vlapz = vlapz * sz2 + vz * z2;
+        wlapz = wlapz * sz2 + wz * z2; tlapz = tlapz * sz2 + tz * z2;
+        const double ulap = ulapx + ulapy + ulapz, vlap = vlapx + vlapy + vlapz;
+        const double wlap = wlapx + wlapy + wlapz, tlap = tlapx + tlapy + tlapz;
+        const double div = ux + vy + wz;
+        const double div3l = div / 3.0;
+        A(i, j, k, 10) = div3l;
+        const double omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
+        const double omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
+        A(i, j, k, 9) = std::sqrt(omod2);
+        const double sig11 = 2.0 * (ux - div3l), sig12 = uy + vx, sig13 = uz + wx;
+        const double sig22 = 2.0 * (vy - div3l), sig23 = vz + wy, sig33 = 2.0 * (wz - div3l);
+        const double sigx = mux * sig11 + muy * sig12 + muz * sig13 + mu * ulap;
+        const double sigy = mux * sig12 + muy * sig22 + muz * sig23 + mu * vlap;
+        const double sigz = mux * sig13 + muy * sig23 + muz * sig33 + mu * wlap;
+        const double sigqt = (mux * tx + muy * ty + muz * tz + mu * tlap) * cploc / prandtl;
+        const double sigah = (sig11 * ux + sig12 * uy + sig13 * uz + sig12 * vx + sig22 * vy + sig23 * vz +
+                              sig13 * wx + sig23 * wy + sig33 * wz) * mu;
+        const double sigq = sigx * uu + sigy * vv + sigz * ww + sigah + sigqt;
+        FL(i, j, k, 2) = FL(i, j, k, 2) - sigx;
+        FL(i, j, k, 3) = FL(i, j, k, 3) - sigy;
+        FL(i, j, k, 4) = FL(i, j, k, 4) - sigz;
+        FL(i, j, k, 5) = FL(i, j, k, 5) - sigq;
+        if (j == 1) {
+          wallprop[(0 * sz + k + ng - 1) * sx + i + ng - 1] = mu * uy;
+          wallprop[(1 * sz + k + ng - 1) * sx + i + ng - 1] = mu * wy;
+          wallprop[(2 * sz + k + ng - 1) * sx + i + ng - 1] = mu * ty * cploc / prandtl;
+        }
+      }
+  });
+}
+
+// visflx_div_subroutine (kernels_cpu.F90:3484-3532)
+void Solver::visflx_div() {
+  const int lmax = s.visc_order / 2;
+  const double* c1 = s.coeff_deriv1[lmax - 1];
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const double uu = A(i, j, k, 2), vv = A(i, j, k, 3), ww = A(i, j, k, 4), mu = A(i, j, k, 7);
+        double divx3l = 0, divy3l = 0, divz3l = 0;
+        for (int l = 1; l <= lmax; ++l) {
+          const double ccl = c1[l - 1];
+          divx3l = divx3l + ccl * (A(i + l, j, k, 10) - A(i - l, j, k, 10));
+          divy3l = divy3l + ccl * (A(i, j + l, k, 10) - A(i, j - l, k, 10));
+          divz3l = divz3l + ccl * (A(i, j, k + l, 10) - A(i, j, k - l, 10));
+        }
+        divx3l = divx3l * s.dcsidx[i - 1];
+        divy3l = divy3l * s.detady[j - 1];
+        divz3l = divz3l * s.dzitdz[k - 1];
+        const double sigx = mu * divx3l, sigy = mu * divy3l, sigz = mu * divz3l;
+        const double sigq = sigx * uu + sigy * vv + sigz * ww;
+        FL(i, j, k, 2) = FL(i, j, k, 2) - sigx;
+        FL(i, j, k, 3) = FL(i, j, k, 3) - sigy;
+        FL(i, j, k, 4) = FL(i, j, k, 4) - sigz;
+        FL(i, j, k, 5) = FL(i, j, k, 5) - sigq;
+      }
+  });
+}
+
 // force_rhs (singleideal_cpu.F90:845-889) with force_rhs_1/2 (kernels_cpu.F90:3157-3193, 3092-3116).
 // The oracle sums each k-plane sequentially and then the planes in k order.
 void Solver::force_rhs() {
@@ -890,7 +1015,7 @@ void Solver::force_var() {
   });
 }
 
-// rk_sync (singleideal_cpu.F90:332-409), conservative_viscous = 1, mode_async = 0
+// rk_sync (singleideal_cpu.F90:332-409), mode_async = 0
 void Solver::rk_sync() {
   if (s.channel_case) dpdx = 0.0;
   for (int istep = 1; istep <= s.nrk; ++istep) {
@@ -904,8 +1029,12 @@ void Solver::rk_sync() {
     bcswap();
     compute_aux(1, 1);
     euler(0);
-    visflx_reduced_ord2(0);
-    visflx_faces();
+    if (s.conservative_viscous == 1) {
+      visflx_reduced_ord2(0);
+      visflx_faces();
+    } else {
+      visflx_nosensor();
+    }
     bcextr_var(10);
     bcswap_var(10);
     euler(1);
@@ -914,7 +1043,10 @@ void Solver::rk_sync() {
       sensor();
       bcswap_var(8);
     }
-    visflx_div_ord2();
+    if (s.conservative_viscous == 1)
+      visflx_div_ord2();
+    else
+      visflx_div();
     // update_flux_subroutine (kernels_cpu.F90:3400-3418)
     for (size_t q = 0; q < fl.size(); ++q) fln[q] = fln[q] - gamdt * fl[q];
     if (s.channel_case) force_rhs();

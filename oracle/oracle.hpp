@@ -86,6 +86,8 @@ class Solver {
   void sensor();
   void bcextr_var(int m);
   void visflx_div_ord2();
+  void visflx_nosensor();
+  void visflx_div();
   void force_rhs();
   void force_var();
   void face_flux(int dir, int i, int j, int k, double fh[5]) const;

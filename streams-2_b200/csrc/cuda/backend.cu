@@ -87,7 +87,7 @@ std::string validate(const streams_b200_params* p) {
   if (p->weno_version != 0 && p->weno_version != 1) return "weno_version must be 0 or 1";
   if (p->weno_version == 1 && p->weno_scheme != 3) return "weno_version 1 requires weno_scheme 3";
   if (p->flux_splitting != 0) return "flux_splitting = 1 (Rusanov) is not implemented on the device path";
-  if (p->conservative_viscous != 1) return "only conservative_viscous = 1 is implemented on the device path";
+  if (p->conservative_viscous != 0 && p->conservative_viscous != 1) return "conservative_viscous must be 0 or 1";
   if (p->calorically_perfect != 1) return "only calorically perfect gas is implemented on the device path";
   if (p->nrk != 3) return "only the Wray RK3 scheme (nrk = 3) is implemented";
   if (p->precision != 0 && p->precision != 1) return "precision must be 0 (FP64) or 1 (mixed)";
@@ -132,6 +132,7 @@ void fill_geom(streams_b200_ctx* c) {
   g.volchan = p.volchan;
   g.t_bulk_target = p.t_bulk_target;
   g.precision = p.precision;
+  g.conservative_viscous = p.conservative_viscous;
   g.march_threads = 148LL * 1024;
   g.march_minseg = 16;
 }
@@ -221,6 +222,23 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
   g.epx = ex; g.epy = ey; g.epz = ez;
   for (int lm = 0; lm < 4; ++lm)
     for (int l = 0; l < 4; ++l) g.coeff[lm][l] = gr->coeff_deriv1 ? gr->coeff_deriv1[lm * 4 + l] : 0.0;
+  if (p->conservative_viscous == 0) {
+    if (!gr->dcsidx2 || !gr->detady2 || !gr->dzitdz2 || !gr->coeff_deriv2) {
+      streams_b200_destroy(c);
+      return set_err(nullptr, STREAMS_B200_EINVAL,
+                     "conservative_viscous = 0 needs dcsidx2, detady2, dzitdz2 and coeff_deriv2 in the grid");
+    }
+    double *s1, *s2, *s3;
+    if ((e = dev_alloc(c, &s1, p->nx)) || (e = dev_alloc(c, &s2, p->ny)) || (e = dev_alloc(c, &s3, p->nz)))
+      return fail(e, "cudaMalloc(grid)");
+    if ((e = cudaMemcpy(s1, gr->dcsidx2, nx * 8, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(s2, gr->detady2, ny * 8, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(s3, gr->dzitdz2, nz * 8, cudaMemcpyHostToDevice)))
+      return fail(e, "cudaMemcpy(grid)");
+    g.dcsidx2 = s1 - 1; g.detady2 = s2 - 1; g.dzitdz2 = s3 - 1;
+    for (int lm = 0; lm < 4; ++lm)
+      for (int l = 0; l < 5; ++l) g.coeff2[lm][l] = gr->coeff_deriv2[lm * 5 + l];
+  }
   // state
   DevState& d = c->d;
   const bool mixed = p->precision == 1;

@@ -35,6 +35,12 @@ struct Geom {
   const int* epy;
   const int* epz;
   double coeff[4][4];     // coeff_deriv1(l, lmax) at [lmax-1][l-1]
+  // non-conservative viscous form (conservative_viscous = 0)
+  int conservative_viscous;
+  const double* dcsidx2;  // [i], i = 1..nx (second-derivative metric terms)
+  const double* detady2;
+  const double* dzitdz2;
+  double coeff2[4][5];    // coeff_deriv2(l, lmax) at [lmax-1][l], l = 0..4
   // boundary handling
   int periodic[3];
   int wall_ymin, wall_ymax;  // staggered isothermal walls

@@ -158,7 +158,8 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
 // Ducros sensor in FP64 from w for the mixed form, so that the central/WENO switch is taken
 // on the same values as in the FP64 form.  mode 0: initial sensor of run() (visflx(mode=2),
 // kernels_cpu.F90:4680-4682); mode 1: sensor_subroutine of stage 3 (:4726-4744), which works
-// from the stored |omega| and div/3.
+// from the stored |omega| and div/3 of visflx_reduced_ord2; mode 2: the same from the
+// visc_order derivatives of visflx_nosensor_subroutine (conservative_viscous = 0).
 __global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restrict__ w, double* __restrict__ out,
                                                   int mode) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
@@ -170,21 +171,41 @@ __global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restri
     const double ri = 1.0 / st[0];
     v[0] = st[1] * ri; v[1] = st[2] * ri; v[2] = st[3] * ri;
   };
-  double xp[3], xm[3], yp[3], ym[3], zp[3], zm[3];
-  vel(i + 1, j, k, xp); vel(i - 1, j, k, xm);
-  vel(i, j + 1, k, yp); vel(i, j - 1, k, ym);
-  vel(i, j, k + 1, zp); vel(i, j, k - 1, zm);
-  double dxl = 1.0 / (g.x[i + 1] - g.x[i - 1]);
-  double dyl = 1.0 / (g.y[j + 1] - g.y[j - 1]);
-  double dzl = 1.0 / (g.z[k + 1] - g.z[k - 1]);
-  double ux = dxl * (xp[0] - xm[0]), vx = dxl * (xp[1] - xm[1]), wx = dxl * (xp[2] - xm[2]);
-  double uy = dyl * (yp[0] - ym[0]), vy = dyl * (yp[1] - ym[1]), wy = dyl * (yp[2] - ym[2]);
-  double uz = dzl * (zp[0] - zm[0]), vz = dzl * (zp[1] - zm[1]), wz = dzl * (zp[2] - zm[2]);
+  double ux, vx, wx, uy, vy, wy, uz, vz, wz;
+  if (mode < 2) {
+    double xp[3], xm[3], yp[3], ym[3], zp[3], zm[3];
+    vel(i + 1, j, k, xp); vel(i - 1, j, k, xm);
+    vel(i, j + 1, k, yp); vel(i, j - 1, k, ym);
+    vel(i, j, k + 1, zp); vel(i, j, k - 1, zm);
+    double dxl = 1.0 / (g.x[i + 1] - g.x[i - 1]);
+    double dyl = 1.0 / (g.y[j + 1] - g.y[j - 1]);
+    double dzl = 1.0 / (g.z[k + 1] - g.z[k - 1]);
+    ux = dxl * (xp[0] - xm[0]); vx = dxl * (xp[1] - xm[1]); wx = dxl * (xp[2] - xm[2]);
+    uy = dyl * (yp[0] - ym[0]); vy = dyl * (yp[1] - ym[1]); wy = dyl * (yp[2] - ym[2]);
+    uz = dzl * (zp[0] - zm[0]); vz = dzl * (zp[1] - zm[1]); wz = dzl * (zp[2] - zm[2]);
+  } else {
+    // the derivatives of visflx_nosensor_subroutine (order visc_order, metric after the sum)
+    const int lv = g.lmax_base;
+    double d[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int l = 1; l <= lv; ++l) {
+      const double ccl = g.coeff[lv - 1][l - 1];
+      double p[3], m[3];
+      vel(i + l, j, k, p); vel(i - l, j, k, m);
+      for (int v = 0; v < 3; ++v) d[0][v] = d[0][v] + ccl * (p[v] - m[v]);
+      vel(i, j + l, k, p); vel(i, j - l, k, m);
+      for (int v = 0; v < 3; ++v) d[1][v] = d[1][v] + ccl * (p[v] - m[v]);
+      vel(i, j, k + l, p); vel(i, j, k - l, m);
+      for (int v = 0; v < 3; ++v) d[2][v] = d[2][v] + ccl * (p[v] - m[v]);
+    }
+    ux = d[0][0] * g.dcsidx[i]; vx = d[0][1] * g.dcsidx[i]; wx = d[0][2] * g.dcsidx[i];
+    uy = d[1][0] * g.detady[j]; vy = d[1][1] * g.detady[j]; wy = d[1][2] * g.detady[j];
+    uz = d[2][0] * g.dzitdz[k]; vz = d[2][1] * g.dzitdz[k]; wz = d[2][2] * g.dzitdz[k];
+  }
   double div = ux + vy + wz;
   double omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
   double omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
   double u0l0 = g.u0 / g.l0;
-  if (mode == 1) {
+  if (mode >= 1) {
     double div3l = div / 3.0;
     double om = sqrt(omod2);
     omod2 = om * om;
@@ -379,12 +400,28 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
           const int j = b, k = c;
           const long long a = gidx(g, i, j, k);
           const R uu = aux[n + a], vv = aux[2 * n + a], ww = aux[3 * n + a], mu = aux[6 * n + a];
-          const R dxl = mu / R(g.x[i + 1] - g.x[i - 1]);
-          const R dyl = mu / R(g.y[j + 1] - g.y[j - 1]);
-          const R dzl = mu / R(g.z[k + 1] - g.z[k - 1]);
-          const R sigx = dxl * (div3_at(g, div3, i + 1, j, k) - div3_at(g, div3, i - 1, j, k));
-          const R sigy = dyl * (div3_at(g, div3, i, j + 1, k) - div3_at(g, div3, i, j - 1, k));
-          const R sigz = dzl * (div3_at(g, div3, i, j, k + 1) - div3_at(g, div3, i, j, k - 1));
+          R sigx, sigy, sigz;
+          if (g.conservative_viscous) {
+            const R dxl = mu / R(g.x[i + 1] - g.x[i - 1]);
+            const R dyl = mu / R(g.y[j + 1] - g.y[j - 1]);
+            const R dzl = mu / R(g.z[k + 1] - g.z[k - 1]);
+            sigx = dxl * (div3_at(g, div3, i + 1, j, k) - div3_at(g, div3, i - 1, j, k));
+            sigy = dyl * (div3_at(g, div3, i, j + 1, k) - div3_at(g, div3, i, j - 1, k));
+            sigz = dzl * (div3_at(g, div3, i, j, k + 1) - div3_at(g, div3, i, j, k - 1));
+          } else {
+            // visflx_div_subroutine (kernels_cpu.F90:3484-3532): order visc_order
+            const int lv = g.lmax_base;
+            R dx3 = R(0), dy3 = R(0), dz3 = R(0);
+            for (int l = 1; l <= lv; ++l) {
+              const R ccl = R(g.coeff[lv - 1][l - 1]);
+              dx3 = dx3 + ccl * (div3_at(g, div3, i + l, j, k) - div3_at(g, div3, i - l, j, k));
+              dy3 = dy3 + ccl * (div3_at(g, div3, i, j + l, k) - div3_at(g, div3, i, j - l, k));
+              dz3 = dz3 + ccl * (div3_at(g, div3, i, j, k + l) - div3_at(g, div3, i, j, k - l));
+            }
+            sigx = mu * (dx3 * R(g.dcsidx[i]));
+            sigy = mu * (dy3 * R(g.detady[j]));
+            sigz = mu * (dz3 * R(g.dzitdz[k]));
+          }
           const R sigq = sigx * uu + sigy * vv + sigz * ww;
           f[1] = f[1] - double(sigx);
           f[2] = f[2] - double(sigy);
@@ -532,6 +569,99 @@ __global__ void __launch_bounds__(256) k_visc(Geom g, const R* __restrict__ aux,
   fl[2 * nI + q] = f3;
   fl[3 * nI + q] = f4;
   fl[4 * nI + q] = f5;
+}
+
+// visflx_nosensor_subroutine (kernels_cpu.F90:3996-4180), the non-conservative viscous form of
+// conservative_viscous = 0: first and second derivatives of u, v, w, T (and first of mu) with the
+// central stencil of order visc_order, the full stress divergence and dissipation, heat flux;
+// div/3 and |omega| for the div term and the stage-3 sensor (sensor_subroutine,
+// kernels_cpu.F90:4726-4744, from |omega| and div/3), wall shear at j = 1.  Arithmetic in R,
+// accumulation into the FP64 register.
+template <class R>
+__global__ void __launch_bounds__(256) k_visc_ns(Geom g, const R* __restrict__ aux, double* __restrict__ fl,
+                                                 R* __restrict__ div3, double* __restrict__ sensor_next,
+                                                 double* __restrict__ wallprop, int do_sensor) {
+  const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (q >= g.nint) return;
+  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+  const long long n = g.nvol, nI = g.nint;
+  const long long c = gidx(g, i, j, k);
+  const long long st[3] = {1, g.sx, (long long)g.sx * g.sy};
+  auto A = [&](long long a, int m) -> R { return __ldg(aux + (m - 1) * n + a); };
+  const int lmax = g.lmax_base;
+  const R uu = A(c, 2), vv = A(c, 3), ww = A(c, 4), tt = A(c, 6), mu = A(c, 7);
+  // d[dir][var]: first derivative of u, v, w, T, mu; lap[dir][var]: second derivative of u, v, w, T
+  R d1[3][5], lap[3][4];
+  const R c20 = R(g.coeff2[lmax - 1][0]);
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) d1[dir][v] = R(0);
+    lap[dir][0] = c20 * uu; lap[dir][1] = c20 * vv; lap[dir][2] = c20 * ww; lap[dir][3] = c20 * tt;
+    for (int l = 1; l <= lmax; ++l) {
+      const R ccl = R(g.coeff[lmax - 1][l - 1]);
+      const R clapl = R(g.coeff2[lmax - 1][l]);
+      const long long ap = c + l * st[dir], am = c - l * st[dir];
+      const int ms[5] = {2, 3, 4, 6, 7};
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const R fp = A(ap, ms[v]), fm = A(am, ms[v]);
+        d1[dir][v] = d1[dir][v] + ccl * (fp - fm);
+        if (v < 4) lap[dir][v] = lap[dir][v] + clapl * (fp + fm);
+      }
+    }
+  }
+  const R m1[3] = {R(g.dcsidx[i]), R(g.detady[j]), R(g.dzitdz[k])};
+  const R ms2[3] = {R(g.dcsidxs[i]), R(g.detadys[j]), R(g.dzitdzs[k])};
+  const R m2[3] = {R(g.dcsidx2[i]), R(g.detady2[j]), R(g.dzitdz2[k])};
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) d1[dir][v] = d1[dir][v] * m1[dir];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) lap[dir][v] = lap[dir][v] * ms2[dir] + d1[dir][v] * m2[dir];
+  }
+  const R ux = d1[0][0], vx = d1[0][1], wx = d1[0][2], tx = d1[0][3], mux = d1[0][4];
+  const R uy = d1[1][0], vy = d1[1][1], wy = d1[1][2], ty = d1[1][3], muy = d1[1][4];
+  const R uz = d1[2][0], vz = d1[2][1], wz = d1[2][2], tz = d1[2][3], muz = d1[2][4];
+  const R ulap = lap[0][0] + lap[1][0] + lap[2][0];
+  const R vlap = lap[0][1] + lap[1][1] + lap[2][1];
+  const R wlap = lap[0][2] + lap[1][2] + lap[2][2];
+  const R tlap = lap[0][3] + lap[1][3] + lap[2][3];
+  const R div = ux + vy + wz;
+  const R div3l = div / R(3);
+  div3[q] = div3l;
+  const R omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
+  const R omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
+  if (do_sensor) {
+    const R om = sqrt(omod2);
+    const R om2 = om * om;
+    const R dv = R(3) * div3l;
+    const R u0l0 = R(g.u0 / g.l0);
+    const R t = fmax(-dv / sqrt(om2 + dv * dv + u0l0 * u0l0), R(0));
+    sensor_next[q] = double(t * t);
+  }
+  const R cploc = R(g.cp0), prandtl = R(g.prandtl);
+  const R sig11 = R(2) * (ux - div3l), sig12 = uy + vx, sig13 = uz + wx;
+  const R sig22 = R(2) * (vy - div3l), sig23 = vz + wy, sig33 = R(2) * (wz - div3l);
+  const R sigx = mux * sig11 + muy * sig12 + muz * sig13 + mu * ulap;
+  const R sigy = mux * sig12 + muy * sig22 + muz * sig23 + mu * vlap;
+  const R sigz = mux * sig13 + muy * sig23 + muz * sig33 + mu * wlap;
+  const R sigqt = (mux * tx + muy * ty + muz * tz + mu * tlap) * cploc / prandtl;
+  const R sigah = (sig11 * ux + sig12 * uy + sig13 * uz + sig12 * vx + sig22 * vy + sig23 * vz + sig13 * wx +
+                   sig23 * wy + sig33 * wz) * mu;
+  const R sigq = sigx * uu + sigy * vv + sigz * ww + sigah + sigqt;
+  fl[nI + q] = fl[nI + q] - double(sigx);
+  fl[2 * nI + q] = fl[2 * nI + q] - double(sigy);
+  fl[3 * nI + q] = fl[3 * nI + q] - double(sigz);
+  fl[4 * nI + q] = fl[4 * nI + q] - double(sigq);
+  if (j == 1) {
+    const long long wp = (long long)(k - 1) * g.nx + (i - 1);
+    const long long nw = (long long)g.nx * g.nz;
+    wallprop[wp] = double(mu * uy);
+    wallprop[nw + wp] = double(mu * wy);
+    wallprop[2 * nw + wp] = double(mu * ty * cploc / prandtl);
+  }
 }
 
 // Initial Ducros sensor of run() (visflx(mode=2), singleideal_cpu.F90:1550-1555):
@@ -1006,12 +1136,18 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   const bool fp64 = sizeof(R) == sizeof(double);
   if (a.run_aux) aux_launch<R>(g, d, a.apply_shift, 0, K_AUX, s, nl);
   SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS><<<xg, xb, 0, s>>>(g, aux, sensor, fl_new));
-  SB_LAUNCH(d, K_VISC, s,
-            k_visc<R><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
-                                                           fp64 && a.istep == 3));
+  if (g.conservative_viscous)
+    SB_LAUNCH(d, K_VISC, s,
+              k_visc<R><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
+                                                             fp64 && a.istep == 3));
+  else
+    SB_LAUNCH(d, K_VISC, s,
+              k_visc_ns<R><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
+                                                                fp64 && a.istep == 3));
   if (!fp64 && a.istep == 3) {
     // the mixed form takes the stage-3 sensor in FP64 from the stage's starting state
-    SB_LAUNCH(d, K_INIT_SENSOR, s, k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, sensor_next, 1));
+    SB_LAUNCH(d, K_INIT_SENSOR, s,
+              k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, sensor_next, g.conservative_viscous ? 1 : 2));
     ++*nl;
   }
   if (gyb > 0)

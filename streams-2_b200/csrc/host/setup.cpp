@@ -644,8 +644,8 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
   s.visc_order = c.get_int("numerics", "visc_order");
   if (s.visc_order != s.ep_order) throw InputError("viscous order must be equal to ep_order");
   s.conservative_viscous = c.get_int("numerics", "conservative_viscous");
-  if (s.conservative_viscous != 1)
-    throw InputError("conservative_viscous = 0 is not supported by the B200 backend");
+  if (s.conservative_viscous != 0 && s.conservative_viscous != 1)
+    throw InputError("conservative_viscous must be 0 or 1");
   for (int i = 0; i < 4; ++i) get_deriv_coeffs(s.coeff_deriv1[i], s.coeff_deriv2[i], 2 * (i + 1), 2 * (i + 1));
   s.sensor_threshold = c.get_double("numerics", "sensor_threshold");
   s.x_split = c.get_int("mpi", "x_split");
@@ -795,6 +795,8 @@ void Setup::fill_grid(streams_b200_grid* g) const {
   g->dcsidxs = dcsidxs.data(); g->detadys = detadys.data(); g->dzitdzs = dzitdzs.data();
   g->coeff_deriv1 = &coeff_deriv1[0][0];
   g->ep_ord_x = ep_ord[0].data(); g->ep_ord_y = ep_ord[1].data(); g->ep_ord_z = ep_ord[2].data();
+  g->dcsidx2 = dcsidx2.data(); g->detady2 = detady2.data(); g->dzitdz2 = dzitdz2.data();
+  g->coeff_deriv2 = &coeff_deriv2[0][0];
 }
 
 void write_restart_inputs(const Setup& s, const std::string& dir) {

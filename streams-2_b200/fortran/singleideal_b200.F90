@@ -73,6 +73,8 @@ contains
       g%dcsidxs = c_loc(f%dcsidxs) ; g%detadys = c_loc(f%detadys) ; g%dzitdzs = c_loc(f%dzitdzs)
       g%coeff_deriv1 = c_loc(eb%coeff_deriv1)
       g%ep_ord_x = c_loc(self%epx) ; g%ep_ord_y = c_loc(self%epy) ; g%ep_ord_z = c_loc(self%epz)
+      g%dcsidx2 = c_loc(f%dcsidx2) ; g%detady2 = c_loc(f%detady2) ; g%dzitdz2 = c_loc(f%dzitdz2)
+      g%coeff_deriv2 = c_loc(eb%coeff_deriv2)
       call self%check(streams_b200_create(p, g, self%ctx), 'create')
       call self%check(streams_b200_copy_from_field(self%ctx, c_loc(f%w)), 'copy_from_field')
       call self%check(streams_b200_set_time(self%ctx, eb%time0), 'set_time')

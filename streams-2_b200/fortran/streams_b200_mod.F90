@@ -36,6 +36,8 @@ module streams_b200_mod
     type(c_ptr) :: dcsidx, detady, dzitdz, dcsidxs, detadys, dzitdzs
     type(c_ptr) :: coeff_deriv1
     type(c_ptr) :: ep_ord_x, ep_ord_y, ep_ord_z
+    type(c_ptr) :: dcsidx2, detady2, dzitdz2
+    type(c_ptr) :: coeff_deriv2
   end type streams_b200_grid
 
   interface

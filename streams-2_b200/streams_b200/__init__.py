@@ -58,7 +58,8 @@ class Grid(C.Structure):
 
     _fields_ = [(n, C.POINTER(C.c_double)) for n in
                 ("x", "y", "z", "yn", "dcsidx", "detady", "dzitdz", "dcsidxs", "detadys", "dzitdzs",
-                 "coeff_deriv1")] + [(n, C.POINTER(C.c_int)) for n in ("ep_ord_x", "ep_ord_y", "ep_ord_z")]
+                 "coeff_deriv1")] + [(n, C.POINTER(C.c_int)) for n in ("ep_ord_x", "ep_ord_y", "ep_ord_z")] + \
+        [(n, C.POINTER(C.c_double)) for n in ("dcsidx2", "detady2", "dzitdz2", "coeff_deriv2")]
 
 
 class BackendError(RuntimeError):

@@ -13,7 +13,8 @@ import random
 def channel_ini(nx=32, ny=24, nz=16, *, lx=6.283185307179586, ly=2.0, lz=3.141592653589793, mach=1.5,
                 re_bulk=3000.0, theta_wall=0.0, visc_model=1, vt_exp=0.76, sensor=0.05, ep_order=6,
                 weno_scheme=3, weno_version=0, nkeep=0, amp=0.1, seed=1, y_stretch=1.5, cfl=0.8,
-                num_iter=100, print_control=1, correct_bound_ord=1, reynolds_tau=None) -> str:
+                num_iter=100, print_control=1, correct_bound_ord=1, reynolds_tau=None,
+                conservative_viscous=1) -> str:
     """Input file of a seeded synthetic channel case (the shape of the benchmark channel).
 
     A [synthetic] section selects the seeded Poiseuille + uniform-noise initial field and the
@@ -67,7 +68,7 @@ num_iter = {num_iter}
 ep_order = {ep_order}
 nkeep = {nkeep}
 visc_order = {ep_order}
-conservative_viscous = 1
+conservative_viscous = {conservative_viscous}
 weno_scheme = {weno_scheme}
 weno_version = {weno_version}
 flux_splitting = 0

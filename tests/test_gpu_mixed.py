@@ -52,6 +52,8 @@ FIXED = [
     ("weno", dict(nx=24, ny=16, nz=12, sensor=-1.0), [1e-5, 1e-5, 2e-5, 2e-5, 1e-5]),
     ("central_sutherland_cold_wall", dict(nx=24, ny=20, nz=12, sensor=1.01, visc_model=2, theta_wall=-2.5,
                                           mach=0.5), [1e-5] * 5),
+    ("central_nonconservative_viscous", dict(nx=32, ny=24, nz=16, sensor=1.01, conservative_viscous=0),
+     [1e-5] * 5),
 ]
 
 

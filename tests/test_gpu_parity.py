@@ -45,6 +45,10 @@ CASES = {
     "order4_weno2": dict(nx=24, ny=16, nz=12, ep_order=4, weno_scheme=2),
     "ragged": dict(nx=37, ny=13, nz=11),
     "no_order_reduction": dict(nx=24, ny=16, nz=12, correct_bound_ord=0),
+    # conservative_viscous = 0: visflx_nosensor + visflx_div at visc_order, stage-3 sensor from them
+    "nonconservative_viscous": dict(nx=32, ny=24, nz=16, conservative_viscous=0),
+    "nonconservative_viscous_order4": dict(nx=24, ny=20, nz=16, conservative_viscous=0, ep_order=4,
+                                           weno_scheme=2),
 }
 
 
@@ -60,7 +64,7 @@ def test_one_step(name, tmp_path):
         assert abs(sg[k] - so[k]) <= 1e-11 * max(abs(so[k]), 1e-30), (name, k, sg[k], so[k])
 
 
-@pytest.mark.parametrize("name", ["hybrid", "full_weno", "full_central_sutherland"])
+@pytest.mark.parametrize("name", ["hybrid", "full_weno", "full_central_sutherland", "nonconservative_viscous"])
 def test_hundred_steps(name, tmp_path):
     o, s = run_pair(tmp_path, channel_ini(**CASES[name]), 100)
     ng = o.ng
