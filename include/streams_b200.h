@@ -75,6 +75,18 @@ typedef struct streams_b200_params {
   double cfl;               /* >0 CFL number, <0 fixed time step -cfl */
   /* arithmetic of the device path: 0 = FP64, 1 = mixed (FP32 fluxes, FP64 state) */
   int precision;
+  /* open boundaries (boundary layer): characteristic non-reflecting type per face (bctags_nr of
+   * equation_base; 0 none, 1, 2, 3, 6 as bc_nr_lat_x/y_kernel), free-stream state winf, p0 */
+  int bctags_nr[6];
+  double winf[5];
+  double p0;
+  /* recycling-rescaling inflow (bctags[0] = 10, recyc_prepare): station i_recyc, last node
+   * below l0 jbl_inflow, betarecyc, and the crandom sequence the inflow plane is drawn from
+   * (seed and the number of draws the set-up took) */
+  int recyc, i_recyc, jbl_inflow;
+  double betarecyc;
+  unsigned int rng_seed;
+  long long rng_draws;
 } streams_b200_params;
 
 /*
@@ -102,6 +114,15 @@ typedef struct streams_b200_grid {
   const double* detady2;    /* detady2(1:ny) */
   const double* dzitdz2;    /* dzitdz2(1:nz) */
   const double* coeff_deriv2; /* coeff_deriv2(0:4,1:4), Fortran order (l fastest) */
+  /* recycling inflow data of recyc_prepare (recyc = 1 only; may be NULL otherwise) */
+  const double* wmean_inflow; /* wmean(1-i, j, m), i = 1..ng, j = 1..ny, m = 1..4: i fastest */
+  const double* yplus_inflow; /* yplus_inflow(1-ng:ny+ng) */
+  const double* eta_inflow;   /* eta_inflow(1-ng:ny+ng) */
+  const double* yplus_recyc;  /* yplus_recyc(1-ng:ny+ng) */
+  const double* eta_recyc;    /* eta_recyc(1-ng:ny+ng) */
+  const double* weta_inflow;  /* weta_inflow(1:ny) */
+  const int* map_j_inn;       /* map_j_inn(1:ny) */
+  const int* map_j_out;       /* map_j_out(1:ny) */
 } streams_b200_grid;
 
 typedef struct streams_b200_ctx streams_b200_ctx;

@@ -248,6 +248,9 @@ Solver::Solver(const Setup& setup) : s(setup) {
   wallprop.assign(static_cast<size_t>(sx) * sz * 3, 0.0);
   time = s.time0;
   icyc = s.icyc0;
+  random_plane.assign(static_cast<size_t>(ny) * nz * 3, 0.5);  // recyc_prepare's neutral plane
+  rng = streams_b200::GlibcRand(s.rng_seed);
+  rng.discard(s.rng_draws);
 }
 
 // base_cpu%bcswap (code/src/base_cpu.F90:1326-1435) on one block: face halos of periodic directions
@@ -306,37 +309,212 @@ void Solver::bcswap_var(int m) {
         }
 }
 
-// update_ghost (singleideal_cpu.F90:1064-1138) with bcwall_staggered (kernels_cpu.F90:6612-6678)
+// update_ghost (singleideal_cpu.F90:1064-1138): the faces in the order ilat = 1..6
 void Solver::update_ghost(int do_swap) {
-  const double twall = s.t_wall, t0 = s.t0, rgas0 = s.rgas0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
-  for (int ilat = 3; ilat <= 4; ++ilat) {
-    if (s.bctags[ilat - 1] != 6) continue;
-    par_for(1, nz, [&](int k) {
-      for (int l = 1; l <= ng; ++l)
-        for (int i = 1; i <= nx; ++i) {
-          const int js = (ilat == 3) ? l : ny + 1 - l;
-          const int jg = (ilat == 3) ? 1 - l : ny + l;
-          double rho = W(i, js, k, 0);
-          double uu = W(i, js, k, 1) / rho;
-          double vv = W(i, js, k, 2) / rho;
-          double ww = W(i, js, k, 3) / rho;
-          double rhoe = W(i, js, k, 4);
-          double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-          double ee = rhoe / rho - qq;
-          double tt = t0 + (ee - cvl * t0) / cv0;
-          double pp = rho * tt * rgas0;
-          tt = 2.0 * twall - tt;
-          ee = (cvl + cv0 * (tt / t0 - 1.0)) * t0;
-          rho = pp / tt / rgas0;
-          W(i, jg, k, 0) = rho;
-          W(i, jg, k, 1) = -rho * uu;
-          W(i, jg, k, 2) = -rho * vv;
-          W(i, jg, k, 3) = -rho * ww;
-          W(i, jg, k, 4) = rho * (ee + qq);
-        }
-    });
+  for (int ilat = 1; ilat <= 6; ++ilat) {
+    switch (s.bctags[ilat - 1]) {
+      case 2: bcextr(ilat); break;
+      case 6: if (s.is_y_staggered) bcwall_staggered(ilat); else bcwall(ilat); break;
+      case 10: if (ilat == 1) bcrecyc(); break;
+      default: break;
+    }
   }
   if (do_swap == 1) bcswap();
+}
+
+// bcwall_staggered_subroutine (kernels_cpu.F90:6612-6678)
+void Solver::bcwall_staggered(int ilat) {
+  if (ilat != 3 && ilat != 4) return;
+  const double twall = s.t_wall, t0 = s.t0, rgas0 = s.rgas0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
+  par_for(1, nz, [&](int k) {
+    for (int l = 1; l <= ng; ++l)
+      for (int i = 1; i <= nx; ++i) {
+        const int js = (ilat == 3) ? l : ny + 1 - l;
+        const int jg = (ilat == 3) ? 1 - l : ny + l;
+        double rho = W(i, js, k, 0);
+        double uu = W(i, js, k, 1) / rho;
+        double vv = W(i, js, k, 2) / rho;
+        double ww = W(i, js, k, 3) / rho;
+        double rhoe = W(i, js, k, 4);
+        double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        double ee = rhoe / rho - qq;
+        double tt = t0 + (ee - cvl * t0) / cv0;
+        double pp = rho * tt * rgas0;
+        tt = 2.0 * twall - tt;
+        ee = (cvl + cv0 * (tt / t0 - 1.0)) * t0;
+        rho = pp / tt / rgas0;
+        W(i, jg, k, 0) = rho;
+        W(i, jg, k, 1) = -rho * uu;
+        W(i, jg, k, 2) = -rho * vv;
+        W(i, jg, k, 3) = -rho * ww;
+        W(i, jg, k, 4) = rho * (ee + qq);
+      }
+  });
+}
+
+// bcwall_subroutine (kernels_cpu.F90:6478-6525): wall node j = 1 at rest and at T_wall, ghosts
+// mirrored about it (T_g = 2 T_w - T, p_g = p, velocity reversed); ymin only, as the reference
+void Solver::bcwall(int ilat) {
+  if (ilat != 3) return;
+  const double twall = s.t_wall, t0 = s.t0, rgas0 = s.rgas0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
+  par_for(1, nz, [&](int k) {
+    for (int i = 1; i <= nx; ++i) {
+      W(i, 1, k, 1) = 0.0;
+      W(i, 1, k, 2) = 0.0;
+      W(i, 1, k, 3) = 0.0;
+      double ee = (cvl + cv0 * (twall / t0 - 1.0)) * t0;
+      W(i, 1, k, 4) = W(i, 1, k, 0) * ee;
+      for (int l = 1; l <= ng; ++l) {
+        double rho = W(i, 1 + l, k, 0);
+        double uu = W(i, 1 + l, k, 1) / rho;
+        double vv = W(i, 1 + l, k, 2) / rho;
+        double ww = W(i, 1 + l, k, 3) / rho;
+        double rhoe = W(i, 1 + l, k, 4);
+        double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        ee = rhoe / rho - qq;
+        double tt = t0 + (ee - cvl * t0) / cv0;
+        double pp = rho * tt * rgas0;
+        tt = 2.0 * twall - tt;
+        ee = (cvl + cv0 * (tt / t0 - 1.0)) * t0;
+        rho = pp / tt / rgas0;
+        W(i, 1 - l, k, 0) = rho;
+        W(i, 1 - l, k, 1) = -rho * uu;
+        W(i, 1 - l, k, 2) = -rho * vv;
+        W(i, 1 - l, k, 3) = -rho * ww;
+        W(i, 1 - l, k, 4) = rho * (ee + qq);
+      }
+    }
+  });
+}
+
+// bcextr_subroutine (kernels_cpu.F90:6323-6390): zeroth-order extrapolation of all variables
+void Solver::bcextr(int ilat) {
+  for (int m = 0; m < 5; ++m) {
+    if (ilat == 1 || ilat == 2) {
+      const int is = ilat == 1 ? 1 : nx;
+      for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+          for (int l = 1; l <= ng; ++l) W(ilat == 1 ? 1 - l : nx + l, j, k, m) = W(is, j, k, m);
+    } else if (ilat == 3 || ilat == 4) {
+      const int js = ilat == 3 ? 1 : ny;
+      for (int k = 1; k <= nz; ++k)
+        for (int i = 1; i <= nx; ++i)
+          for (int l = 1; l <= ng; ++l) W(i, ilat == 3 ? 1 - l : ny + l, k, m) = W(i, js, k, m);
+    } else {
+      const int ks = ilat == 5 ? 1 : nz;
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i)
+          for (int l = 1; l <= ng; ++l) W(i, j, ilat == 5 ? 1 - l : nz + l, m) = W(i, j, ks, m);
+    }
+  }
+}
+
+// recyc_exchange (singleideal_cpu.F90:935-999) on one block: the plane i_recyc+1-i, i = 1..ng,
+// shifted in z by nzmax/2 (recyc_exchange_subroutine_1..3, kernels_cpu.F90:5003-5060), then
+// bcrecyc_subroutine_1..3 (:5810-5947): spanwise means, fluctuations, rescaled inflow ghosts.
+void Solver::bcrecyc() {
+  const int kshift = s.nzmax / 2;
+  const int ir = s.i_recyc;
+  const size_t pl = static_cast<size_t>(ng) * ny * nz;
+  std::vector<double> wr(pl * 5);
+  auto WR = [&](int i, int j, int k, int m) -> double& {
+    return wr[(static_cast<size_t>(m - 1) * nz + (k - 1)) * ny * ng + static_cast<size_t>(j - 1) * ng + (i - 1)];
+  };
+  for (int k = 1; k <= nz; ++k) {
+    const int ks = ((k - kshift - 1) % nz + nz) % nz + 1;
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= ng; ++i)
+        for (int m = 1; m <= 5; ++m) WR(i, j, k, m) = W(ir + 1 - i, j, ks, m - 1);
+  }
+  std::vector<double> av(static_cast<size_t>(ng) * ny * 5);
+  auto AV = [&](int i, int j, int m) -> double& { return av[(static_cast<size_t>(m - 1) * ny + (j - 1)) * ng + (i - 1)]; };
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= ng; ++i)
+      for (int m = 1; m <= 5; ++m) {
+        double a = 0.0;
+        for (int k = 1; k <= nz; ++k) a = a + WR(i, j, k, m);
+        AV(i, j, m) = a;
+      }
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= ng; ++i) {
+      const double ufav = AV(i, j, 2) / AV(i, j, 1);
+      const double vfav = AV(i, j, 3) / AV(i, j, 1);
+      const double wfav = AV(i, j, 4) / AV(i, j, 1);
+      const double rhom = AV(i, j, 1) / s.nzmax;
+      for (int k = 1; k <= nz; ++k) {
+        WR(i, j, k, 2) = WR(i, j, k, 2) / WR(i, j, k, 1) - ufav;
+        WR(i, j, k, 3) = WR(i, j, k, 3) / WR(i, j, k, 1) - vfav;
+        WR(i, j, k, 4) = WR(i, j, k, 4) / WR(i, j, k, 1) - wfav;
+        WR(i, j, k, 1) = WR(i, j, k, 1) - rhom;
+      }
+    }
+  const double p0 = s.p0, rgas0 = s.rgas0, betarecyc = s.betarecyc;
+  double u0_02 = 0.02 * s.u0;
+  if (s.rand_type == 0) u0_02 = 0.0;
+  auto yo = [&](const std::vector<double>& v, int j) { return v[static_cast<size_t>(j + ng - 1)]; };
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const double eta = yo(s.eta_inflow, j);
+      const double etamin = std::min(eta, 1.0);
+      const double weta = s.weta_inflow[j - 1];
+      const double weta1 = 1.0 - weta;
+      const double bdamp = 0.5 * (1.0 - std::tanh(4.0 * (yo(s.eta_inflow, j) - 2.0)));
+      const int j_inn = s.map_j_inn[j - 1], j_out = s.map_j_out[j - 1];
+      const double disty_inn = (yo(s.yplus_inflow, j) - yo(s.yplus_recyc, j_inn)) /
+                               (yo(s.yplus_recyc, j_inn + 1) - yo(s.yplus_recyc, j_inn));
+      const double disty_out = (yo(s.eta_inflow, j) - yo(s.eta_recyc, j_out)) /
+                               (yo(s.eta_recyc, j_out + 1) - yo(s.eta_recyc, j_out));
+      for (int i = 1; i <= ng; ++i) {
+        auto WMI = [&](int m) { return s.wmean_inflow[(static_cast<size_t>(m - 1) * ny + (j - 1)) * ng + (i - 1)]; };
+        const double rhomean = WMI(1);
+        const double uumean = WMI(2) / rhomean, vvmean = WMI(3) / rhomean, wwmean = WMI(4) / rhomean;
+        double rhofluc, ufluc, vfluc, wfluc;
+        if (j == 1 || j_inn >= ny || j_out >= ny) {
+          rhofluc = ufluc = vfluc = wfluc = 0.0;
+        } else {
+          auto mix = [&](int m, int jj, double d) { return WR(i, jj, k, m) * (1.0 - d) + WR(i, jj + 1, k, m) * d; };
+          const double rhof_inn = mix(1, j_inn, disty_inn), rhof_out = mix(1, j_out, disty_out);
+          const double uf_inn = mix(2, j_inn, disty_inn), uf_out = mix(2, j_out, disty_out);
+          const double vf_inn = mix(3, j_inn, disty_inn), vf_out = mix(3, j_out, disty_out);
+          const double wf_inn = mix(4, j_inn, disty_inn), wf_out = mix(4, j_out, disty_out);
+          rhofluc = rhof_inn * weta1 + rhof_out * weta;
+          ufluc = uf_inn * weta1 + uf_out * weta;
+          vfluc = vf_inn * weta1 + vf_out * weta;
+          wfluc = wf_inn * weta1 + wf_out * weta;
+          rhofluc = rhofluc * bdamp;
+          ufluc = ufluc * bdamp * betarecyc;
+          vfluc = vfluc * bdamp * betarecyc;
+          wfluc = wfluc * bdamp * betarecyc;
+          auto RP = [&](int c) { return random_plane[(static_cast<size_t>(c - 1) * nz + (k - 1)) * ny + (j - 1)]; };
+          ufluc = ufluc + u0_02 * (RP(1) - 0.5) * etamin;
+          vfluc = vfluc + u0_02 * (RP(2) - 0.5) * etamin;
+          wfluc = wfluc + u0_02 * (RP(3) - 0.5) * etamin;
+        }
+        rhofluc = std::max(-0.75 * rhomean, rhofluc);
+        rhofluc = std::min(4.0 * rhomean, rhofluc);
+        const double rho = rhomean + rhofluc;
+        const double tt = p0 / rho / rgas0;
+        const double uu = uumean + ufluc, vv = vvmean + vfluc, ww = wwmean + wfluc;
+        const double rhou = rho * uu, rhov = rho * vv, rhow = rho * ww;
+        const double ee = (s.cv_coeff[1] + s.cv_coeff[0] * (tt / s.t0 - 1.0)) * s.t0;
+        W(1 - i, j, k, 0) = rho;
+        W(1 - i, j, k, 1) = rhou;
+        W(1 - i, j, k, 2) = rhov;
+        W(1 - i, j, k, 3) = rhow;
+        W(1 - i, j, k, 4) = rho * ee + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;
+      }
+    }
+}
+
+// euler_z's draw of the recycling plane (singleideal_cpu.F90:841): get_crandom_f on
+// inflow_random_plane(2:jbl_inflow, 1:nz, 1:3), first index outermost (crandom_f.F90:81-93)
+void Solver::draw_random_plane() {
+  const double rescale = s.rng_seed == 0 ? 0.0 : 1.0;
+  for (int j = 2; j <= s.jbl_inflow; ++j)
+    for (int k = 1; k <= nz; ++k)
+      for (int c = 1; c <= 3; ++c)
+        random_plane[(static_cast<size_t>(c - 1) * nz + (k - 1)) * ny + (j - 1)] =
+            rescale * static_cast<double>(rng()) / RAND_MAX;
 }
 
 // eval_aux_subroutine (kernels_cpu.F90:6960-7011), calorically perfect gas
@@ -910,6 +1088,42 @@ void Solver::visflx_nosensor() {
   });
 }
 
+// The Ducros sensor that visflx_subroutine (kernels_cpu.F90:3598-3777) stores at run()'s start for
+// conservative_viscous = 0 (its flux contribution is discarded by zero_flux): visc_order
+// derivatives, theta from div and omega directly.
+void Solver::sensor_visc_order() {
+  const int lmax = s.visc_order / 2;
+  const double* c1 = s.coeff_deriv1[lmax - 1];
+  const double u0 = s.u0, l0 = s.l0;
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double ux = 0, vx = 0, wx = 0, uy = 0, vy = 0, wy = 0, uz = 0, vz = 0, wz = 0;
+        for (int l = 1; l <= lmax; ++l) {
+          const double ccl = c1[l - 1];
+          ux = ux + ccl * (A(i + l, j, k, 2) - A(i - l, j, k, 2));
+          vx = vx + ccl * (A(i + l, j, k, 3) - A(i - l, j, k, 3));
+          wx = wx + ccl * (A(i + l, j, k, 4) - A(i - l, j, k, 4));
+          uy = uy + ccl * (A(i, j + l, k, 2) - A(i, j - l, k, 2));
+          vy = vy + ccl * (A(i, j + l, k, 3) - A(i, j - l, k, 3));
+          wy = wy + ccl * (A(i, j + l, k, 4) - A(i, j - l, k, 4));
+          uz = uz + ccl * (A(i, j, k + l, 2) - A(i, j, k - l, 2));
+          vz = vz + ccl * (A(i, j, k + l, 3) - A(i, j, k - l, 3));
+          wz = wz + ccl * (A(i, j, k + l, 4) - A(i, j, k - l, 4));
+        }
+        const double dx = s.dcsidx[i - 1], dy = s.detady[j - 1], dz = s.dzitdz[k - 1];
+        ux = ux * dx; vx = vx * dx; wx = wx * dx;
+        uy = uy * dy; vy = vy * dy; wy = wy * dy;
+        uz = uz * dz; vz = vz * dz; wz = wz * dz;
+        const double div = ux + vy + wz;
+        const double omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
+        const double omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
+        const double t = std::max(-div / std::sqrt(omod2 + div * div + (u0 / l0) * (u0 / l0)), 0.0);
+        A(i, j, k, 8) = t * t;
+      }
+  });
+}
+
 // visflx_div_subroutine (kernels_cpu.F90:3484-3532)
 void Solver::visflx_div() {
   const int lmax = s.visc_order / 2;
@@ -936,6 +1150,114 @@ void Solver::visflx_div() {
         FL(i, j, k, 5) = FL(i, j, k, 5) - sigq;
       }
   });
+}
+
+// bc_nr (singleideal_cpu.F90:1001-1062) with bc_nr_lat_x_kernel / bc_nr_lat_y_kernel
+// (kernels_cpu.F90:5169-5283, 5420-5540): characteristic correction of fl at the boundary
+// points of the faces with a non-reflecting type (1: outgoing waves only; 2: incoming waves from
+// the ghost point; 3: incoming waves towards the free stream; 6: the acoustic reflection of
+// type-6), one-sided second-order normal derivatives of w.
+void Solver::bc_nr() {
+  const double rgas0 = s.rgas0, gamloc = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
+  for (int ilat = 1; ilat <= 4; ++ilat) {
+    const int nr_type = s.bctags_nr[ilat - 1];
+    if (nr_type <= 0) continue;
+    const int dir = (ilat - 1) / 2;            // 0 x, 1 y
+    const int start_or_end = (ilat - 1) % 2 + 1;
+    const int sgn = start_or_end == 1 ? 1 : -1;
+    const int n1 = dir == 0 ? ny : nx;
+    for (int k = 1; k <= nz; ++k)
+      for (int t = 1; t <= n1; ++t) {
+        const int i = dir == 0 ? (start_or_end == 1 ? 1 : nx) : t;
+        const int j = dir == 1 ? (start_or_end == 1 ? 1 : ny) : t;
+        const double c_one[3] = {-1.5, 2.0, -0.5};
+        double dw_dn[5], dw_dn_outer[5];
+        for (int m = 0; m < 5; ++m) {
+          dw_dn[m] = 0.0;
+          for (int l = 1; l <= 3; ++l) {
+            const int o = sgn * (l - 1);
+            dw_dn[m] = dw_dn[m] + sgn * c_one[l - 1] * W(i + (dir == 0 ? o : 0), j + (dir == 1 ? o : 0), k, m);
+          }
+          double w_target = 0.0;
+          if (nr_type == 2) w_target = W(i - (dir == 0 ? sgn : 0), j - (dir == 1 ? sgn : 0), k, m);
+          else if (nr_type == 3) w_target = s.winf[m];
+          dw_dn_outer[m] = sgn * (W(i, j, k, m) - w_target);
+        }
+        const double rho = A(i, j, k, 1), uu = A(i, j, k, 2), vv = A(i, j, k, 3), ww = A(i, j, k, 4);
+        const double h = A(i, j, k, 5), tt = A(i, j, k, 6);
+        const double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        const double cc = gamloc * tt * rgas0;
+        const double c = std::sqrt(cc);
+        const double ci = 1.0 / c;
+        const double p_rho = tt * rgas0;
+        const double p_e = rho * (gamloc - 1.0);
+        const double etot = h - tt * rgas0;
+        const double b3 = etot - rho * p_rho / p_e;
+        const double b2 = p_e / (rho * cc);
+        const double b1 = p_rho / cc - b2 * (etot - 2.0 * qq);
+        // eigenvectors_x / eigenvectors_y (kernels_cpu.F90:2728-2782, 2842-2896): el(var, char), er(char, var)
+        double el[5][5], er[5][5];
+        const double vn = dir == 0 ? uu : vv;
+        const double vt1 = dir == 0 ? vv : uu;  // first tangential velocity (v for x, u for y)
+        const int t1 = dir == 0 ? 2 : 1;        // its conserved slot
+        const int nslot = dir == 0 ? 1 : 2;
+        for (int a = 0; a < 5; ++a)
+          for (int b = 0; b < 5; ++b) el[a][b] = er[a][b] = 0.0;
+        const double vel[3] = {uu, vv, ww};
+        el[0][0] = 0.5 * (b1 + vn * ci);
+        for (int d = 0; d < 3; ++d) el[1 + d][0] = -0.5 * (b2 * vel[d] + (1 + d == nslot ? ci : 0.0));
+        el[4][0] = 0.5 * b2;
+        el[0][1] = 1.0 - b1;
+        for (int d = 0; d < 3; ++d) el[1 + d][1] = b2 * vel[d];
+        el[4][1] = -b2;
+        el[0][2] = -vt1; el[t1][2] = 1.0;
+        el[0][3] = -ww; el[3][3] = 1.0;
+        el[0][4] = 0.5 * (b1 - vn * ci);
+        for (int d = 0; d < 3; ++d) el[1 + d][4] = -0.5 * (b2 * vel[d] - (1 + d == nslot ? ci : 0.0));
+        el[4][4] = 0.5 * b2;
+        er[0][0] = 1.0; er[1][0] = 1.0; er[4][0] = 1.0;
+        for (int d = 0; d < 3; ++d) {
+          er[0][1 + d] = vel[d] - (1 + d == nslot ? c : 0.0);
+          er[1][1 + d] = vel[d];
+          er[4][1 + d] = vel[d] + (1 + d == nslot ? c : 0.0);
+        }
+        er[2][1] = er[2][2] = er[2][3] = 0.0;
+        er[3][1] = er[3][2] = er[3][3] = 0.0;
+        er[2][t1] = 1.0;
+        er[3][3] = 1.0;
+        er[0][4] = h - vn * c;
+        er[1][4] = b3;
+        er[2][4] = vt1;
+        er[3][4] = ww;
+        er[4][4] = h + vn * c;
+        double dwc_dn[5], dwc_dn_outer[5], ev[5];
+        for (int m = 0; m < 5; ++m) {
+          dwc_dn[m] = 0.0;
+          dwc_dn_outer[m] = 0.0;
+          for (int mm = 0; mm < 5; ++mm) {
+            dwc_dn[m] = dwc_dn[m] + el[mm][m] * dw_dn[mm];
+            dwc_dn_outer[m] = dwc_dn_outer[m] + el[mm][m] * dw_dn_outer[mm];
+          }
+        }
+        ev[0] = vn - c; ev[1] = vn; ev[2] = ev[1]; ev[3] = ev[1]; ev[4] = vn + c;
+        if (nr_type == 1)
+          for (int l = 0; l < 5; ++l) ev[l] = start_or_end == 1 ? std::min(ev[l], 0.0) : std::max(ev[l], 0.0);
+        if (nr_type == 2 || nr_type == 3)
+          for (int m = 0; m < 5; ++m)
+            if (sgn * ev[m] > 0.0) dwc_dn[m] = dwc_dn_outer[m];
+        for (int m = 0; m < 5; ++m) dwc_dn[m] = ev[m] * dwc_dn[m];
+        if (nr_type == 6) {
+          dwc_dn[1] = dwc_dn[2] = dwc_dn[3] = 0.0;
+          if (start_or_end == 1) dwc_dn[4] = dwc_dn[0]; else dwc_dn[0] = dwc_dn[4];
+        }
+        const double met = dir == 0 ? s.dcsidx[i - 1] : s.detady[j - 1];
+        for (int m = 0; m < 5; ++m) {
+          double df = 0.0;
+          for (int mm = 0; mm < 5; ++mm) df = df + er[mm][m] * dwc_dn[mm];
+          FL(i, j, k, m + 1) = FL(i, j, k, m + 1) + df * met;
+        }
+      }
+  }
 }
 
 // force_rhs (singleideal_cpu.F90:845-889) with force_rhs_1/2 (kernels_cpu.F90:3157-3193, 3092-3116).
@@ -1039,6 +1361,7 @@ void Solver::rk_sync() {
     bcswap_var(10);
     euler(1);
     euler(2);
+    if (s.recyc) draw_random_plane();
     if (istep == 3) {
       sensor();
       bcswap_var(8);
@@ -1047,6 +1370,7 @@ void Solver::rk_sync() {
       visflx_div_ord2();
     else
       visflx_div();
+    bc_nr();
     // update_flux_subroutine (kernels_cpu.F90:3400-3418)
     for (size_t q = 0; q < fl.size(); ++q) fln[q] = fln[q] - gamdt * fl[q];
     if (s.channel_case) force_rhs();
@@ -1128,7 +1452,10 @@ void Solver::compute_residual() {
 void Solver::init_run() {
   update_ghost(1);
   compute_aux(1, 1);
-  visflx_reduced_ord2(1);
+  if (s.conservative_viscous == 1)
+    visflx_reduced_ord2(1);
+  else
+    sensor_visc_order();
   bcswap_var(8);
   std::fill(fl.begin(), fl.end(), 0.0);
   compute_dt();

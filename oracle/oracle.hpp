@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 
+#include "glibc_rand.hpp"
 #include "setup.hpp"
 
 namespace streams_oracle {
@@ -56,6 +57,10 @@ class Solver {
   double residual_rhou = 0, rhomin = 0, rhomax = 0, tmin = 0, tmax = 0, pmin = 0, pmax = 0;
   int icyc = 0;
   std::vector<ProgressRow> rows;
+  // recycling inflow: the random plane inflow_random_plane(1:ny,1:nz,1:3) and the crandom
+  // sequence it is drawn from (continued from the set-up's draws)
+  std::vector<double> random_plane;
+  streams_b200::GlibcRand rng{1};
 
   size_t gi(int i, int j, int k) const {
     return (static_cast<size_t>(k + ng - 1) * sy + (j + ng - 1)) * sx + (i + ng - 1);
@@ -87,10 +92,17 @@ class Solver {
   void bcextr_var(int m);
   void visflx_div_ord2();
   void visflx_nosensor();
+  void sensor_visc_order();
   void visflx_div();
   void force_rhs();
   void force_var();
   void face_flux(int dir, int i, int j, int k, double fh[5]) const;
+  void bcextr(int ilat);
+  void bcwall(int ilat);
+  void bcwall_staggered(int ilat);
+  void bcrecyc();
+  void draw_random_plane();
+  void bc_nr();
 };
 
 }  // namespace streams_oracle

@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "glibc_rand.hpp"
 #include "kernels.hpp"
 #include "streams_b200.h"
 
@@ -94,11 +95,23 @@ std::string validate(const streams_b200_params* p) {
   if (p->visc_model < 0 || p->visc_model > 2) return "visc_model must be 0, 1 or 2";
   for (int d = 0; d < 3; ++d) {
     const int a = p->bctags[2 * d], b = p->bctags[2 * d + 1];
-    const bool per = (a == 0 && b == 0);
-    if (per) continue;
-    if (d == 1 && a == 6 && b == 6 && p->is_y_staggered) continue;
-    return "boundary tags: only periodic directions and staggered isothermal y walls (6) are implemented";
+    if ((a == 0) != (b == 0)) return "a periodic direction needs tag 0 on both faces";
   }
+  for (int l = 0; l < 6; ++l) {
+    const int t = p->bctags[l];
+    if (t != 0 && t != 2 && t != 6 && t != 10)
+      return "boundary tags: periodic (0), extrapolation (2), isothermal wall (6) and recycling inflow (10)";
+    if (t == 6 && l != 2 && l != 3) return "isothermal walls (6) are implemented on the y faces";
+    if (t == 6 && !p->is_y_staggered && l != 2) return "a node-based wall (6, not staggered) is implemented at ymin";
+    if (t == 10 && l != 0) return "recycling inflow (10) is implemented at xmin";
+    const int nr = p->bctags_nr[l];
+    if (nr != 0 && nr != 1 && nr != 2 && nr != 3 && nr != 6) return "non-reflecting types: 0, 1, 2, 3, 6";
+    if (nr != 0 && l >= 4) return "non-reflecting treatment is implemented on the x and y faces";
+    if (nr != 0 && t == 0) return "a periodic face cannot be non-reflecting";
+  }
+  if (p->bctags[0] == 10 && (p->recyc != 1 || p->i_recyc < p->ng || p->i_recyc > p->nx || p->jbl_inflow < 1 ||
+                             p->jbl_inflow > p->ny || p->bctags[4] != 0))
+    return "recycling inflow needs recyc = 1, ng <= i_recyc <= nx, 1 <= jbl_inflow <= ny and periodic z";
   if (p->channel_case && !(p->volchan > 0)) return "channel forcing needs volchan > 0";
   return "";
 }
@@ -111,8 +124,19 @@ void fill_geom(streams_b200_ctx* c) {
   g.nvol = (long long)g.sx * g.sy * g.sz;
   g.nint = (long long)p.nx * p.ny * p.nz;
   for (int d = 0; d < 3; ++d) g.periodic[d] = (p.bctags[2 * d] == 0 && p.bctags[2 * d + 1] == 0);
-  g.wall_ymin = p.bctags[2] == 6;
-  g.wall_ymax = p.bctags[3] == 6;
+  g.wall_ymin = p.bctags[2] == 6 && p.is_y_staggered;
+  g.wall_ymax = p.bctags[3] == 6 && p.is_y_staggered;
+  for (int l = 0; l < 6; ++l) {
+    g.bctag[l] = p.bctags[l];
+    g.nr[l] = p.bctags_nr[l];
+  }
+  for (int m = 0; m < 5; ++m) g.winf[m] = p.winf[m];
+  g.p0 = p.p0;
+  g.recyc = p.bctags[0] == 10;
+  g.i_recyc = p.i_recyc;
+  g.jbl_inflow = p.jbl_inflow;
+  g.betarecyc = p.betarecyc;
+  g.rand_scale = p.rng_seed == 0 ? 0.0 : 1.0;
   for (int l = 0; l < 6; ++l) g.fzf[l] = p.force_zero_flux[l];
   g.eul_imin = p.eul_imin; g.eul_imax = p.eul_imax; g.eul_jmin = p.eul_jmin;
   g.eul_jmax = p.eul_jmax; g.eul_kmin = p.eul_kmin; g.eul_kmax = p.eul_kmax;
@@ -239,6 +263,30 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
     for (int lm = 0; lm < 4; ++lm)
       for (int l = 0; l < 5; ++l) g.coeff2[lm][l] = gr->coeff_deriv2[lm * 5 + l];
   }
+  if (p->bctags[0] == 10) {
+    if (!gr->wmean_inflow || !gr->yplus_inflow || !gr->eta_inflow || !gr->yplus_recyc || !gr->eta_recyc ||
+        !gr->weta_inflow || !gr->map_j_inn || !gr->map_j_out) {
+      streams_b200_destroy(c);
+      return set_err(nullptr, STREAMS_B200_EINVAL, "recycling inflow needs the recyc_prepare arrays in the grid");
+    }
+    const size_t nyg = ny + g2;
+    double *wm, *yi, *ei, *yr, *er, *we;
+    int *mi, *mo;
+    if ((e = dev_alloc(c, &wm, (size_t)p->ng * ny * 4)) || (e = dev_alloc(c, &yi, nyg)) ||
+        (e = dev_alloc(c, &ei, nyg)) || (e = dev_alloc(c, &yr, nyg)) || (e = dev_alloc(c, &er, nyg)) ||
+        (e = dev_alloc(c, &we, ny)) || (e = dev_alloc(c, &mi, ny)) || (e = dev_alloc(c, &mo, ny)))
+      return fail(e, "cudaMalloc(inflow)");
+    struct Cp2 { void* d; const void* h; size_t b; } ins[] = {
+        {wm, gr->wmean_inflow, (size_t)p->ng * ny * 4 * 8}, {yi, gr->yplus_inflow, nyg * 8},
+        {ei, gr->eta_inflow, nyg * 8}, {yr, gr->yplus_recyc, nyg * 8}, {er, gr->eta_recyc, nyg * 8},
+        {we, gr->weta_inflow, ny * 8}, {mi, gr->map_j_inn, ny * 4}, {mo, gr->map_j_out, ny * 4}};
+    for (auto& cp : ins)
+      if ((e = cudaMemcpy(cp.d, cp.h, cp.b, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e, "cudaMemcpy(inflow)");
+    g.wmean_inflow = wm;
+    g.yplus_inflow = yi + (ng - 1); g.eta_inflow = ei + (ng - 1);
+    g.yplus_recyc = yr + (ng - 1); g.eta_recyc = er + (ng - 1);
+    g.weta_inflow = we - 1; g.map_j_inn = mi - 1; g.map_j_out = mo - 1;
+  }
   // state
   DevState& d = c->d;
   const bool mixed = p->precision == 1;
@@ -255,6 +303,21 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
       (e = dev_alloc(c, &c->fl_b, g.nint * 5)) || (e = dev_alloc(c, &d.wallprop, (size_t)p->nx * p->nz * 3)) ||
       (e = dev_alloc(c, &d.sc, 1)))
     return fail(e, "cudaMalloc(state)");
+  if (g.recyc) {
+    const size_t npl = (size_t)p->ny * p->nz * 3;
+    if ((e = dev_alloc(c, &d.rplane, npl)) || (e = dev_alloc(c, &d.recyc_av, (size_t)p->ng * p->ny * 5)) ||
+        (e = dev_alloc(c, &d.rng, 1)))
+      return fail(e, "cudaMalloc(inflow state)");
+    std::vector<double> half(npl, 0.5);  // recyc_prepare's neutral plane
+    streams_b200::GlibcRand r(p->rng_seed);
+    r.discard(p->rng_draws);
+    RngState hs;
+    for (int q = 0; q < 34; ++q) hs.ring[q] = r.ring()[q];
+    hs.pos = r.position();
+    if ((e = cudaMemcpy(d.rplane, half.data(), npl * 8, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(d.rng, &hs, sizeof(RngState), cudaMemcpyHostToDevice)))
+      return fail(e, "cudaMemcpy(inflow state)");
+  }
   d.red_capacity = reduction_slots(g);
   if ((e = dev_alloc(c, &d.red, d.red_capacity))) return fail(e, "cudaMalloc(reductions)");
   d.fl_a = c->fl_a;
@@ -325,6 +388,8 @@ int streams_b200_copy_to_device(streams_b200_ctx* c, double* w) {
 int streams_b200_init_run(streams_b200_ctx* c) {
   if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
   cudaSetDevice(c->device);
+  // run() starts with update_ghost (singleideal_cpu.F90:1546)
+  if (has_stored_ghosts(c->g)) SB_CHECK(c, launch_bc_fill(c->g, c->d, c->stream, &c->launches));
   SB_CHECK(c, launch_aux(c->g, c->d, c->shift_pending ? 1 : 0, c->stream, &c->launches));
   c->shift_pending = false;
   c->aux_current = true;

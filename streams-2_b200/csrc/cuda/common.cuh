@@ -43,7 +43,20 @@ struct Geom {
   double coeff2[4][5];    // coeff_deriv2(l, lmax) at [lmax-1][l], l = 0..4
   // boundary handling
   int periodic[3];
-  int wall_ymin, wall_ymax;  // staggered isothermal walls
+  int wall_ymin, wall_ymax;  // staggered isothermal walls (ghosts mirrored on the fly)
+  int bctag[6], nr[6];       // boundary tags and non-reflecting types per face
+  double winf[5], p0;        // free stream (non-reflecting type 3), reference pressure
+  // recycling-rescaling inflow (bctag[0] = 10)
+  int recyc, i_recyc, jbl_inflow;
+  double betarecyc, rand_scale;
+  const double* wmean_inflow;  // [(m-1)*ny + (j-1)]*ng + (i-1), wmean(1-i, j, m)
+  const double* yplus_inflow;  // [j], j = 1-ng..ny+ng
+  const double* eta_inflow;
+  const double* yplus_recyc;
+  const double* eta_recyc;
+  const double* weta_inflow;   // [j], j = 1..ny
+  const int* map_j_inn;        // [j], j = 1..ny
+  const int* map_j_out;
   int fzf[6];                // force_zero_flux
   int eul_imin, eul_imax, eul_jmin, eul_jmax, eul_kmin, eul_kmax;
   // numerics
@@ -64,6 +77,13 @@ struct Geom {
   long long march_threads;
   int march_minseg;
 };
+// State of the crandom sequence on the device (glibc's additive feedback generator, continued
+// from the host set-up's draws): the 34-word ring and the position of the next word.
+struct RngState {
+  unsigned int ring[34];
+  long long pos;
+};
+
 // smallest march segment length a context may be tuned to (sizes the reduction scratch)
 constexpr int MARCH_MINSEG_MIN = 4;
 

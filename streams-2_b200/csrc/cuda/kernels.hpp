@@ -46,6 +46,11 @@ struct DevState {
   double* red = nullptr;      // block partials of the reductions
   Scalars* sc = nullptr;      // device scalars
   long long red_capacity = 0; // doubles in red
+  // recycling inflow: the random plane inflow_random_plane(j,k,c) at [(c*nz + k-1)*ny + j-1],
+  // the spanwise means of the recycling plane [(m*ny + j-1)*ng + i-1], the generator state
+  double* rplane = nullptr;
+  double* recyc_av = nullptr;
+  RngState* rng = nullptr;
   Prof* prof = nullptr;       // optional per-kernel timing
 };
 
@@ -73,6 +78,11 @@ cudaError_t launch_count_weno(const Geom& g, DevState& d, cudaStream_t s, long l
 cudaError_t launch_add_time(DevState& d, cudaStream_t s, long long* nl);
 
 // partial-sum slots needed for a geometry
+// open boundaries (bc_kernels.cu)
+cudaError_t launch_bc_fill(const Geom& g, DevState& d, cudaStream_t s, long long* nl);
+cudaError_t launch_rand_plane(const Geom& g, DevState& d, cudaStream_t s, long long* nl);
+cudaError_t launch_bc_nr(const Geom& g, DevState& d, double* fl, cudaStream_t s, long long* nl);
+bool has_stored_ghosts(const Geom& g);
 long long reduction_slots(const Geom& g);
 
 }  // namespace sb200

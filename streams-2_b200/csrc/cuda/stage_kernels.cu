@@ -90,13 +90,16 @@ __device__ __forceinline__ void point_state(const Geom& g, const double* __restr
   const int ox = (i < 1 || i > g.nx), oy = (j < 1 || j > g.ny), oz = (k < 1 || k > g.nz);
   int si = i, sj = j, sk = k;
   int wall = 0;
-  if (ox) si = wrap(i, g.nx);
-  if (oz) sk = wrap(k, g.nz);
+  // periodic faces wrap, staggered walls mirror; any other face reads its stored ghost
+  if (ox && g.periodic[0]) si = wrap(i, g.nx);
+  if (oz && g.periodic[2]) sk = wrap(k, g.nz);
   if (oy) {
     if (j < 1) {
-      if (g.periodic[1]) sj = j + g.ny; else { sj = 1 - j; wall = 1; }
+      if (g.periodic[1]) sj = j + g.ny;
+      else if (g.wall_ymin) { sj = 1 - j; wall = 1; }
     } else {
-      if (g.periodic[1]) sj = j - g.ny; else { sj = 2 * g.ny + 1 - j; wall = 1; }
+      if (g.periodic[1]) sj = j - g.ny;
+      else if (g.wall_ymax) { sj = 2 * g.ny + 1 - j; wall = 1; }
     }
   }
   const long long src = gidx(g, si, sj, sk);
@@ -159,7 +162,9 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
 // on the same values as in the FP64 form.  mode 0: initial sensor of run() (visflx(mode=2),
 // kernels_cpu.F90:4680-4682); mode 1: sensor_subroutine of stage 3 (:4726-4744), which works
 // from the stored |omega| and div/3 of visflx_reduced_ord2; mode 2: the same from the
-// visc_order derivatives of visflx_nosensor_subroutine (conservative_viscous = 0).
+// visc_order derivatives of visflx_nosensor_subroutine (conservative_viscous = 0); mode 3: the
+// initial sensor of run() for conservative_viscous = 0 (visflx(mode=0), visflx_subroutine,
+// kernels_cpu.F90:3598-3777: visc_order derivatives, theta from div and omega directly).
 __global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restrict__ w, double* __restrict__ out,
                                                   int mode) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
@@ -205,7 +210,7 @@ __global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restri
   double omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
   double omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
   double u0l0 = g.u0 / g.l0;
-  if (mode >= 1) {
+  if (mode == 1 || mode == 2) {
     double div3l = div / 3.0;
     double om = sqrt(omod2);
     omod2 = om * om;
@@ -1087,7 +1092,9 @@ cudaError_t launch_apply_shift(const Geom& g, DevState& d, cudaStream_t s, long 
 }
 
 cudaError_t launch_init_sensor(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
-  if (g.precision == 1)
+  if (!g.conservative_viscous)
+    SB_LAUNCH(d, K_INIT_SENSOR, s, k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, d.sensor, 3));
+  else if (g.precision == 1)
     SB_LAUNCH(d, K_INIT_SENSOR, s, k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, d.sensor, 0));
   else
     SB_LAUNCH(d, K_INIT_SENSOR, s, k_init_sensor<double><<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.aux, d.sensor));
@@ -1158,6 +1165,8 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
             k_march<R, 2, LB, WS><<<gzb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                         a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
   *nl += 4;
+  if (g.recyc) launch_rand_plane(g, d, s, nl);  // euler_z draws the inflow plane of the stage
+  launch_bc_nr(g, d, fl_new, s, nl);
   if (g.channel_case) {
     SB_LAUNCH(d, K_FINISH_RHS, s, k_finish_rhs<<<1, FIN_NT, 0, s>>>(g, d.red, (long long)gzb, a.istep == 1, d.sc));
     ++*nl;
@@ -1168,6 +1177,7 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
                                             a.want_stats, d.red, sensor_next, sensor));
   SB_LAUNCH(d, K_FINISH_UPD, s, k_finish_upd<<<1, FIN_NT, 0, s>>>(g, d.red, nbu, a.want_stats, a.add_time, d.sc));
   *nl += 2;
+  if (has_stored_ghosts(g)) launch_bc_fill(g, d, s, nl);  // update_ghost
   return cudaGetLastError();
 }
 

@@ -2,6 +2,8 @@
 // restates (paths relative to the STREAmS-2 repository).
 #include "setup.hpp"
 
+#include "glibc_rand.hpp"
+
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -13,7 +15,7 @@ namespace streams_b200 {
 
 namespace {
 
-constexpr int GRID_FROMFILE = 1, GRID_UNIFORM = 2, GRID_CHA = 3;
+constexpr int GRID_FROMFILE = 1, GRID_UNIFORM = 2, GRID_CHA = 3, GRID_BL = 4, GRID_SBLI = 5;
 constexpr double TOL_ITER = 0.000000001;  // parameters.F90:43 (REAL64 build)
 
 double pi() { return std::acos(-1.0); }
@@ -132,6 +134,65 @@ void generate_grid_tanh(Setup& s, double b) {
     s.yg(nymax + j) = 2.0 - s.yg(nymax + 1 - j);
     s.yg(1 - j) = -2.0 - s.yg(j);
   }
+}
+
+// generate_grid_bl (code/src/grid.F90:310-336), followed by generate_grid_geoprogression
+// (:338-368, GRID_BL) or generate_grid_uni_extension (:370-386, GRID_SBLI) above the wall-resolved
+// part, and generate_yg (:388-429): smoothing, staggered or node-based yg, mirrored ghosts.
+void generate_grid_bl(Setup& s, double jbgrid, double dyptarget, int nymaxwr, double rlywr, double retau,
+                      int nsmooy, bool sbli) {
+  const int nymax = s.nymax, ng = s.ng;
+  const double alfc = 4.0 / 3.0 * std::pow(retau * rlywr, 0.75) / (nymaxwr + 1);
+  for (int j = 1; j <= nymaxwr + 1 + ng; ++j) {
+    const double rj = static_cast<double>(j - 1);
+    const double q = rj / jbgrid;
+    s.yn(j) = 1.0 / (1.0 + q * q);
+    s.yn(j) = s.yn(j) * (rj * dyptarget + std::pow(0.75 * alfc * rj, 4.0 / 3.0) * (q * q));
+  }
+  const double ynf = s.yn(nymaxwr + 1);
+  for (int j = 1; j <= nymaxwr + ng + 1; ++j) s.yn(j) = s.yn(j) / ynf * rlywr;
+  if (nymaxwr < nymax) {
+    const double dy1 = s.yn(nymaxwr + 2) - s.yn(nymaxwr + 1);
+    if (!sbli) {
+      const double rlygp = s.domain_size[1] - rlywr;
+      const int nygp = nymax + 1 - (nymaxwr + 1);
+      double rgp = 1.01;
+      for (int it = 0; it < 100000; ++it) {
+        const double rgpold = rgp;
+        rgp = 1.0 - (1.0 - rgp) / dy1 * rlygp;
+        rgp = std::pow(rgp, 1.0 / nygp);
+        if (std::fabs(rgp - rgpold) < TOL_ITER) break;
+      }
+      for (int j = 1; j <= nygp + ng; ++j) s.yn(nymaxwr + 1 + j) = s.yn(nymaxwr + j) + dy1 * std::pow(rgp, j - 1.0);
+    } else {
+      for (int j = nymaxwr + 2; j <= nymax + 1 + ng; ++j) s.yn(j) = s.yn(j - 1) + dy1;
+    }
+  }
+  std::vector<double> tmp(static_cast<size_t>(nymax + 2 + ng));
+  for (int l = 1; l <= nsmooy; ++l) {
+    for (int j = 1; j <= nymax + 1 + ng; ++j) tmp[j] = s.yn(j);
+    for (int j = 2; j <= nymax + ng; ++j) s.yn(j) = (tmp[j - 1] + 4.0 * tmp[j] + tmp[j + 1]) / 6.0;
+  }
+  if (s.is_y_staggered) {
+    for (int j = 1; j <= nymax + ng; ++j) s.yg(j) = 0.5 * (s.yn(j) + s.yn(j + 1));
+    s.domain_size[1] = s.yn(nymax + 1) - s.yn(1);
+    for (int j = 1; j <= ng; ++j) s.yg(1 - j) = -s.yg(j);
+  } else {
+    for (int j = 1; j <= nymax + ng; ++j) s.yg(j) = s.yn(j);
+    s.domain_size[1] = s.yg(nymax) - s.yg(1);
+    for (int j = 1; j <= ng; ++j) s.yg(1 - j) = -s.yg(1 + j);
+  }
+}
+
+// locateval (code/src/parameters.F90:145-164): bisection index il with xx(il) <= x < xx(il+1)
+// for an ascending table (1-based; 0 below the table, n at or above its end).
+int locateval(const double* xx, int n, double x) {
+  int il = 0, juu = n + 1;
+  while (juu - il > 1) {
+    const int jm = (juu + il) / 2;
+    if ((xx[n - 1] > xx[0]) == (x > xx[jm - 1])) il = jm; else juu = jm;
+  }
+  return il;
 }
 
 // read_grid (code/src/grid.F90:877-959)
@@ -290,8 +351,16 @@ void set_flow_params(Setup& s, double reynolds_bulk_target) {
     }
     s.reynolds_friction = s.reynolds;
     s.reynolds = rebulk(s.reynolds_friction);
+  } else if (s.flow_init == 1) {
+    // set_bl_prop (singleideal.F90:2858-2892) converts the input friction Reynolds number into
+    // the free-stream one with hasan_meanprofile; the synthetic boundary layer states both
+    const IniFile& ci = s.ini;
+    if (!ci.has_section("synthetic"))
+      throw InputError("flow_init = 1 needs the [synthetic] boundary-layer initialisation");
+    s.reynolds_friction = ci.get_double_or("synthetic", "reynolds_tau", s.reynolds);
+    s.reynolds = ci.get_double("synthetic", "reynolds_delta");
   } else {
-    throw InputError("flow_init other than 0 (channel) is not supported yet");
+    throw InputError("flow_init other than 0 (channel) or 1 (boundary layer) is not supported");
   }
   s.p0 = s.rho0 * s.rgas0 * s.t0;
   s.c0 = std::sqrt(s.gam * s.rgas0 * s.t0);
@@ -314,40 +383,7 @@ void set_flow_params(Setup& s, double reynolds_bulk_target) {
   }
 }
 
-// glibc's rand() (the additive feedback generator behind random(), TYPE_3: degree 31,
-// separation 3), restated as a per-call object so that case set-ups running in several threads
-// do not share one global sequence.  Seeding: r0 = seed (1 if 0), r_i = 16807 r_{i-1} mod
-// (2^31 - 1) for i < 31, r_i = r_{i-31} for i = 31..33; then r_i = r_{i-31} + r_{i-3} (mod 2^32)
-// and output k is r_{k+344} >> 1.  crandom.c (code/third-party/crandom/crandom.c:12-29) calls
-// srand/rand, so the draws are those of the reference.
-class GlibcRand {
- public:
-  explicit GlibcRand(unsigned seed) {
-    int32_t r[34];
-    r[0] = seed == 0 ? 1 : static_cast<int32_t>(seed);
-    for (int i = 1; i < 31; ++i) {
-      const int32_t hi = r[i - 1] / 127773, lo = r[i - 1] % 127773;
-      int32_t word = 16807 * lo - 2836 * hi;
-      if (word < 0) word += 2147483647;
-      r[i] = word;
-    }
-    for (int i = 31; i < 34; ++i) r[i] = r[i - 31];
-    for (int i = 0; i < 34; ++i) ring_[i] = static_cast<uint32_t>(r[i]);
-    pos_ = 34;
-    for (int i = 34; i < 344; ++i) next_raw();
-  }
-  int operator()() { return static_cast<int>(next_raw() >> 1); }
 
- private:
-  uint32_t next_raw() {
-    const uint32_t v = ring_[(pos_ - 31) % 34] + ring_[(pos_ - 3) % 34];
-    ring_[pos_ % 34] = v;
-    ++pos_;
-    return v;
-  }
-  uint32_t ring_[34];
-  long long pos_;
-};
 
 // init_channel (singleideal.F90:4344-4419) with the per-rank seeding of an MPI run
 void init_channel(Setup& s) {
@@ -429,6 +465,138 @@ void init_channel_synthetic(Setup& s, double amp, int seed) {
         s.w[s.widx(i, j, k, 3)] = rhoww;
         s.w[s.widx(i, j, k, 4)] = rho * ee + 0.5 * (rhouu * rhouu + rhovv * rhovv + rhoww * rhoww) / rho;
       }
+}
+
+// Synthetic spatially developing boundary layer (the benchmark's boundary-layer workload; it
+// replaces init_bl, singleideal.F90:3252-3423, whose hasan_meanprofile is not restated):
+//   thickness   delta(x) = l0 (1 + (x/l0) 0.27^1.2 / Re^0.2)^(5/6)   (the Urbin-Knight growth that
+//               recyc_prepare reports), viscous length deltav(x) = (l0/Re_tau) (delta/l0)^(1/8)
+//   mean flow   u = u0 min(y/delta, 1)^(1/7), Crocco-Busemann temperature
+//               T = T_w + (T_r - T_w) u/u0 + (t0 - T_r) (u/u0)^2, rho = p0 / (R T),
+//               v from continuity exactly as init_bl integrates it, w = 0
+//   field       mean + uniform random perturbations of +-amp u0 on u, v, w (glibc rand, seed of
+//               the single rank, 3 draws per cell in k, j, i order, as init_bl draws them)
+void init_bl_synthetic(Setup& s, double amp) {
+  const int nx = s.nxmax, ny = s.nymax, nz = s.nzmax, ng = s.ng;
+  const int nxg = nx + 2 * ng + 1;  // xg(1-ng : nx+ng+1)
+  s.deltavec.assign(nxg, 0.0);
+  s.deltavvec.assign(nxg, 0.0);
+  const double grow = std::pow(0.27, 1.2) / std::pow(s.reynolds, 0.2);
+  for (int i = 1 - ng; i <= nx + ng + 1; ++i) {
+    const double d = s.l0 * std::pow(1.0 + s.xg(i) / s.l0 * grow, 5.0 / 6.0);
+    s.deltavec[i + ng - 1] = d;
+    s.deltavvec[i + ng - 1] = s.l0 / s.reynolds_friction * std::pow(d / s.l0, 0.125);
+  }
+  // wmean(1-ng:nx+ng+1, 1:ny, 4)
+  const int wi = nx + 2 * ng + 1;
+  s.wmean.assign(static_cast<size_t>(wi) * ny * 4, 0.0);
+  auto WM = [&](int i, int j, int m) -> double& {
+    return s.wmean[(static_cast<size_t>(m - 1) * ny + (j - 1)) * wi + (i + ng - 1)];
+  };
+  for (int i = 1 - ng; i <= nx + ng + 1; ++i) {
+    const double delta = s.deltavec[i + ng - 1];
+    for (int j = 1; j <= ny; ++j) {
+      const double yy = s.yg(j);
+      const double eta = std::min(std::max(yy, 0.0) / delta, 1.0);
+      const double ub = std::pow(eta, 1.0 / 7.0);
+      const double tt = s.t_wall + (s.t_recovery - s.t_wall) * ub + (s.t0 - s.t_recovery) * ub * ub;
+      const double rho = s.p0 / (s.rgas0 * tt);
+      WM(i, j, 1) = rho;
+      WM(i, j, 2) = rho * ub * s.u0;
+    }
+  }
+  for (int i = 1 - ng; i <= nx + ng; ++i)
+    for (int j = 2; j <= ny; ++j) {
+      const double vi_j = -(WM(i + 1, j, 2) - WM(i, j, 2)) / (s.xg(i + 1) - s.xg(i));
+      const double vi_jm = -(WM(i + 1, j - 1, 2) - WM(i, j - 1, 2)) / (s.xg(i + 1) - s.xg(i));
+      const double vi = 0.5 * (vi_j + vi_jm);
+      WM(i, j, 3) = WM(i, j - 1, 3) + vi * (s.yg(j) - s.yg(j - 1));
+    }
+  const unsigned seed = s.rand_type == 0 ? 0u : 1u;
+  const double rescale = s.rand_type == 0 ? 0.0 : 1.0;
+  GlibcRand rnd(seed);
+  const double ua = 2.0 * amp * s.u0;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const double rho = WM(i, j, 1);
+        double rr[3];
+        for (int l = 0; l < 3; ++l) rr[l] = rescale * static_cast<double>(rnd()) / RAND_MAX - 0.5;
+        const double uu = WM(i, j, 2) / rho + ua * rr[0];
+        const double vv = WM(i, j, 3) / rho + ua * rr[1];
+        const double ww = WM(i, j, 4) / rho + ua * rr[2];
+        const double rhouu = rho * uu, rhovv = rho * vv, rhoww = rho * ww;
+        s.w[s.widx(i, j, k, 0)] = rho;
+        s.w[s.widx(i, j, k, 1)] = rhouu;
+        s.w[s.widx(i, j, k, 2)] = rhovv;
+        s.w[s.widx(i, j, k, 3)] = rhoww;
+        const double tt = s.p0 / s.rgas0 / rho;
+        const double ee = e_from_t(s, tt);
+        s.w[s.widx(i, j, k, 4)] = rho * ee + 0.5 * (rhouu * rhouu + rhovv * rhovv + rhoww * rhoww) / rho;
+      }
+  s.rng_seed = seed;
+  s.rng_draws = 3LL * nx * ny * nz;
+}
+
+// recyc_prepare (singleideal.F90:1512-1588), single block
+void recyc_prepare(Setup& s) {
+  const int nx = s.nxmax, ny = s.nymax, ng = s.ng;
+  s.x_recyc = s.ini.get_double("bc", "x_recyc") * s.l0;
+  const double bexprecyc_base = 0.13, my_eta0 = 0.08, my_deltablend = 1.10;
+  std::vector<double> xg1(static_cast<size_t>(nx));
+  for (int i = 1; i <= nx; ++i) xg1[i - 1] = s.xg(i);
+  int ig_recyc = locateval(xg1.data(), nx, s.x_recyc);
+  s.i_recyc = ig_recyc;
+  if (s.i_recyc < ng) {
+    s.i_recyc = ng;
+    ig_recyc = s.i_recyc;
+  }
+  auto DV = [&](int i) { return s.deltavec[i + ng - 1]; };
+  auto DVV = [&](int i) { return s.deltavvec[i + ng - 1]; };
+  s.betarecyc = DVV(ig_recyc) / DVV(1);
+  s.glund1 = std::pow(DV(ig_recyc) / DV(1), bexprecyc_base);
+  const int n = ny + 2 * ng;
+  s.yplus_inflow.assign(n, 0.0); s.eta_inflow.assign(n, 0.0); s.yplus_recyc.assign(n, 0.0);
+  s.eta_recyc.assign(n, 0.0); s.eta_recyc_blend.assign(n, 0.0);
+  for (int j = 1 - ng; j <= ny + ng; ++j) {
+    const double y = s.yg(j);
+    const size_t q = static_cast<size_t>(j + ng - 1);
+    s.yplus_inflow[q] = y / DVV(1);
+    s.eta_inflow[q] = y / DV(1);
+    s.yplus_recyc[q] = y / DVV(ig_recyc);
+    s.eta_recyc[q] = y / DV(ig_recyc);
+    const double r = DV(1) / DV(ig_recyc);
+    s.eta_recyc_blend[q] = y * (std::pow(r, bexprecyc_base) +
+                                0.5 * (1.0 + std::tanh(std::log(std::fabs(s.eta_recyc[q]) / my_eta0) / my_deltablend)) *
+                                    (r - std::pow(r, bexprecyc_base)));
+  }
+  const double alfa_blend = 4.0, beta_blend = 0.2, c_blend = 1.0 - 2.0 * beta_blend;
+  s.map_j_inn.assign(ny, 0); s.map_j_out.assign(ny, 0); s.map_j_out_blend.assign(ny, 0);
+  s.weta_inflow.assign(ny, 0.0);
+  const double* yr = &s.yplus_recyc[ng];  // yplus_recyc(1:ny)
+  const double* er = &s.eta_recyc[ng];
+  const double* eb = &s.eta_recyc_blend[ng];
+  for (int j = 1; j <= ny; ++j) {
+    const size_t q = static_cast<size_t>(j + ng - 1);
+    s.map_j_inn[j - 1] = locateval(yr, ny, s.yplus_inflow[q]);
+    s.map_j_out[j - 1] = locateval(er, ny, s.eta_inflow[q]);
+    s.map_j_out_blend[j - 1] = locateval(eb, ny, s.eta_inflow[q]);
+    s.weta_inflow[j - 1] = 0.5 * (1.0 + std::tanh((alfa_blend * (s.eta_inflow[q] - beta_blend)) /
+                                                  (beta_blend + s.eta_inflow[q] * c_blend)) /
+                                            std::tanh(alfa_blend));
+  }
+  // jbl_inflow (init_bl, singleideal.F90:3281): last y node below l0
+  std::vector<double> y1(static_cast<size_t>(ny));
+  for (int j = 1; j <= ny; ++j) y1[j - 1] = s.yg(j);
+  s.jbl_inflow = locateval(y1.data(), ny, s.l0);
+  // the mean inflow planes wmean(1-i, j, m), i = 1..ng, that bcrecyc_subroutine_3 rescales
+  const int wi = nx + 2 * ng + 1;
+  s.wmean_inflow.assign(static_cast<size_t>(4) * ny * ng, 0.0);
+  for (int m = 1; m <= 4; ++m)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= ng; ++i)
+        s.wmean_inflow[(static_cast<size_t>(m - 1) * ny + (j - 1)) * ng + (i - 1)] =
+            s.wmean[(static_cast<size_t>(m - 1) * ny + (j - 1)) * wi + (1 - i + ng - 1)];
 }
 
 // read_field (code/src/field.F90:1853-1905): rst.bin = nv global arrays, Fortran order, native REAL64
@@ -611,6 +779,11 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
       generate_grid_cha(s, c.get_double("grid", "jbgrid"), c.get_double("grid", "dyptarget"),
                         static_cast<int>(std::lround(c.get_double("grid", "ysmoosteps"))),
                         c.get_double("flow", "Reynolds"));
+    } else if (s.grid_type == GRID_BL || s.grid_type == GRID_SBLI) {
+      generate_grid_bl(s, c.get_double("grid", "jbgrid"), c.get_double("grid", "dyptarget"),
+                       static_cast<int>(std::lround(c.get_double("grid", "nywr"))), c.get_double("grid", "lywr"),
+                       c.get_double("flow", "Reynolds"),
+                       static_cast<int>(std::lround(c.get_double("grid", "ysmoosteps"))), s.grid_type == GRID_SBLI);
     } else {
       throw InputError("grid_type " + std::to_string(s.grid_type) + " is not supported by the B200 backend");
     }
@@ -672,12 +845,18 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
     }
   }
   for (int l = 0; l < 6; ++l) {
-    if (s.bctags[l] != 0 && s.bctags[l] != 6)
-      throw InputError("boundary tag " + std::to_string(s.bctags[l]) + " is not supported by the B200 backend yet");
-    if (s.bctags_nr[l] != 0) throw InputError("non-reflecting boundary treatment is not supported yet");
+    const int t = s.bctags[l];
+    if (t != 0 && t != 2 && t != 6 && t != 10)
+      throw InputError("boundary tag " + std::to_string(t) + " is not supported by the B200 backend yet");
+    const int nr = s.bctags_nr[l];
+    if (nr != 0 && nr != 1 && nr != 2 && nr != 3 && nr != 6)
+      throw InputError("non-reflecting type " + std::to_string(nr) + " is not supported");
+    if (nr != 0 && l >= 4) throw InputError("non-reflecting treatment is supported on x and y boundaries");
   }
   if (s.bctags[0] == 6 || s.bctags[1] == 6 || s.bctags[4] == 6 || s.bctags[5] == 6)
     throw InputError("viscous walls are supported on the y boundaries only");
+  for (int l = 1; l < 6; ++l)
+    if (s.bctags[l] == 10) throw InputError("recycling inflow (tag 10) is supported at xmin only");
 
   // correct_bc_order (singleideal.F90:946-993)
   const int n3[3] = {s.nxmax, s.nymax, s.nzmax};
@@ -746,8 +925,15 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
       std::istringstream is(c.raw("synthetic", "kind"));
       is >> kind;
     }
-    if (kind != "channel_poiseuille") throw InputError("unknown synthetic initial field " + kind);
-    init_channel_synthetic(s, c.get_double_or("synthetic", "amp", 0.1), c.get_int_or("synthetic", "seed", 1));
+    if (kind == "channel_poiseuille") {
+      if (s.flow_init != 0) throw InputError("the synthetic channel field needs flow_init = 0");
+      init_channel_synthetic(s, c.get_double_or("synthetic", "amp", 0.1), c.get_int_or("synthetic", "seed", 1));
+    } else if (kind == "bl_powerlaw") {
+      if (s.flow_init != 1) throw InputError("the synthetic boundary-layer field needs flow_init = 1");
+      init_bl_synthetic(s, c.get_double_or("synthetic", "amp", 0.05));
+    } else {
+      throw InputError("unknown synthetic initial field " + kind);
+    }
   } else {
     init_channel(s);
     if (s.restart_type == 1) {
@@ -756,6 +942,11 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
     } else if (s.restart_type == 2) {
       throw InputError("restart_type = 2 (statistics restart) is not supported by the B200 backend");
     }
+  }
+  s.recyc = s.bctags[0] == 10;
+  if (s.recyc) {
+    if (s.flow_init != 1 || s.wmean.empty()) throw InputError("recycling inflow needs the boundary-layer initialisation");
+    recyc_prepare(s);
   }
   return s;
 }
@@ -787,6 +978,15 @@ void Setup::fill_params(streams_b200_params* p, int precision) const {
   }
   p->cfl = cfl;
   p->precision = precision;
+  for (int l = 0; l < 6; ++l) p->bctags_nr[l] = bctags_nr[l];
+  for (int m = 0; m < 5; ++m) p->winf[m] = winf[m];
+  p->p0 = p0;
+  p->recyc = recyc ? 1 : 0;
+  p->i_recyc = i_recyc;
+  p->jbl_inflow = jbl_inflow;
+  p->betarecyc = betarecyc;
+  p->rng_seed = rng_seed;
+  p->rng_draws = rng_draws;
 }
 
 void Setup::fill_grid(streams_b200_grid* g) const {
@@ -797,6 +997,13 @@ void Setup::fill_grid(streams_b200_grid* g) const {
   g->ep_ord_x = ep_ord[0].data(); g->ep_ord_y = ep_ord[1].data(); g->ep_ord_z = ep_ord[2].data();
   g->dcsidx2 = dcsidx2.data(); g->detady2 = detady2.data(); g->dzitdz2 = dzitdz2.data();
   g->coeff_deriv2 = &coeff_deriv2[0][0];
+  if (recyc) {
+    g->wmean_inflow = wmean_inflow.data();
+    g->yplus_inflow = yplus_inflow.data(); g->eta_inflow = eta_inflow.data();
+    g->yplus_recyc = yplus_recyc.data(); g->eta_recyc = eta_recyc.data();
+    g->weta_inflow = weta_inflow.data();
+    g->map_j_inn = map_j_inn.data(); g->map_j_out = map_j_out.data();
+  }
 }
 
 void write_restart_inputs(const Setup& s, const std::string& dir) {

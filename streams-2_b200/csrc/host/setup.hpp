@@ -84,6 +84,22 @@ struct Setup {
   int restart_type = 0, num_iter = 0, iter_dt_recompute = 1, print_control = 1, icyc0 = 0;
   double cfl = 0, time0 = 0;
 
+  // boundary layer (flow_init = 1): recycling-rescaling inflow (recyc_prepare,
+  // singleideal.F90:1512-1588) and the mean profile it rescales
+  bool recyc = false;
+  double x_recyc = 0, betarecyc = 1, glund1 = 1;
+  int i_recyc = 0, jbl_inflow = 1;
+  std::vector<double> deltavec, deltavvec;  // BL thickness / viscous length at xg(1-ng .. nxmax+ng+1)
+  std::vector<double> wmean;                // wmean(1-ng:nx+ng+1, 1:ny, 4), Fortran order
+  std::vector<double> yplus_inflow, eta_inflow, yplus_recyc, eta_recyc, eta_recyc_blend;  // (1-ng:ny+ng)
+  std::vector<int> map_j_inn, map_j_out, map_j_out_blend;  // (1:ny)
+  std::vector<double> weta_inflow;          // (1:ny)
+  std::vector<double> wmean_inflow;         // wmean(1-i, j, m), i = 1..ng: [m][j][i-1] (C order)
+  // state of the crandom sequence after the set-up (seed and draws taken): the solver draws the
+  // recycling plane's random perturbations from it at every stage
+  unsigned rng_seed = 1;
+  long long rng_draws = 0;
+
   // initial conserved field w(1-ng:nx+ng,1-ng:ny+ng,1-ng:nz+ng,5), Fortran order
   std::vector<double> w;
 

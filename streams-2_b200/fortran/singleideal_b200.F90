@@ -17,6 +17,11 @@ module streams_equation_singleideal_b200_object
     type(equation_singleideal_object) :: equation_base
     type(c_ptr) :: ctx = c_null_ptr
     integer, allocatable, dimension(:) :: epx, epy, epz
+    ! recycling inflow: wmean(1-i, j, 1:4), i = 1..ng, of the equation object, contiguous
+    real(c_double), allocatable, dimension(:,:,:) :: wmean_inflow
+    ! rank of this process and the crandom draws the set-up took (init_bl: 3 per cell)
+    integer(c_int) :: myrank = 0
+    integer(c_long_long) :: crandom_draws = 0
   contains
     procedure, pass(self) :: initialize
     procedure, pass(self) :: run
@@ -64,6 +69,11 @@ contains
       p%nrk = eb%nrk ; p%rhork = 0._rkind ; p%gamrk = 0._rkind
       p%rhork(1:eb%nrk) = eb%rhork ; p%gamrk(1:eb%nrk) = eb%gamrk
       p%cfl = eb%cfl ; p%precision = 0
+      p%bctags_nr = eb%bctags_nr ; p%winf = eb%winf ; p%p0 = eb%p0
+      p%recyc = merge(1, 0, eb%recyc) ; p%i_recyc = eb%i_recyc ; p%jbl_inflow = eb%jbl_inflow
+      p%betarecyc = eb%betarecyc
+      ! the crandom sequence continues on the device: seed of this rank and the draws taken so far
+      p%rng_seed = self%myrank + 1 ; p%rng_draws = self%crandom_draws
       allocate(self%epx(0:f%nx), self%epy(0:f%ny), self%epz(0:f%nz))
       do i = 0, f%nx ; self%epx(i) = eb%ep_ord_change(i,1,1,1) ; enddo
       do j = 0, f%ny ; self%epy(j) = eb%ep_ord_change(1,j,1,2) ; enddo
@@ -75,6 +85,17 @@ contains
       g%ep_ord_x = c_loc(self%epx) ; g%ep_ord_y = c_loc(self%epy) ; g%ep_ord_z = c_loc(self%epz)
       g%dcsidx2 = c_loc(f%dcsidx2) ; g%detady2 = c_loc(f%detady2) ; g%dzitdz2 = c_loc(f%dzitdz2)
       g%coeff_deriv2 = c_loc(eb%coeff_deriv2)
+      if (eb%recyc) then
+        allocate(self%wmean_inflow(f%grid%ng, f%ny, 4))
+        do i = 1, f%grid%ng
+          self%wmean_inflow(i, :, :) = eb%wmean(1-i, 1:f%ny, 1:4)
+        enddo
+        self%crandom_draws = 3_c_long_long * f%nx * f%ny * f%nz
+        g%wmean_inflow = c_loc(self%wmean_inflow) ; g%weta_inflow = c_loc(eb%weta_inflow)
+        g%yplus_inflow = c_loc(eb%yplus_inflow) ; g%eta_inflow = c_loc(eb%eta_inflow)
+        g%yplus_recyc = c_loc(eb%yplus_recyc) ; g%eta_recyc = c_loc(eb%eta_recyc)
+        g%map_j_inn = c_loc(eb%map_j_inn) ; g%map_j_out = c_loc(eb%map_j_out)
+      endif
       call self%check(streams_b200_create(p, g, self%ctx), 'create')
       call self%check(streams_b200_copy_from_field(self%ctx, c_loc(f%w)), 'copy_from_field')
       call self%check(streams_b200_set_time(self%ctx, eb%time0), 'set_time')

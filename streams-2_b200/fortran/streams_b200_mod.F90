@@ -29,6 +29,13 @@ module streams_b200_mod
     real(c_double) :: rhork(4), gamrk(4)
     real(c_double) :: cfl
     integer(c_int) :: precision
+    integer(c_int) :: bctags_nr(6)
+    real(c_double) :: winf(5)
+    real(c_double) :: p0
+    integer(c_int) :: recyc, i_recyc, jbl_inflow
+    real(c_double) :: betarecyc
+    integer(c_int) :: rng_seed
+    integer(c_long_long) :: rng_draws
   end type streams_b200_params
 
   type, bind(c) :: streams_b200_grid
@@ -38,6 +45,8 @@ module streams_b200_mod
     type(c_ptr) :: ep_ord_x, ep_ord_y, ep_ord_z
     type(c_ptr) :: dcsidx2, detady2, dzitdz2
     type(c_ptr) :: coeff_deriv2
+    type(c_ptr) :: wmean_inflow, yplus_inflow, eta_inflow, yplus_recyc, eta_recyc, weta_inflow
+    type(c_ptr) :: map_j_inn, map_j_out
   end type streams_b200_grid
 
   interface

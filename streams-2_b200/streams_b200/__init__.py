@@ -50,6 +50,9 @@ class Params(C.Structure):
         ("rhork", C.c_double * 4), ("gamrk", C.c_double * 4),
         ("cfl", C.c_double),
         ("precision", C.c_int),
+        ("bctags_nr", C.c_int * 6), ("winf", C.c_double * 5), ("p0", C.c_double),
+        ("recyc", C.c_int), ("i_recyc", C.c_int), ("jbl_inflow", C.c_int),
+        ("betarecyc", C.c_double), ("rng_seed", C.c_uint), ("rng_draws", C.c_longlong),
     ]
 
 
@@ -59,7 +62,10 @@ class Grid(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_double)) for n in
                 ("x", "y", "z", "yn", "dcsidx", "detady", "dzitdz", "dcsidxs", "detadys", "dzitdzs",
                  "coeff_deriv1")] + [(n, C.POINTER(C.c_int)) for n in ("ep_ord_x", "ep_ord_y", "ep_ord_z")] + \
-        [(n, C.POINTER(C.c_double)) for n in ("dcsidx2", "detady2", "dzitdz2", "coeff_deriv2")]
+        [(n, C.POINTER(C.c_double)) for n in ("dcsidx2", "detady2", "dzitdz2", "coeff_deriv2",
+                                               "wmean_inflow", "yplus_inflow", "eta_inflow", "yplus_recyc",
+                                               "eta_recyc", "weta_inflow")] + \
+        [(n, C.POINTER(C.c_int)) for n in ("map_j_inn", "map_j_out")]
 
 
 class BackendError(RuntimeError):

@@ -111,6 +111,121 @@ enable_vtk = 0
 """
 
 
+def bl_ini(nx=64, ny=48, nz=16, *, lx=100.0, ly=12.0, lz=8.0, mach=2.0, reynolds_tau=400.0,
+           reynolds_delta=None, theta_wall=1.0, visc_model=1, vt_exp=0.76, sensor=0.05, ep_order=6,
+           weno_scheme=3, weno_version=0, amp=0.05, x_recyc=None, nr_outflow=1, nr_top=1, cfl=0.8,
+           jbgrid=None, dyptarget=0.7, nywr=None, lywr=None, ysmoosteps=10, conservative_viscous=1,
+           num_iter=100, print_control=1, correct_bound_ord=1, rand_type=1) -> str:
+    """Input file of a spatially developing supersonic boundary layer (the benchmark's boundary
+    layer workload): box lx x ly x lz inflow thicknesses, BL grid (grid_type 4, wall-resolved part
+    of nywr points up to lywr), recycling-rescaling inflow at xmin, extrapolation with a
+    characteristic non-reflecting treatment at the outflow and top (types nr_outflow / nr_top),
+    isothermal wall at theta_wall (1 = recovery temperature), periodic z, and the synthetic
+    power-law initial field ([synthetic] kind = bl_powerlaw)."""
+    if reynolds_delta is None:
+        reynolds_delta = 25.0 * reynolds_tau ** 1.1  # free-stream Re_delta of a Mach-2 layer of that Re_tau
+    if x_recyc is None:
+        x_recyc = 0.8 * lx
+    if nywr is None:
+        nywr = max(8, (3 * ny) // 4)
+    if lywr is None:
+        lywr = 2.5
+    if jbgrid is None:
+        jbgrid = max(4.0, nywr / 4.0)
+    return f"""[grid]
+grid_dim = 1
+domain_size_x = {lx!r}
+domain_size_y = {ly!r}
+domain_size_z = {lz!r}
+nxmax = {nx}
+nymax = {ny}
+nzmax = {nz}
+ng = 3
+metrics_order = {ep_order}
+grid_type = 4
+jbgrid = {jbgrid!r}
+dyptarget = {dyptarget!r}
+nywr = {nywr}
+lywr = {lywr!r}
+ysmoosteps = {ysmoosteps}
+
+[bc]
+xmin = 10
+xmax = 2
+ymin = 6
+ymax = 2
+zmin = 0
+zmax = 0
+xmin_nr = 0
+xmax_nr = {nr_outflow}
+ymin_nr = 0
+ymax_nr = {nr_top}
+zmin_nr = 0
+zmax_nr = 0
+x_recyc = {x_recyc!r}
+correct_bound_ord = {correct_bound_ord}
+
+[mpi]
+x_split = 1
+y_split = 1
+z_split = 1
+
+[controls]
+restart_type = 0
+cfl = {cfl!r}
+iter_dt_recompute = 1
+num_iter = {num_iter}
+
+[numerics]
+ep_order = {ep_order}
+nkeep = 0
+visc_order = {ep_order}
+conservative_viscous = {conservative_viscous}
+weno_scheme = {weno_scheme}
+weno_version = {weno_version}
+flux_splitting = 0
+sensor_threshold = {sensor!r}
+rk_type = 1
+rand_type = {rand_type}
+
+[flow]
+flow_init = 1
+Mach = {mach!r}
+Reynolds = {reynolds_tau!r}
+theta_wall = {theta_wall!r}
+xshock_imp = 0.
+shock_angle = 0.
+T_ref = 220.
+aoa = 0.
+
+[fluid]
+gam = 1.4
+Prandtl = 0.72
+visc_model = {visc_model}
+vt_exp = {vt_exp!r}
+s_suth = 110.4
+calorically_perfect = 1
+
+[output]
+print_control = {print_control}
+dtsave_restart = 50.
+dtsave = 50.
+dtstat = 50.
+dtslice = 50.
+igslice = 0
+jgslice = 0
+kgslice = 0
+enable_plot3d = 0
+enable_vtk = 0
+
+[synthetic]
+kind = bl_powerlaw
+amp = {amp!r}
+reynolds_delta = {reynolds_delta!r}
+reynolds_tau = {reynolds_tau!r}
+"""
+
+
 # grid choices of the batched workload (48 boxes)
 BATCH_NX = (64, 96, 128)
 BATCH_NY = (64, 96)

@@ -37,3 +37,22 @@ def test_nonconservative_mass_conservation(tmp_path):
     o = run(tmp_path, "c", 5, nx=24, ny=16, nz=12, conservative_viscous=0)
     s = o.scalars()
     assert abs(s["rhobulk"] - 1.0) < 1e-12
+
+
+def test_bl_setup_and_oracle_run(tmp_path):
+    """The synthetic boundary layer: set-up, recycling data and a few oracle steps on the CPU."""
+    from oracle_py import Oracle
+    from streams_b200 import Case
+    from streams_b200.cases import bl_ini
+    ini = bl_ini(nx=32, ny=32, nz=8)
+    case = Case(tmp_path, ini)
+    p = case.params()
+    assert list(p.bctags) == [10, 2, 6, 2, 0, 0] and p.recyc == 1 and p.is_y_staggered == 0
+    assert p.eul_imax == 31 and p.eul_jmax == 31  # non-reflecting outflow and top (bc_preproc)
+    assert 3 <= p.i_recyc <= 32 and p.rng_draws == 3 * 32 * 32 * 8
+    o = Oracle(tmp_path, ini)
+    o.init_run()
+    o.run(3)
+    w = o.w()
+    assert np.all(np.isfinite(w))
+    assert np.all(w[1:4, 3:-3, 3, 3:-3] == 0.0)  # wall node at rest
