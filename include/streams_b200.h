@@ -87,6 +87,10 @@ typedef struct streams_b200_params {
   double betarecyc;
   unsigned int rng_seed;
   long long rng_draws;
+  /* impinging oblique shock at the top (bctags[3] = 7, set_oblique_shock): impingement point,
+   * shock angle [rad], tanh smoothing length, post-shock conserved state */
+  double xshock_imp, shock_angle, tanhfacs;
+  double winf_past_shock[5];
 } streams_b200_params;
 
 /*

@@ -315,6 +315,7 @@ void Solver::update_ghost(int do_swap) {
     switch (s.bctags[ilat - 1]) {
       case 2: bcextr(ilat); break;
       case 6: if (s.is_y_staggered) bcwall_staggered(ilat); else bcwall(ilat); break;
+      case 7: if (ilat == 4) bcshock(); break;
       case 10: if (ilat == 1) bcrecyc(); break;
       default: break;
     }
@@ -385,6 +386,26 @@ void Solver::bcwall(int ilat) {
       }
     }
   });
+}
+
+// bcshock_subroutine (kernels_cpu.F90:6159-6196), ymax
+void Solver::bcshock() {
+  const double tanhlen = 8.0 * s.tanhfacs;
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i)
+      for (int l = 0; l <= ng; ++l) {
+        const double xsh = s.xshock_imp - Y(ny + l) / std::tan(s.shock_angle);
+        const double xx = X(i) - xsh;
+        if (std::fabs(xx) > tanhlen) {
+          for (int m = 0; m < 5; ++m) W(i, ny + l, k, m) = W(i, ny, k, m);
+        } else {
+          const double tanhf = 0.5 * (1.0 + std::tanh(xx / s.tanhfacs));
+          for (int m = 0; m < 5; ++m) {
+            const double dwinf = s.winf_past_shock[m] - s.winf[m];
+            W(i, ny + l, k, m) = s.winf[m] + dwinf * tanhf;
+          }
+        }
+      }
 }
 
 // bcextr_subroutine (kernels_cpu.F90:6323-6390): zeroth-order extrapolation of all variables

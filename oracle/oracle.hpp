@@ -101,6 +101,7 @@ class Solver {
   void bcwall(int ilat);
   void bcwall_staggered(int ilat);
   void bcrecyc();
+  void bcshock();
   void draw_random_plane();
   void bc_nr();
 };

@@ -99,8 +99,9 @@ std::string validate(const streams_b200_params* p) {
   }
   for (int l = 0; l < 6; ++l) {
     const int t = p->bctags[l];
-    if (t != 0 && t != 2 && t != 6 && t != 10)
-      return "boundary tags: periodic (0), extrapolation (2), isothermal wall (6) and recycling inflow (10)";
+    if (t != 0 && t != 2 && t != 6 && t != 10 && !(t == 7 && l == 3))
+      return "boundary tags: periodic (0), extrapolation (2), isothermal wall (6), shock at ymax (7) and "
+             "recycling inflow (10)";
     if (t == 6 && l != 2 && l != 3) return "isothermal walls (6) are implemented on the y faces";
     if (t == 6 && !p->is_y_staggered && l != 2) return "a node-based wall (6, not staggered) is implemented at ymin";
     if (t == 10 && l != 0) return "recycling inflow (10) is implemented at xmin";
@@ -137,6 +138,8 @@ void fill_geom(streams_b200_ctx* c) {
   g.jbl_inflow = p.jbl_inflow;
   g.betarecyc = p.betarecyc;
   g.rand_scale = p.rng_seed == 0 ? 0.0 : 1.0;
+  g.xshock_imp = p.xshock_imp; g.shock_angle = p.shock_angle; g.tanhfacs = p.tanhfacs;
+  for (int m = 0; m < 5; ++m) g.winf_past_shock[m] = p.winf_past_shock[m];
   for (int l = 0; l < 6; ++l) g.fzf[l] = p.force_zero_flux[l];
   g.eul_imin = p.eul_imin; g.eul_imax = p.eul_imax; g.eul_jmin = p.eul_jmin;
   g.eul_jmax = p.eul_jmax; g.eul_kmin = p.eul_kmin; g.eul_kmax = p.eul_kmax;

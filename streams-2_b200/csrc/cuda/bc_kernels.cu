@@ -67,6 +67,33 @@ __global__ void __launch_bounds__(BC_NT) k_bc_wall(Geom g, double* __restrict__ 
   }
 }
 
+// bcshock_subroutine (kernels_cpu.F90:6159-6196), ymax: within 8 tanhfacs of the shock's foot
+// the top row and its ghosts take the tanh blend of the free stream and the post-shock state,
+// elsewhere the ghosts copy the top row (l = 0 is the row itself)
+__global__ void __launch_bounds__(BC_NT) k_bc_shock(Geom g, double* __restrict__ w) {
+  const long long q = (long long)blockIdx.x * BC_NT + threadIdx.x;
+  if (q >= (long long)g.nx * g.nz) return;
+  const int i = (int)(q % g.nx) + 1, k = (int)(q / g.nx) + 1;
+  const long long n = g.nvol, top = gidx(g, i, g.ny, k);
+  const double tanhlen = 8.0 * g.tanhfacs;
+  for (int l = 0; l <= g.ng; ++l) {
+    const double xsh = g.xshock_imp - g.y[g.ny + l] / tan(g.shock_angle);
+    const double xx = g.x[i] - xsh;
+    const long long d = gidx(g, i, g.ny + l, k);
+    if (fabs(xx) > tanhlen) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) w[m * n + d] = w[m * n + top];
+    } else {
+      const double tanhf = 0.5 * (1.0 + tanh(xx / g.tanhfacs));
+#pragma unroll
+      for (int m = 0; m < 5; ++m) {
+        const double dwinf = g.winf_past_shock[m] - g.winf[m];
+        w[m * n + d] = g.winf[m] + dwinf * tanhf;
+      }
+    }
+  }
+}
+
 // z index of the recycling plane that feeds inflow plane k: recyc_exchange shifts by nzmax/2
 // (singleideal_cpu.F90:935-999 on one block)
 __device__ __forceinline__ int recyc_k(const Geom& g, int k) {
@@ -319,6 +346,9 @@ cudaError_t launch_bc_fill(const Geom& g, DevState& d, cudaStream_t s, long long
       const long long np = (long long)(dir == 0 ? g.ny : g.nx) * (dir == 2 ? g.ny : g.nz);
       k_bc_extr<<<nb(np), BC_NT, 0, s>>>(g, d.w, ilat);
       ++*nl;
+    } else if (t == 7 && ilat == 4) {
+      k_bc_shock<<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w);
+      ++*nl;
     } else if (t == 6 && ilat == 3 && !g.wall_ymin) {
       k_bc_wall<<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w);
       ++*nl;
@@ -330,7 +360,7 @@ cudaError_t launch_bc_fill(const Geom& g, DevState& d, cudaStream_t s, long long
 bool has_stored_ghosts(const Geom& g) {
   for (int l = 0; l < 6; ++l) {
     const int t = g.bctag[l];
-    if (t == 2 || t == 10 || (t == 6 && !(l == 2 ? g.wall_ymin : g.wall_ymax))) return true;
+    if (t == 2 || t == 7 || t == 10 || (t == 6 && !(l == 2 ? g.wall_ymin : g.wall_ymax))) return true;
   }
   return false;
 }

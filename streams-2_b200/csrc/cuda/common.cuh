@@ -46,6 +46,7 @@ struct Geom {
   int wall_ymin, wall_ymax;  // staggered isothermal walls (ghosts mirrored on the fly)
   int bctag[6], nr[6];       // boundary tags and non-reflecting types per face
   double winf[5], p0;        // free stream (non-reflecting type 3), reference pressure
+  double xshock_imp, shock_angle, tanhfacs, winf_past_shock[5];  // impinging shock (bctag[3] = 7)
   // recycling-rescaling inflow (bctag[0] = 10)
   int recyc, i_recyc, jbl_inflow;
   double betarecyc, rand_scale;

@@ -318,13 +318,53 @@ ChanPre chan_prop_pre(Setup& s) {
   return {rmb, tw_over_tr};
 }
 
+// set_oblique_shock (singleideal.F90:2953-3016): post-shock state of the impinging shock of
+// angle shock_angle through the free stream, and the tanh smoothing length at the top
+void set_oblique_shock(Setup& s) {
+  const IniFile& c = s.ini;
+  const double gam = s.gam, gm1 = s.gm1, mach = s.mach;
+  s.xshock_imp = c.get_double("flow", "xshock_imp") * s.l0;
+  s.shock_angle = c.get_double("flow", "shock_angle") * pi() / 180.0;
+  const double xshock_top = s.xshock_imp - s.yg(s.nymax) / std::tan(s.shock_angle);
+  std::vector<double> xg1(static_cast<size_t>(s.nxmax));
+  for (int i = 1; i <= s.nxmax; ++i) xg1[i - 1] = s.xg(i);
+  const int ig_shock = locateval(xg1.data(), s.nxmax, xshock_top);
+  if (ig_shock < 1) throw InputError("the shock meets the top boundary upstream of the domain");
+  s.tanhfacs = s.dxg(ig_shock);
+  const double sins = std::sin(s.shock_angle), coss = std::cos(s.shock_angle);
+  const double mach_normal = mach * sins;
+  const double mach_normal2 = mach_normal * mach_normal;
+  double mach_normal_past = (1.0 + 0.5 * gm1 * mach_normal2) / (gam * mach_normal2 - 0.5 * gm1);
+  mach_normal_past = std::sqrt(mach_normal_past);
+  const double vel_ratio = (2.0 + gm1 * mach_normal2) / ((gam + 1.0) * mach_normal2);
+  const double rho_ratio = 1.0 / vel_ratio;
+  const double p_ratio = 1.0 + 2.0 * gam / (gam + 1.0) * (mach_normal2 - 1.0);
+  const double t_ratio = p_ratio / rho_ratio;
+  const double defl_tan = 2.0 * coss / sins * ((mach * mach) * (sins * sins) - 1.0) /
+                          (2.0 + (mach * mach) * (gam + std::cos(2.0 * s.shock_angle)));
+  const double defl = std::atan(defl_tan);
+  const double mach_past = mach_normal_past / std::sin(s.shock_angle - defl);
+  const double t_past = s.t0 * t_ratio;
+  const double c_past = std::sqrt(gam * s.rgas0 * t_past);
+  const double u_past = mach_past * c_past * std::cos(defl);
+  const double v_past = mach_past * c_past * std::sin(defl);
+  const double rho_past = s.rho0 * rho_ratio;
+  const double e_past = e_from_t(s, t_past);
+  const double etot_past = e_past + 0.5 * (u_past * u_past + v_past * v_past);
+  s.winf_past_shock[0] = rho_past;
+  s.winf_past_shock[1] = rho_past * u_past;
+  s.winf_past_shock[2] = -rho_past * v_past;
+  s.winf_past_shock[3] = 0.0;
+  s.winf_past_shock[4] = rho_past * etot_past;
+}
+
 // set_flow_params (singleideal.F90:2776-2856) for the channel
 void set_flow_params(Setup& s, double reynolds_bulk_target) {
   const IniFile& c = s.ini;
   s.reynolds = c.get_double("flow", "Reynolds");
   s.mach = c.get_double("flow", "Mach");
   s.theta_wall = c.get_double("flow", "theta_wall");
-  if (s.bctags[3] == 7) throw InputError("oblique-shock top boundary (bc ymax = 7) is not supported yet");
+  if (s.bctags[3] == 7) set_oblique_shock(s);
   double gm1h = 0.5 * s.gm1;
   s.t_recovery = s.t0 * (1.0 + gm1h * s.rfac * (s.mach * s.mach));
   s.t_wall = s.theta_wall * (s.t_recovery - s.t0) + s.t0;
@@ -846,7 +886,7 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
   }
   for (int l = 0; l < 6; ++l) {
     const int t = s.bctags[l];
-    if (t != 0 && t != 2 && t != 6 && t != 10)
+    if (t != 0 && t != 2 && t != 6 && t != 10 && !(t == 7 && l == 3))
       throw InputError("boundary tag " + std::to_string(t) + " is not supported by the B200 backend yet");
     const int nr = s.bctags_nr[l];
     if (nr != 0 && nr != 1 && nr != 2 && nr != 3 && nr != 6)
@@ -987,6 +1027,8 @@ void Setup::fill_params(streams_b200_params* p, int precision) const {
   p->betarecyc = betarecyc;
   p->rng_seed = rng_seed;
   p->rng_draws = rng_draws;
+  p->xshock_imp = xshock_imp; p->shock_angle = shock_angle; p->tanhfacs = tanhfacs;
+  for (int m = 0; m < 5; ++m) p->winf_past_shock[m] = winf_past_shock[m];
 }
 
 void Setup::fill_grid(streams_b200_grid* g) const {

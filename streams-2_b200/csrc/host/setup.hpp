@@ -99,6 +99,9 @@ struct Setup {
   // recycling plane's random perturbations from it at every stage
   unsigned rng_seed = 1;
   long long rng_draws = 0;
+  // impinging oblique shock (bc ymax = 7, set_oblique_shock singleideal.F90:2953-3016)
+  double xshock_imp = 0, shock_angle = 0, tanhfacs = 1;
+  double winf_past_shock[5] = {0, 0, 0, 0, 0};
 
   // initial conserved field w(1-ng:nx+ng,1-ng:ny+ng,1-ng:nz+ng,5), Fortran order
   std::vector<double> w;

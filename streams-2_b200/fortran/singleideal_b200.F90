@@ -72,6 +72,8 @@ contains
       p%bctags_nr = eb%bctags_nr ; p%winf = eb%winf ; p%p0 = eb%p0
       p%recyc = merge(1, 0, eb%recyc) ; p%i_recyc = eb%i_recyc ; p%jbl_inflow = eb%jbl_inflow
       p%betarecyc = eb%betarecyc
+      p%xshock_imp = eb%xshock_imp ; p%shock_angle = eb%shock_angle ; p%tanhfacs = eb%tanhfacs
+      p%winf_past_shock = eb%winf_past_shock
       ! the crandom sequence continues on the device: seed of this rank and the draws taken so far
       p%rng_seed = self%myrank + 1 ; p%rng_draws = self%crandom_draws
       allocate(self%epx(0:f%nx), self%epy(0:f%ny), self%epz(0:f%nz))

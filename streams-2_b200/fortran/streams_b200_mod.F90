@@ -36,6 +36,8 @@ module streams_b200_mod
     real(c_double) :: betarecyc
     integer(c_int) :: rng_seed
     integer(c_long_long) :: rng_draws
+    real(c_double) :: xshock_imp, shock_angle, tanhfacs
+    real(c_double) :: winf_past_shock(5)
   end type streams_b200_params
 
   type, bind(c) :: streams_b200_grid

@@ -53,6 +53,8 @@ class Params(C.Structure):
         ("bctags_nr", C.c_int * 6), ("winf", C.c_double * 5), ("p0", C.c_double),
         ("recyc", C.c_int), ("i_recyc", C.c_int), ("jbl_inflow", C.c_int),
         ("betarecyc", C.c_double), ("rng_seed", C.c_uint), ("rng_draws", C.c_longlong),
+        ("xshock_imp", C.c_double), ("shock_angle", C.c_double), ("tanhfacs", C.c_double),
+        ("winf_past_shock", C.c_double * 5),
     ]
 
 

@@ -115,7 +115,8 @@ def bl_ini(nx=64, ny=48, nz=16, *, lx=100.0, ly=12.0, lz=8.0, mach=2.0, reynolds
            reynolds_delta=None, theta_wall=1.0, visc_model=1, vt_exp=0.76, sensor=0.05, ep_order=6,
            weno_scheme=3, weno_version=0, amp=0.05, x_recyc=None, nr_outflow=1, nr_top=1, cfl=0.8,
            jbgrid=None, dyptarget=0.7, nywr=None, lywr=None, ysmoosteps=10, conservative_viscous=1,
-           num_iter=100, print_control=1, correct_bound_ord=1, rand_type=1) -> str:
+           num_iter=100, print_control=1, correct_bound_ord=1, rand_type=1, shock_angle=None,
+           xshock_imp=None) -> str:
     """Input file of a spatially developing supersonic boundary layer (the benchmark's boundary
     layer workload): box lx x ly x lz inflow thicknesses, BL grid (grid_type 4, wall-resolved part
     of nywr points up to lywr), recycling-rescaling inflow at xmin, extrapolation with a
@@ -132,6 +133,12 @@ def bl_ini(nx=64, ny=48, nz=16, *, lx=100.0, ly=12.0, lz=8.0, mach=2.0, reynolds
         lywr = 2.5
     if jbgrid is None:
         jbgrid = max(4.0, nywr / 4.0)
+    # an impinging oblique shock at the top (SBLI) replaces the top's extrapolation (tag 7)
+    ymax_tag, shock = (2, 0.0) if shock_angle is None else (7, shock_angle)
+    if shock_angle is not None:
+        nr_top = 0
+        if xshock_imp is None:
+            xshock_imp = 0.6 * lx
     return f"""[grid]
 grid_dim = 1
 domain_size_x = {lx!r}
@@ -153,7 +160,7 @@ ysmoosteps = {ysmoosteps}
 xmin = 10
 xmax = 2
 ymin = 6
-ymax = 2
+ymax = {ymax_tag}
 zmin = 0
 zmax = 0
 xmin_nr = 0
@@ -193,8 +200,8 @@ flow_init = 1
 Mach = {mach!r}
 Reynolds = {reynolds_tau!r}
 theta_wall = {theta_wall!r}
-xshock_imp = 0.
-shock_angle = 0.
+xshock_imp = {xshock_imp if xshock_imp is not None else 0.0!r}
+shock_angle = {shock!r}
 T_ref = 220.
 aoa = 0.
 

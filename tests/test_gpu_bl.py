@@ -1,7 +1,8 @@
 """The boundary-layer boundary set on the GPU against the oracle: recycling-rescaling inflow
 (z-shifted recycling plane, spanwise means, inner/outer rescaling, random plane drawn from the
 continued glibc sequence every stage), zeroth-order extrapolation with the characteristic
-non-reflecting correction at the outflow and top, and the node-based isothermal wall.
+non-reflecting correction at the outflow and top, the node-based isothermal wall, and the
+impinging oblique shock at the top (shock / boundary-layer interaction).
 
 Bounds as for the channel: relative L2 of every conserved variable <= 1e-12 after one step and
 <= 1e-11 after 100 steps (FP64), including the stored inflow ghost planes.
@@ -51,9 +52,12 @@ def compare(o, s, tol):
     return errs
 
 
+SBLI = dict(mach=2.28, shock_angle=32.6, lx=60.0)  # an 8-degree deflection at Mach 2.28
+
+
 @pytest.mark.parametrize("kw", [dict(), dict(nr_outflow=2, nr_top=3), dict(nr_outflow=6, nr_top=1),
-                                dict(sensor=-1.0), dict(conservative_viscous=0)],
-                         ids=["nr1", "nr2_nr3", "nr6", "full_weno", "nonconservative"])
+                                dict(sensor=-1.0), dict(conservative_viscous=0), SBLI],
+                         ids=["nr1", "nr2_nr3", "nr6", "full_weno", "nonconservative", "sbli"])
 def test_bl_one_step(kw, tmp_path):
     o, s = pair(tmp_path, bl(**kw), 1)
     compare(o, s, 1e-12)
@@ -61,8 +65,9 @@ def test_bl_one_step(kw, tmp_path):
     assert abs(sg["dt"] - so["dt"]) <= 1e-12 * so["dt"]
 
 
-def test_bl_hundred_steps(tmp_path):
-    o, s = pair(tmp_path, bl(), 100)
+@pytest.mark.parametrize("kw", [dict(), SBLI], ids=["bl", "sbli"])
+def test_bl_hundred_steps(kw, tmp_path):
+    o, s = pair(tmp_path, bl(**kw), 100)
     compare(o, s, 1e-11)
 
 
