@@ -1,22 +1,28 @@
 #!/usr/bin/env python
 """Benchmark of the B200 backend: throughput of the per-RK-stage RHS + update of the Cartesian
-channel in Mcell-steps/s (1 cell-step = one interior cell advanced one full RK3 step).
+solver in Mcell-steps/s (1 cell-step = one interior cell advanced one full RK3 step).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size NXxNYxNZ]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload bl|channel|sbli] [--size NXxNYxNZ]
 
-Default workload: the supersonic turbulent channel of the benchmark suite at its largest
-single-GPU size, 512x256x256 (the enlarged channel), in FP64: domain 2pi x 2 x pi, tanh-stretched
-staggered y (factor 1.5), isothermal walls, gamma 1.4, Pr 0.72, power-law viscosity 0.76, bulk
-Mach 1.5, bulk Reynolds 3000 with bulk-flow and bulk-temperature forcing, hybrid 6th-order central /
-WENO5 with Ducros threshold 0.05, CFL 0.8.  Seeded synthetic initial field: Poiseuille u (peak
-1.5 u_b), v = w = 0, uniform density and wall temperature, +-10% uniform random velocity noise.
+Default workload (--workload bl): the Mach 2 spatially developing turbulent boundary layer of the
+benchmark suite at its size, 1024x256x192, FP64: box 100 x 12 x 8 inflow thicknesses, BL grid
+(wall-resolved tanh-law part plus geometric stretching), recycling-rescaling inflow, zeroth-order
+extrapolation with characteristic non-reflecting outflow and top, isothermal wall at the recovery
+temperature, periodic z, power-law viscosity, hybrid 6th-order central / WENO5 with Ducros
+threshold 0.05, CFL 0.8.  Seeded synthetic initial field: 1/7 power-law mean velocity,
+Crocco-Busemann temperature, +-5 % uniform random velocity noise (no dataset exists).
+--workload channel is the supersonic channel at 512x256x256 (Mach_b 1.5, Re_b 3000, Poiseuille +
++-10 % noise); --workload sbli the Mach 2.28 shock / boundary-layer interaction at 1024x256x128.
 
 The b200 arm prints one JSON line with: device-timed throughput (value, CUDA events on the
 context's stream, max over ranks), the end-to-end throughput through the C ABI with pinned host
 buffers (e2e), the roofline of the dominant kernel from live per-kernel CUDA events, the CPU
-oracle timed on the host cores (cpu_baseline), and the SM clocks sampled during the timed region.
-With --gpus N > 1 each rank advances an independent replica (the path has no exchange step).
---impl reference times the CPU restatement of the reference's CPU backend (oracle/) on the host.
+oracle timed on the host cores (cpu_baseline), the SM clocks sampled during the timed region, the
+mixed-precision form on the three workloads, the batched form (48 channel boxes) and the served
+form (a Poisson stream of solves).  With --gpus N > 1 each rank advances an independent replica
+(the path has no exchange step).  --impl reference times the CPU restatement of the reference's
+CPU backend (oracle/) on the host.
 """
 from __future__ import annotations
 
@@ -121,6 +127,29 @@ def channel_case_ini(nx, ny, nz, steps, **kw):
     return channel_ini(nx, ny, nz, num_iter=steps, print_control=max(1, steps), **kw)
 
 
+# Boundary-layer workload: Mach 2 spatially developing turbulent boundary layer, box 100 x 12 x 8
+# inflow thicknesses, BL grid, recycling-rescaling inflow, non-reflecting outflow and top,
+# isothermal wall at the recovery temperature, periodic z; the SBLI variant adds an impinging
+# shock of 8-degree deflection at Mach 2.28 on the top boundary.
+SBLI_KW = dict(mach=2.28, shock_angle=32.6)
+
+
+def bl_case_ini(nx, ny, nz, steps, **kw):
+    from streams_b200.cases import bl_ini
+    return bl_ini(nx, ny, nz, num_iter=steps, print_control=max(1, steps), **kw)
+
+
+def case_ini(workload, nx, ny, nz, steps):
+    if workload == "channel":
+        return channel_case_ini(nx, ny, nz, steps)
+    if workload == "sbli":
+        return bl_case_ini(nx, ny, nz, steps, **SBLI_KW)
+    return bl_case_ini(nx, ny, nz, steps)
+
+
+DEFAULT_SIZE = {"bl": "1024x256x192", "channel": "512x256x256", "sbli": "1024x256x128"}
+
+
 def run_batched(torch, precision, steps, warmup, tune_cache):
     """The batched form: 48 channel boxes of uneven grids and flow parameters (seeded mix),
     autotuned launch shapes, one CUDA graph per 10 steps of all boxes.  Device time from CUDA
@@ -202,10 +231,10 @@ def run_serving(torch, duration_s, step_scale, single_rate, tune_cache):
             "host_batch_build_s": out["batch_build_s"]}
 
 
-def cpu_oracle_rate(nx, ny, nz, nsteps, budget_s=20.0):
+def cpu_oracle_rate(workload, nx, ny, nz, nsteps, budget_s=20.0):
     """Oracle (restated CPU backend) throughput on a slab of the workload: all host threads."""
     from oracle_py import Oracle
-    ini = channel_case_ini(nx, ny, nz, nsteps)
+    ini = case_ini(workload, nx, ny, nz, nsteps)
     with tempfile.TemporaryDirectory() as d:
         o = Oracle(d, ini)
         o.init_run()
@@ -235,7 +264,7 @@ def run_reference(args):
     sx, sy, sz = sample_dims(nx, ny, nz)
     from oracle_py import Oracle
     threads = os.environ.get("ORACLE_THREADS") or str(os.cpu_count() or 1)
-    ini = channel_case_ini(sx, sy, sz, args.steps)
+    ini = case_ini(args.workload, sx, sy, sz, args.steps)
     with tempfile.TemporaryDirectory() as d:
         o = Oracle(d, ini)
         o.init_run()
@@ -250,9 +279,10 @@ def run_reference(args):
         "impl": "reference", "metric": "Mcell-steps/s", "value": value, "unit": "Mcell-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(nx, ny, nz),
+        "config": workload_config(args.workload, nx, ny, nz),
         "cpu_baseline": {"value": value, "unit": "Mcell-steps/s", "cores": int(threads), "kind": "port",
-                         "sample": f"{sx}x{sy}x{sz} slab of the {nx}x{ny}x{nz} channel, {args.steps} RK3 steps"},
+                         "sample": f"{sx}x{sy}x{sz} slab of the {nx}x{ny}x{nz} {args.workload}, "
+                                   f"{args.steps} RK3 steps"},
         "e2e": {"value": value, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's Fortran/MPI CPU backend cannot be built on this image (no Fortran compiler, "
                 "no MPI); this arm times the C++ restatement of that backend (oracle/), pinned to the "
@@ -262,10 +292,18 @@ def run_reference(args):
     return 0
 
 
-def workload_config(nx, ny, nz):
-    return {"workload": f"supersonic channel {nx}x{ny}x{nz} FP64, hybrid central-6/WENO5 (Ducros 0.05), "
-                        "Mach_b 1.5, Re_b 3000, power-law mu, CFL 0.8",
-            "grid": [nx, ny, nz], "cells": nx * ny * nz, "precision": "fp64",
+def workload_config(workload, nx, ny, nz):
+    if workload == "channel":
+        desc = (f"supersonic channel {nx}x{ny}x{nz} FP64, hybrid central-6/WENO5 (Ducros 0.05), "
+                "Mach_b 1.5, Re_b 3000, power-law mu, CFL 0.8")
+    elif workload == "sbli":
+        desc = (f"Mach 2.28 shock / boundary-layer interaction {nx}x{ny}x{nz} FP64, 8-degree impinging shock, "
+                "recycling inflow, NR outflow, hybrid central-6/WENO5 (Ducros 0.05), CFL 0.8")
+    else:
+        desc = (f"Mach 2 spatially developing boundary layer {nx}x{ny}x{nz} FP64, box 100x12x8 delta, "
+                "recycling-rescaling inflow, NR outflow and top, isothermal wall at T_recovery, "
+                "hybrid central-6/WENO5 (Ducros 0.05), power-law mu, CFL 0.8")
+    return {"workload": desc, "grid": [nx, ny, nz], "cells": nx * ny * nz, "precision": "fp64",
             "l2_policy": "inputs larger than L2 (state ~12 x 8 B per cell)"}
 
 
@@ -275,7 +313,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--size", default="512x256x256")
+    ap.add_argument("--workload", default="bl", choices=["bl", "channel", "sbli"])
+    ap.add_argument("--size", default=None, help="NXxNYxNZ (default: the workload's benchmark size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form measurement")
@@ -286,6 +325,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.size is None:
+        args.size = DEFAULT_SIZE[args.workload]
     if args.impl == "reference":
         return run_reference(args)
 
@@ -307,7 +348,7 @@ def main():
     nx, ny, nz = parse_size(args.size)
     ncell = nx * ny * nz
     with tempfile.TemporaryDirectory() as d:
-        case = Case(d, channel_case_ini(nx, ny, nz, args.steps))
+        case = Case(d, case_ini(args.workload, nx, ny, nz, args.steps))
     info = case.info()
     s = Solver.from_case(case)
     s.init_run()
@@ -400,25 +441,28 @@ def main():
     e2e_val = ncell * args.steps * world / (e2e_ms / 1e3) / 1e6
     s2.close()
 
-    # mixed form (FP32 fluxes, FP64 state): throughput on the same workload, and its error against
-    # the FP64 form after 100 steps of the 128x96x64 channel (relative L2 per conserved variable)
-    mixed = None
-    if not args.no_mixed:
-        sm = Solver.from_case(case, precision=1)
-        sm.init_run()
-        sm.advance(args.warmup, 1, 0, 0)
-        stm = torch.cuda.ExternalStream(sm.stream_handle)
-        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # mixed form (FP32 fluxes, FP64 state): throughput on the headline workload and on the two
+    # mixed-precision workloads (the channel at 512x256x256, the shock / boundary-layer interaction at
+    # 1024x256x128), each with its error against the FP64 form after 100 steps of a smaller case
+    def device_rate(cs, precision):
+        sv = Solver.from_case(cs, precision=precision)
+        sv.init_run()
+        sv.advance(args.warmup, 1, 0, 0)
+        st_ = torch.cuda.ExternalStream(sv.stream_handle)
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
-        m0.record(stm)
-        sm.advance(args.steps, 1, args.warmup, 0)
-        m1.record(stm)
-        sm.synchronize()
-        mms = max_over_ranks(m0.elapsed_time(m1))
-        mval = ncell * args.steps * world / (mms / 1e3) / 1e6
-        sm.close()
+        a0.record(st_)
+        sv.advance(args.steps, 1, args.warmup, 0)
+        a1.record(st_)
+        sv.synchronize()
+        t_ms = max_over_ranks(a0.elapsed_time(a1))
+        n_ = cs.shape[0] * cs.shape[1] * cs.shape[2]
+        sv.close()
+        return n_ * args.steps * world / (t_ms / 1e3) / 1e6, t_ms
+
+    def mixed_error(wl, dims):
         with tempfile.TemporaryDirectory() as d:
-            c0 = Case(d, channel_case_ini(128, 96, 64, 100))
+            c0 = Case(d, case_ini(wl, *dims, 100))
         fields = []
         for prec in (0, 1):
             sv = Solver.from_case(c0, precision=prec)
@@ -426,10 +470,31 @@ def main():
             sv.advance(100, 1, 0, 0)
             fields.append(sv.copy_to_field()[:, 3:-3, 3:-3, 3:-3])
             sv.close()
-        errs = [float(np.linalg.norm(fields[1][m] - fields[0][m]) / np.linalg.norm(fields[0][m])) for m in range(5)]
+        return [float(np.linalg.norm(fields[1][m] - fields[0][m]) / np.linalg.norm(fields[0][m])) for m in range(5)]
+
+    small = {"bl": (128, 64, 32), "channel": (128, 96, 64), "sbli": (128, 64, 32)}
+    mixed = None
+    if not args.no_mixed:
+        mval, mms = device_rate(case, 1)
+        errs = mixed_error(args.workload, small[args.workload])
         mixed = {"value": mval, "unit": "Mcell-steps/s", "ms_per_step": mms / args.steps, "speedup_vs_fp64": mval / value,
-                 "rel_l2_vs_fp64_100_steps_128x96x64": errs, "max_rel_l2": max(errs),
-                 "precision": "FP32 flux/viscous arithmetic, FP64 state, RK register, T recovery, dt, reductions"}
+                 "rel_l2_vs_fp64_100_steps": errs, "error_case": "x".join(map(str, small[args.workload])),
+                 "max_rel_l2": max(errs),
+                 "precision": "FP32 flux/viscous arithmetic, FP64 state, RK register, T recovery, sensor, dt, "
+                              "reductions"}
+        for wl in ("channel", "sbli"):
+            if wl == args.workload:
+                continue
+            dims = parse_size(DEFAULT_SIZE[wl])
+            with tempfile.TemporaryDirectory() as d:
+                cw = Case(d, case_ini(wl, *dims, args.steps))
+            f64, _ = device_rate(cw, 0)
+            f32, _ = device_rate(cw, 1)
+            e = mixed_error(wl, small[wl])
+            mixed[f"{wl}_{DEFAULT_SIZE[wl]}"] = {
+                "fp64": f64, "mixed": f32, "speedup_vs_fp64": f32 / f64, "rel_l2_vs_fp64_100_steps": e,
+                "error_case": "x".join(map(str, small[wl])), "max_rel_l2": max(e)}
+            del cw
 
     # batched and served forms (rank 0 of a replica run measures them on its own GPU)
     tune_cache = {}
@@ -451,11 +516,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             sx, sy, sz = sample_dims(nx, ny, nz)
-            rate, nst, sec = cpu_oracle_rate(sx, sy, sz, 5)
+            rate, nst, sec = cpu_oracle_rate(args.workload, sx, sy, sz, 5)
             cpu = {"value": rate, "unit": "Mcell-steps/s", "cores": int(os.environ.get("ORACLE_THREADS") or
                                                                        (os.cpu_count() or 1)),
-                   "kind": "port", "sample": f"{sx}x{sy}x{sz} slab of the {nx}x{ny}x{nz} channel, {nst} RK3 steps "
-                                             f"in {sec:.1f} s"}
+                   "kind": "port", "sample": f"{sx}x{sy}x{sz} slab of the {nx}x{ny}x{nz} {args.workload}, "
+                                             f"{nst} RK3 steps in {sec:.1f} s"}
         except Exception as e:  # the baseline is reported, not required
             cpu = {"value": None, "unit": "Mcell-steps/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
 
@@ -466,7 +531,7 @@ def main():
             "metric": "Mcell-steps/s", "value": value, "unit": "Mcell-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(nx, ny, nz),
+            "config": workload_config(args.workload, nx, ny, nz),
             "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": nbytes / args.steps,
                     "d2h_bytes_per_step": (nbytes + 56 * args.steps) / args.steps, "wall_s": wall,
                     "what": "copy_from_field (pinned) + init_run + K x (rk step + scalar read) + copy_to_field"},
