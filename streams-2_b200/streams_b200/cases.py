@@ -252,12 +252,30 @@ def batch_mix(nboxes: int = 48, seed: int = 2024) -> list[dict]:
     return out
 
 
+def shock_angle_for(mach: float, deflection_deg: float = 8.0, gam: float = 1.4) -> float:
+    """Weak-shock angle [deg] of the theta-beta-Mach relation for a given flow deflection."""
+    th = math.radians(deflection_deg)
+
+    def f(b):
+        return 2.0 / math.tan(b) * (mach ** 2 * math.sin(b) ** 2 - 1.0) / (mach ** 2 * (gam + math.cos(2 * b)) + 2.0) - math.tan(th)
+    lo, hi = math.asin(1.0 / mach) + 1e-9, math.radians(64.0)
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if f(mid) > 0.0:
+            hi = mid
+        else:
+            lo = mid
+    return math.degrees(0.5 * (lo + hi))
+
+
 def serve_mix(nreq: int, rate_per_s: float, seed: int = 7, cells_min: int = 48 ** 3,
-              cells_max: int = 384 * 192 * 128, steps=(200, 2000), mixed_fraction: float = 0.5) -> list[dict]:
-    """A Poisson stream of channel solve requests: arrival offsets with exponential gaps at
-    rate_per_s, grids log-uniform in cell count between cells_min and cells_max (aspect
-    2:1:1 rounded to multiples of 16), bulk Mach uniform in [0.5, 2.5], step counts uniform in
-    `steps`, and FP64 or mixed precision."""
+              cells_max: int = 384 * 192 * 128, steps=(200, 2000), mixed_fraction: float = 0.5,
+              sbli_fraction: float = 0.3) -> list[dict]:
+    """A Poisson stream of solve requests: arrival offsets with exponential gaps at rate_per_s;
+    70 % channels and 30 % shock / boundary-layer interactions (an 8-degree impinging shock);
+    grids log-uniform in cell count between cells_min and cells_max (aspect 2:1:1 rounded to
+    multiples of 16); Mach uniform in [0.5, 2.5] (channels, bulk Mach) or [1.8, 2.5] (SBLI, where
+    the 8-degree shock stays attached); step counts uniform in `steps`; FP64 or mixed precision."""
     rng = random.Random(seed)
     t = 0.0
     out = []
@@ -268,7 +286,13 @@ def serve_mix(nreq: int, rate_per_s: float, seed: int = 7, cells_min: int = 48 *
         nx = max(32, int(round(2 * base / 16)) * 16)
         ny = max(32, int(round(base / 16)) * 16)
         nz = max(32, int(round(base / 16)) * 16)
-        out.append(dict(rid=r, arrival=t, nx=nx, ny=ny, nz=nz, mach=round(rng.uniform(0.5, 2.5), 6),
-                        nsteps=rng.randint(*steps), precision=1 if rng.random() < mixed_fraction else 0,
-                        seed=r + 1))
+        sbli = rng.random() < sbli_fraction
+        mach = round(rng.uniform(1.8, 2.5) if sbli else rng.uniform(0.5, 2.5), 6)
+        req = dict(rid=r, arrival=t, nx=nx, ny=ny, nz=nz, mach=mach, nsteps=rng.randint(*steps),
+                   precision=1 if rng.random() < mixed_fraction else 0)
+        if sbli:
+            req.update(kind="sbli", shock_angle=round(shock_angle_for(mach), 6))
+        else:
+            req.update(kind="channel", seed=r + 1)
+        out.append(req)
     return out

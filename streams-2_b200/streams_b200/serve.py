@@ -25,7 +25,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import Batch, Case, Solver, lib
-from .cases import channel_ini
+from .cases import bl_ini, channel_ini
 
 
 @dataclass
@@ -53,9 +53,11 @@ def footprint_of(case: Case, precision: int) -> int:
 
 def prepare(req: dict, workdir: str) -> Case:
     """Host set-up of one request (runs in a worker thread; the C++ set-up releases the GIL)."""
-    kw = {k: v for k, v in req.items() if k not in ("rid", "arrival", "nsteps", "precision")}
+    kw = {k: v for k, v in req.items() if k not in ("rid", "arrival", "nsteps", "precision", "kind")}
     d = os.path.join(workdir, f"req{req['rid']}")
     os.makedirs(d, exist_ok=True)
+    if req.get("kind", "channel") == "sbli":
+        return Case(d, bl_ini(num_iter=req["nsteps"], **kw))
     return Case(d, channel_ini(num_iter=req["nsteps"], **kw))
 
 

@@ -22,6 +22,18 @@ def test_serve_mix_is_a_poisson_stream():
     for r in reqs:
         assert 32 <= r["ny"] and r["nx"] % 16 == 0 and 0.5 <= r["mach"] <= 2.5
         assert 200 <= r["nsteps"] <= 2000 and r["precision"] in (0, 1)
+    frac = sum(r["kind"] == "sbli" for r in reqs) / len(reqs)
+    assert 0.2 < frac < 0.4
+
+
+def test_shock_angle_gives_the_deflection():
+    import math
+    from streams_b200.cases import shock_angle_for
+    for m in (1.8, 2.0, 2.28, 2.5):
+        b = math.radians(shock_angle_for(m))
+        th = math.atan(2.0 / math.tan(b) * (m * m * math.sin(b) ** 2 - 1.0) / (m * m * (1.4 + math.cos(2 * b)) + 2.0))
+        assert abs(math.degrees(th) - 8.0) < 1e-6
+    assert abs(shock_angle_for(2.28) - 32.6) < 0.5
 
 
 def test_admission_is_fifo_by_footprint():
