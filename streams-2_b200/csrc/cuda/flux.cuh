@@ -113,21 +113,21 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
         bm[l] = betascale * bm[l];
       }
       if (version == 0) {
-        R sump = R(0), summ = R(0);
+        // omega_l = (d_l / t_l) / sum_k (d_k / t_k), t_l = (eps + beta_l)^2, formed with one
+        // division per side: omega_l = d_l prod_{m != l} t_m / sum_k d_k prod_{m != k} t_m
+        // (the same weights; the products stay far inside the exponent range for eps = 1e-6)
+        R tp[3], tm[3];
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
-          R tp = eps6 + bp[l], tm = eps6 + bm[l];
-          bp[l] = dwe[l] / (tp * tp);
-          bm[l] = dwe[l] / (tm * tm);
-          sump = sump + bp[l];
-          summ = summ + bm[l];
+          const R a = eps6 + bp[l], b = eps6 + bm[l];
+          tp[l] = a * a;
+          tm[l] = b * b;
         }
-        const R rsp = R(1) / sump, rsm = R(1) / summ;
-#pragma unroll
-        for (int l = 0; l < 3; ++l) {
-          bp[l] = bp[l] * rsp;
-          bm[l] = bm[l] * rsm;
-        }
+        const R np0 = dwe[0] * (tp[1] * tp[2]), np1 = dwe[1] * (tp[0] * tp[2]), np2 = dwe[2] * (tp[0] * tp[1]);
+        const R nm0 = dwe[0] * (tm[1] * tm[2]), nm1 = dwe[1] * (tm[0] * tm[2]), nm2 = dwe[2] * (tm[0] * tm[1]);
+        const R rsp = R(1) / ((np0 + np1) + np2), rsm = R(1) / ((nm0 + nm1) + nm2);
+        bp[0] = np0 * rsp; bp[1] = np1 * rsp; bp[2] = np2 * rsp;
+        bm[0] = nm0 * rsm; bm[1] = nm1 * rsm; bm[2] = nm2 * rsm;
       } else {
         // eps40 is a single-precision literal in the reference
         const R eps40 = R(static_cast<double>(1.e-35f));
@@ -232,7 +232,9 @@ __device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>&
 #pragma unroll
   for (int q = 0; q < 2 * S; ++q) {
     pp[q] = st.t[q] * st.rho[q] * rgas0;
-    ee[q] = st.h[q] - pp[q] / st.rho[q] - R(0.5) * (st.u[q] * st.u[q] + st.v[q] * st.v[q] + st.w[q] * st.w[q]);
+    // e = H - p/rho - |u|^2/2 with p/rho = R T taken directly (the reference divides p by rho;
+    // the two differ in the last bit only and the division is the costliest operation here)
+    ee[q] = st.h[q] - st.t[q] * rgas0 - R(0.5) * (st.u[q] * st.u[q] + st.v[q] * st.v[q] + st.w[q] * st.w[q]);
   }
   R ft1 = 0, ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
   R lt1 = 0, lt2 = 0, lt3 = 0, lt4 = 0, lt5 = 0, lt6 = 0;  // compensation (mixed form)
