@@ -320,7 +320,7 @@ __device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>&
 // of |u_n -+ c| (:614-675) and wenorec_1d; back-projection with the right eigenvectors (:677-683).
 template <class R, int DIR, int WS, int S>
 __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5],
-                                          R (&fl)[5]) {
+                                          R (&fl)[5], R* __restrict__ gs, int gstride) {
   const R rgas0 = R(g.rgas0);
   const int o0 = S - 1, o1 = S;  // the two points adjacent to the face
   // Roe average
@@ -363,87 +363,88 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   }
   const R betascale_a = R(1) / (R(g.rho0) * R(g.rho0) * (R(g.u0) * R(g.u0)));
   const R betascale_b = R(1) / (R(g.rho0) * R(g.rho0) * (R(g.u0) * R(g.u0)) * (R(g.u0) * R(g.u0)));
+  // Projection of the stencil's conserved states U and fluxes F onto the five characteristic
+  // fields, point by point, using the structure of the left eigenvectors (the reference forms
+  // the five dot products el(:,m).U one field at a time): with dq = Roe velocity . X(2:4),
+  // s = b1 X1 + b2 (X5 - dq) and a = ci (vn X1 - X(normal momentum)),
+  //   P1 = (s + a)/2, P2 = X1 - s, P3 = X(t1) - v_t1 X1, P4 = X(t2) - v_t2 X1, P5 = (s - a)/2.
+  // The split values g+- = (P(F) +- lambda_m P(U))/2 of every point and field go to this
+  // thread's scratch gs[((m*2WS + l)*2 + side) * gstride].
+  const R lam[5] = {ev0, ev1, ev1, ev1, ev4};
+  const R vel[3] = {uu, vv, ww};
 #pragma unroll
-  for (int m = 0; m < 5; ++m) fh[m] = fl[m] = R(0);
-  // one characteristic field per iteration; the loop is kept rolled so that the reconstruction
-  // is emitted once (the unrolled form overflows the instruction cache)
+  for (int l = 0; l < 2 * WS; ++l) {
+    const int q = l + S - WS;
+    const R rr = st.rho[q], u1 = st.u[q], v1 = st.v[q], w1 = st.w[q], h1 = st.h[q];
+    const R vq[3] = {u1, v1, w1};
+    const R rhovn = rr * vq[DIR];
+    const R pp = rr * st.t[q] * rgas0;
+    R U[5], F[5];
+    U[0] = rr; U[1] = rr * u1; U[2] = rr * v1; U[3] = rr * w1; U[4] = rr * h1 - pp;
+    F[0] = rhovn; F[1] = u1 * rhovn; F[2] = v1 * rhovn; F[3] = w1 * rhovn; F[4] = h1 * rhovn;
+    F[1 + DIR] = F[1 + DIR] + pp;
+    R PU[5], PF[5];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const R* X = side == 0 ? U : F;
+      R* P = side == 0 ? PU : PF;
+      const R dq = uu * X[1] + vv * X[2] + ww * X[3];
+      const R sv = b1 * X[0] + b2 * (X[4] - dq);
+      const R av = ci * (vn * X[0] - X[1 + DIR]);
+      P[0] = R(0.5) * (sv + av);
+      P[1] = X[0] - sv;
+      P[2] = X[1 + t1] - vel[t1] * X[0];
+      P[3] = X[1 + t2] - vel[t2] * X[0];
+      P[4] = R(0.5) * (sv - av);
+    }
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      const R cm = R(0.5) * (PF[m] + lam[m] * PU[m]);
+      gs[((m * 2 * WS + l) * 2) * gstride] = cm;
+      gs[((m * 2 * WS + l) * 2 + 1) * gstride] = PF[m] - cm;
+    }
+  }
+  // reconstruction, one characteristic field per iteration (rolled: one copy of wenorec)
+  R fi[5];
 #pragma unroll 1
   for (int m = 0; m < 5; ++m) {
-    // column m of the left eigenvector matrix el(1:5, m)
-    R e0, e1, e2, e3, e4;
-    if (m == 0 || m == 4) {
-      const R sgn = m == 0 ? R(1) : R(-1);
-      e0 = R(0.5) * (b1 + sgn * (vn * ci));
-      e1 = R(-0.5) * (DIR == 0 ? b2 * uu + sgn * ci : b2 * uu);
-      e2 = R(-0.5) * (DIR == 1 ? b2 * vv + sgn * ci : b2 * vv);
-      e3 = R(-0.5) * (DIR == 2 ? b2 * ww + sgn * ci : b2 * ww);
-      e4 = R(0.5) * b2;
-    } else if (m == 1) {
-      e0 = R(1) - b1; e1 = b2 * uu; e2 = b2 * vv; e3 = b2 * ww; e4 = -b2;
-    } else {
-      const int tt_ = m == 2 ? t1 : t2;
-      e0 = -(tt_ == 0 ? uu : (tt_ == 1 ? vv : ww));
-      e1 = tt_ == 0 ? R(1) : R(0);
-      e2 = tt_ == 1 ? R(1) : R(0);
-      e3 = tt_ == 2 ? R(1) : R(0);
-      e4 = R(0);
-    }
-    const R evm = m == 0 ? ev0 : (m == 4 ? ev4 : ev1);
     R gp[2 * WS], gm[2 * WS];
 #pragma unroll
     for (int l = 0; l < 2 * WS; ++l) {
-      const int q = l + S - WS;
-      const R rr = st.rho[q], u1 = st.u[q], v1 = st.v[q], w1 = st.w[q], h1 = st.h[q];
-      const R vnq = DIR == 0 ? u1 : (DIR == 1 ? v1 : w1);
-      const R rhovn = rr * vnq;
-      const R pp = rr * st.t[q] * rgas0;
-      R f1 = u1 * rhovn, f2 = v1 * rhovn, f3 = w1 * rhovn;
-      if (DIR == 0) f1 = f1 + pp;
-      if (DIR == 1) f2 = f2 + pp;
-      if (DIR == 2) f3 = f3 + pp;
-      const R f4 = h1 * rhovn;
-      R wc = R(0), gc = R(0);
-      wc = wc + e0 * rr;
-      gc = gc + e0 * rhovn;
-      wc = wc + e1 * rr * u1;
-      gc = gc + e1 * f1;
-      wc = wc + e2 * rr * v1;
-      gc = gc + e2 * f2;
-      wc = wc + e3 * rr * w1;
-      gc = gc + e3 * f3;
-      wc = wc + e4 * (rr * h1 - pp);
-      gc = gc + e4 * f4;
-      R cm = R(0.5) * (gc + evm * wc);
-      gp[l] = cm;
-      gm[l] = gc - cm;
+      gp[l] = gs[((m * 2 * WS + l) * 2) * gstride];
+      gm[l] = gs[((m * 2 * WS + l) * 2 + 1) * gstride];
     }
     const R bs = (m == 2 || m == 3) ? betascale_b : betascale_a;
-    const R fi = wenorec<R, WS>(gp, gm, ord, g.weno_version, bs);
-    // row m of the right eigenvector matrix er(m, 1:5)
-    R r0, r1, r2, r3, r4;
-    if (m == 0 || m == 4) {
-      const R sc = m == 0 ? -c : c;
-      r0 = R(1);
-      r1 = DIR == 0 ? uu + sc : uu;
-      r2 = DIR == 1 ? vv + sc : vv;
-      r3 = DIR == 2 ? ww + sc : ww;
-      r4 = m == 0 ? h - vn * c : h + vn * c;
-    } else if (m == 1) {
-      r0 = R(1); r1 = uu; r2 = vv; r3 = ww; r4 = b3;
-    } else {
-      const int tt_ = m == 2 ? t1 : t2;
-      r0 = R(0);
-      r1 = tt_ == 0 ? R(1) : R(0);
-      r2 = tt_ == 1 ? R(1) : R(0);
-      r3 = tt_ == 2 ? R(1) : R(0);
-      r4 = tt_ == 0 ? uu : (tt_ == 1 ? vv : ww);
-    }
-    acc_prod(fh[0], fl[0], r0, fi);
-    acc_prod(fh[1], fl[1], r1, fi);
-    acc_prod(fh[2], fl[2], r2, fi);
-    acc_prod(fh[3], fl[3], r3, fi);
-    acc_prod(fh[4], fl[4], r4, fi);
+    const R f = wenorec<R, WS>(gp, gm, ord, g.weno_version, bs);
+#pragma unroll
+    for (int mm = 0; mm < 5; ++mm)
+      if (mm == m) fi[mm] = f;
   }
+  // back-projection with the right eigenvectors, er(m,:) = (1, u - c n, h - vn c) for m = 1,
+  // (1, u, b3) for m = 2, (0, e_t, v_t) for m = 3, 4, (1, u + c n, h + vn c) for m = 5,
+  // accumulated term by term (compensated in the mixed form)
+#pragma unroll
+  for (int m = 0; m < 5; ++m) fh[m] = fl[m] = R(0);
+  acc_add(fh[0], fl[0], fi[0]);
+  acc_add(fh[0], fl[0], fi[1]);
+  acc_add(fh[0], fl[0], fi[4]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    acc_prod(fh[1 + d], fl[1 + d], vel[d], fi[0]);
+    acc_prod(fh[1 + d], fl[1 + d], vel[d], fi[1]);
+    acc_prod(fh[1 + d], fl[1 + d], vel[d], fi[4]);
+    if (d == DIR) {
+      acc_prod(fh[1 + d], fl[1 + d], -c, fi[0]);
+      acc_prod(fh[1 + d], fl[1 + d], c, fi[4]);
+    }
+    if (d == t1) acc_add(fh[1 + d], fl[1 + d], fi[2]);
+    if (d == t2) acc_add(fh[1 + d], fl[1 + d], fi[3]);
+  }
+  acc_prod(fh[4], fl[4], h - vn * c, fi[0]);
+  acc_prod(fh[4], fl[4], b3, fi[1]);
+  acc_prod(fh[4], fl[4], vel[t1], fi[2]);
+  acc_prod(fh[4], fl[4], vel[t2], fi[3]);
+  acc_prod(fh[4], fl[4], h + vn * c, fi[4]);
 }
 
 }  // namespace sb200

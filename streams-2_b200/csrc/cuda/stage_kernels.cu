@@ -246,6 +246,18 @@ __device__ __forceinline__ R div3_at(const Geom& g, const R* __restrict__ d, int
   return d[iidx(g, i, j, k)];
 }
 
+// Per-thread scratch of the WENO characteristic projections (dynamic shared memory of the flux
+// kernels, 5 fields x 2WS points x 2 sides per thread, thread-interleaved)
+template <class R>
+__device__ __forceinline__ R* weno_scratch() {
+  extern __shared__ __align__(16) unsigned char sb_dyn_smem[];
+  return reinterpret_cast<R*>(sb_dyn_smem);
+}
+template <class R, int WS>
+constexpr size_t weno_scratch_bytes(int nthreads) {
+  return (size_t)nthreads * 5 * 2 * WS * 2 * sizeof(R);
+}
+
 template <int DIR>
 __device__ __forceinline__ int face_ep(const Geom& g, int p) {
   return DIR == 0 ? g.epx[p] : (DIR == 1 ? g.epy[p] : g.epz[p]);
@@ -255,7 +267,7 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
 // hi + lo is the face flux (lo = 0 in the FP64 form).
 template <class R, int DIR, int LB, int WS, int S>
 __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& st, bool ishk, int p,
-                                            R (&hi)[5], R (&lo)[5]) {
+                                            R (&hi)[5], R (&lo)[5], R* __restrict__ gs, int gstride) {
   const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
   const int ep = face_ep<DIR>(g, p);
   if (!ishk) {
@@ -264,7 +276,7 @@ __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& 
     central_flux<R, DIR, LB, S>(g, st, lmax, g.nkeep, zf, hi, lo);
   } else {
     const int ord = max(WS + ep, 1);
-    weno_flux<R, DIR, WS, S>(g, st, ord, hi, lo);
+    weno_flux<R, DIR, WS, S>(g, st, ord, hi, lo, gs, gstride);
   }
 }
 
@@ -313,7 +325,7 @@ __global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F)
     const long long base = gidx(g, p, j, k);
 #pragma unroll
     for (int q = 0; q < 2 * S; ++q) load_point<R, S>(g, st, q, aux, g.nvol, base + (q - (S - 1)));
-    window_flux<R, 0, LB, WS, S>(g, st, ishk, p, fh, fo);
+    window_flux<R, 0, LB, WS, S>(g, st, ishk, p, fh, fo, weno_scratch<R>() + threadIdx.y * XF_TX + lane, XF_NT);
   }
   R hu[5], lu[5];
 #pragma unroll
@@ -393,7 +405,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
       load_point<R, S>(g, st, NP - 1, aux, n, base0 + (long long)(c + S) * sd);
       mask = (mask >> 1) | (sensor_bit(c + WS) << (2 * WS - 1));
       R hhi[5], lhi[5];
-      window_flux<R, DIR, LB, WS, S>(g, st, mask != 0u, c, hhi, lhi);
+      window_flux<R, DIR, LB, WS, S>(g, st, mask != 0u, c, hhi, lhi, weno_scratch<R>() + threadIdx.x, MT_NT);
       if (c >= c0) {
         // cell c lies between the faces c-1 (lo) and c (hi)
         const long long ic = DIR == 1 ? iidx(g, i, c, b) : iidx(g, i, b, c);
@@ -1142,7 +1154,18 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   R* div3 = div3_of<R>(d);
   const bool fp64 = sizeof(R) == sizeof(double);
   if (a.run_aux) aux_launch<R>(g, d, a.apply_shift, 0, K_AUX, s, nl);
-  SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS><<<xg, xb, 0, s>>>(g, aux, sensor, fl_new));
+  const size_t xsm = weno_scratch_bytes<R, WS>(XF_NT), msm = weno_scratch_bytes<R, WS>(MT_NT);
+  // per instantiation and device: allow more than 48 KB of dynamic shared memory
+  static unsigned long long smem_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !(smem_set & (1ULL << dev))) {
+    cudaFuncSetAttribute(k_xflux<R, LB, WS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm);
+    cudaFuncSetAttribute(k_march<R, 1, LB, WS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+    cudaFuncSetAttribute(k_march<R, 2, LB, WS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+    smem_set |= 1ULL << dev;
+  }
+  SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS><<<xg, xb, xsm, s>>>(g, aux, sensor, fl_new));
   if (g.conservative_viscous)
     SB_LAUNCH(d, K_VISC, s,
               k_visc<R><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
@@ -1159,10 +1182,10 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   }
   if (gyb > 0)
     SB_LAUNCH(d, K_EULER_Y, s,
-              k_march<R, 1, LB, WS><<<gyb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
+              k_march<R, 1, LB, WS><<<gyb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                           a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
   SB_LAUNCH(d, K_EULER_Z, s,
-            k_march<R, 2, LB, WS><<<gzb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
+            k_march<R, 2, LB, WS><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                         a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
   *nl += 4;
   if (g.recyc) launch_rand_plane(g, d, s, nl);  // euler_z draws the inflow plane of the stage
