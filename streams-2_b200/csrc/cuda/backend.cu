@@ -309,7 +309,7 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
   if (g.recyc) {
     const size_t npl = (size_t)p->ny * p->nz * 3;
     if ((e = dev_alloc(c, &d.rplane, npl)) || (e = dev_alloc(c, &d.recyc_av, (size_t)p->ng * p->ny * 5)) ||
-        (e = dev_alloc(c, &d.rng, 1)))
+        (e = dev_alloc(c, &d.rng, 1)) || (e = dev_alloc(c, &d.rwords, npl)))
       return fail(e, "cudaMalloc(inflow state)");
     std::vector<double> half(npl, 0.5);  // recyc_prepare's neutral plane
     streams_b200::GlibcRand r(p->rng_seed);

@@ -190,25 +190,60 @@ __global__ void __launch_bounds__(BC_NT) k_recyc_fill(Geom g, double* __restrict
 
 // The random plane of one stage (euler_z's get_crandom_f on inflow_random_plane(2:jbl_inflow,
 // 1:nz, 1:3), singleideal_cpu.F90:841; first index outermost, code/third-party/crandom/
-// crandom_f.F90:81-93), drawn from the continued glibc sequence by one thread: the draws are
-// strictly sequential.
-__global__ void k_rand_plane(Geom g, RngState* __restrict__ st, double* __restrict__ rplane) {
+// crandom_f.F90:81-93), drawn from the continued glibc sequence.  The draws are strictly
+// sequential, so one thread produces the raw words (k_rand_words) and a second kernel converts
+// and scatters them in parallel (k_rand_scatter).  The 34-word ring is rotated into registers
+// so that slot s holds the word of the positions congruent to pos + s (mod 34); blocks of 34
+// draws are unrolled with compile-time slots: new word of slot s = slot (s+3) + slot (s+31).
+__global__ void k_rand_words(RngState* __restrict__ st, unsigned int* __restrict__ words, long long total) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  unsigned int ring[34];
-  for (int q = 0; q < 34; ++q) ring[q] = st->ring[q];
-  long long pos = st->pos;
-  const long long pn = (long long)g.ny * g.nz;
-  for (int j = 2; j <= g.jbl_inflow; ++j)
-    for (int k = 1; k <= g.nz; ++k)
-      for (int c = 0; c < 3; ++c) {
-        const unsigned int v = ring[(pos - 31) % 34] + ring[(pos - 3) % 34];
-        ring[pos % 34] = v;
-        ++pos;
-        const int r = (int)(v >> 1);
-        rplane[c * pn + (long long)(k - 1) * g.ny + (j - 1)] = g.rand_scale * (double)r / 2147483647.0;
-      }
-  for (int q = 0; q < 34; ++q) st->ring[q] = ring[q];
-  st->pos = pos;
+  unsigned int r[34];
+  const long long pos0 = st->pos;
+  const int p0 = (int)(pos0 % 34);
+#pragma unroll
+  for (int s = 0; s < 34; ++s) {
+    int idx = p0 + s;
+    if (idx >= 34) idx -= 34;
+    r[s] = st->ring[idx];
+  }
+  const long long nblk = total / 34;
+  for (long long b = 0; b < nblk; ++b) {
+#pragma unroll
+    for (int s = 0; s < 34; ++s) {
+      r[s] = r[(s + 3) % 34] + r[(s + 31) % 34];
+      words[b * 34 + s] = r[s] >> 1;
+    }
+  }
+  const int rem = (int)(total - nblk * 34);
+#pragma unroll
+  for (int s = 0; s < 34; ++s) {
+    if (s < rem) {
+      r[s] = r[(s + 3) % 34] + r[(s + 31) % 34];
+      words[nblk * 34 + s] = r[s] >> 1;
+    }
+  }
+  // the ring after `total` draws: slot s now holds the latest word of its residue class except
+  // for the slots >= rem of the last (partial) block, which still hold the block before; both
+  // are the words of the last 34 positions, stored at ring[(position) mod 34]
+#pragma unroll
+  for (int s = 0; s < 34; ++s) {
+    int idx = p0 + s;
+    if (idx >= 34) idx -= 34;
+    st->ring[idx] = r[s];
+  }
+  st->pos = pos0 + total;
+}
+
+// draw d of the stage: component c = d mod 3, k = (d / 3) mod nz + 1, j = d / (3 nz) + 2
+__global__ void __launch_bounds__(256) k_rand_scatter(Geom g, const unsigned int* __restrict__ words,
+                                                      double* __restrict__ rplane, long long total) {
+  const long long d = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (d >= total) return;
+  const int c = (int)(d % 3);
+  const long long jk = d / 3;
+  const int k = (int)(jk % g.nz) + 1, j = (int)(jk / g.nz) + 2;
+  const int v = (int)words[d];
+  rplane[(long long)c * g.ny * g.nz + (long long)(k - 1) * g.ny + (j - 1)] = g.rand_scale * (double)v / 2147483647.0;
 }
 
 // bc_nr_lat_x_kernel / bc_nr_lat_y_kernel (kernels_cpu.F90:5169-5283, 5420-5540): characteristic
@@ -338,19 +373,20 @@ cudaError_t launch_bc_fill(const Geom& g, DevState& d, cudaStream_t s, long long
   for (int ilat = 1; ilat <= 6; ++ilat) {
     const int t = g.bctag[ilat - 1];
     if (t == 10 && ilat == 1) {
-      k_recyc_mean<<<nb((long long)g.ng * g.ny * 5), BC_NT, 0, s>>>(g, d.w, d.recyc_av);
-      k_recyc_fill<<<nb((long long)g.ny * g.nz), BC_NT, 0, s>>>(g, d.w, d.recyc_av, d.rplane);
+      SB_LAUNCH(d, K_BC_FILL, s, k_recyc_mean<<<nb((long long)g.ng * g.ny * 5), BC_NT, 0, s>>>(g, d.w, d.recyc_av));
+      SB_LAUNCH(d, K_BC_FILL, s,
+                k_recyc_fill<<<nb((long long)g.ny * g.nz), BC_NT, 0, s>>>(g, d.w, d.recyc_av, d.rplane));
       *nl += 2;
     } else if (t == 2) {
       const int dir = (ilat - 1) / 2;
       const long long np = (long long)(dir == 0 ? g.ny : g.nx) * (dir == 2 ? g.ny : g.nz);
-      k_bc_extr<<<nb(np), BC_NT, 0, s>>>(g, d.w, ilat);
+      SB_LAUNCH(d, K_BC_FILL, s, k_bc_extr<<<nb(np), BC_NT, 0, s>>>(g, d.w, ilat));
       ++*nl;
     } else if (t == 7 && ilat == 4) {
-      k_bc_shock<<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w);
+      SB_LAUNCH(d, K_BC_FILL, s, k_bc_shock<<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w));
       ++*nl;
     } else if (t == 6 && ilat == 3 && !g.wall_ymin) {
-      k_bc_wall<<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w);
+      SB_LAUNCH(d, K_BC_FILL, s, k_bc_wall<<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w));
       ++*nl;
     }
   }
@@ -366,8 +402,12 @@ bool has_stored_ghosts(const Geom& g) {
 }
 
 cudaError_t launch_rand_plane(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
-  k_rand_plane<<<1, 32, 0, s>>>(g, d.rng, d.rplane);
-  ++*nl;
+  const long long total = (long long)(g.jbl_inflow - 1) * g.nz * 3;
+  if (total <= 0) return cudaSuccess;
+  SB_LAUNCH(d, K_RAND_PLANE, s, k_rand_words<<<1, 32, 0, s>>>(d.rng, d.rwords, total));
+  SB_LAUNCH(d, K_RAND_PLANE, s,
+            k_rand_scatter<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, d.rwords, d.rplane, total));
+  *nl += 2;
   return cudaGetLastError();
 }
 
@@ -377,9 +417,9 @@ cudaError_t launch_bc_nr(const Geom& g, DevState& d, double* fl, cudaStream_t s,
     if (g.nr[ilat - 1] <= 0) continue;
     const long long np = (long long)((ilat <= 2) ? g.ny : g.nx) * g.nz;
     if (g.precision == 1)
-      k_bc_nr<float><<<nb(np), BC_NT, 0, s>>>(g, d.w, d.auxf, fl, ilat);
+      SB_LAUNCH(d, K_BC_NR, s, k_bc_nr<float><<<nb(np), BC_NT, 0, s>>>(g, d.w, d.auxf, fl, ilat));
     else
-      k_bc_nr<double><<<nb(np), BC_NT, 0, s>>>(g, d.w, d.aux, fl, ilat);
+      SB_LAUNCH(d, K_BC_NR, s, k_bc_nr<double><<<nb(np), BC_NT, 0, s>>>(g, d.w, d.aux, fl, ilat));
     ++*nl;
   }
   return cudaGetLastError();

@@ -12,7 +12,7 @@ namespace sb200 {
 // Kernel identifiers of the optional per-kernel event profiler.
 enum KernelId {
   K_AUX = 0, K_EULER_X, K_VISC, K_EULER_Y, K_EULER_Z, K_FINISH_RHS, K_UPDATE, K_FINISH_UPD, K_DT, K_DT_FINISH,
-  K_INIT_SENSOR, K_APPLY_SHIFT, K_FILL_GHOSTS, K_COUNT_WENO, K_ADD_TIME, K_NUM
+  K_INIT_SENSOR, K_APPLY_SHIFT, K_FILL_GHOSTS, K_COUNT_WENO, K_ADD_TIME, K_BC_FILL, K_BC_NR, K_RAND_PLANE, K_NUM
 };
 const char* kernel_name(int kid);
 
@@ -49,10 +49,19 @@ struct DevState {
   // recycling inflow: the random plane inflow_random_plane(j,k,c) at [(c*nz + k-1)*ny + j-1],
   // the spanwise means of the recycling plane [(m*ny + j-1)*ng + i-1], the generator state
   double* rplane = nullptr;
+  unsigned int* rwords = nullptr;  // raw draws of one stage
   double* recyc_av = nullptr;
   RngState* rng = nullptr;
   Prof* prof = nullptr;       // optional per-kernel timing
 };
+
+// Launch with optional per-kernel event timing on the launching stream
+#define SB_LAUNCH(dst, kid, s, ...)                                  \
+  do {                                                               \
+    if ((dst).prof && (dst).prof->on) (dst).prof->begin((kid), (s)); \
+    __VA_ARGS__;                                                     \
+    if ((dst).prof && (dst).prof->on) (dst).prof->end((s));          \
+  } while (0)
 
 struct StageArgs {
   int istep;           // 1..nrk

@@ -983,19 +983,15 @@ __global__ void __launch_bounds__(256) k_count_weno(Geom g, const double* __rest
 inline unsigned nblocks(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
 // Wrap one launch with profiler events when profiling is on.
-#define SB_LAUNCH(dst, kid, s, ...)                                  \
-  do {                                                               \
-    if ((dst).prof && (dst).prof->on) (dst).prof->begin((kid), (s)); \
-    __VA_ARGS__;                                                     \
-    if ((dst).prof && (dst).prof->on) (dst).prof->end((s));          \
-  } while (0)
+
 
 }  // namespace
 
 const char* kernel_name(int kid) {
   static const char* names[K_NUM] = {"k_aux", "k_euler_x", "k_visc", "k_euler_y", "k_euler_z", "k_finish_rhs",
                                      "k_update", "k_finish_upd", "k_dt", "k_dt_finish", "k_init_sensor",
-                                     "k_apply_shift", "k_fill_ghosts", "k_count_weno", "k_add_time"};
+                                     "k_apply_shift", "k_fill_ghosts", "k_count_weno", "k_add_time",
+                                     "k_bc_fill", "k_bc_nr", "k_rand_plane"};
   return (kid >= 0 && kid < K_NUM) ? names[kid] : "?";
 }
 
