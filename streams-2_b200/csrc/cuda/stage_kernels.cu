@@ -47,6 +47,11 @@ constexpr int MT_NT = 128;                                     // march kernels
 #ifndef MT_MINB_F
 #define MT_MINB_F 4
 #endif
+// the viscous pass: 4 blocks of 256 threads per SM (64 registers, a little spilling) measured
+// faster than 2 blocks at 128 registers
+#ifndef VISC_MINB
+#define VISC_MINB 4
+#endif
 constexpr int FIN_NT = 1024;
 
 // Apply force_var_2 (kernels_cpu.F90:3285-3314) to the conserved values of one interior point:
@@ -349,7 +354,7 @@ __global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F)
 // point loaded per face), computes every face of the segment once and adds the divergence to fl.
 // The z pass also applies the grad(mu div/3) term of visflx_div_ord2_subroutine
 // (kernels_cpu.F90:3446-3480) and emits the force_rhs block partials (:3157-3193).
-template <class R, int DIR, int LB, int WS>
+template <class R, int DIR, int LB, int WS, bool CH = false>
 __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F) k_march(Geom g, const R* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl,
                                                  const R* __restrict__ div3,
@@ -444,7 +449,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
           f[2] = f[2] - double(sigy);
           f[3] = f[3] - double(sigz);
           f[4] = f[4] - double(sigq);
-          if (g.channel_case) {
+          if constexpr (CH) {
             const double dt = sc->dt;
             const double rhodt = rhork * dt, gamdt = gamrk * dt;
             double fln1 = (istep > 1 ? -(rhodt * fl_prev[ic]) : 0.0) - gamdt * f[0];
@@ -469,7 +474,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
       }
     }
   }
-  if (DIR == 2 && g.channel_case) {
+  if constexpr (DIR == 2 && CH) {
     block_reduce_sum<5, MT_NT>(part, rsh);
     if (threadIdx.x == 0)
 #pragma unroll
@@ -482,7 +487,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
 // sensor_subroutine (:4726-4744) into the next sensor buffer.  Arithmetic in R, accumulation
 // into the FP64 register.
 template <class R>
-__global__ void __launch_bounds__(256) k_visc(Geom g, const R* __restrict__ aux, double* __restrict__ fl,
+__global__ void __launch_bounds__(256, VISC_MINB) k_visc(Geom g, const R* __restrict__ aux, double* __restrict__ fl,
                                               R* __restrict__ div3, double* __restrict__ sensor_next,
                                               double* __restrict__ wallprop, int do_sensor) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
@@ -1158,7 +1163,8 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   if (dev < 64 && !(smem_set & (1ULL << dev))) {
     cudaFuncSetAttribute(k_xflux<R, LB, WS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm);
     cudaFuncSetAttribute(k_march<R, 1, LB, WS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
-    cudaFuncSetAttribute(k_march<R, 2, LB, WS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+    cudaFuncSetAttribute(k_march<R, 2, LB, WS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+    cudaFuncSetAttribute(k_march<R, 2, LB, WS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
     smem_set |= 1ULL << dev;
   }
   SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS><<<xg, xb, xsm, s>>>(g, aux, sensor, fl_new));
@@ -1180,9 +1186,15 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
     SB_LAUNCH(d, K_EULER_Y, s,
               k_march<R, 1, LB, WS><<<gyb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                           a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
-  SB_LAUNCH(d, K_EULER_Z, s,
-            k_march<R, 2, LB, WS><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
-                                                        a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
+  // the channel's force_rhs partials are a separate instantiation (fewer registers without them)
+  if (g.channel_case)
+    SB_LAUNCH(d, K_EULER_Z, s,
+              k_march<R, 2, LB, WS, true><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
+                                                                  a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
+  else
+    SB_LAUNCH(d, K_EULER_Z, s,
+              k_march<R, 2, LB, WS, false><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
+                                                                   a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
   *nl += 4;
   if (g.recyc) launch_rand_plane(g, d, s, nl);  // euler_z draws the inflow plane of the stage
   launch_bc_nr(g, d, fl_new, s, nl);
