@@ -6,6 +6,12 @@
 
 #include "common.cuh"
 
+// keep the sound speed of every stencil point in the window (1) or recompute it in the WENO
+// branch (0, default: fewer registers and spills in the march kernels, measured 2-7 % faster)
+#ifndef SB_CACHE_C
+#define SB_CACHE_C 0
+#endif
+
 namespace sb200 {
 
 // Error-free transformations for the mixed form: the face fluxes are accumulated as float-float
@@ -45,7 +51,9 @@ __device__ __forceinline__ void acc_add(double& hi, double& lo, double b) {
 template <class R, int S>
 struct Stencil {
   R rho[2 * S], u[2 * S], v[2 * S], w[2 * S], h[2 * S], t[2 * S];
+#if SB_CACHE_C
   R c[2 * S];  // sound speed sqrt(gamma R T) of each point, computed once when the point is loaded
+#endif
 };
 
 // wenorec_1d (kernels_cpu.F90:2526-2724) for one characteristic variable.  The nonlinear weights
@@ -356,7 +364,11 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   for (int l = 0; l < 2 * WS; ++l) {
     const int q = l + S - WS;
     const R vnq = DIR == 0 ? st.u[q] : (DIR == 1 ? st.v[q] : st.w[q]);
+#if SB_CACHE_C
     const R cs = st.c[q];
+#else
+    const R cs = sqrt(R(g.gamloc) * R(g.rgas0) * st.t[q]);
+#endif
     ev0 = fmax(fabs(vnq - cs), ev0);
     ev1 = fmax(fabs(vnq), ev1);
     ev4 = fmax(fabs(vnq + cs), ev4);

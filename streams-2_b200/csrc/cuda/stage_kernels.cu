@@ -294,7 +294,9 @@ __device__ __forceinline__ void load_point(const Geom& g, Stencil<R, S>& st, int
   st.w[q] = __ldg(aux + 3 * n + a);
   st.h[q] = __ldg(aux + 4 * n + a);
   st.t[q] = __ldg(aux + 5 * n + a);
+#if SB_CACHE_C
   st.c[q] = sqrt(R(g.gamloc) * R(g.rgas0) * st.t[q]);
+#endif
 }
 
 // Divergence of one variable between a face pair, in FP64: (hi_up - hi_lo) + (lo_up - lo_lo).
@@ -405,7 +407,10 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
 #pragma unroll
       for (int q = 0; q < NP - 1; ++q) {
         st.rho[q] = st.rho[q + 1]; st.u[q] = st.u[q + 1]; st.v[q] = st.v[q + 1];
-        st.w[q] = st.w[q + 1]; st.h[q] = st.h[q + 1]; st.t[q] = st.t[q + 1]; st.c[q] = st.c[q + 1];
+        st.w[q] = st.w[q + 1]; st.h[q] = st.h[q + 1]; st.t[q] = st.t[q + 1];
+#if SB_CACHE_C
+        st.c[q] = st.c[q + 1];
+#endif
       }
       load_point<R, S>(g, st, NP - 1, aux, n, base0 + (long long)(c + S) * sd);
       mask = (mask >> 1) | (sensor_bit(c + WS) << (2 * WS - 1));
