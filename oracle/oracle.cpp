@@ -14,7 +14,7 @@ namespace {
 
 // wenorec_1d (kernels_cpu.F90:2526-2724).  vp, vm: [5][8] with Fortran index l = 1..8 at [m][l-1].
 void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], int iweno, int ord, int version,
-                double rho0, double u0) {
+                double rho0, double u0, bool rusanov = false) {
   auto VP = [&](int m, int l) { return vp[m][l - 1]; };
   auto VM = [&](int m, int l) { return vm[m][l - 1]; };
   double u0_2 = u0 * u0;
@@ -26,6 +26,14 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
   betascale[2] = 1.0 / rho0_2u0_4;
   betascale[3] = betascale[2];
   betascale[4] = betascale[0];
+  if (rusanov) {
+    // wenorec_1d_rusanov (kernels_cpu.F90:2325-2523): scales of the conserved variables
+    betascale[0] = 1.0 / rho0_2u0_2;
+    betascale[1] = 1.0 / rho0_2u0_4;
+    betascale[2] = betascale[1];
+    betascale[3] = betascale[1];
+    betascale[4] = betascale[1] / u0_2;
+  }
   const int i = iweno;
   if (ord == 1) {
     for (int m = 0; m < 5; ++m) vhat[m] = VP(m, i) + VM(m, i + 1);
@@ -679,6 +687,45 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
     if ((pos == 0 && s.force_zero_flux[2 * dir] == 1) || (pos == nd && s.force_zero_flux[2 * dir + 1] == 1))
       for (int m = 0; m < 5; ++m) fh[m] = 0.0;
     fh[1 + dir] = fh[1 + dir] + 0.5 * ft6;
+  } else if (s.flux_splitting == 1) {
+    // Rusanov (component-wise local Lax-Friedrichs) WENO branch of the *_hybrid_rusanov kernels
+    // (kernels_cpu.F90:692-941 for x): stencil maximum of |u_n -+ c|, split of the conserved
+    // fluxes, wenorec_1d_rusanov
+    const double gamloc = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
+    double evmax = -1.0;
+    for (int l = 1; l <= 2 * ws; ++l) {
+      const int o = l - ws;
+      const double un = at(o, 2 + dir), tt = at(o, 6);
+      const double c = std::sqrt(gamloc * rgas0 * tt);
+      const double evm = std::max(std::fabs(un - c), std::fabs(un + c));
+      evmax = std::max(evm, evmax);
+    }
+    double gp[5][8], gm[5][8];
+    for (int l = 1; l <= 2 * ws; ++l) {
+      const int o = l - ws;
+      const double rho = at(o, 1), h = at(o, 5);
+      const double vel[3] = {at(o, 2), at(o, 3), at(o, 4)};
+      const double rhou = rho * vel[dir];
+      const double pp = rho * at(o, 6) * rgas0;
+      const double rhoevm = rho * evmax;
+      double evm = rhou;
+      double c = 0.5 * (evm + rhoevm);
+      gp[0][l - 1] = c;
+      gm[0][l - 1] = evm - c;
+      for (int d = 0; d < 3; ++d) {
+        evm = vel[d] * rhou;
+        if (d == dir) evm = evm + pp;
+        c = 0.5 * (evm + rhoevm * vel[d]);
+        gp[1 + d][l - 1] = c;
+        gm[1 + d][l - 1] = evm - c;
+      }
+      evm = h * rhou;
+      c = 0.5 * (evm + evmax * (rho * h - pp));
+      gp[4][l - 1] = c;
+      gm[4][l - 1] = evm - c;
+    }
+    const int ord = std::max(ws + epo, 1);
+    wenorec_1d(gp, gm, fh, ws, ord, s.weno_version, s.rho0, s.u0, true);
   } else {
     // compute_roe_average (kernels_cpu.F90:3013-3089), calorically perfect gas
     double uu = at(0, 2), vv = at(0, 3), ww = at(0, 4);

@@ -87,7 +87,9 @@ std::string validate(const streams_b200_params* p) {
   if (p->nx < p->ng || p->ny < p->ng || p->nz < p->ng) return "every block dimension must be >= ng";
   if (p->weno_version != 0 && p->weno_version != 1) return "weno_version must be 0 or 1";
   if (p->weno_version == 1 && p->weno_scheme != 3) return "weno_version 1 requires weno_scheme 3";
-  if (p->flux_splitting != 0) return "flux_splitting = 1 (Rusanov) is not implemented on the device path";
+  if (p->flux_splitting != 0 && p->flux_splitting != 1) return "flux_splitting must be 0 or 1";
+  if (p->flux_splitting == 1 && !(p->ep_order == 6 && p->weno_scheme == 3))
+    return "flux_splitting = 1 (Rusanov) is implemented for ep_order 6 with weno_scheme 3";
   if (p->conservative_viscous != 0 && p->conservative_viscous != 1) return "conservative_viscous must be 0 or 1";
   if (p->calorically_perfect != 1) return "only calorically perfect gas is implemented on the device path";
   if (p->nrk != 3) return "only the Wray RK3 scheme (nrk = 3) is implemented";
@@ -160,6 +162,7 @@ void fill_geom(streams_b200_ctx* c) {
   g.t_bulk_target = p.t_bulk_target;
   g.precision = p.precision;
   g.conservative_viscous = p.conservative_viscous;
+  g.flux_splitting = p.flux_splitting;
   g.march_threads = 148LL * 1024;
   g.march_minseg = 16;
 }

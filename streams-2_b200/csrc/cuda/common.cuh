@@ -62,6 +62,7 @@ struct Geom {
   int eul_imin, eul_imax, eul_jmin, eul_jmax, eul_kmin, eul_kmax;
   // numerics
   int lmax_base, nkeep, weno_scheme, weno_version;
+  int flux_splitting;  // 0: characteristic WENO, 1: component-wise (Rusanov) WENO
   double sensor_threshold;
   // fluid
   int visc_model;

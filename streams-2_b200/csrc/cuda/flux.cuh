@@ -459,4 +459,63 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   acc_prod(fh[4], fl[4], h + vn * c, fi[4]);
 }
 
+// Rusanov (component-wise local Lax-Friedrichs) WENO flux of the *_hybrid_rusanov kernels
+// (kernels_cpu.F90:692-941 for x, same in y and z): stencil maximum of |u_n -+ c|, split
+// values of the conserved fluxes, wenorec with the scales of wenorec_1d_rusanov (:2325-2523).
+template <class R, int DIR, int WS, int S>
+__device__ __forceinline__ void rusanov_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5], R (&fl)[5]) {
+  const R rgas0 = R(g.rgas0);
+  R evmax = R(-1);
+#pragma unroll
+  for (int l = 0; l < 2 * WS; ++l) {
+    const int q = l + S - WS;
+    const R un = DIR == 0 ? st.u[q] : (DIR == 1 ? st.v[q] : st.w[q]);
+    const R c = sqrt(R(g.gamloc) * rgas0 * st.t[q]);
+    const R evm = fmax(fabs(un - c), fabs(un + c));
+    evmax = fmax(evm, evmax);
+  }
+  const R u02 = R(g.u0) * R(g.u0);
+  const R r2u2 = R(g.rho0) * R(g.rho0) * u02;
+  const R r2u4 = r2u2 * u02;
+  R bsc[5];
+  bsc[0] = R(1) / r2u2;
+  bsc[1] = R(1) / r2u4;
+  bsc[2] = bsc[1];
+  bsc[3] = bsc[1];
+  bsc[4] = bsc[1] / u02;
+#pragma unroll 1
+  for (int m = 0; m < 5; ++m) {
+    R gp[2 * WS], gm[2 * WS];
+#pragma unroll
+    for (int l = 0; l < 2 * WS; ++l) {
+      const int q = l + S - WS;
+      const R rho = st.rho[q], h = st.h[q];
+      const R vel[3] = {st.u[q], st.v[q], st.w[q]};
+      const R rhou = rho * vel[DIR];
+      const R pp = rho * st.t[q] * rgas0;
+      const R rhoevm = rho * evmax;
+      R evm, c;
+      if (m == 0) {
+        evm = rhou;
+        c = R(0.5) * (evm + rhoevm);
+      } else if (m == 4) {
+        evm = h * rhou;
+        c = R(0.5) * (evm + evmax * (rho * h - pp));
+      } else {
+        const R vd = m == 1 ? vel[0] : (m == 2 ? vel[1] : vel[2]);
+        evm = vd * rhou;
+        if (m == 1 + DIR) evm = evm + pp;
+        c = R(0.5) * (evm + rhoevm * vd);
+      }
+      gp[l] = c;
+      gm[l] = evm - c;
+    }
+    const R bs = m == 0 ? bsc[0] : (m == 4 ? bsc[4] : bsc[1]);
+    const R f = wenorec<R, WS>(gp, gm, ord, g.weno_version, bs);
+#pragma unroll
+    for (int mm = 0; mm < 5; ++mm)
+      if (mm == m) { fh[mm] = f; fl[mm] = R(0); }
+  }
+}
+
 }  // namespace sb200

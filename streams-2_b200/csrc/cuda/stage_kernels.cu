@@ -270,7 +270,7 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
 
 // Flux at a face from a loaded stencil window (points p-(S-1) .. p+S of face p):
 // hi + lo is the face flux (lo = 0 in the FP64 form).
-template <class R, int DIR, int LB, int WS, int S>
+template <class R, int DIR, int LB, int WS, int S, int FS = 0>
 __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& st, bool ishk, int p,
                                             R (&hi)[5], R (&lo)[5], R* __restrict__ gs, int gstride) {
   const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
@@ -281,7 +281,10 @@ __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& 
     central_flux<R, DIR, LB, S>(g, st, lmax, g.nkeep, zf, hi, lo);
   } else {
     const int ord = max(WS + ep, 1);
-    weno_flux<R, DIR, WS, S>(g, st, ord, hi, lo, gs, gstride);
+    if constexpr (FS == 1)
+      rusanov_flux<R, DIR, WS, S>(g, st, ord, hi, lo);
+    else
+      weno_flux<R, DIR, WS, S>(g, st, ord, hi, lo, gs, gstride);
   }
 }
 
@@ -313,7 +316,7 @@ __device__ __forceinline__ double face_diff(R hup, R lup, R hlo, R llo) {
 // cells between them; the upper face of a cell comes from the neighbouring lane by a shuffle,
 // so no shared memory and no block barrier are needed.  fl is written (first contribution of the
 // stage, euler_x after init_flux).
-template <class R, int LB, int WS>
+template <class R, int LB, int WS, int FS = 0>
 __global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F) k_xflux(Geom g, const R* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl) {
   constexpr int S = LB > WS ? LB : WS;
@@ -332,7 +335,7 @@ __global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F)
     const long long base = gidx(g, p, j, k);
 #pragma unroll
     for (int q = 0; q < 2 * S; ++q) load_point<R, S>(g, st, q, aux, g.nvol, base + (q - (S - 1)));
-    window_flux<R, 0, LB, WS, S>(g, st, ishk, p, fh, fo, weno_scratch<R>() + threadIdx.y * XF_TX + lane, XF_NT);
+    window_flux<R, 0, LB, WS, S, FS>(g, st, ishk, p, fh, fo, weno_scratch<R>() + threadIdx.y * XF_TX + lane, XF_NT);
   }
   R hu[5], lu[5];
 #pragma unroll
@@ -356,7 +359,7 @@ __global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F)
 // point loaded per face), computes every face of the segment once and adds the divergence to fl.
 // The z pass also applies the grad(mu div/3) term of visflx_div_ord2_subroutine
 // (kernels_cpu.F90:3446-3480) and emits the force_rhs block partials (:3157-3193).
-template <class R, int DIR, int LB, int WS, bool CH = false>
+template <class R, int DIR, int LB, int WS, bool CH = false, int FS = 0>
 __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F) k_march(Geom g, const R* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl,
                                                  const R* __restrict__ div3,
@@ -415,7 +418,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
       load_point<R, S>(g, st, NP - 1, aux, n, base0 + (long long)(c + S) * sd);
       mask = (mask >> 1) | (sensor_bit(c + WS) << (2 * WS - 1));
       R hhi[5], lhi[5];
-      window_flux<R, DIR, LB, WS, S>(g, st, mask != 0u, c, hhi, lhi, weno_scratch<R>() + threadIdx.x, MT_NT);
+      window_flux<R, DIR, LB, WS, S, FS>(g, st, mask != 0u, c, hhi, lhi, weno_scratch<R>() + threadIdx.x, MT_NT);
       if (c >= c0) {
         // cell c lies between the faces c-1 (lo) and c (hi)
         const long long ic = DIR == 1 ? iidx(g, i, c, b) : iidx(g, i, b, c);
@@ -1144,7 +1147,7 @@ cudaError_t launch_count_weno(const Geom& g, DevState& d, cudaStream_t s, long l
   return cudaGetLastError();
 }
 
-template <class R, int LB, int WS>
+template <class R, int LB, int WS, int FS = 0>
 static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
                               cudaStream_t s, long long* nl) {
   const dim3 xb(XF_TX, XF_TY);
@@ -1166,13 +1169,13 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !(smem_set & (1ULL << dev))) {
-    cudaFuncSetAttribute(k_xflux<R, LB, WS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm);
-    cudaFuncSetAttribute(k_march<R, 1, LB, WS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
-    cudaFuncSetAttribute(k_march<R, 2, LB, WS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
-    cudaFuncSetAttribute(k_march<R, 2, LB, WS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+    cudaFuncSetAttribute(k_xflux<R, LB, WS, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm);
+    cudaFuncSetAttribute(k_march<R, 1, LB, WS, false, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+    cudaFuncSetAttribute(k_march<R, 2, LB, WS, false, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+    cudaFuncSetAttribute(k_march<R, 2, LB, WS, true, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
     smem_set |= 1ULL << dev;
   }
-  SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS><<<xg, xb, xsm, s>>>(g, aux, sensor, fl_new));
+  SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS, FS><<<xg, xb, xsm, s>>>(g, aux, sensor, fl_new));
   if (g.conservative_viscous)
     SB_LAUNCH(d, K_VISC, s,
               k_visc<R><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
@@ -1189,16 +1192,16 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   }
   if (gyb > 0)
     SB_LAUNCH(d, K_EULER_Y, s,
-              k_march<R, 1, LB, WS><<<gyb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
+              k_march<R, 1, LB, WS, false, FS><<<gyb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                           a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
   // the channel's force_rhs partials are a separate instantiation (fewer registers without them)
   if (g.channel_case)
     SB_LAUNCH(d, K_EULER_Z, s,
-              k_march<R, 2, LB, WS, true><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
+              k_march<R, 2, LB, WS, true, FS><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                                   a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
   else
     SB_LAUNCH(d, K_EULER_Z, s,
-              k_march<R, 2, LB, WS, false><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
+              k_march<R, 2, LB, WS, false, FS><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                                    a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
   *nl += 4;
   if (g.recyc) launch_rand_plane(g, d, s, nl);  // euler_z draws the inflow plane of the stage
@@ -1220,6 +1223,11 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
 template <class R>
 static cudaError_t stage_dispatch(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
                                   cudaStream_t s, long long* nl) {
+  if (g.flux_splitting == 1) {
+    // the Rusanov splitting is instantiated for the sixth-order central / WENO5 scheme
+    if (g.lmax_base == 3 && g.weno_scheme == 3) return stage_impl<R, 3, 3, 1>(g, d, a, fl_prev, fl_new, s, nl);
+    return cudaErrorInvalidValue;
+  }
   if (g.lmax_base == 3 && g.weno_scheme == 3) return stage_impl<R, 3, 3>(g, d, a, fl_prev, fl_new, s, nl);
   if (g.lmax_base == 2 && g.weno_scheme == 2) return stage_impl<R, 2, 2>(g, d, a, fl_prev, fl_new, s, nl);
   if (g.lmax_base == 4 && g.weno_scheme == 4) return stage_impl<R, 4, 4>(g, d, a, fl_prev, fl_new, s, nl);

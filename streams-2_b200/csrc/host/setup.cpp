@@ -853,7 +853,7 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
   s.weno_version = c.get_int("numerics", "weno_version");
   if (s.weno_scheme != 3 && s.weno_version == 1) throw InputError("weno_version 1 supported only for weno_scheme = 3");
   s.flux_splitting = c.get_int_or("numerics", "flux_splitting", 0);
-  if (s.flux_splitting != 0) throw InputError("flux_splitting = 1 (Rusanov) is not supported by the B200 backend");
+  if (s.flux_splitting != 0 && s.flux_splitting != 1) throw InputError("flux_splitting must be 0 or 1");
   s.visc_order = c.get_int("numerics", "visc_order");
   if (s.visc_order != s.ep_order) throw InputError("viscous order must be equal to ep_order");
   s.conservative_viscous = c.get_int("numerics", "conservative_viscous");

@@ -14,7 +14,7 @@ def channel_ini(nx=32, ny=24, nz=16, *, lx=6.283185307179586, ly=2.0, lz=3.14159
                 re_bulk=3000.0, theta_wall=0.0, visc_model=1, vt_exp=0.76, sensor=0.05, ep_order=6,
                 weno_scheme=3, weno_version=0, nkeep=0, amp=0.1, seed=1, y_stretch=1.5, cfl=0.8,
                 num_iter=100, print_control=1, correct_bound_ord=1, reynolds_tau=None,
-                conservative_viscous=1) -> str:
+                conservative_viscous=1, flux_splitting=0) -> str:
     """Input file of a seeded synthetic channel case (the shape of the benchmark channel).
 
     A [synthetic] section selects the seeded Poiseuille + uniform-noise initial field and the
@@ -71,7 +71,7 @@ visc_order = {ep_order}
 conservative_viscous = {conservative_viscous}
 weno_scheme = {weno_scheme}
 weno_version = {weno_version}
-flux_splitting = 0
+flux_splitting = {flux_splitting}
 sensor_threshold = {sensor!r}
 rk_type = 1
 rand_type = 1
@@ -116,7 +116,7 @@ def bl_ini(nx=64, ny=48, nz=16, *, lx=100.0, ly=12.0, lz=8.0, mach=2.0, reynolds
            weno_scheme=3, weno_version=0, amp=0.05, x_recyc=None, nr_outflow=1, nr_top=1, cfl=0.8,
            jbgrid=None, dyptarget=0.7, nywr=None, lywr=None, ysmoosteps=10, conservative_viscous=1,
            num_iter=100, print_control=1, correct_bound_ord=1, rand_type=1, shock_angle=None,
-           xshock_imp=None) -> str:
+           xshock_imp=None, flux_splitting=0) -> str:
     """Input file of a spatially developing supersonic boundary layer (the benchmark's boundary
     layer workload): box lx x ly x lz inflow thicknesses, BL grid (grid_type 4, wall-resolved part
     of nywr points up to lywr), recycling-rescaling inflow at xmin, extrapolation with a
@@ -190,7 +190,7 @@ visc_order = {ep_order}
 conservative_viscous = {conservative_viscous}
 weno_scheme = {weno_scheme}
 weno_version = {weno_version}
-flux_splitting = 0
+flux_splitting = {flux_splitting}
 sensor_threshold = {sensor!r}
 rk_type = 1
 rand_type = {rand_type}

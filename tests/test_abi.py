@@ -57,8 +57,11 @@ def test_case_load_and_params(tmp_path):
 
 def test_case_rejects_unsupported_input(tmp_path):
     import streams_b200
-    bad = channel_ini(16, 12, 8).replace("flux_splitting = 0", "flux_splitting = 1")
-    with pytest.raises(streams_b200.BackendError, match="Rusanov"):
+    bad = channel_ini(16, 12, 8).replace("flux_splitting = 0", "flux_splitting = 3")
+    with pytest.raises(streams_b200.BackendError, match="flux_splitting"):
+        streams_b200.Case(tmp_path, bad)
+    bad = channel_ini(16, 12, 8).replace("rk_type = 1", "rk_type = 2")
+    with pytest.raises(streams_b200.BackendError, match="rk_type"):
         streams_b200.Case(tmp_path, bad)
     with pytest.raises(streams_b200.BackendError, match="missing input key"):
         streams_b200.Case(tmp_path, "[grid]\nnxmax = 4\n")

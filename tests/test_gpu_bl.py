@@ -56,8 +56,8 @@ SBLI = dict(mach=2.28, shock_angle=32.6, lx=60.0)  # an 8-degree deflection at M
 
 
 @pytest.mark.parametrize("kw", [dict(), dict(nr_outflow=2, nr_top=3), dict(nr_outflow=6, nr_top=1),
-                                dict(sensor=-1.0), dict(conservative_viscous=0), SBLI],
-                         ids=["nr1", "nr2_nr3", "nr6", "full_weno", "nonconservative", "sbli"])
+                                dict(sensor=-1.0), dict(conservative_viscous=0), SBLI, dict(flux_splitting=1)],
+                         ids=["nr1", "nr2_nr3", "nr6", "full_weno", "nonconservative", "sbli", "rusanov"])
 def test_bl_one_step(kw, tmp_path):
     o, s = pair(tmp_path, bl(**kw), 1)
     compare(o, s, 1e-12)

@@ -49,6 +49,9 @@ CASES = {
     "nonconservative_viscous": dict(nx=32, ny=24, nz=16, conservative_viscous=0),
     "nonconservative_viscous_order4": dict(nx=24, ny=20, nz=16, conservative_viscous=0, ep_order=4,
                                            weno_scheme=2),
+    # flux_splitting = 1: component-wise (Rusanov) WENO instead of the characteristic one
+    "rusanov": dict(nx=32, ny=24, nz=16, flux_splitting=1),
+    "rusanov_full_weno": dict(nx=24, ny=16, nz=12, sensor=-1.0, flux_splitting=1),
 }
 
 
@@ -64,7 +67,8 @@ def test_one_step(name, tmp_path):
         assert abs(sg[k] - so[k]) <= 1e-11 * max(abs(so[k]), 1e-30), (name, k, sg[k], so[k])
 
 
-@pytest.mark.parametrize("name", ["hybrid", "full_weno", "full_central_sutherland", "nonconservative_viscous"])
+@pytest.mark.parametrize("name", ["hybrid", "full_weno", "full_central_sutherland", "nonconservative_viscous",
+                                  "rusanov"])
 def test_hundred_steps(name, tmp_path):
     o, s = run_pair(tmp_path, channel_ini(**CASES[name]), 100)
     ng = o.ng
