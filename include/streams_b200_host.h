@@ -39,6 +39,14 @@ const double* streams_b200_case_field(const streams_b200_case* c);
 int streams_b200_case_info(const streams_b200_case* c, double out[12]);
 /* Write x.dat, y.dat, z.dat, yn.dat, rst.bin and field_info0.dat of the case into dir. */
 int streams_b200_case_write_restart(const streams_b200_case* c, const char* dir);
+/*
+ * Restart files of a running solve: w (the ghosted field of streams_b200_copy_to_field) at step
+ * icyc and time, written as x/y/z/yn.dat, rst.bin, field_info0.dat (the keys read_field_info of
+ * code/src/singleideal/singleideal.F90:2546-2590 reads) and singleideal.ini = the case's input
+ * with restart_type = 1, so that the case resumes from dir here or in the reference.
+ */
+int streams_b200_case_write_state(const streams_b200_case* c, const double* w, int icyc, double time,
+                                  const char* dir);
 
 /*
  * The run() loop of the solver on the device: initial ghost fill and sensor, then nsteps time

@@ -77,6 +77,18 @@ int streams_b200_case_write_restart(const streams_b200_case* c, const char* dir)
   return STREAMS_B200_OK;
 }
 
+int streams_b200_case_write_state(const streams_b200_case* c, const double* w, int icyc, double time,
+                                  const char* dir) {
+  if (!c || !w || !dir) return STREAMS_B200_EINVAL;
+  try {
+    streams_b200::write_restart_state(c->s, w, icyc, time, dir);
+  } catch (const std::exception& e) {
+    g_case_err = e.what();
+    return STREAMS_B200_EINVAL;
+  }
+  return STREAMS_B200_OK;
+}
+
 int streams_b200_run_case(const streams_b200_case* c, int nsteps, int precision, const char* progress_path,
                           double* last_row, double* w_out) {
   if (!c) return STREAMS_B200_EINVAL;

@@ -974,15 +974,21 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
     } else {
       throw InputError("unknown synthetic initial field " + kind);
     }
+    // a synthetic case restarted from its own rst.bin: the set-up above fixes the parameters,
+    // grid and inflow data, the field and the clock come from the restart files
+    if (s.restart_type == 1) {
+      read_rst(s);
+      read_field_info(s);
+    }
   } else {
     init_channel(s);
     if (s.restart_type == 1) {
       read_rst(s);
       read_field_info(s);
-    } else if (s.restart_type == 2) {
-      throw InputError("restart_type = 2 (statistics restart) is not supported by the B200 backend");
     }
   }
+  if (s.restart_type == 2)
+    throw InputError("restart_type = 2 (statistics restart) is not supported by the B200 backend");
   s.recyc = s.bctags[0] == 10;
   if (s.recyc) {
     if (s.flow_init != 1 || s.wmean.empty()) throw InputError("recycling inflow needs the boundary-layer initialisation");
@@ -1049,6 +1055,15 @@ void Setup::fill_grid(streams_b200_grid* g) const {
 }
 
 void write_restart_inputs(const Setup& s, const std::string& dir) {
+  write_restart_state(s, s.w.data(), s.icyc0, s.time0, dir);
+}
+
+// The files of a restart (restart_type = 1) from a conserved field w of the case: grid files,
+// rst.bin (per variable, Fortran order, interior points: the single-block layout of the
+// reference's MPI-IO file, code/src/field.F90:1853-1966), field_info0.dat with every key that
+// read_field_info (singleideal.F90:2546-2590) reads unconditionally (the output clocks start
+// afresh), and singleideal.ini = the case's input with restart_type = 1.
+void write_restart_state(const Setup& s, const double* w, int icyc, double time, const std::string& dir) {
   auto col = [&](const std::string& name, const OffsetArray& a, int lo, int hi) {
     FILE* f = std::fopen((dir + "/" + name).c_str(), "w");
     if (!f) throw InputError("cannot write " + dir + "/" + name);
@@ -1065,13 +1080,25 @@ void write_restart_inputs(const Setup& s, const std::string& dir) {
   for (int m = 0; m < 5; ++m)
     for (int k = 1; k <= s.nzmax; ++k)
       for (int j = 1; j <= s.nymax; ++j) {
-        for (int i = 1; i <= s.nxmax; ++i) plane[i - 1] = s.w[s.widx(i, j, k, m)];
+        for (int i = 1; i <= s.nxmax; ++i) plane[i - 1] = w[s.widx(i, j, k, m)];
         std::fwrite(plane.data(), sizeof(double), plane.size(), f);
       }
   std::fclose(f);
   FILE* fi = std::fopen((dir + "/field_info0.dat").c_str(), "w");
-  std::fprintf(fi, "[field_info]\nicyc0 = %d\ntime0 = %.17e\nitav = 0\nistore = 1\n", s.icyc0, s.time0);
+  if (!fi) throw InputError("cannot write field_info0.dat");
+  std::fprintf(fi,
+               "[field_info]\nicyc0 = %d\ntime0 = %.17e\nitav = 0\nitslice_p3d = 0\ntime_from_last_rst = 0.0\n"
+               "time_from_last_write = 0.0\ntime_from_last_stat = 0.0\ntime_from_last_slice = 0.0\n"
+               "time_from_last_probe = 0.0\nistore = 1\n",
+               icyc, time);
   std::fclose(fi);
+  IniFile ini = s.ini;
+  ini.set("controls", "restart_type", "1");
+  FILE* fin = std::fopen((dir + "/singleideal.ini").c_str(), "w");
+  if (!fin) throw InputError("cannot write singleideal.ini");
+  const std::string text = ini.to_text();
+  std::fwrite(text.data(), 1, text.size(), fin);
+  std::fclose(fin);
 }
 
 }  // namespace streams_b200

@@ -132,5 +132,8 @@ double get_reynolds_cha(double retau, double rm, double trat, double s2tinf, dou
 // Write the files with which the reference itself starts the same case:
 // x.dat, y.dat, z.dat, yn.dat (with ghosts), rst.bin and field_info0.dat.
 void write_restart_inputs(const Setup& s, const std::string& dir);
+// The same from a conserved field w (ghosted, Fortran order) at step icyc and time, plus a
+// singleideal.ini of the case with restart_type = 1: a run resumes from dir.
+void write_restart_state(const Setup& s, const double* w, int icyc, double time, const std::string& dir);
 
 }  // namespace streams_b200

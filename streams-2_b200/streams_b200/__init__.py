@@ -120,6 +120,7 @@ def _load() -> C.CDLL:
         "streams_b200_case_field": (D, [P]),
         "streams_b200_case_info": (I, [P, D]),
         "streams_b200_case_write_restart": (I, [P, C.c_char_p]),
+        "streams_b200_case_write_state": (I, [P, D, I, C.c_double, C.c_char_p]),
         "streams_b200_run_case": (I, [P, I, I, C.c_char_p, D, D]),
         "streams_b200_set_tuning": (I, [P, LL, I]),
         "streams_b200_get_tuning": (I, [P, C.POINTER(LL), C.POINTER(I)]),
@@ -152,7 +153,8 @@ EXPORTED = [
     "streams_b200_profile_enable", "streams_b200_profile_read", "streams_b200_kernel_count",
     "streams_b200_kernel_name", "streams_b200_compute_dt_noalloc", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
     "streams_b200_case_params", "streams_b200_case_grid", "streams_b200_case_field", "streams_b200_case_info",
-    "streams_b200_case_write_restart", "streams_b200_run_case", "streams_b200_set_tuning",
+    "streams_b200_case_write_restart", "streams_b200_case_write_state", "streams_b200_run_case",
+    "streams_b200_set_tuning",
     "streams_b200_get_tuning", "streams_b200_batch_create", "streams_b200_batch_advance",
     "streams_b200_batch_synchronize", "streams_b200_batch_invalidate", "streams_b200_batch_stats",
     "streams_b200_batch_last_error", "streams_b200_batch_destroy",
@@ -211,6 +213,17 @@ class Case:
 
     def write_restart(self, directory: str | os.PathLike) -> None:
         rc = lib.streams_b200_case_write_restart(self._h, str(directory).encode())
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_case_error().decode())
+
+    def write_state(self, w: np.ndarray, icyc: int, time: float, directory: str | os.PathLike) -> None:
+        """Restart files (rst.bin, field_info0.dat, grid files, singleideal.ini with
+        restart_type = 1) of the field w at step icyc and time; Case(directory) resumes it."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        nx, ny, nz, ng = self.shape
+        if w.shape != (5, nz + 2 * ng, ny + 2 * ng, nx + 2 * ng):
+            raise ValueError("w must be the ghosted field of this case")
+        rc = lib.streams_b200_case_write_state(self._h, _dptr(w), int(icyc), float(time), str(directory).encode())
         if rc != OK:
             raise BackendError(rc, lib.streams_b200_case_error().decode())
 

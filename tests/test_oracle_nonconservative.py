@@ -56,3 +56,26 @@ def test_bl_setup_and_oracle_run(tmp_path):
     w = o.w()
     assert np.all(np.isfinite(w))
     assert np.all(w[1:4, 3:-3, 3, 3:-3] == 0.0)  # wall node at rest
+
+
+def test_restart_files_round_trip(tmp_path):
+    """write_state -> Case(dir) restores the field bit for bit and the clock of the run."""
+    from oracle_py import Oracle
+    from streams_b200 import Case
+    from streams_b200.cases import channel_ini
+    (tmp_path / "a").mkdir()
+    (tmp_path / "r").mkdir()
+    ini = channel_ini(nx=24, ny=16, nz=8)
+    case = Case(tmp_path / "a", ini)
+    o = Oracle(tmp_path / "a", ini)
+    o.init_run()
+    o.run(4)
+    w = o.w()
+    t = o.scalars()["time"]
+    case.write_state(w, 4, t, tmp_path / "r")
+    back = Case(tmp_path / "r")
+    g = 3
+    assert np.array_equal(back.field()[:, g:-g, g:-g, g:-g], w[:, g:-g, g:-g, g:-g])
+    info = back.info()
+    assert info["icyc0"] == 4 and info["time0"] == t
+    assert back.params().mu0 == case.params().mu0
