@@ -204,6 +204,30 @@ int streams_b200_count_weno(streams_b200_ctx* ctx, double out[3]);
 /* Wall shear / heat flux at j=1 (wallprop(1:nx,1:nz,2:4) of visflx_reduced_ord2). */
 int streams_b200_get_wallprop(streams_b200_ctx* ctx, double* out /* nx*nz*3 */);
 
+/*
+ * Running statistics.  Replace equation_singleideal_object%compute_stats
+ * (code/src/singleideal/singleideal.F90:2003-2179) and compute_stats_3d (:2513-2543) as
+ * manage_output calls them (singleideal_gpu.F90:2012-2034): right after a completed rk_sync,
+ * before the next step's compute_dt, with no upload in between (a download is allowed);
+ * otherwise STREAMS_B200_EINVAL.  itav is the number of samples already averaged (the caller
+ * increments it after the call, as manage_output does).  compute_stats adds the z-average of 70
+ * point quantities (velocity derivatives of order visc_order, T and mu of the stage-3 aux pass,
+ * Reynolds stresses, vorticity, viscous stresses, ...) to w_stat(70, nx, ny):
+ *   w_stat = (w_stat*itav + w_stat_z)/(itav + 1);
+ * compute_stats_3d does the same per cell for the 14 quantities of w_stat_3d(14, nx, ny, nz).
+ * The arrays live on the device (allocated on first use, zero-initialised: 2*70*nx*ny and
+ * 14*nx*ny*nz doubles) in the reference's layout, statistic index fastest.  get_stats /
+ * set_stats copy which = 0 (w_stat), 1 (w_stat_z of the last sample, read only) or
+ * 2 (w_stat_3d); n is the buffer size in doubles (set_stats: exactly the array size), e.g. to
+ * restore w_stat from stat.bin on a restart with restart_type = 2 (read_stats, :1646-1700).
+ */
+#define STREAMS_B200_NV_STAT 70
+#define STREAMS_B200_NV_STAT_3D 14
+int streams_b200_compute_stats(streams_b200_ctx* ctx, int itav);
+int streams_b200_compute_stats_3d(streams_b200_ctx* ctx, int itav);
+int streams_b200_get_stats(streams_b200_ctx* ctx, int which, double* out, long long n);
+int streams_b200_set_stats(streams_b200_ctx* ctx, int which, const double* in, long long n);
+
 /* Synchronise the context's stream and report any asynchronous error. */
 int streams_b200_synchronize(streams_b200_ctx* ctx);
 

@@ -49,14 +49,46 @@ int streams_b200_case_write_state(const streams_b200_case* c, const double* w, i
                                   const char* dir);
 
 /*
+ * The same with running statistics: stat.bin (and stat3d.bin when w_stat_3d is non-NULL) with
+ * w_stat(70, nx, ny), w_stat_3d(14, nx, ny, nz) (statistic index fastest), field_info0.dat with
+ * itav and time_from_last_stat, and singleideal.ini with restart_type = 2, so that the
+ * averaging continues on resume (read_stats, singleideal.F90:1646-1700).
+ */
+int streams_b200_case_write_state_stats(const streams_b200_case* c, const double* w, int icyc, double time,
+                                        const double* w_stat, const double* w_stat_3d, int itav,
+                                        double time_from_last_stat, const char* dir);
+/*
+ * Statistics settings and restart state of the case: out[0..4] = dtstat (< 0 when [output] has
+ * no dtstat), enable_stat_time, enable_stat_3d, itav, time_from_last_stat.
+ */
+int streams_b200_case_stats_info(const streams_b200_case* c, double out[5]);
+/*
+ * Averages read on a restart with restart_type = 2: which = 0 w_stat (70*nx*ny doubles),
+ * 2 w_stat_3d (14*nx*ny*nz); zeros when the case starts the averages afresh.
+ */
+int streams_b200_case_stats(const streams_b200_case* c, int which, double* out, long long n);
+
+/*
  * The run() loop of the solver on the device: initial ghost fill and sensor, then nsteps time
  * steps (num_iter when nsteps < 0); every print_control steps compute_residual and a progress
  * row.  Rows (14 columns of progress.out) are written to progress_path when it is non-NULL and
  * the last row is returned in last_row[14] when non-NULL.  The final field is written to
- * w_out when non-NULL.  Returns STREAMS_B200_ENAN when the residual becomes NaN.
+ * w_out when non-NULL.  Returns STREAMS_B200_ENAN when the residual becomes NaN.  When the
+ * input sets [output] dtstat, the statistics are sampled as manage_output does
+ * (singleideal_gpu.F90:2012-2034: time_from_last_stat += dt after every step, a sample when it
+ * reaches dtstat), starting from the case's restart averages.
  */
 int streams_b200_run_case(const streams_b200_case* c, int nsteps, int precision, const char* progress_path,
                           double* last_row, double* w_out);
+/*
+ * run_case that also returns the statistics at the end: w_stat_out (70*nx*ny), w_stat_3d_out
+ * (14*nx*ny*nz) and stat_clock[2] = itav, time_from_last_stat (each may be NULL).  With
+ * output_dir non-NULL the files that the end of run() writes are written there
+ * (singleideal_gpu.F90:1660-1683: rst.bin, stat.bin, stat3d.bin, field_info0.dat).
+ */
+int streams_b200_run_case_stats(const streams_b200_case* c, int nsteps, int precision, const char* progress_path,
+                                double* last_row, double* w_out, double* w_stat_out, double* w_stat_3d_out,
+                                double* stat_clock, const char* output_dir);
 
 #ifdef __cplusplus
 }

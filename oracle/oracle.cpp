@@ -1547,6 +1547,123 @@ void Solver::run(int nsteps) {
 }
 
 // print_progress (singleideal_cpu.F90:1695-1732), channel row
+// compute_stats (singleideal.F90:2003-2179) on one block (the z all-reduce is the identity):
+// visc_order velocity derivatives from w including its ghost layers as the step left them, T and
+// mu from w_aux(6), w_aux(7); the 70 per-point quantities are summed over k for every (i,j), divided
+// by nzmax and averaged in time with the itav samples already in w_stat.
+void Solver::compute_stats(int itav) {
+  const int nv = NV_STAT;
+  const int lmax = s.visc_order / 2;
+  if (w_stat.empty()) w_stat.assign(static_cast<size_t>(nv) * nx * ny, 0.0);
+  w_stat_z.assign(static_cast<size_t>(nv) * nx * ny, 0.0);
+  const double rgas0 = s.rgas0;
+  // get_gamloc (singleideal.F90:4752-4771), calorically perfect
+  const double cploc0 = s.cp_coeff[0];
+  par_for(1, ny, [&](int j) {
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nx; ++i) {
+        double ux = 0, vx = 0, wx = 0, uy = 0, vy = 0, wy = 0, uz = 0, vz = 0, wz = 0;
+        for (int l = 1; l <= lmax; ++l) {
+          const double ccl = s.coeff_deriv1[lmax - 1][l - 1];
+          ux = ux + ccl * (W(i + l, j, k, 1) / W(i + l, j, k, 0) - W(i - l, j, k, 1) / W(i - l, j, k, 0));
+          vx = vx + ccl * (W(i + l, j, k, 2) / W(i + l, j, k, 0) - W(i - l, j, k, 2) / W(i - l, j, k, 0));
+          wx = wx + ccl * (W(i + l, j, k, 3) / W(i + l, j, k, 0) - W(i - l, j, k, 3) / W(i - l, j, k, 0));
+          uy = uy + ccl * (W(i, j + l, k, 1) / W(i, j + l, k, 0) - W(i, j - l, k, 1) / W(i, j - l, k, 0));
+          vy = vy + ccl * (W(i, j + l, k, 2) / W(i, j + l, k, 0) - W(i, j - l, k, 2) / W(i, j - l, k, 0));
+          wy = wy + ccl * (W(i, j + l, k, 3) / W(i, j + l, k, 0) - W(i, j - l, k, 3) / W(i, j - l, k, 0));
+          uz = uz + ccl * (W(i, j, k + l, 1) / W(i, j, k + l, 0) - W(i, j, k - l, 1) / W(i, j, k - l, 0));
+          vz = vz + ccl * (W(i, j, k + l, 2) / W(i, j, k + l, 0) - W(i, j, k - l, 2) / W(i, j, k - l, 0));
+          wz = wz + ccl * (W(i, j, k + l, 3) / W(i, j, k + l, 0) - W(i, j, k - l, 3) / W(i, j, k - l, 0));
+        }
+        const double dx = s.dcsidx[i - 1], dy = s.detady[j - 1], dz = s.dzitdz[k - 1];
+        ux = ux * dx; vx = vx * dx; wx = wx * dx;
+        uy = uy * dy; vy = vy * dy; wy = wy * dy;
+        uz = uz * dz; vz = vz * dz; wz = wz * dz;
+        const double omx = wy - vz, omy = uz - wx, omz = vx - uy;
+        const double rho = W(i, j, k, 0), rhou = W(i, j, k, 1), rhov = W(i, j, k, 2), rhow = W(i, j, k, 3);
+        const double ri = 1.0 / rho;
+        const double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
+        const double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+        const double tt = A(i, j, k, 6);
+        const double pp = rho * rgas0 * tt;
+        const double mu = A(i, j, k, 7);
+        const double nu = mu / rho;
+        const double gamloc = cploc0 / (cploc0 - rgas0);
+        const double cploc = gamloc / (gamloc - 1.0) * rgas0;
+        const double c = std::sqrt(gamloc * rgas0 * tt);
+        const double machlocal = std::sqrt(2.0 * qq) / c;
+        const double t_tot = tt + qq * (gamloc - 1.0) / gamloc;
+        const double rho2 = rho * rho, uu2 = uu * uu, vv2 = vv * vv, ww2 = ww * ww, pp2 = pp * pp, tt2 = tt * tt;
+        const double divl = ux + vy + wz;
+        const double div3l = divl / 3.0;
+        double sg[3][3];
+        sg[0][0] = 2.0 * (ux - div3l);
+        sg[0][1] = uy + vx;
+        sg[0][2] = uz + wx;
+        sg[1][0] = sg[0][1];
+        sg[1][1] = 2.0 * (vy - div3l);
+        sg[1][2] = vz + wy;
+        sg[2][0] = sg[0][2];
+        sg[2][1] = sg[1][2];
+        sg[2][2] = 2.0 * (wz - div3l);
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) sg[a][b] = sg[a][b] * mu;
+        const double v[NV_STAT] = {
+            rho, uu, vv, ww, pp, tt, rho2, uu2, vv2, ww2, pp2, tt2, rhou, rhov, rhow,
+            rhou * uu, rhov * vv, rhow * ww, rhou * vv, mu, nu, omx * omx, omy * omy, omz * omz,
+            rho * tt, rho * tt2, t_tot, rho * t_tot, t_tot * t_tot, rhou * tt, rhov * tt, rhow * tt,
+            machlocal, machlocal * machlocal, rhou * uu2, rhov * uu2, rhou * vv2, rhov * vv2, rhou * ww2,
+            rhov * ww2, pp * uu, pp * vv, sg[0][0], sg[0][1], sg[0][2], sg[1][1], sg[1][2], sg[2][2],
+            sg[0][0] * uu, sg[0][1] * uu, sg[1][0] * vv, sg[1][1] * vv, sg[2][0] * ww, sg[2][1] * ww,
+            sg[0][0] * vv, sg[0][1] * vv, sg[0][0] * ux, sg[1][0] * vx, sg[2][0] * wx, sg[0][0] * vx,
+            pp * ux, pp * vy, pp * wz, pp * (uy + vx), divl * divl, rho * tt2 * tt, rho * tt2 * tt2,
+            rhou * uu2 * uu, cploc, gamloc};
+        double* acc = &w_stat_z[(static_cast<size_t>(j - 1) * nx + (i - 1)) * nv];
+        for (int l = 0; l < nv; ++l) acc[l] = acc[l] + v[l];
+        // statistics 55-60 add several terms, left to right as the source line reads
+        acc[54] = acc[54] + sg[1][0] * uu;
+        acc[55] = acc[55] + sg[1][1] * uu;
+        acc[56] = acc[56] + sg[0][1] * uy;
+        acc[56] = acc[56] + sg[0][2] * uz;
+        acc[57] = acc[57] + sg[1][1] * vy;
+        acc[57] = acc[57] + sg[1][2] * vz;
+        acc[58] = acc[58] + sg[2][1] * wy;
+        acc[58] = acc[58] + sg[2][2] * wz;
+        acc[59] = acc[59] + sg[0][1] * (ux + vy);
+        acc[59] = acc[59] + sg[1][1] * uy;
+        acc[59] = acc[59] + sg[0][2] * vz;
+        acc[59] = acc[59] + sg[1][2] * uz;
+      }
+  });
+  const double nzmax = static_cast<double>(s.nzmax);
+  const double rav = static_cast<double>(itav);
+  for (size_t q = 0; q < w_stat_z.size(); ++q) {
+    w_stat_z[q] = w_stat_z[q] / nzmax;
+    w_stat[q] = w_stat[q] * rav + w_stat_z[q];
+    w_stat[q] = w_stat[q] / (rav + 1.0);
+  }
+}
+
+// compute_stats_3d (singleideal.F90:2513-2543): 14 point statistics averaged in time
+void Solver::compute_stats_3d(int itav) {
+  const int nv = NV_STAT_3D;
+  if (w_stat_3d.empty()) w_stat_3d.assign(static_cast<size_t>(nv) * nint_(), 0.0);
+  const double rav = static_cast<double>(itav);
+  par_for(1, nz, [&](int k) {
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const double r = W(i, j, k, 0), ru = W(i, j, k, 1), rv = W(i, j, k, 2), rw = W(i, j, k, 3);
+        const double t = A(i, j, k, 6);
+        const double v[NV_STAT_3D] = {r,           ru,          rv,          rw,          r * t,
+                                      r * r,       ru * ru / r, rv * rv / r, rw * rw / r, ru * rv / r,
+                                      ru * rw / r, rv * rw / r, r * (t * t), (r * t) * (r * t)};
+        double* o = &w_stat_3d[ii(i, j, k) * nv];
+        for (int l = 0; l < nv; ++l) o[l] = o[l] * rav + v[l];
+      }
+  });
+  for (double& x : w_stat_3d) x = x / (rav + 1.0);
+}
+
 ProgressRow Solver::progress_row() const {
   ProgressRow r;
   r.icyc = icyc;

@@ -45,6 +45,14 @@ class Solver {
   void compute_residual();
   ProgressRow progress_row() const;
 
+  // running statistics, as manage_output calls them after a step (itav samples already averaged):
+  // compute_stats (singleideal.F90:2003-2179) and compute_stats_3d (:2513-2543)
+  static constexpr int NV_STAT = 70, NV_STAT_3D = 14;
+  void compute_stats(int itav);
+  void compute_stats_3d(int itav);
+  std::vector<double> w_stat, w_stat_z;  // (nv_stat, nx, ny), statistic index fastest
+  std::vector<double> w_stat_3d;         // (nv_stat_3d, nx, ny, nz)
+
   // state (Fortran layouts)
   const Setup& s;
   int nx, ny, nz, ng, sx, sy, sz;

@@ -111,6 +111,22 @@ void oracle_get_residual(void* hp, double* out) {
   out[4] = s->tmax; out[5] = s->pmin; out[6] = s->pmax;
 }
 
+// running statistics: compute_stats / compute_stats_3d with itav samples already averaged; then
+// w_stat(70,nx,ny), w_stat_z(70,nx,ny) or w_stat_3d(14,nx,ny,nz) (which = 0, 1, 2)
+void oracle_compute_stats(void* hp, int itav) { static_cast<Handle*>(hp)->solver->compute_stats(itav); }
+void oracle_compute_stats_3d(void* hp, int itav) { static_cast<Handle*>(hp)->solver->compute_stats_3d(itav); }
+void oracle_set_stats(void* hp, int which, const double* in) {
+  auto* s = static_cast<Handle*>(hp)->solver;
+  const size_t n2 = static_cast<size_t>(Solver::NV_STAT) * s->nx * s->ny;
+  if (which == 0) s->w_stat.assign(in, in + n2);
+  if (which == 2) s->w_stat_3d.assign(in, in + static_cast<size_t>(Solver::NV_STAT_3D) * s->nint_());
+}
+void oracle_get_stats(void* hp, int which, double* out) {
+  auto* s = static_cast<Handle*>(hp)->solver;
+  const std::vector<double>& v = which == 0 ? s->w_stat : (which == 1 ? s->w_stat_z : s->w_stat_3d);
+  std::memcpy(out, v.data(), v.size() * sizeof(double));
+}
+
 // case parameters used by the tests: u0, rho0, l0, mu0, volchan, t_bulk_target, num_iter, print_control
 void oracle_case_info(void* hp, double* out) {
   const auto& st = static_cast<Handle*>(hp)->setup;

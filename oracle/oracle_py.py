@@ -42,6 +42,10 @@ def _load():
         "oracle_last_progress": (I, [P, D]),
         "oracle_get_residual": (None, [P, D]),
         "oracle_case_info": (None, [P, D]),
+        "oracle_compute_stats": (None, [P, I]),
+        "oracle_compute_stats_3d": (None, [P, I]),
+        "oracle_set_stats": (None, [P, I, D]),
+        "oracle_get_stats": (None, [P, I, D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -142,3 +146,22 @@ class Oracle:
         lib.oracle_case_info(self._h, _d(a))
         return dict(zip(["u0", "rho0", "l0", "mu0", "volchan", "t_bulk_target", "num_iter", "print_control"],
                         a.tolist()))
+
+    def compute_stats(self, itav: int):
+        lib.oracle_compute_stats(self._h, itav)
+
+    def compute_stats_3d(self, itav: int):
+        lib.oracle_compute_stats_3d(self._h, itav)
+
+    def _stats_shape(self, which: int):
+        return (self.ny, self.nx, 70) if which in (0, 1) else (self.nz, self.ny, self.nx, 14)
+
+    def stats(self, which: int = 0) -> np.ndarray:
+        """w_stat (0), w_stat_z (1) as (ny, nx, 70) or w_stat_3d (2) as (nz, ny, nx, 14) arrays."""
+        a = np.zeros(self._stats_shape(which))
+        lib.oracle_get_stats(self._h, which, _d(a))
+        return a
+
+    def set_stats(self, which: int, a: np.ndarray):
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(self._stats_shape(which))
+        lib.oracle_set_stats(self._h, which, _d(a))

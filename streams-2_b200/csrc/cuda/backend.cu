@@ -26,6 +26,9 @@ struct streams_b200_ctx {
   bool shift_pending = false;  // force_var energy shift not applied to w yet
   bool aux_current = false;    // aux matches w (no update since the last aux pass)
   bool have_stats = false;
+  // the state is the one manage_output samples statistics from: a completed rk_sync and no aux
+  // pass or upload since
+  bool stats_ready = false;
   long long launches = 0;
   Prof prof;
   std::vector<void*> allocs;
@@ -116,6 +119,14 @@ std::string validate(const streams_b200_params* p) {
                              p->jbl_inflow > p->ny || p->bctags[4] != 0))
     return "recycling inflow needs recyc = 1, ng <= i_recyc <= nx, 1 <= jbl_inflow <= ny and periodic z";
   if (p->channel_case && !(p->volchan > 0)) return "channel forcing needs volchan > 0";
+  if (p->channel_case && p->theta_wall >= -1.0)
+    for (int l = 0; l < 6; ++l) {
+      // the force_var energy shift is applied to the interior lazily, before the next aux pass;
+      // ghosts stored by update_ghost would miss it
+      const int t = p->bctags[l];
+      if (t == 2 || t == 7 || t == 10 || (t == 6 && !p->is_y_staggered))
+        return "bulk-temperature forcing (theta_wall >= -1) needs periodic faces and staggered walls";
+    }
   return "";
 }
 
@@ -349,6 +360,7 @@ int streams_b200_copy_from_field(streams_b200_ctx* c, const double* w) {
   SB_CHECK(c, cudaMemcpyAsync(c->d.w, w, c->g.nvol * 5 * 8, cudaMemcpyHostToDevice, c->stream));
   c->shift_pending = false;
   c->aux_current = false;
+  c->stats_ready = false;
   return STREAMS_B200_OK;
 }
 
@@ -358,17 +370,18 @@ int streams_b200_copy_from_device(streams_b200_ctx* c, const double* w) {
   SB_CHECK(c, cudaMemcpyAsync(c->d.w, w, c->g.nvol * 5 * 8, cudaMemcpyDeviceToDevice, c->stream));
   c->shift_pending = false;
   c->aux_current = false;
+  c->stats_ready = false;
   return STREAMS_B200_OK;
 }
 
 static int finalize_w(streams_b200_ctx* c) {
-  // apply a pending force_var shift and rebuild the ghost layers (update_ghost + bcswap)
+  // apply a pending force_var shift and rebuild the ghost layers of w (update_ghost + bcswap);
+  // aux is left alone, so that the statistics of the step can still be sampled after a download
   if (c->shift_pending) {
     SB_CHECK(c, launch_apply_shift(c->g, c->d, c->stream, &c->launches));
     c->shift_pending = false;
   }
   SB_CHECK(c, launch_fill_ghosts(c->g, c->d, c->stream, &c->launches));
-  c->aux_current = true;
   return STREAMS_B200_OK;
 }
 
@@ -399,6 +412,7 @@ int streams_b200_init_run(streams_b200_ctx* c) {
   SB_CHECK(c, launch_aux(c->g, c->d, c->shift_pending ? 1 : 0, c->stream, &c->launches));
   c->shift_pending = false;
   c->aux_current = true;
+  c->stats_ready = false;
   SB_CHECK(c, launch_init_sensor(c->g, c->d, c->stream, &c->launches));
   SB_CHECK(c, cudaMemsetAsync(c->fl_a, 0, c->g.nint * 40, c->stream));
   SB_CHECK(c, cudaMemsetAsync(c->fl_b, 0, c->g.nint * 40, c->stream));
@@ -416,6 +430,7 @@ static int do_compute_dt(streams_b200_ctx* c) {
     SB_CHECK(c, launch_aux(c->g, c->d, c->shift_pending ? 1 : 0, c->stream, &c->launches));
     c->shift_pending = false;
     c->aux_current = true;
+    c->stats_ready = false;
   }
   SB_CHECK(c, launch_dt(c->g, c->d, c->p.cfl, c->stream, &c->launches));
   return STREAMS_B200_OK;
@@ -469,6 +484,7 @@ static int do_rk_sync(streams_b200_ctx* c, bool add_time) {
     c->aux_current = false;
   }
   c->have_stats = true;
+  c->stats_ready = true;
   return STREAMS_B200_OK;
 }
 
@@ -608,6 +624,91 @@ int streams_b200_synchronize(streams_b200_ctx* c) {
   cudaSetDevice(c->device);
   SB_CHECK(c, cudaStreamSynchronize(c->stream));
   SB_CHECK(c, cudaGetLastError());
+  return STREAMS_B200_OK;
+}
+
+static int ensure_stats(streams_b200_ctx* c, bool three_d) {
+  const size_t n2 = (size_t)NV_STAT * c->p.nx * c->p.ny;
+  if (!c->d.wstat) {
+    SB_CHECK(c, dev_alloc(c, &c->d.wstat, n2));
+    SB_CHECK(c, dev_alloc(c, &c->d.wstat_z, n2));
+    SB_CHECK(c, cudaMemsetAsync(c->d.wstat, 0, n2 * 8, c->stream));
+    SB_CHECK(c, cudaMemsetAsync(c->d.wstat_z, 0, n2 * 8, c->stream));
+  }
+  if (three_d && !c->d.wstat3d) {
+    const size_t n3 = (size_t)NV_STAT_3D * c->g.nint;
+    SB_CHECK(c, dev_alloc(c, &c->d.wstat3d, n3));
+    SB_CHECK(c, cudaMemsetAsync(c->d.wstat3d, 0, n3 * 8, c->stream));
+  }
+  return STREAMS_B200_OK;
+}
+
+static int stats_sample_check(streams_b200_ctx* c, int itav) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  if (itav < 0) return set_err(c, STREAMS_B200_EINVAL, "itav must be >= 0");
+  if (!c->stats_ready)
+    return set_err(c, STREAMS_B200_EINVAL,
+                   "statistics are sampled right after a completed rk_sync, before the next step's compute_dt "
+                   "and with no upload in between");
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_compute_stats(streams_b200_ctx* c, int itav) {
+  int rc = stats_sample_check(c, itav);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  if ((rc = ensure_stats(c, false))) return rc;
+  SB_CHECK(c, launch_stats(c->g, c->d, c->fl_b, c->fl_a, c->p.rhork[2], c->p.gamrk[2], c->shift_pending ? 1 : 0,
+                           itav, c->stream, &c->launches));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_compute_stats_3d(streams_b200_ctx* c, int itav) {
+  int rc = stats_sample_check(c, itav);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  if ((rc = ensure_stats(c, true))) return rc;
+  SB_CHECK(c, launch_stats3d(c->g, c->d, itav, c->stream, &c->launches));
+  return STREAMS_B200_OK;
+}
+
+static int stats_buffer(streams_b200_ctx* c, int which, double** buf, long long* cnt) {
+  const long long n2 = (long long)NV_STAT * c->p.nx * c->p.ny;
+  int rc = ensure_stats(c, which == 2);
+  if (rc) return rc;
+  switch (which) {
+    case 0: *buf = c->d.wstat; *cnt = n2; break;
+    case 1: *buf = c->d.wstat_z; *cnt = n2; break;
+    case 2: *buf = c->d.wstat3d; *cnt = (long long)NV_STAT_3D * c->g.nint; break;
+    default: return set_err(c, STREAMS_B200_EINVAL, "statistics array: 0 w_stat, 1 w_stat_z, 2 w_stat_3d");
+  }
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_get_stats(streams_b200_ctx* c, int which, double* out, long long n) {
+  if (!c || !out) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  cudaSetDevice(c->device);
+  double* buf = nullptr;
+  long long cnt = 0;
+  int rc = stats_buffer(c, which, &buf, &cnt);
+  if (rc) return rc;
+  if (n < cnt) return set_err(c, STREAMS_B200_EINVAL, "output buffer too small");
+  SB_CHECK(c, cudaMemcpyAsync(out, buf, cnt * 8, cudaMemcpyDeviceToHost, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_set_stats(streams_b200_ctx* c, int which, const double* in, long long n) {
+  if (!c || !in) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  if (which == 1) return set_err(c, STREAMS_B200_EINVAL, "w_stat_z is recomputed by every sample");
+  cudaSetDevice(c->device);
+  double* buf = nullptr;
+  long long cnt = 0;
+  int rc = stats_buffer(c, which, &buf, &cnt);
+  if (rc) return rc;
+  if (n != cnt) return set_err(c, STREAMS_B200_EINVAL, "statistics array size mismatch");
+  SB_CHECK(c, cudaMemcpyAsync(buf, in, cnt * 8, cudaMemcpyHostToDevice, c->stream));
+  SB_CHECK(c, cudaStreamSynchronize(c->stream));
   return STREAMS_B200_OK;
 }
 

@@ -13,6 +13,9 @@ constexpr int NV = 5;
 // Number of FP64 reduction slots produced per block by the stage kernels.
 constexpr int NRED_RHS = 5;   // force_rhs: sum fln1*dy, fln2*dy, rho*dy, rhou*dy, rhou*T*dy
 constexpr int NRED_UPD = 8;   // force_var sum rhou*T*dy, residual sum, rho/T/p min and max
+// running statistics per (i,j) column and per cell (nv_stat, nv_stat_3d of singleideal.F90:474-478)
+constexpr int NV_STAT = 70;
+constexpr int NV_STAT_3D = 14;
 
 struct Geom {
   // block sizes and padded strides (ghosted arrays: index (i,j,k), i in 1-ng..nx+ng)
@@ -122,6 +125,20 @@ __device__ __forceinline__ double e_from_t(const Geom& g, double tt) {
   double ee = g.cv_last;
   ee = ee + g.cv0 * (tt / g.t0 - 1.0);
   return ee * g.t0;
+}
+
+// Apply force_var_2 (kernels_cpu.F90:3285-3314) to the conserved values of one interior point:
+// temperature from the (unshifted) state as force_var_1 computes it (:3241-3282), shifted by tbdiff.
+__device__ __forceinline__ double shifted_rhoe(const Geom& g, double rho, double rhou, double rhov, double rhow,
+                                               double rhoe, double tbdiff) {
+  double ri = 1.0 / rho;
+  double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
+  double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+  double ee = rhoe / rho - qq;
+  double tt = t_from_e(g, ee);
+  double ttnew = tt + tbdiff;
+  double en = e_from_t(g, ttnew);
+  return rho * en + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;
 }
 
 // viscosity law of eval_aux_subroutine (kernels_cpu.F90:6995-7002)

@@ -12,7 +12,8 @@ namespace sb200 {
 // Kernel identifiers of the optional per-kernel event profiler.
 enum KernelId {
   K_AUX = 0, K_EULER_X, K_VISC, K_EULER_Y, K_EULER_Z, K_FINISH_RHS, K_UPDATE, K_FINISH_UPD, K_DT, K_DT_FINISH,
-  K_INIT_SENSOR, K_APPLY_SHIFT, K_FILL_GHOSTS, K_COUNT_WENO, K_ADD_TIME, K_BC_FILL, K_BC_NR, K_RAND_PLANE, K_NUM
+  K_INIT_SENSOR, K_APPLY_SHIFT, K_FILL_GHOSTS, K_COUNT_WENO, K_ADD_TIME, K_BC_FILL, K_BC_NR, K_RAND_PLANE,
+  K_STATS, K_STATS3D, K_NUM
 };
 const char* kernel_name(int kid);
 
@@ -52,6 +53,11 @@ struct DevState {
   unsigned int* rwords = nullptr;  // raw draws of one stage
   double* recyc_av = nullptr;
   RngState* rng = nullptr;
+  // running statistics (allocated on first use), statistic index fastest:
+  // w_stat(70, nx, ny), w_stat_z(70, nx, ny), w_stat_3d(14, nx, ny, nz)
+  double* wstat = nullptr;
+  double* wstat_z = nullptr;
+  double* wstat3d = nullptr;
   Prof* prof = nullptr;       // optional per-kernel timing
 };
 
@@ -92,6 +98,11 @@ cudaError_t launch_bc_fill(const Geom& g, DevState& d, cudaStream_t s, long long
 cudaError_t launch_rand_plane(const Geom& g, DevState& d, cudaStream_t s, long long* nl);
 cudaError_t launch_bc_nr(const Geom& g, DevState& d, double* fl, cudaStream_t s, long long* nl);
 bool has_stored_ghosts(const Geom& g);
+// running statistics (stats_kernels.cu), sampled after a completed step: fl2 / fl3 are the RK
+// registers written by stages 2 and 3, pending says whether the force_var shift is still pending
+cudaError_t launch_stats(const Geom& g, DevState& d, const double* fl2, const double* fl3, double rhork3,
+                         double gamrk3, int pending, int itav, cudaStream_t s, long long* nl);
+cudaError_t launch_stats3d(const Geom& g, DevState& d, int itav, cudaStream_t s, long long* nl);
 long long reduction_slots(const Geom& g);
 
 }  // namespace sb200

@@ -54,20 +54,6 @@ constexpr int MT_NT = 128;                                     // march kernels
 #endif
 constexpr int FIN_NT = 1024;
 
-// Apply force_var_2 (kernels_cpu.F90:3285-3314) to the conserved values of one interior point:
-// temperature from the (unshifted) state as force_var_1 computes it (:3241-3282), shifted by tbdiff.
-__device__ __forceinline__ double shifted_rhoe(const Geom& g, double rho, double rhou, double rhov, double rhow,
-                                               double rhoe, double tbdiff) {
-  double ri = 1.0 / rho;
-  double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
-  double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-  double ee = rhoe / rho - qq;
-  double tt = t_from_e(g, ee);
-  double ttnew = tt + tbdiff;
-  double en = e_from_t(g, ttnew);
-  return rho * en + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;
-}
-
 // Primitive state of an interior point recomputed from w in FP64, with the operations of
 // eval_aux_subroutine (kernels_cpu.F90:6960-7011).
 struct Prim {
@@ -128,7 +114,8 @@ __device__ __forceinline__ void point_state(const Geom& g, const double* __restr
 }
 
 // w -> aux at all interior and face-ghost points (eval_aux_subroutine, kernels_cpu.F90:6960-7011),
-// computed in FP64 and stored as A; with write_ghost_w the ghost states are also stored into w.
+// computed in FP64 and stored as A; with write_ghost_w = 1 the ghost states are also stored into
+// w, with write_ghost_w = 2 only they are (aux is left as it is).
 template <class A>
 __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, A* __restrict__ aux,
                                                 int write_ghost_w) {
@@ -141,6 +128,7 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   const int i = ii - g.ng + 1, j = jj - g.ng + 1, k = kk - g.ng + 1;
   const int ox = (i < 1 || i > g.nx), oy = (j < 1 || j > g.ny), oz = (k < 1 || k > g.nz);
   if (ox + oy + oz > 1) return;  // halo edges and corners are never read
+  if (write_ghost_w == 2 && !(ox | oy | oz)) return;
   double st[5];
   point_state(g, w, i, j, k, st);
   double rho = st[0], rhou = st[1], rhov = st[2], rhow = st[3], rhoe = st[4];
@@ -148,6 +136,7 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   if (write_ghost_w && (ox | oy | oz)) {
     w[dst] = rho; w[n + dst] = rhou; w[2 * n + dst] = rhov; w[3 * n + dst] = rhow; w[4 * n + dst] = rhoe;
   }
+  if (write_ghost_w == 2) return;  // ghost layers of w only; aux keeps its values
   double ri = 1.0 / rho;
   double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
   double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
@@ -830,7 +819,7 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
                                                 const double* __restrict__ fl_new, const Scalars* __restrict__ sc,
                                                 double rhork, double gamrk, int istep, int stats,
                                                 double* __restrict__ red, const double* __restrict__ sensor_next,
-                                                double* __restrict__ sensor) {
+                                                double* __restrict__ sensor, R* __restrict__ aux) {
   __shared__ double sm[2 * 8];
   __shared__ double smn[3 * 8];
   __shared__ double smx[3 * 8];
@@ -874,6 +863,8 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
       double tt = t_from_e(g, ee);
       s2[0] = wn[1] * tt * dy;
       tstat = tt;
+      // force_var_1 leaves this temperature in w_aux(6), where the statistics read it
+      if (istep == 3) aux[5 * n + c] = R(tt);
     }
     if (stats) {
       double r = fln[1] / dt;
@@ -1004,7 +995,7 @@ const char* kernel_name(int kid) {
   static const char* names[K_NUM] = {"k_aux", "k_euler_x", "k_visc", "k_euler_y", "k_euler_z", "k_finish_rhs",
                                      "k_update", "k_finish_upd", "k_dt", "k_dt_finish", "k_init_sensor",
                                      "k_apply_shift", "k_fill_ghosts", "k_count_weno", "k_add_time",
-                                     "k_bc_fill", "k_bc_nr", "k_rand_plane"};
+                                     "k_bc_fill", "k_bc_nr", "k_rand_plane", "k_stats", "k_stats3d"};
   return (kid >= 0 && kid < K_NUM) ? names[kid] : "?";
 }
 
@@ -1101,8 +1092,8 @@ cudaError_t launch_aux(const Geom& g, DevState& d, int apply_shift, cudaStream_t
 }
 
 cudaError_t launch_fill_ghosts(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
-  if (g.precision == 1) aux_launch<float>(g, d, 0, 1, K_FILL_GHOSTS, s, nl);
-  else aux_launch<double>(g, d, 0, 1, K_FILL_GHOSTS, s, nl);
+  if (g.precision == 1) aux_launch<float>(g, d, 0, 2, K_FILL_GHOSTS, s, nl);
+  else aux_launch<double>(g, d, 0, 2, K_FILL_GHOSTS, s, nl);
   return cudaGetLastError();
 }
 
@@ -1213,7 +1204,7 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   const unsigned nbu = nblocks(g.nint, 256);
   SB_LAUNCH(d, K_UPDATE, s,
             k_update<R><<<nbu, 256, 0, s>>>(g, d.w, fl_prev, fl_new, d.sc, a.rhork, a.gamrk, a.istep,
-                                            a.want_stats, d.red, sensor_next, sensor));
+                                            a.want_stats, d.red, sensor_next, sensor, aux));
   SB_LAUNCH(d, K_FINISH_UPD, s, k_finish_upd<<<1, FIN_NT, 0, s>>>(g, d.red, nbu, a.want_stats, a.add_time, d.sc));
   *nl += 2;
   if (has_stored_ghosts(g)) launch_bc_fill(g, d, s, nl);  // update_ghost

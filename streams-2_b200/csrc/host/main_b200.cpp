@@ -1,5 +1,6 @@
 // Stand-alone driver: the counterpart of main_<backend>.F90 (code/src/singleideal/main_cpu.F90:1-18)
-// for the B200 backend.  Runs <dir>/singleideal.ini on the current GPU, writes <dir>/progress.out.
+// for the B200 backend.  Runs <dir>/singleideal.ini on the current GPU, writes <dir>/progress.out
+// and, at the end, the restart files of the reference's run() into <dir>.
 //   streams_b200_run <dir> [nsteps] [precision]
 #include <cstdio>
 #include <cstdlib>
@@ -22,7 +23,9 @@ int main(int argc, char** argv) {
   }
   double row[14];
   const std::string prog = dir + "/progress.out";
-  int rc = streams_b200_run_case(c, nsteps, prec, prog.c_str(), row, nullptr);
+  // as run() ends: rst.bin, stat.bin / stat3d.bin (when [output] dtstat is set) and field_info0.dat
+  int rc = streams_b200_run_case_stats(c, nsteps, prec, prog.c_str(), row, nullptr, nullptr, nullptr, nullptr,
+                                       dir.c_str());
   if (rc) {
     std::fprintf(stderr, "run failed (%d): %s\n", rc, streams_b200_case_error());
     streams_b200_case_free(c);

@@ -661,6 +661,31 @@ void read_field_info(Setup& s) {
   IniFile fi = IniFile::parse_file(s.dir + "/field_info0.dat");
   s.icyc0 = fi.get_int("field_info", "icyc0");
   s.time0 = fi.get_double("field_info", "time0");
+  s.itav = fi.get_int_or("field_info", "itav", 0);
+  s.time_from_last_stat = fi.get_double_or("field_info", "time_from_last_stat", 0.0);
+}
+
+// read_stats / read_stats_3d (singleideal.F90:1646-1700, 1728-1783): per statistic one global
+// plane (nx*ny) or volume (nx*ny*nz) in Fortran order, transposed into w_stat(l, i, j[, k])
+void read_stats_files(Setup& s) {
+  auto read_blocks = [&](const std::string& name, int nv, size_t block, std::vector<double>& out) {
+    const std::string path = s.dir + "/" + name;
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw InputError("cannot open " + path + " (restart_type = 2)");
+    out.assign(static_cast<size_t>(nv) * block, 0.0);
+    std::vector<double> b(block);
+    for (int l = 0; l < nv; ++l) {
+      if (std::fread(b.data(), sizeof(double), block, f) != block) {
+        std::fclose(f);
+        throw InputError(name + " is too short");
+      }
+      for (size_t q = 0; q < block; ++q) out[q * nv + l] = b[q];
+    }
+    std::fclose(f);
+  };
+  const size_t n2 = static_cast<size_t>(s.nxmax) * s.nymax;
+  if (s.enable_stat_time > 0) read_blocks("stat.bin", 70, n2, s.w_stat);
+  if (s.enable_stat_3d > 0) read_blocks("stat3d.bin", 14, n2 * s.nzmax, s.w_stat_3d);
 }
 
 }  // namespace
@@ -776,6 +801,11 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
   }
   for (int l = 0; l < 6; ++l) s.bctags_nr[l] = c.get_int("bc", std::string(bcn[l]) + "_nr");
   s.restart_type = c.get_int("controls", "restart_type");
+  if (s.restart_type < 0 || s.restart_type > 2) throw InputError("restart_type must be 0, 1 or 2");
+  // [output] statistics keys (singleideal.F90:542-551, 818)
+  s.dtstat = c.get_double_or("output", "dtstat", -1.0);
+  s.enable_stat_time = c.get_int_or("output", "enable_stat_time", 1);
+  s.enable_stat_3d = c.get_int_or("output", "enable_stat_3d", 0);
   s.grid_type = c.get_int("grid", "grid_type");
   bool rebuild_ghost = (s.grid_type == GRID_FROMFILE);
   if (s.restart_type > 0) s.grid_type = GRID_FROMFILE;
@@ -987,8 +1017,12 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
       read_field_info(s);
     }
   }
-  if (s.restart_type == 2)
-    throw InputError("restart_type = 2 (statistics restart) is not supported by the B200 backend");
+  if (s.restart_type == 2) {
+    // restart with statistics: the field and clock as for restart_type = 1, then the averages
+    read_rst(s);
+    read_field_info(s);
+    read_stats_files(s);
+  }
   s.recyc = s.bctags[0] == 10;
   if (s.recyc) {
     if (s.flow_init != 1 || s.wmean.empty()) throw InputError("recycling inflow needs the boundary-layer initialisation");
@@ -1058,22 +1092,9 @@ void write_restart_inputs(const Setup& s, const std::string& dir) {
   write_restart_state(s, s.w.data(), s.icyc0, s.time0, dir);
 }
 
-// The files of a restart (restart_type = 1) from a conserved field w of the case: grid files,
-// rst.bin (per variable, Fortran order, interior points: the single-block layout of the
-// reference's MPI-IO file, code/src/field.F90:1853-1966), field_info0.dat with every key that
-// read_field_info (singleideal.F90:2546-2590) reads unconditionally (the output clocks start
-// afresh), and singleideal.ini = the case's input with restart_type = 1.
-void write_restart_state(const Setup& s, const double* w, int icyc, double time, const std::string& dir) {
-  auto col = [&](const std::string& name, const OffsetArray& a, int lo, int hi) {
-    FILE* f = std::fopen((dir + "/" + name).c_str(), "w");
-    if (!f) throw InputError("cannot write " + dir + "/" + name);
-    for (int i = lo; i <= hi; ++i) std::fprintf(f, "%.17e\n", a(i));
-    std::fclose(f);
-  };
-  col("x.dat", s.xg, 1 - s.ng, s.nxmax + s.ng + 1);
-  col("y.dat", s.yg, 1 - s.ng, s.nymax + s.ng);
-  col("z.dat", s.zg, 1 - s.ng, s.nzmax + s.ng);
-  col("yn.dat", s.yn, 1, s.nymax + 1);
+namespace {
+
+void write_rst(const Setup& s, const double* w, const std::string& dir) {
   FILE* f = std::fopen((dir + "/rst.bin").c_str(), "wb");
   if (!f) throw InputError("cannot write rst.bin");
   std::vector<double> plane(static_cast<size_t>(s.nxmax));
@@ -1084,21 +1105,75 @@ void write_restart_state(const Setup& s, const double* w, int icyc, double time,
         std::fwrite(plane.data(), sizeof(double), plane.size(), f);
       }
   std::fclose(f);
+}
+
+// field_info0.dat with every key that read_field_info (singleideal.F90:2546-2590) reads
+// unconditionally; the output clocks other than the statistics' start afresh
+void write_field_info(const std::string& dir, int icyc, double time, const StatsOut* st) {
   FILE* fi = std::fopen((dir + "/field_info0.dat").c_str(), "w");
   if (!fi) throw InputError("cannot write field_info0.dat");
   std::fprintf(fi,
-               "[field_info]\nicyc0 = %d\ntime0 = %.17e\nitav = 0\nitslice_p3d = 0\ntime_from_last_rst = 0.0\n"
-               "time_from_last_write = 0.0\ntime_from_last_stat = 0.0\ntime_from_last_slice = 0.0\n"
+               "[field_info]\nicyc0 = %d\ntime0 = %.17e\nitav = %d\nitslice_p3d = 0\ntime_from_last_rst = 0.0\n"
+               "time_from_last_write = 0.0\ntime_from_last_stat = %.17e\ntime_from_last_slice = 0.0\n"
                "time_from_last_probe = 0.0\nistore = 1\n",
-               icyc, time);
+               icyc, time, st ? st->itav : 0, st ? st->time_from_last_stat : 0.0);
   std::fclose(fi);
+}
+
+// write_stats / write_stats_3d (singleideal.F90:1786-1834, 1922-1965): one block per statistic
+void write_stats_files(const Setup& s, const std::string& dir, const StatsOut& st) {
+  auto write_blocks = [&](const std::string& name, const double* a, int nv, size_t block) {
+    FILE* f = std::fopen((dir + "/" + name).c_str(), "wb");
+    if (!f) throw InputError("cannot write " + name);
+    std::vector<double> b(block);
+    for (int l = 0; l < nv; ++l) {
+      for (size_t q = 0; q < block; ++q) b[q] = a[q * nv + l];
+      std::fwrite(b.data(), sizeof(double), block, f);
+    }
+    std::fclose(f);
+  };
+  const size_t n2 = static_cast<size_t>(s.nxmax) * s.nymax;
+  if (st.w_stat) write_blocks("stat.bin", st.w_stat, 70, n2);
+  if (st.w_stat_3d) write_blocks("stat3d.bin", st.w_stat_3d, 14, n2 * s.nzmax);
+}
+
+}  // namespace
+
+// The files of a restart from a conserved field w of the case: grid files, rst.bin (per
+// variable, Fortran order, interior points: the single-block layout of the reference's MPI-IO
+// file, code/src/field.F90:1853-1966), field_info0.dat, the statistics files when given, and
+// singleideal.ini = the case's input with restart_type = 1, or 2 with statistics.
+void write_restart_state(const Setup& s, const double* w, int icyc, double time, const std::string& dir,
+                         const StatsOut* st) {
+  auto col = [&](const std::string& name, const OffsetArray& a, int lo, int hi) {
+    FILE* f = std::fopen((dir + "/" + name).c_str(), "w");
+    if (!f) throw InputError("cannot write " + dir + "/" + name);
+    for (int i = lo; i <= hi; ++i) std::fprintf(f, "%.17e\n", a(i));
+    std::fclose(f);
+  };
+  col("x.dat", s.xg, 1 - s.ng, s.nxmax + s.ng + 1);
+  col("y.dat", s.yg, 1 - s.ng, s.nymax + s.ng);
+  col("z.dat", s.zg, 1 - s.ng, s.nzmax + s.ng);
+  col("yn.dat", s.yn, 1, s.nymax + 1);
+  write_run_output(s, w, icyc, time, dir, st);
   IniFile ini = s.ini;
-  ini.set("controls", "restart_type", "1");
+  ini.set("controls", "restart_type", st ? "2" : "1");
+  if (st) {
+    ini.set("output", "enable_stat_time", st->w_stat ? "1" : "0");
+    ini.set("output", "enable_stat_3d", st->w_stat_3d ? "1" : "0");
+  }
   FILE* fin = std::fopen((dir + "/singleideal.ini").c_str(), "w");
   if (!fin) throw InputError("cannot write singleideal.ini");
   const std::string text = ini.to_text();
   std::fwrite(text.data(), 1, text.size(), fin);
   std::fclose(fin);
+}
+
+void write_run_output(const Setup& s, const double* w, int icyc, double time, const std::string& dir,
+                      const StatsOut* st) {
+  write_rst(s, w, dir);
+  if (st) write_stats_files(s, dir, *st);
+  write_field_info(dir, icyc, time, st);
 }
 
 }  // namespace streams_b200

@@ -103,6 +103,15 @@ struct Setup {
   double xshock_imp = 0, shock_angle = 0, tanhfacs = 1;
   double winf_past_shock[5] = {0, 0, 0, 0, 0};
 
+  // running statistics ([output] dtstat, enable_stat_time, enable_stat_3d): the averaging clock
+  // and, on a restart with restart_type = 2, the averages read from stat.bin / stat3d.bin in the
+  // reference's layouts w_stat(70, nx, ny), w_stat_3d(14, nx, ny, nz) (empty: start from zero)
+  double dtstat = -1.0;  // < 0: the key is absent and the stand-alone run loop samples nothing
+  int enable_stat_time = 1, enable_stat_3d = 0;
+  int itav = 0;
+  double time_from_last_stat = 0.0;
+  std::vector<double> w_stat, w_stat_3d;
+
   // initial conserved field w(1-ng:nx+ng,1-ng:ny+ng,1-ng:nz+ng,5), Fortran order
   std::vector<double> w;
 
@@ -132,8 +141,20 @@ double get_reynolds_cha(double retau, double rm, double trat, double s2tinf, dou
 // Write the files with which the reference itself starts the same case:
 // x.dat, y.dat, z.dat, yn.dat (with ghosts), rst.bin and field_info0.dat.
 void write_restart_inputs(const Setup& s, const std::string& dir);
+// Running statistics to write with a restart (null arrays are not written).
+struct StatsOut {
+  const double* w_stat = nullptr;     // (70, nx, ny)
+  const double* w_stat_3d = nullptr;  // (14, nx, ny, nz)
+  int itav = 0;
+  double time_from_last_stat = 0.0;
+};
 // The same from a conserved field w (ghosted, Fortran order) at step icyc and time, plus a
-// singleideal.ini of the case with restart_type = 1: a run resumes from dir.
-void write_restart_state(const Setup& s, const double* w, int icyc, double time, const std::string& dir);
+// singleideal.ini of the case with restart_type = 1 (2 with statistics): a run resumes from dir.
+void write_restart_state(const Setup& s, const double* w, int icyc, double time, const std::string& dir,
+                         const StatsOut* st = nullptr);
+// The files the end of run() writes (singleideal_gpu.F90:1660-1683): rst.bin, stat.bin and
+// stat3d.bin when given, field_info0.dat.
+void write_run_output(const Setup& s, const double* w, int icyc, double time, const std::string& dir,
+                      const StatsOut* st);
 
 }  // namespace streams_b200

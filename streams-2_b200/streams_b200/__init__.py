@@ -103,6 +103,10 @@ def _load() -> C.CDLL:
         "streams_b200_compute_residual": (I, [P, D]),
         "streams_b200_count_weno": (I, [P, D]),
         "streams_b200_get_wallprop": (I, [P, D]),
+        "streams_b200_compute_stats": (I, [P, I]),
+        "streams_b200_compute_stats_3d": (I, [P, I]),
+        "streams_b200_get_stats": (I, [P, I, D, LL]),
+        "streams_b200_set_stats": (I, [P, I, D, LL]),
         "streams_b200_synchronize": (I, [P]),
         "streams_b200_launch_count": (LL, [P]),
         "streams_b200_debug_fetch": (I, [P, I, D, LL]),
@@ -122,6 +126,10 @@ def _load() -> C.CDLL:
         "streams_b200_case_write_restart": (I, [P, C.c_char_p]),
         "streams_b200_case_write_state": (I, [P, D, I, C.c_double, C.c_char_p]),
         "streams_b200_run_case": (I, [P, I, I, C.c_char_p, D, D]),
+        "streams_b200_run_case_stats": (I, [P, I, I, C.c_char_p, D, D, D, D, D, C.c_char_p]),
+        "streams_b200_case_write_state_stats": (I, [P, D, I, C.c_double, D, D, I, C.c_double, C.c_char_p]),
+        "streams_b200_case_stats_info": (I, [P, D]),
+        "streams_b200_case_stats": (I, [P, I, D, LL]),
         "streams_b200_set_tuning": (I, [P, LL, I]),
         "streams_b200_get_tuning": (I, [P, C.POINTER(LL), C.POINTER(I)]),
         "streams_b200_batch_create": (I, [C.POINTER(P), I, I, I, C.POINTER(P)]),
@@ -149,11 +157,15 @@ EXPORTED = [
     "streams_b200_init_run", "streams_b200_compute_dt", "streams_b200_set_dt", "streams_b200_rk_sync",
     "streams_b200_advance", "streams_b200_get_scalars", "streams_b200_set_time", "streams_b200_compute_residual",
     "streams_b200_count_weno", "streams_b200_get_wallprop", "streams_b200_synchronize",
+    "streams_b200_compute_stats", "streams_b200_compute_stats_3d", "streams_b200_get_stats",
+    "streams_b200_set_stats",
     "streams_b200_launch_count", "streams_b200_debug_fetch", "streams_b200_get_stream",
     "streams_b200_profile_enable", "streams_b200_profile_read", "streams_b200_kernel_count",
     "streams_b200_kernel_name", "streams_b200_compute_dt_noalloc", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
     "streams_b200_case_params", "streams_b200_case_grid", "streams_b200_case_field", "streams_b200_case_info",
     "streams_b200_case_write_restart", "streams_b200_case_write_state", "streams_b200_run_case",
+    "streams_b200_run_case_stats", "streams_b200_case_write_state_stats", "streams_b200_case_stats_info",
+    "streams_b200_case_stats",
     "streams_b200_set_tuning",
     "streams_b200_get_tuning", "streams_b200_batch_create", "streams_b200_batch_advance",
     "streams_b200_batch_synchronize", "streams_b200_batch_invalidate", "streams_b200_batch_stats",
@@ -241,6 +253,58 @@ class Case:
         if rc != OK:
             raise BackendError(rc, lib.streams_b200_case_error().decode())
         return row, w
+
+    def stats_info(self) -> dict:
+        """[output] statistics settings and the restart's averaging clock."""
+        out = np.zeros(5)
+        lib.streams_b200_case_stats_info(self._h, _dptr(out))
+        return dict(zip(["dtstat", "enable_stat_time", "enable_stat_3d", "itav", "time_from_last_stat"],
+                        out.tolist()))
+
+    def restart_stats(self, which: int = 0) -> np.ndarray:
+        """Averages read on a restart_type = 2 restart (zeros otherwise): w_stat as (ny, nx, 70),
+        w_stat_3d (which = 2) as (nz, ny, nx, 14)."""
+        nx, ny, nz, _ = self.shape
+        shape = (ny, nx, 70) if which == 0 else (nz, ny, nx, 14)
+        out = np.zeros(shape)
+        rc = lib.streams_b200_case_stats(self._h, which, _dptr(out), out.size)
+        if rc != OK:
+            raise BackendError(rc, "case statistics: which must be 0 or 2")
+        return out
+
+    def write_state_stats(self, w: np.ndarray, icyc: int, time: float, w_stat: np.ndarray | None,
+                          w_stat_3d: np.ndarray | None, itav: int, time_from_last_stat: float,
+                          directory: str | os.PathLike) -> None:
+        """write_state plus stat.bin / stat3d.bin and the averaging clock (restart_type = 2)."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        a2 = None if w_stat is None else np.ascontiguousarray(w_stat, dtype=np.float64)
+        a3 = None if w_stat_3d is None else np.ascontiguousarray(w_stat_3d, dtype=np.float64)
+        rc = lib.streams_b200_case_write_state_stats(
+            self._h, _dptr(w), int(icyc), float(time), _dptr(a2) if a2 is not None else None,
+            _dptr(a3) if a3 is not None else None, int(itav), float(time_from_last_stat), str(directory).encode())
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_case_error().decode())
+
+    def run_stats(self, nsteps: int = -1, precision: int = 0, progress_path: str | None = None,
+                  output_dir: str | os.PathLike | None = None) -> dict:
+        """run() with the statistics of [output] dtstat: returns the last progress row, the final
+        field, w_stat (ny, nx, 70), w_stat_3d (nz, ny, nx, 14) and the averaging clock; with
+        output_dir the end-of-run files are written there."""
+        nx, ny, nz, ng = self.shape
+        row = np.zeros(14)
+        w = np.zeros((5, nz + 2 * ng, ny + 2 * ng, nx + 2 * ng))
+        s2 = np.zeros((ny, nx, 70))
+        info = self.stats_info()
+        s3 = np.zeros((nz, ny, nx, 14)) if info["enable_stat_3d"] > 0 else None
+        clock = np.zeros(2)
+        rc = lib.streams_b200_run_case_stats(
+            self._h, nsteps, precision, progress_path.encode() if progress_path else None, _dptr(row), _dptr(w),
+            _dptr(s2), _dptr(s3) if s3 is not None else None, _dptr(clock),
+            str(output_dir).encode() if output_dir is not None else None)
+        if rc != OK:
+            raise BackendError(rc, lib.streams_b200_case_error().decode())
+        return {"row": row, "w": w, "w_stat": s2, "w_stat_3d": s3, "itav": int(clock[0]),
+                "time_from_last_stat": float(clock[1])}
 
 
 class Solver:
@@ -343,6 +407,36 @@ class Solver:
 
     def synchronize(self):
         self._check(lib.streams_b200_synchronize(self._h))
+
+    NV_STAT, NV_STAT_3D = 70, 14
+
+    def compute_stats(self, itav: int) -> None:
+        """compute_stats after a step: fold the step's z-averaged statistics into w_stat, which
+        already averages itav samples (manage_output then increments itav)."""
+        self._check(lib.streams_b200_compute_stats(self._h, int(itav)))
+
+    def compute_stats_3d(self, itav: int) -> None:
+        """compute_stats_3d after a step: the 14 point statistics averaged in time."""
+        self._check(lib.streams_b200_compute_stats_3d(self._h, int(itav)))
+
+    def _stats_shape(self, which: int):
+        nx, ny, nz, _ = self.shape
+        if which in (0, 1):
+            return (ny, nx, self.NV_STAT)
+        if which == 2:
+            return (nz, ny, nx, self.NV_STAT_3D)
+        raise ValueError("which: 0 w_stat, 1 w_stat_z, 2 w_stat_3d")
+
+    def stats(self, which: int = 0) -> np.ndarray:
+        """w_stat (0) or w_stat_z (1) as (ny, nx, 70) arrays, w_stat_3d (2) as (nz, ny, nx, 14):
+        the reference's Fortran arrays w_stat(70, nx, ny) ... with the index order reversed."""
+        out = np.zeros(self._stats_shape(which))
+        self._check(lib.streams_b200_get_stats(self._h, which, _dptr(out), out.size))
+        return out
+
+    def set_stats(self, which: int, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(self._stats_shape(which))
+        self._check(lib.streams_b200_set_stats(self._h, which, _dptr(a), a.size))
 
     def debug_fetch(self, which: int) -> np.ndarray:
         """Internal arrays: 0 aux (7 ghosted), 1 last stage RHS fl (5), 2 sensor, 3 div/3."""
