@@ -105,20 +105,42 @@ contains
   endsubroutine initialize
 
   ! run() of singleideal_cpu.F90:1519-1693 for the channel: the device advances print_control
-  ! steps at a time without host synchronisation; progress rows as print_progress writes them.
+  ! steps at a time without host synchronisation (one at a time while statistics are sampled:
+  ! the clock of manage_output needs every step's dt); progress rows as print_progress writes
+  ! them; statistics sampled on the device as manage_output samples them
+  ! (singleideal_gpu.F90:2012-2034) and brought back for write_stats at the end.
   subroutine run(self, filename)
     class(equation_singleideal_b200_object), intent(inout), target :: self
     character(*), intent(in) :: filename
     real(c_double) :: sc(7), res(7)
     integer(c_int) :: chunk, rc
+    logical :: stats
     call self%initialize(filename)
     associate(eb => self%equation_base)
+      stats = eb%enable_stat_time > 0 .or. eb%enable_stat_3d > 0
+      if (eb%restart_type == 2) then
+        if (eb%enable_stat_time > 0) call self%check(streams_b200_set_stats(self%ctx, 0, c_loc(eb%w_stat), &
+                                     int(size(eb%w_stat), c_long_long)), 'set_stats')
+        if (eb%enable_stat_3d > 0) call self%check(streams_b200_set_stats(self%ctx, 2, c_loc(eb%w_stat_3d), &
+                                     int(size(eb%w_stat_3d), c_long_long)), 'set_stats')
+      endif
       call self%check(streams_b200_init_run(self%ctx), 'init_run')
       do while (eb%icyc - eb%icyc0 < eb%num_iter)
         chunk = min(eb%print_control - mod(eb%icyc - eb%icyc0, eb%print_control), &
                     eb%num_iter - (eb%icyc - eb%icyc0))
+        if (stats) chunk = 1
         call self%check(streams_b200_advance(self%ctx, chunk, eb%iter_dt_recompute, eb%icyc, eb%icyc0), 'advance')
         eb%icyc = eb%icyc + chunk
+        if (stats) then
+          call self%check(streams_b200_get_scalars(self%ctx, sc), 'get_scalars')
+          eb%time_from_last_stat = eb%time_from_last_stat + sc(1)
+          if (eb%time_from_last_stat >= eb%dtstat) then
+            if (eb%enable_stat_time > 0) call self%check(streams_b200_compute_stats(self%ctx, eb%itav), 'stats')
+            if (eb%enable_stat_3d > 0) call self%check(streams_b200_compute_stats_3d(self%ctx, eb%itav), 'stats_3d')
+            eb%time_from_last_stat = 0._rkind
+            eb%itav = eb%itav + 1
+          endif
+        endif
         if (mod(eb%icyc - eb%icyc0, eb%print_control) == 0) then
           rc = streams_b200_compute_residual(self%ctx, res)
           call self%check(streams_b200_get_scalars(self%ctx, sc), 'get_scalars')
@@ -136,6 +158,16 @@ contains
       enddo
       call self%check(streams_b200_copy_to_field(self%ctx, c_loc(eb%field%w)), 'copy_to_field')
       call eb%field%write_field()
+      if (eb%enable_stat_time > 0) then
+        call self%check(streams_b200_get_stats(self%ctx, 0, c_loc(eb%w_stat), int(size(eb%w_stat), c_long_long)), &
+                        'get_stats')
+        call eb%write_stats()
+      endif
+      if (eb%enable_stat_3d > 0) then
+        call self%check(streams_b200_get_stats(self%ctx, 2, c_loc(eb%w_stat_3d), &
+                        int(size(eb%w_stat_3d), c_long_long)), 'get_stats')
+        call eb%write_stats_3d()
+      endif
       call eb%write_field_info()
     endassociate
     call self%check(streams_b200_destroy(self%ctx), 'destroy')

@@ -121,6 +121,36 @@ module streams_b200_mod
       real(c_double), intent(out) :: out(3)
       integer(c_int) :: streams_b200_count_weno
     end function
+    ! running statistics (compute_stats / compute_stats_3d after a completed step)
+    function streams_b200_compute_stats(ctx, itav) bind(c, name="streams_b200_compute_stats")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: itav
+      integer(c_int) :: streams_b200_compute_stats
+    end function
+    function streams_b200_compute_stats_3d(ctx, itav) bind(c, name="streams_b200_compute_stats_3d")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: itav
+      integer(c_int) :: streams_b200_compute_stats_3d
+    end function
+    ! which = 0: w_stat(70,nx,ny), 1: w_stat_z, 2: w_stat_3d(14,nx,ny,nz); n in doubles
+    function streams_b200_get_stats(ctx, which, out, n) bind(c, name="streams_b200_get_stats")
+      import :: c_int, c_ptr, c_long_long
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: which
+      type(c_ptr), value :: out
+      integer(c_long_long), value :: n
+      integer(c_int) :: streams_b200_get_stats
+    end function
+    function streams_b200_set_stats(ctx, which, in, n) bind(c, name="streams_b200_set_stats")
+      import :: c_int, c_ptr, c_long_long
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: which
+      type(c_ptr), value :: in
+      integer(c_long_long), value :: n
+      integer(c_int) :: streams_b200_set_stats
+    end function
     function streams_b200_last_error(ctx) bind(c, name="streams_b200_last_error")
       import :: c_ptr
       type(c_ptr), value :: ctx
