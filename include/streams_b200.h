@@ -27,7 +27,9 @@
 extern "C" {
 #endif
 
-#define STREAMS_B200_ABI_VERSION 2
+#define STREAMS_B200_ABI_VERSION 3
+/* largest number of cp(T) polynomial coefficients (indx_cp_r - indx_cp_l + 2) */
+#define STREAMS_B200_MAX_CP 12
 
 /* error codes */
 #define STREAMS_B200_OK 0
@@ -61,7 +63,7 @@ typedef struct streams_b200_params {
   int is_y_staggered;       /* staggered y walls (channel) */
   /* fluid (set_fluid_prop, singleideal.F90:2685-2774) */
   int visc_model;           /* 0 inviscid, 1 power law, 2 Sutherland */
-  int calorically_perfect;  /* 1 constant cp (the only one on the device path) */
+  int calorically_perfect;  /* 1 constant cp, 0 cp(T) polynomial (thermally perfect, FP64 form) */
   double mu0, t0, rgas0, rho0, u0, l0;
   double sutherland_s, t_ref_dim, powerlaw_vtexp, prandtl;
   double cp0, cv0;          /* cp_coeff(0), cv_coeff(0) */
@@ -91,6 +93,13 @@ typedef struct streams_b200_params {
    * shock angle [rad], tanh smoothing length, post-shock conserved state */
   double xshock_imp, shock_angle, tanhfacs;
   double winf_past_shock[5];
+  /* thermally perfect gas (calorically_perfect = 0): cp(T)/rgas0 = sum of cp_coeff(l) (T/t0)^l,
+   * l = indx_cp_l..indx_cp_r, and the energy datum at l = indx_cp_r+1, as set_fluid_prop leaves
+   * cp_coeff and cv_coeff (times rgas0); stored at [l - indx_cp_l].  For calorically_perfect = 1
+   * indx_cp_l = indx_cp_r = 0 and the two entries equal cp0, cp_last (cv0, cv_last). */
+  int indx_cp_l, indx_cp_r;
+  double cp_coeff[STREAMS_B200_MAX_CP];
+  double cv_coeff[STREAMS_B200_MAX_CP];
 } streams_b200_params;
 
 /*
@@ -216,7 +225,8 @@ int streams_b200_get_wallprop(streams_b200_ctx* ctx, double* out /* nx*nz*3 */);
  *   w_stat = (w_stat*itav + w_stat_z)/(itav + 1);
  * compute_stats_3d does the same per cell for the 14 quantities of w_stat_3d(14, nx, ny, nz).
  * The arrays live on the device (allocated on first use, zero-initialised: 2*70*nx*ny and
- * 14*nx*ny*nz doubles) in the reference's layout, statistic index fastest.  get_stats /
+ * 14*nx*ny*nz doubles, plus a scratch of 3 doubles per ghosted point for the velocities of a
+ * sample) in the reference's layout, statistic index fastest.  get_stats /
  * set_stats copy which = 0 (w_stat), 1 (w_stat_z of the last sample, read only) or
  * 2 (w_stat_3d); n is the buffer size in doubles (set_stats: exactly the array size), e.g. to
  * restore w_stat from stat.bin on a restart with restart_type = 2 (read_stats, :1646-1700).

@@ -261,6 +261,61 @@ Solver::Solver(const Setup& setup) : s(setup) {
   rng.discard(s.rng_draws);
 }
 
+// get_temperature_from_e_dev (kernels_cpu.F90:7116-7152)
+double Solver::temp_from_e(double ee, double t_start) const {
+  const double t0 = s.t0;
+  const double ebar = ee - cv(s.indx_cp_r + 1) * t0;
+  if (s.calorically_perfect == 1) return t0 + ebar / cv(0);
+  double t_old = t_start, tt = t_start;
+  for (int iter = 1; iter <= 50; ++iter) {
+    double den = 0.0, num = 0.0;
+    for (int l = s.indx_cp_l; l <= s.indx_cp_r; ++l) {
+      const double t_pow = std::pow(t_old / t0, l);
+      if (l == -1) {
+        den = den + cv(l) * t_pow;
+        num = num + cv(l) * std::log(t_old / t0);
+      } else {
+        const double t_powp = (t_old / t0) * t_pow;
+        den = den + cv(l) * t_pow;
+        num = num + cv(l) * (t_powp - 1.0) / (l + 1.0);
+      }
+    }
+    num = num * t0;
+    tt = t_old + (ebar - num) / den;
+    if (std::fabs(tt - t_old) < 1e-12) break;
+    t_old = tt;
+  }
+  return tt;
+}
+
+// get_e_from_temperature_dev (kernels_cpu.F90:7155-7176)
+double Solver::e_from_temp(double tt) const {
+  const double t0 = s.t0;
+  double ee = cv(s.indx_cp_r + 1);
+  if (s.calorically_perfect == 1) {
+    ee = ee + cv(0) * (tt / t0 - 1.0);
+  } else {
+    for (int l = s.indx_cp_l; l <= s.indx_cp_r; ++l) {
+      if (l == -1) ee = ee + cv(l) * std::log(tt / t0);
+      else ee = ee + cv(l) / (l + 1.0) * (std::pow(tt / t0, l + 1) - 1.0);
+    }
+  }
+  return ee * t0;
+}
+
+// cp(T) of get_gamloc_dev (kernels_cpu.F90:7096-7113) and of the viscous routines
+double Solver::cploc_at(double tt) const {
+  if (s.calorically_perfect == 1) return cp(0);
+  double cploc = 0.0;
+  for (int l = s.indx_cp_l; l <= s.indx_cp_r; ++l) cploc = cploc + cp(l) * std::pow(tt / s.t0, l);
+  return cploc;
+}
+
+double Solver::gamloc_at(double tt) const {
+  const double cploc = cploc_at(tt);
+  return cploc / (cploc - s.rgas0);
+}
+
 // base_cpu%bcswap (code/src/base_cpu.F90:1326-1435) on one block: face halos of periodic directions
 void Solver::bcswap() {
   if (s.periodic[0])
@@ -334,7 +389,7 @@ void Solver::update_ghost(int do_swap) {
 // bcwall_staggered_subroutine (kernels_cpu.F90:6612-6678)
 void Solver::bcwall_staggered(int ilat) {
   if (ilat != 3 && ilat != 4) return;
-  const double twall = s.t_wall, t0 = s.t0, rgas0 = s.rgas0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
+  const double twall = s.t_wall, rgas0 = s.rgas0;
   par_for(1, nz, [&](int k) {
     for (int l = 1; l <= ng; ++l)
       for (int i = 1; i <= nx; ++i) {
@@ -347,10 +402,10 @@ void Solver::bcwall_staggered(int ilat) {
         double rhoe = W(i, js, k, 4);
         double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
         double ee = rhoe / rho - qq;
-        double tt = t0 + (ee - cvl * t0) / cv0;
+        double tt = temp_from_e(ee, A(i, js, k, 6));
         double pp = rho * tt * rgas0;
         tt = 2.0 * twall - tt;
-        ee = (cvl + cv0 * (tt / t0 - 1.0)) * t0;
+        ee = e_from_temp(tt);
         rho = pp / tt / rgas0;
         W(i, jg, k, 0) = rho;
         W(i, jg, k, 1) = -rho * uu;
@@ -365,13 +420,13 @@ void Solver::bcwall_staggered(int ilat) {
 // mirrored about it (T_g = 2 T_w - T, p_g = p, velocity reversed); ymin only, as the reference
 void Solver::bcwall(int ilat) {
   if (ilat != 3) return;
-  const double twall = s.t_wall, t0 = s.t0, rgas0 = s.rgas0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
+  const double twall = s.t_wall, rgas0 = s.rgas0;
   par_for(1, nz, [&](int k) {
     for (int i = 1; i <= nx; ++i) {
       W(i, 1, k, 1) = 0.0;
       W(i, 1, k, 2) = 0.0;
       W(i, 1, k, 3) = 0.0;
-      double ee = (cvl + cv0 * (twall / t0 - 1.0)) * t0;
+      double ee = e_from_temp(twall);
       W(i, 1, k, 4) = W(i, 1, k, 0) * ee;
       for (int l = 1; l <= ng; ++l) {
         double rho = W(i, 1 + l, k, 0);
@@ -381,10 +436,10 @@ void Solver::bcwall(int ilat) {
         double rhoe = W(i, 1 + l, k, 4);
         double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
         ee = rhoe / rho - qq;
-        double tt = t0 + (ee - cvl * t0) / cv0;
+        double tt = temp_from_e(ee, A(i, 1 + l, k, 6));
         double pp = rho * tt * rgas0;
         tt = 2.0 * twall - tt;
-        ee = (cvl + cv0 * (tt / t0 - 1.0)) * t0;
+        ee = e_from_temp(tt);
         rho = pp / tt / rgas0;
         W(i, 1 - l, k, 0) = rho;
         W(i, 1 - l, k, 1) = -rho * uu;
@@ -525,7 +580,7 @@ void Solver::bcrecyc() {
         const double tt = p0 / rho / rgas0;
         const double uu = uumean + ufluc, vv = vvmean + vfluc, ww = wwmean + wfluc;
         const double rhou = rho * uu, rhov = rho * vv, rhow = rho * ww;
-        const double ee = (s.cv_coeff[1] + s.cv_coeff[0] * (tt / s.t0 - 1.0)) * s.t0;
+        const double ee = e_from_temp(tt);
         W(1 - i, j, k, 0) = rho;
         W(1 - i, j, k, 1) = rhou;
         W(1 - i, j, k, 2) = rhov;
@@ -546,9 +601,9 @@ void Solver::draw_random_plane() {
             rescale * static_cast<double>(rng()) / RAND_MAX;
 }
 
-// eval_aux_subroutine (kernels_cpu.F90:6960-7011), calorically perfect gas
+// eval_aux_subroutine (kernels_cpu.F90:6960-7011)
 void Solver::eval_aux(int i0, int i1, int j0, int j1, int k0, int k1) {
-  const double t0 = s.t0, rgas0 = s.rgas0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
+  const double t0 = s.t0, rgas0 = s.rgas0;
   const double mu0 = s.mu0, vtexp = s.powerlaw_vtexp, ss = s.sutherland_s, trd = s.t_ref_dim;
   const int vm = s.visc_model;
   par_for(k0, k1, [&](int k) {
@@ -560,7 +615,7 @@ void Solver::eval_aux(int i0, int i1, int j0, int j1, int k0, int k1) {
         double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
         double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
         double ee = rhoe / rho - qq;
-        double tt = t0 + (ee - cvl * t0) / cv0;
+        double tt = temp_from_e(ee, A(i, j, k, 6));
         double pp = rho * tt * rgas0;
         A(i, j, k, 1) = rho;
         A(i, j, k, 2) = uu;
@@ -691,12 +746,11 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
     // Rusanov (component-wise local Lax-Friedrichs) WENO branch of the *_hybrid_rusanov kernels
     // (kernels_cpu.F90:692-941 for x): stencil maximum of |u_n -+ c|, split of the conserved
     // fluxes, wenorec_1d_rusanov
-    const double gamloc = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
     double evmax = -1.0;
     for (int l = 1; l <= 2 * ws; ++l) {
       const int o = l - ws;
       const double un = at(o, 2 + dir), tt = at(o, 6);
-      const double c = std::sqrt(gamloc * rgas0 * tt);
+      const double c = std::sqrt(gamloc_at(tt) * rgas0 * tt);
       const double evm = std::max(std::fabs(un - c), std::fabs(un + c));
       evmax = std::max(evm, evmax);
     }
@@ -727,7 +781,7 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
     const int ord = std::max(ws + epo, 1);
     wenorec_1d(gp, gm, fh, ws, ord, s.weno_version, s.rho0, s.u0, true);
   } else {
-    // compute_roe_average (kernels_cpu.F90:3013-3089), calorically perfect gas
+    // compute_roe_average (kernels_cpu.F90:3013-3089)
     double uu = at(0, 2), vv = at(0, 3), ww = at(0, 4);
     double h = at(0, 5);
     double up = at(1, 2), vp = at(1, 3), wp = at(1, 4);
@@ -741,9 +795,36 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
     ww = (r * wp + ww) * rp1;
     h = (r * hp + h) * rp1;
     double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-    double hbar = h - qq - s.cp_coeff[1] * s.t0;
-    double tt = s.t0 + hbar / s.cp_coeff[0];
-    double gamloc = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
+    double hbar = h - qq - cp(s.indx_cp_r + 1) * s.t0;
+    double tt, gamloc;
+    if (s.calorically_perfect == 1) {
+      tt = s.t0 + hbar / cp(0);
+      gamloc = cp(0) / (cp(0) - rgas0);
+    } else {
+      tt = at(0, 6);
+      const double ttp = at(1, 6);
+      tt = (r * ttp + tt) * rp1;
+      double told = tt;
+      for (int iter = 1; iter <= 50; ++iter) {
+        double num = 0.0, den = 0.0;
+        for (int ll = s.indx_cp_l; ll <= s.indx_cp_r; ++ll) {
+          const double tpow = std::pow(told / s.t0, ll);
+          if (ll == -1) {
+            den = den + cp(ll) * tpow;
+            num = num + cp(ll) * std::log(told / s.t0);
+          } else {
+            const double tpowp = (told / s.t0) * tpow;
+            den = den + cp(ll) * tpow;
+            num = num + cp(ll) * (tpowp - 1.0) / (ll + 1.0);
+          }
+        }
+        num = num * s.t0;
+        tt = told + (hbar - num) / den;
+        if (std::fabs(tt - told) < 1e-12) break;
+        told = tt;
+      }
+      gamloc = gamloc_at(tt);
+    }
     double cc = gamloc * tt * rgas0;
     double gm1loc = gamloc - 1.0;
     double c = std::sqrt(cc);
@@ -763,7 +844,7 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
       const int o = l - ws;
       double vn = at(o, 2 + dir);
       double t = at(o, 6);
-      double gl = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
+      double gl = gamloc_at(t);
       double cs = std::sqrt(gl * rgas0 * t);
       evmax[0] = std::max(std::fabs(vn - cs), evmax[0]);
       evmax[1] = std::max(std::fabs(vn), evmax[1]);
@@ -848,7 +929,7 @@ void Solver::euler(int dir) {
 
 // visflx_reduced_ord2_subroutine (kernels_cpu.F90:4623-4721)
 void Solver::visflx_reduced_ord2(int update_sensor) {
-  const double prandtl = s.prandtl, u0 = s.u0, l0 = s.l0, cploc = s.cp_coeff[0];
+  const double prandtl = s.prandtl, u0 = s.u0, l0 = s.l0;
   par_for(1, nz, [&](int k) {
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
@@ -872,7 +953,7 @@ void Solver::visflx_reduced_ord2(int update_sensor) {
         if (j == 1) {
           wallprop[(0 * sz + k + ng - 1) * sx + i + ng - 1] = mu * uy;
           wallprop[(1 * sz + k + ng - 1) * sx + i + ng - 1] = mu * wy;
-          wallprop[(2 * sz + k + ng - 1) * sx + i + ng - 1] = mu * ty * cploc / prandtl;
+          wallprop[(2 * sz + k + ng - 1) * sx + i + ng - 1] = mu * ty * cploc_at(A(i, j, k, 6)) / prandtl;
         }
         double div = ux + vy + wz;
         double div3l = div / 3.0;
@@ -904,7 +985,7 @@ void Solver::visflx_reduced_ord2(int update_sensor) {
 
 // visflx_x / _y / _z_subroutine (kernels_cpu.F90:4779-4999): conservative face Laplacian
 void Solver::visflx_faces() {
-  const double prandtl = s.prandtl, cploc = s.cp_coeff[0];
+  const double prandtl = s.prandtl;
   // x: face fluxes into fhat(2:5), then the divergence
   par_for(1, nz, [&](int k) {
     for (int j = 1; j <= ny; ++j)
@@ -920,7 +1001,7 @@ void Solver::visflx_faces() {
         sigx = sigx * muf;
         sigy = sigy * muf;
         sigz = sigz * muf;
-        double sigq = (sigq_tt * cploc / prandtl + sigq_qq) * muf;
+        double sigq = (sigq_tt * cploc_at(0.5 * (tt + ttp)) / prandtl + sigq_qq) * muf;
         FH(i, j, k, 2) = -sigx;
         FH(i, j, k, 3) = -sigy;
         FH(i, j, k, 4) = -sigz;
@@ -950,7 +1031,7 @@ void Solver::visflx_faces() {
         sigx = sigx * muf;
         sigy = sigy * muf;
         sigz = sigz * muf;
-        double sigq = (sigq_tt * cploc / prandtl + sigq_qq) * muf;
+        double sigq = (sigq_tt * cploc_at(0.5 * (tt + ttp)) / prandtl + sigq_qq) * muf;
         if (j > 0) {
           FL(i, j, k, 2) = FL(i, j, k, 2) + fl2o - sigx * dyhl;
           FL(i, j, k, 3) = FL(i, j, k, 3) + fl3o - sigy * dyhl;
@@ -983,7 +1064,7 @@ void Solver::visflx_faces() {
         sigx = sigx * muf;
         sigy = sigy * muf;
         sigz = sigz * muf;
-        double sigq = (sigq_tt * cploc / prandtl + sigq_qq) * muf;
+        double sigq = (sigq_tt * cploc_at(0.5 * (tt + ttp)) / prandtl + sigq_qq) * muf;
         if (k > 0) {
           FL(i, j, k, 2) = FL(i, j, k, 2) + fl2o - sigx * dzhl;
           FL(i, j, k, 3) = FL(i, j, k, 3) + fl3o - sigy * dzhl;
@@ -1063,7 +1144,7 @@ void Solver::visflx_div_ord2() {
 // (conservative_viscous = 0, calorically perfect gas)
 void Solver::visflx_nosensor() {
   const int lmax = s.visc_order / 2;
-  const double prandtl = s.prandtl, cploc = s.cp_coeff[0];
+  const double prandtl = s.prandtl;
   const double* c1 = s.coeff_deriv1[lmax - 1];
   const double* c2 = s.coeff_deriv2[lmax - 1];
   par_for(1, nz, [&](int k) {
@@ -1139,6 +1220,7 @@ void Solver::visflx_nosensor() {
         const double sigx = mux * sig11 + muy * sig12 + muz * sig13 + mu * ulap;
         const double sigy = mux * sig12 + muy * sig22 + muz * sig23 + mu * vlap;
         const double sigz = mux * sig13 + muy * sig23 + muz * sig33 + mu * wlap;
+        const double cploc = cploc_at(tt);
         const double sigqt = (mux * tx + muy * ty + muz * tz + mu * tlap) * cploc / prandtl;
         const double sigah = (sig11 * ux + sig12 * uy + sig13 * uz + sig12 * vx + sig22 * vy + sig23 * vz +
                               sig13 * wx + sig23 * wy + sig33 * wz) * mu;
@@ -1226,7 +1308,7 @@ void Solver::visflx_div() {
 // the ghost point; 3: incoming waves towards the free stream; 6: the acoustic reflection of
 // type-6), one-sided second-order normal derivatives of w.
 void Solver::bc_nr() {
-  const double rgas0 = s.rgas0, gamloc = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
+  const double rgas0 = s.rgas0;
   for (int ilat = 1; ilat <= 4; ++ilat) {
     const int nr_type = s.bctags_nr[ilat - 1];
     if (nr_type <= 0) continue;
@@ -1253,6 +1335,7 @@ void Solver::bc_nr() {
         }
         const double rho = A(i, j, k, 1), uu = A(i, j, k, 2), vv = A(i, j, k, 3), ww = A(i, j, k, 4);
         const double h = A(i, j, k, 5), tt = A(i, j, k, 6);
+        const double gamloc = gamloc_at(tt);
         const double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
         const double cc = gamloc * tt * rgas0;
         const double c = std::sqrt(cc);
@@ -1369,7 +1452,6 @@ void Solver::force_rhs() {
 // force_var (singleideal_cpu.F90:890-933) with force_var_1/2 (kernels_cpu.F90:3241-3314)
 void Solver::force_var() {
   if (!(s.theta_wall >= -1.0)) return;
-  const double t0 = s.t0, cv0 = s.cv_coeff[0], cvl = s.cv_coeff[1];
   std::vector<double> part(static_cast<size_t>(nz), 0.0);
   par_for(1, nz, [&](int k) {
     double b5 = 0;
@@ -1382,7 +1464,7 @@ void Solver::force_var() {
         double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
         double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
         double ee = rhoe / rho - qq;
-        double tt = t0 + (ee - cvl * t0) / cv0;
+        double tt = temp_from_e(ee, A(i, j, k, 6));
         A(i, j, k, 6) = tt;
         b5 = b5 + rhou * tt * dy;
       }
@@ -1399,7 +1481,7 @@ void Solver::force_var() {
         double rho = W(i, j, k, 0), rhou = W(i, j, k, 1), rhov = W(i, j, k, 2), rhow = W(i, j, k, 3);
         double tt = A(i, j, k, 6);
         double ttnew = tt + tbdiff;
-        double ee = (cvl + cv0 * (ttnew / t0 - 1.0)) * t0;
+        double ee = e_from_temp(ttnew);
         W(i, j, k, 4) = rho * ee + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;
       }
   });
@@ -1461,7 +1543,6 @@ void Solver::compute_dt() {
   }
   std::vector<double> part(static_cast<size_t>(nz) * 9, 0.0);
   const double rgas0 = s.rgas0, prandtl = s.prandtl;
-  const double gamloc = s.cp_coeff[0] / (s.cp_coeff[0] - rgas0);
   par_for(1, nz, [&](int k) {
     double mx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int j = 1; j <= ny; ++j)
@@ -1471,7 +1552,7 @@ void Solver::compute_dt() {
         double uu = A(i, j, k, 2), vv = A(i, j, k, 3), ww = A(i, j, k, 4), tt = A(i, j, k, 6), mu = A(i, j, k, 7);
         double nu = ri * mu;
         double k_over_rhocp = nu / prandtl;
-        double c = std::sqrt(gamloc * rgas0 * tt);
+        double c = std::sqrt(gamloc_at(tt) * rgas0 * tt);
         double v[9] = {(std::fabs(uu) + c) * s.dcsidx[i - 1], (std::fabs(vv) + c) * s.detady[j - 1],
                        (std::fabs(ww) + c) * s.dzitdz[k - 1], nu * s.dcsidxs[i - 1],
                        nu * s.detadys[j - 1], nu * s.dzitdzs[k - 1],
@@ -1557,8 +1638,6 @@ void Solver::compute_stats(int itav) {
   if (w_stat.empty()) w_stat.assign(static_cast<size_t>(nv) * nx * ny, 0.0);
   w_stat_z.assign(static_cast<size_t>(nv) * nx * ny, 0.0);
   const double rgas0 = s.rgas0;
-  // get_gamloc (singleideal.F90:4752-4771), calorically perfect
-  const double cploc0 = s.cp_coeff[0];
   par_for(1, ny, [&](int j) {
     for (int k = 1; k <= nz; ++k)
       for (int i = 1; i <= nx; ++i) {
@@ -1588,7 +1667,8 @@ void Solver::compute_stats(int itav) {
         const double pp = rho * rgas0 * tt;
         const double mu = A(i, j, k, 7);
         const double nu = mu / rho;
-        const double gamloc = cploc0 / (cploc0 - rgas0);
+        // get_gamloc (singleideal.F90:4752-4771)
+        const double gamloc = gamloc_at(tt);
         const double cploc = gamloc / (gamloc - 1.0) * rgas0;
         const double c = std::sqrt(gamloc * rgas0 * tt);
         const double machlocal = std::sqrt(2.0 * qq) / c;

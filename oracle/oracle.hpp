@@ -112,6 +112,14 @@ class Solver {
   void bcshock();
   void draw_random_plane();
   void bc_nr();
+  // thermodynamics (kernels_cpu.F90:7096-7176): get_temperature_from_e_dev (Newton from t_start
+  // for a thermally perfect gas), get_e_from_temperature_dev, get_gamloc_dev, cp(T)
+  double temp_from_e(double ee, double t_start) const;
+  double e_from_temp(double tt) const;
+  double cploc_at(double tt) const;
+  double gamloc_at(double tt) const;
+  double cp(int l) const { return s.cp_coeff[static_cast<size_t>(l - s.indx_cp_l)]; }
+  double cv(int l) const { return s.cv_coeff[static_cast<size_t>(l - s.indx_cp_l)]; }
 };
 
 }  // namespace streams_oracle

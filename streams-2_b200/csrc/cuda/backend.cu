@@ -14,6 +14,8 @@
 
 using namespace sb200;
 
+static_assert(MAX_CP == STREAMS_B200_MAX_CP, "cp polynomial sizes of the ABI and the device differ");
+
 struct streams_b200_ctx {
   streams_b200_params p{};
   Geom g{};
@@ -94,7 +96,14 @@ std::string validate(const streams_b200_params* p) {
   if (p->flux_splitting == 1 && !(p->ep_order == 6 && p->weno_scheme == 3))
     return "flux_splitting = 1 (Rusanov) is implemented for ep_order 6 with weno_scheme 3";
   if (p->conservative_viscous != 0 && p->conservative_viscous != 1) return "conservative_viscous must be 0 or 1";
-  if (p->calorically_perfect != 1) return "only calorically perfect gas is implemented on the device path";
+  if (p->calorically_perfect != 0 && p->calorically_perfect != 1) return "calorically_perfect must be 0 or 1";
+  if (p->calorically_perfect == 0) {
+    if (p->indx_cp_l > 0 || p->indx_cp_r < 0 || p->indx_cp_r - p->indx_cp_l + 2 > STREAMS_B200_MAX_CP)
+      return "cp polynomial: indx_cp_l <= 0 <= indx_cp_r with at most STREAMS_B200_MAX_CP coefficients";
+    if (p->precision != 0) return "the thermally perfect gas (calorically_perfect = 0) is an FP64 (precision 0) path";
+    if (!(p->ep_order == 6 && p->weno_scheme == 3))
+      return "the thermally perfect gas is implemented for ep_order 6 with weno_scheme 3";
+  }
   if (p->nrk != 3) return "only the Wray RK3 scheme (nrk = 3) is implemented";
   if (p->precision != 0 && p->precision != 1) return "precision must be 0 (FP64) or 1 (mixed)";
   if (p->visc_model < 0 || p->visc_model > 2) return "visc_model must be 0, 1 or 2";
@@ -166,6 +175,13 @@ void fill_geom(streams_b200_ctx* c) {
   g.sutherland_s = p.sutherland_s; g.t_ref_dim = p.t_ref_dim; g.vtexp = p.powerlaw_vtexp; g.prandtl = p.prandtl;
   g.cp0 = p.cp0; g.cv0 = p.cv0; g.cp_last = p.cp_last; g.cv_last = p.cv_last;
   g.gamloc = p.cp0 / (p.cp0 - p.rgas0);
+  g.calorically_perfect = p.calorically_perfect;
+  g.cp_l = p.indx_cp_l;
+  g.cp_r = p.indx_cp_r;
+  for (int q = 0; q < MAX_CP; ++q) {
+    g.cpc[q] = p.cp_coeff[q];
+    g.cvc[q] = p.cv_coeff[q];
+  }
   g.t_wall = p.t_wall;
   g.channel_case = p.channel_case;
   g.force_var = p.channel_case && p.theta_wall >= -1.0;
@@ -632,6 +648,7 @@ static int ensure_stats(streams_b200_ctx* c, bool three_d) {
   if (!c->d.wstat) {
     SB_CHECK(c, dev_alloc(c, &c->d.wstat, n2));
     SB_CHECK(c, dev_alloc(c, &c->d.wstat_z, n2));
+    SB_CHECK(c, dev_alloc(c, &c->d.wstat_vel, (size_t)c->g.nvol * 3));
     SB_CHECK(c, cudaMemsetAsync(c->d.wstat, 0, n2 * 8, c->stream));
     SB_CHECK(c, cudaMemsetAsync(c->d.wstat_z, 0, n2 * 8, c->stream));
   }

@@ -37,8 +37,10 @@ __global__ void __launch_bounds__(BC_NT) k_bc_extr(Geom g, double* __restrict__ 
 }
 
 // bcwall_subroutine (kernels_cpu.F90:6478-6525), ymin: wall node at rest and at T_wall, ghosts
-// mirrored about it (T_g = 2 T_w - T, p_g = p, velocity reversed)
-__global__ void __launch_bounds__(BC_NT) k_bc_wall(Geom g, double* __restrict__ w) {
+// mirrored about it (T_g = 2 T_w - T, p_g = p, velocity reversed); the Newton iteration of a
+// thermally perfect gas starts from the interior point's temperature in aux, as w_aux(6) there
+template <class A>
+__global__ void __launch_bounds__(BC_NT) k_bc_wall(Geom g, double* __restrict__ w, const A* __restrict__ aux) {
   const long long q = (long long)blockIdx.x * BC_NT + threadIdx.x;
   if (q >= (long long)g.nx * g.nz) return;
   const int i = (int)(q % g.nx) + 1, k = (int)(q / g.nx) + 1;
@@ -54,7 +56,7 @@ __global__ void __launch_bounds__(BC_NT) k_bc_wall(Geom g, double* __restrict__ 
     const double rhoe = w[4 * n + s];
     const double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
     double ee = rhoe / rho - qq;
-    double tt = t_from_e(g, ee);
+    double tt = t_from_e(g, ee, double(aux[5 * n + s]));
     const double pp = rho * tt * g.rgas0;
     tt = 2.0 * g.t_wall - tt;
     ee = e_of_t(g, tt);
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(BC_NT) k_bc_nr(Geom g, const double* __restric
   const double rho = double(aux[c0]), uu = double(aux[n + c0]), vv = double(aux[2 * n + c0]);
   const double ww = double(aux[3 * n + c0]), h = double(aux[4 * n + c0]), tt = double(aux[5 * n + c0]);
   const double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-  const double gamloc = g.gamloc, rgas0 = g.rgas0;
+  const double gamloc = gamloc_of_t(g, tt), rgas0 = g.rgas0;
   const double cc = gamloc * tt * rgas0;
   const double c = sqrt(cc);
   const double ci = 1.0 / c;
@@ -386,7 +388,10 @@ cudaError_t launch_bc_fill(const Geom& g, DevState& d, cudaStream_t s, long long
       SB_LAUNCH(d, K_BC_FILL, s, k_bc_shock<<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w));
       ++*nl;
     } else if (t == 6 && ilat == 3 && !g.wall_ymin) {
-      SB_LAUNCH(d, K_BC_FILL, s, k_bc_wall<<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w));
+      if (g.precision == 1)
+        SB_LAUNCH(d, K_BC_FILL, s, k_bc_wall<float><<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w, d.auxf));
+      else
+        SB_LAUNCH(d, K_BC_FILL, s, k_bc_wall<double><<<nb((long long)g.nx * g.nz), BC_NT, 0, s>>>(g, d.w, d.aux));
       ++*nl;
     }
   }

@@ -9,6 +9,8 @@
 namespace sb200 {
 
 constexpr int NV = 5;
+constexpr int MAX_CP = 12;           // cp(T) polynomial coefficients (STREAMS_B200_MAX_CP)
+constexpr double TOL_ITER_NR = 1e-12;  // Newton tolerance of the temperature (tol_iter_nr)
 
 // Number of FP64 reduction slots produced per block by the stage kernels.
 constexpr int NRED_RHS = 5;   // force_rhs: sum fln1*dy, fln2*dy, rho*dy, rhou*dy, rhou*T*dy
@@ -71,6 +73,10 @@ struct Geom {
   int visc_model;
   double mu0, t0, rgas0, rho0, u0, l0, sutherland_s, t_ref_dim, vtexp, prandtl;
   double cp0, cv0, cp_last, cv_last, gamloc;
+  // thermally perfect gas (calorically_perfect = 0): cp(T) = sum of cpc[l - cp_l] (T/t0)^l for
+  // l = cp_l..cp_r, cv likewise (set_fluid_prop's cp_coeff / cv_coeff, times rgas0)
+  int calorically_perfect, cp_l, cp_r;
+  double cpc[MAX_CP], cvc[MAX_CP];
   double t_wall;
   // channel forcing
   int channel_case, force_var;
@@ -115,27 +121,94 @@ struct Scalars {
   int pad;
 };
 
-// get_temperature_from_e_dev / get_e_from_temperature_dev (kernels_cpu.F90:7116-7176),
-// calorically perfect branch
-__device__ __forceinline__ double t_from_e(const Geom& g, double ee) {
-  double ebar = ee - g.cv_last * g.t0;
-  return g.t0 + ebar / g.cv0;
+// x^l for an integer exponent (Fortran's ** with an integer power)
+__host__ __device__ __forceinline__ double ipow_d(double x, int l) {
+  double r = 1.0;
+  for (int q = 0; q < (l < 0 ? -l : l); ++q) r = r * x;
+  return l < 0 ? 1.0 / r : r;
 }
+
+// Newton iteration for the temperature of a thermally perfect gas, as get_temperature_from_e_dev
+// (kernels_cpu.F90:7116-7152, coefficients cv, ebar = e - cv(r+1) t0) and compute_roe_average
+// (:3049-3069, coefficients cp, hbar = h - q - cp(r+1) t0) do it: at most 50 steps, stop when the
+// step is below tol_iter_nr
+__device__ __forceinline__ double tp_newton(const Geom& g, const double* c, double ebar, double t_start) {
+  const double t0 = g.t0;
+  // a start that is not a temperature (aux before its first pass holds zeros) becomes t0, the
+  // value initial_conditions gives w_aux(6)
+  if (!(t_start > 0.0)) t_start = t0;
+  double t_old = t_start, tt = t_start;
+  for (int iter = 0; iter < 50; ++iter) {
+    const double tr = t_old / t0;
+    double den = 0.0, num = 0.0, tp = ipow_d(tr, g.cp_l);
+    for (int l = g.cp_l; l <= g.cp_r; ++l) {
+      const double cl = c[l - g.cp_l];
+      den = den + cl * tp;
+      if (l == -1) num = num + cl * log(tr);
+      else num = num + cl * (tr * tp - 1.0) / (l + 1.0);
+      tp = tp * tr;
+    }
+    num = num * t0;
+    tt = t_old + (ebar - num) / den;
+    if (fabs(tt - t_old) < TOL_ITER_NR) break;
+    t_old = tt;
+  }
+  return tt;
+}
+
+// get_temperature_from_e_dev / get_e_from_temperature_dev (kernels_cpu.F90:7116-7176): closed
+// form for the calorically perfect gas, Newton from t_start (the caller's previous temperature of
+// the point) for the thermally perfect one.  TPA = false compiles the thermally perfect branch
+// out (kernel instantiations that never run it keep their registers).
+template <bool TPA = true>
+__device__ __forceinline__ double t_from_e(const Geom& g, double ee, double t_start) {
+  double ebar = ee - g.cv_last * g.t0;
+  if (!TPA || g.calorically_perfect) return g.t0 + ebar / g.cv0;
+  return tp_newton(g, g.cvc, ebar, t_start);
+}
+template <bool TPA = true>
 __device__ __forceinline__ double e_from_t(const Geom& g, double tt) {
   double ee = g.cv_last;
-  ee = ee + g.cv0 * (tt / g.t0 - 1.0);
+  if (!TPA || g.calorically_perfect) {
+    ee = ee + g.cv0 * (tt / g.t0 - 1.0);
+  } else {
+    const double tr = tt / g.t0;
+    double tp = ipow_d(tr, g.cp_l + 1);  // (T/t0)^(l+1)
+    for (int l = g.cp_l; l <= g.cp_r; ++l) {
+      const double cl = g.cvc[l - g.cp_l];
+      if (l == -1) ee = ee + cl * log(tr);
+      else ee = ee + cl / (l + 1.0) * (tp - 1.0);
+      tp = tp * tr;
+    }
+  }
   return ee * g.t0;
+}
+// cp(T) and gamma(T) (get_gamloc_dev, kernels_cpu.F90:7096-7113; the cploc of the viscous terms)
+__device__ __forceinline__ double cp_of_t(const Geom& g, double tt) {
+  if (g.calorically_perfect) return g.cp0;
+  const double tr = tt / g.t0;
+  double cploc = 0.0, tp = ipow_d(tr, g.cp_l);
+  for (int l = g.cp_l; l <= g.cp_r; ++l) {
+    cploc = cploc + g.cpc[l - g.cp_l] * tp;
+    tp = tp * tr;
+  }
+  return cploc;
+}
+__device__ __forceinline__ double gamloc_of_t(const Geom& g, double tt) {
+  if (g.calorically_perfect) return g.gamloc;
+  const double cploc = cp_of_t(g, tt);
+  return cploc / (cploc - g.rgas0);
 }
 
 // Apply force_var_2 (kernels_cpu.F90:3285-3314) to the conserved values of one interior point:
 // temperature from the (unshifted) state as force_var_1 computes it (:3241-3282), shifted by tbdiff.
 __device__ __forceinline__ double shifted_rhoe(const Geom& g, double rho, double rhou, double rhov, double rhow,
-                                               double rhoe, double tbdiff) {
+                                               double rhoe, double tbdiff, double t_start) {
   double ri = 1.0 / rho;
   double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
   double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
   double ee = rhoe / rho - qq;
-  double tt = t_from_e(g, ee);
+  double tt = t_from_e(g, ee, t_start);
   double ttnew = tt + tbdiff;
   double en = e_from_t(g, ttnew);
   return rho * en + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;

@@ -326,9 +326,11 @@ __device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>&
 // Characteristic WENO flux: compute_roe_average (kernels_cpu.F90:3013-3089), eigenvectors_{x,y,z}
 // (:2728-2782, :2842-2896, :2956-3010), local Lax-Friedrichs splitting with the stencil maximum
 // of |u_n -+ c| (:614-675) and wenorec_1d; back-projection with the right eigenvectors (:677-683).
-template <class R, int DIR, int WS, int S>
+// TP: thermally perfect gas (Newton for the Roe-averaged temperature, gamma(T) per point; FP64).
+template <class R, int DIR, int WS, int S, bool TP = false>
 __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5],
                                           R (&fl)[5], R* __restrict__ gs, int gstride) {
+  static_assert(!TP || sizeof(R) == sizeof(double), "the thermally perfect gas is an FP64 path");
   const R rgas0 = R(g.rgas0);
   const int o0 = S - 1, o1 = S;  // the two points adjacent to the face
   // Roe average
@@ -343,8 +345,16 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   h = (r * st.h[o1] + h) * rp1;
   R qq = R(0.5) * (uu * uu + vv * vv + ww * ww);
   R hbar = h - qq - R(g.cp_last) * R(g.t0);
-  R tt = R(g.t0) + hbar / R(g.cp0);
-  R gamloc = R(g.gamloc);
+  R tt, gamloc;
+  if constexpr (TP) {
+    // Newton on h(T) from the Roe average of the two temperatures (compute_roe_average)
+    const R t_start = (r * st.t[o1] + st.t[o0]) * rp1;
+    tt = tp_newton(g, g.cpc, hbar, t_start);
+    gamloc = gamloc_of_t(g, tt);
+  } else {
+    tt = R(g.t0) + hbar / R(g.cp0);
+    gamloc = R(g.gamloc);
+  }
   R cc = gamloc * tt * rgas0;
   R gm1loc = gamloc - R(1);
   R c = sqrt(cc);
@@ -365,9 +375,11 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
     const int q = l + S - WS;
     const R vnq = DIR == 0 ? st.u[q] : (DIR == 1 ? st.v[q] : st.w[q]);
 #if SB_CACHE_C
+    static_assert(!TP, "the cached sound speed assumes a calorically perfect gas");
     const R cs = st.c[q];
 #else
-    const R cs = sqrt(R(g.gamloc) * R(g.rgas0) * st.t[q]);
+    const R gq = TP ? R(gamloc_of_t(g, double(st.t[q]))) : R(g.gamloc);
+    const R cs = sqrt(gq * R(g.rgas0) * st.t[q]);
 #endif
     ev0 = fmax(fabs(vnq - cs), ev0);
     ev1 = fmax(fabs(vnq), ev1);
@@ -462,15 +474,17 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
 // Rusanov (component-wise local Lax-Friedrichs) WENO flux of the *_hybrid_rusanov kernels
 // (kernels_cpu.F90:692-941 for x, same in y and z): stencil maximum of |u_n -+ c|, split
 // values of the conserved fluxes, wenorec with the scales of wenorec_1d_rusanov (:2325-2523).
-template <class R, int DIR, int WS, int S>
+template <class R, int DIR, int WS, int S, bool TP = false>
 __device__ __forceinline__ void rusanov_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5], R (&fl)[5]) {
+  static_assert(!TP || sizeof(R) == sizeof(double), "the thermally perfect gas is an FP64 path");
   const R rgas0 = R(g.rgas0);
   R evmax = R(-1);
 #pragma unroll
   for (int l = 0; l < 2 * WS; ++l) {
     const int q = l + S - WS;
     const R un = DIR == 0 ? st.u[q] : (DIR == 1 ? st.v[q] : st.w[q]);
-    const R c = sqrt(R(g.gamloc) * rgas0 * st.t[q]);
+    const R gq = TP ? R(gamloc_of_t(g, double(st.t[q]))) : R(g.gamloc);
+    const R c = sqrt(gq * rgas0 * st.t[q]);
     const R evm = fmax(fabs(un - c), fabs(un + c));
     evmax = fmax(evm, evmax);
   }

@@ -58,6 +58,7 @@ struct DevState {
   double* wstat = nullptr;
   double* wstat_z = nullptr;
   double* wstat3d = nullptr;
+  double* wstat_vel = nullptr;  // scratch of a sample: velocities at interior and ghost points (3 x nvol)
   Prof* prof = nullptr;       // optional per-kernel timing
 };
 

@@ -59,7 +59,9 @@ constexpr int FIN_NT = 1024;
 struct Prim {
   double rho, uu, vv, ww, tt;
 };
-__device__ __forceinline__ Prim prim_from_w(const Geom& g, const double* __restrict__ w, long long c) {
+template <bool TPA = true>
+__device__ __forceinline__ Prim prim_from_w(const Geom& g, const double* __restrict__ w, long long c,
+                                            double t_start) {
   const long long n = g.nvol;
   Prim p;
   p.rho = w[c];
@@ -68,15 +70,16 @@ __device__ __forceinline__ Prim prim_from_w(const Geom& g, const double* __restr
   p.vv = w[2 * n + c] * ri;
   p.ww = w[3 * n + c] * ri;
   const double qq = 0.5 * (p.uu * p.uu + p.vv * p.vv + p.ww * p.ww);
-  p.tt = t_from_e(g, w[4 * n + c] / p.rho - qq);
+  p.tt = t_from_e<TPA>(g, w[4 * n + c] / p.rho - qq, t_start);
   return p;
 }
 
 // Conserved state at an interior or face-ghost point (i,j,k): the stored value, a periodic copy
 // (bcswap, code/src/base_cpu.F90:1326-1435) or the staggered-wall mirror of
-// bcwall_staggered_subroutine (kernels_cpu.F90:6612-6678).
+// bcwall_staggered_subroutine (kernels_cpu.F90:6612-6678); t_src is the start of the Newton
+// iteration for the mirrored point's temperature (thermally perfect gas).
 __device__ __forceinline__ void point_state(const Geom& g, const double* __restrict__ w, int i, int j, int k,
-                                            double (&st)[5]) {
+                                            double (&st)[5], double t_src) {
   const long long n = g.nvol;
   const int ox = (i < 1 || i > g.nx), oy = (j < 1 || j > g.ny), oz = (k < 1 || k > g.nz);
   int si = i, sj = j, sk = k;
@@ -100,7 +103,7 @@ __device__ __forceinline__ void point_state(const Geom& g, const double* __restr
     double uu = rhou / rho, vv = rhov / rho, ww = rhow / rho;
     double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
     double ee = rhoe / rho - qq;
-    double tt = t_from_e(g, ee);
+    double tt = t_from_e(g, ee, t_src);
     double pp = rho * tt * g.rgas0;
     tt = 2.0 * g.t_wall - tt;
     ee = e_from_t(g, tt);
@@ -129,10 +132,16 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   const int ox = (i < 1 || i > g.nx), oy = (j < 1 || j > g.ny), oz = (k < 1 || k > g.nz);
   if (ox + oy + oz > 1) return;  // halo edges and corners are never read
   if (write_ghost_w == 2 && !(ox | oy | oz)) return;
-  double st[5];
-  point_state(g, w, i, j, k, st);
-  double rho = st[0], rhou = st[1], rhov = st[2], rhow = st[3], rhoe = st[4];
   const long long dst = gidx(g, i, j, k);
+  // Newton starts (thermally perfect gas): the point's previous temperature, as eval_aux starts
+  // from w_aux(6); for a wall ghost the mirror of it estimates the interior source point's
+  double t_old = double(aux[5 * n + dst]);
+  if (!(t_old > 0.0)) t_old = g.t0;
+  double t_src = 2.0 * g.t_wall - t_old;
+  if (!(t_src > 0.0)) t_src = g.t0;
+  double st[5];
+  point_state(g, w, i, j, k, st, t_src);
+  double rho = st[0], rhou = st[1], rhov = st[2], rhow = st[3], rhoe = st[4];
   if (write_ghost_w && (ox | oy | oz)) {
     w[dst] = rho; w[n + dst] = rhou; w[2 * n + dst] = rhov; w[3 * n + dst] = rhow; w[4 * n + dst] = rhoe;
   }
@@ -141,7 +150,7 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
   double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
   double ee = rhoe / rho - qq;
-  double tt = t_from_e(g, ee);
+  double tt = t_from_e(g, ee, t_old);
   double pp = rho * tt * g.rgas0;
   aux[dst] = A(rho);
   aux[n + dst] = A(uu);
@@ -166,7 +175,7 @@ __global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restri
   const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
   auto vel = [&](int a, int b, int c, double (&v)[3]) {
     double st[5];
-    point_state(g, w, a, b, c, st);
+    point_state(g, w, a, b, c, st, g.t_wall);
     const double ri = 1.0 / st[0];
     v[0] = st[1] * ri; v[1] = st[2] * ri; v[2] = st[3] * ri;
   };
@@ -213,14 +222,17 @@ __global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restri
   double t = fmax(-div / sqrt(omod2 + div * div + u0l0 * u0l0), 0.0);
   out[q] = t * t;
 }
-// Pending energy shift on interior points only (before a download).
-__global__ void __launch_bounds__(AUX_NT) k_apply_shift(Geom g, double* __restrict__ w,
+// Pending energy shift on interior points only (before a download).  The Newton start of the
+// thermally perfect gas is the point's temperature in aux, as force_var_1 starts from w_aux(6).
+template <class A>
+__global__ void __launch_bounds__(AUX_NT) k_apply_shift(Geom g, double* __restrict__ w, const A* __restrict__ aux,
                                                         const Scalars* __restrict__ sc) {
   const long long q = (long long)blockIdx.x * AUX_NT + threadIdx.x;
   if (q >= g.nint) return;
   const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
   const long long n = g.nvol, s = gidx(g, i, j, k);
-  w[4 * n + s] = shifted_rhoe(g, w[s], w[n + s], w[2 * n + s], w[3 * n + s], w[4 * n + s], sc->tbdiff);
+  w[4 * n + s] = shifted_rhoe(g, w[s], w[n + s], w[2 * n + s], w[3 * n + s], w[4 * n + s], sc->tbdiff,
+                              double(aux[5 * n + s]));
 }
 
 // Readers of the interior-only sensor and div/3 arrays at a stencil point that may be a ghost.
@@ -258,7 +270,9 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
 }
 
 // Flux at a face from a loaded stencil window (points p-(S-1) .. p+S of face p):
-// hi + lo is the face flux (lo = 0 in the FP64 form).
+// hi + lo is the face flux (lo = 0 in the FP64 form).  FS holds the flux variant flags of a
+// kernel instantiation: bit 0 the component-wise (Rusanov) WENO splitting, bit 1 the thermally
+// perfect gas.
 template <class R, int DIR, int LB, int WS, int S, int FS = 0>
 __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& st, bool ishk, int p,
                                             R (&hi)[5], R (&lo)[5], R* __restrict__ gs, int gstride) {
@@ -270,10 +284,10 @@ __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& 
     central_flux<R, DIR, LB, S>(g, st, lmax, g.nkeep, zf, hi, lo);
   } else {
     const int ord = max(WS + ep, 1);
-    if constexpr (FS == 1)
-      rusanov_flux<R, DIR, WS, S>(g, st, ord, hi, lo);
+    if constexpr ((FS & 1) != 0)
+      rusanov_flux<R, DIR, WS, S, (FS & 2) != 0>(g, st, ord, hi, lo);
     else
-      weno_flux<R, DIR, WS, S>(g, st, ord, hi, lo, gs, gstride);
+      weno_flux<R, DIR, WS, S, (FS & 2) != 0>(g, st, ord, hi, lo, gs, gstride);
   }
 }
 
@@ -452,7 +466,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
             double fln1 = (istep > 1 ? -(rhodt * fl_prev[ic]) : 0.0) - gamdt * f[0];
             double fln2 = (istep > 1 ? -(rhodt * fl_prev[nI + ic]) : 0.0) - gamdt * f[1];
             double dy = g.yn[j + 1] - g.yn[j];
-            const Prim pr = prim_from_w(g, w, a);
+            const Prim pr = prim_from_w<(FS & 2) != 0>(g, w, a, double(aux[5 * n + a]));
             double rhou = w[n + a];
             part[0] += fln1 * dy;
             part[1] += fln2 * dy;
@@ -483,7 +497,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
 // visflx_x/y/z_subroutine (:4779-4999), in the reference's accumulation order; at stage 3 also
 // sensor_subroutine (:4726-4744) into the next sensor buffer.  Arithmetic in R, accumulation
 // into the FP64 register.
-template <class R>
+template <class R, bool TP = false>
 __global__ void __launch_bounds__(256, VISC_MINB) k_visc(Geom g, const R* __restrict__ aux, double* __restrict__ fl,
                                               R* __restrict__ div3, double* __restrict__ sensor_next,
                                               double* __restrict__ wallprop, int do_sensor) {
@@ -495,7 +509,9 @@ __global__ void __launch_bounds__(256, VISC_MINB) k_visc(Geom g, const R* __rest
   const long long sX = 1, sY = g.sx, sZ = (long long)g.sx * g.sy;
   auto A = [&](long long a, int m) -> R { return __ldg(aux + (m - 1) * n + a); };
   const R uu = A(c, 2), vv = A(c, 3), ww = A(c, 4), mu = A(c, 7);
-  const R cploc = R(g.cp0), prandtl = R(g.prandtl);
+  // cp at the point (visflx_reduced_ord2) and at a face's mean temperature (visflx_x/y/z);
+  // a constant for the calorically perfect gas
+  const R cploc = TP ? R(cp_of_t(g, double(A(c, 6)))) : R(g.cp0), prandtl = R(g.prandtl);
   R dxl = R(1) / R(g.x[i + 1] - g.x[i - 1]);
   R dyl = R(1) / R(g.y[j + 1] - g.y[j - 1]);
   R dzl = R(1) / R(g.z[k + 1] - g.z[k - 1]);
@@ -558,7 +574,8 @@ __global__ void __launch_bounds__(256, VISC_MINB) k_visc(Geom g, const R* __rest
     s[0] = double((u2 - u1) * muf);
     s[1] = double((v2 - v1) * muf);
     s[2] = double((w2 - w1) * muf);
-    s[3] = double(((t2 - t1) * cploc / prandtl + (qq2 - qq1)) * muf);
+    const R cpf = TP ? R(cp_of_t(g, double(R(0.5) * (t1 + t2)))) : R(g.cp0);
+    s[3] = double(((t2 - t1) * cpf / prandtl + (qq2 - qq1)) * muf);
   };
   double lo[4], hi[4];
   // x: fl += dxhl*(fhat(i) - fhat(i-1)), fhat = -sigma
@@ -596,7 +613,7 @@ __global__ void __launch_bounds__(256, VISC_MINB) k_visc(Geom g, const R* __rest
 // div/3 and |omega| for the div term and the stage-3 sensor (sensor_subroutine,
 // kernels_cpu.F90:4726-4744, from |omega| and div/3), wall shear at j = 1.  Arithmetic in R,
 // accumulation into the FP64 register.
-template <class R>
+template <class R, bool TP = false>
 __global__ void __launch_bounds__(256) k_visc_ns(Geom g, const R* __restrict__ aux, double* __restrict__ fl,
                                                  R* __restrict__ div3, double* __restrict__ sensor_next,
                                                  double* __restrict__ wallprop, int do_sensor) {
@@ -660,7 +677,7 @@ __global__ void __launch_bounds__(256) k_visc_ns(Geom g, const R* __restrict__ a
     const R t = fmax(-dv / sqrt(om2 + dv * dv + u0l0 * u0l0), R(0));
     sensor_next[q] = double(t * t);
   }
-  const R cploc = R(g.cp0), prandtl = R(g.prandtl);
+  const R cploc = TP ? R(cp_of_t(g, double(A(c, 6)))) : R(g.cp0), prandtl = R(g.prandtl);
   const R sig11 = R(2) * (ux - div3l), sig12 = uy + vx, sig13 = uz + wx;
   const R sig22 = R(2) * (vy - div3l), sig23 = vz + wy, sig33 = R(2) * (wz - div3l);
   const R sigx = mux * sig11 + muy * sig12 + muz * sig13 + mu * ulap;
@@ -730,12 +747,12 @@ __global__ void __launch_bounds__(256) k_dt(Geom g, const double* __restrict__ w
     if constexpr (sizeof(R) == sizeof(double)) {
       uu = aux[n + c]; vv = aux[2 * n + c]; ww = aux[3 * n + c]; tt = aux[5 * n + c]; mu = aux[6 * n + c];
     } else {
-      const Prim p = prim_from_w(g, w, c);
+      const Prim p = prim_from_w<false>(g, w, c, double(aux[5 * n + c]));  // mixed form only
       uu = p.uu; vv = p.vv; ww = p.ww; tt = p.tt; mu = viscosity(g, tt);
     }
     double nu = ri * mu;
     double kr = nu / g.prandtl;
-    double cs = sqrt(g.gamloc * g.rgas0 * tt);
+    double cs = sqrt(gamloc_of_t(g, tt) * g.rgas0 * tt);
     v[0] = (fabs(uu) + cs) * g.dcsidx[i];
     v[1] = (fabs(vv) + cs) * g.detady[j];
     v[2] = (fabs(ww) + cs) * g.dzitdz[k];
@@ -832,7 +849,9 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
     const long long n = g.nvol, nI = g.nint, c = gidx(g, i, j, k);
     const double dt = sc->dt;
     const double rhodt = rhork * dt, gamdt = gamrk * dt;
-    const Prim old = prim_from_w(g, w, c);
+    // the stage's starting temperature is in aux (Newton start of the thermally perfect gas)
+    const double t_aux = double(aux[5 * n + c]);
+    const Prim old = prim_from_w<sizeof(R) == sizeof(double)>(g, w, c, t_aux);
     double fln[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
@@ -860,7 +879,7 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
       double uu = wn[1] * ri, vv = wn[2] * ri, ww = wn[3] * ri;
       double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
       double ee = wn[4] / wn[0] - qq;
-      double tt = t_from_e(g, ee);
+      double tt = t_from_e<sizeof(R) == sizeof(double)>(g, ee, t_aux);
       s2[0] = wn[1] * tt * dy;
       tstat = tt;
       // force_var_1 leaves this temperature in w_aux(6), where the statistics read it
@@ -1078,7 +1097,7 @@ template <class R>
 static void aux_launch(const Geom& g, DevState& d, int apply_shift, int write_ghost, int kid, cudaStream_t s,
                        long long* nl) {
   if (apply_shift) {
-    SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.sc));
+    SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<R><<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), d.sc));
     ++*nl;
   }
   SB_LAUNCH(d, kid, s, k_aux<R><<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), write_ghost));
@@ -1098,7 +1117,10 @@ cudaError_t launch_fill_ghosts(const Geom& g, DevState& d, cudaStream_t s, long 
 }
 
 cudaError_t launch_apply_shift(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
-  SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.sc));
+  if (g.precision == 1)
+    SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<float><<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.auxf, d.sc));
+  else
+    SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<double><<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc));
   ++*nl;
   return cudaGetLastError();
 }
@@ -1169,11 +1191,11 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS, FS><<<xg, xb, xsm, s>>>(g, aux, sensor, fl_new));
   if (g.conservative_viscous)
     SB_LAUNCH(d, K_VISC, s,
-              k_visc<R><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
+              k_visc<R, (FS & 2) != 0><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
                                                              fp64 && a.istep == 3));
   else
     SB_LAUNCH(d, K_VISC, s,
-              k_visc_ns<R><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
+              k_visc_ns<R, (FS & 2) != 0><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
                                                                 fp64 && a.istep == 3));
   if (!fp64 && a.istep == 3) {
     // the mixed form takes the stage-3 sensor in FP64 from the stage's starting state
@@ -1214,6 +1236,15 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
 template <class R>
 static cudaError_t stage_dispatch(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
                                   cudaStream_t s, long long* nl) {
+  if (!g.calorically_perfect) {
+    // the thermally perfect gas is instantiated for the FP64 sixth-order central / WENO5 scheme
+    if constexpr (sizeof(R) == sizeof(double)) {
+      if (g.lmax_base == 3 && g.weno_scheme == 3)
+        return g.flux_splitting == 1 ? stage_impl<R, 3, 3, 3>(g, d, a, fl_prev, fl_new, s, nl)
+                                     : stage_impl<R, 3, 3, 2>(g, d, a, fl_prev, fl_new, s, nl);
+    }
+    return cudaErrorInvalidValue;
+  }
   if (g.flux_splitting == 1) {
     // the Rusanov splitting is instantiated for the sixth-order central / WENO5 scheme
     if (g.lmax_base == 3 && g.weno_scheme == 3) return stage_impl<R, 3, 3, 1>(g, d, a, fl_prev, fl_new, s, nl);

@@ -39,7 +39,8 @@ struct StatStep {
 
 // (rho, rho u, rho v, rho w) at a stencil point as described above; the point is interior or lies
 // outside the block in one direction only.
-__device__ __forceinline__ void stat_point(const Geom& g, const double* __restrict__ w,
+template <class A>
+__device__ __forceinline__ void stat_point(const Geom& g, const double* __restrict__ w, const A* __restrict__ aux,
                                            const double* __restrict__ fl2, const double* __restrict__ fl3,
                                            const StatStep& a, int i, int j, int k, double (&v)[4]) {
   const long long n = g.nvol, nI = g.nint;
@@ -78,10 +79,11 @@ __device__ __forceinline__ void stat_point(const Geom& g, const double* __restri
     const long long s = gidx(g, i, sj, k);
     const double rho = w[s], rhou = w[n + s], rhov = w[2 * n + s], rhow = w[3 * n + s];
     double rhoe = w[4 * n + s];
-    if (a.pending) rhoe = shifted_rhoe(g, rho, rhou, rhov, rhow, rhoe, a.tbdiff);
+    const double ts = double(aux[5 * n + s]);  // Newton start (thermally perfect gas)
+    if (a.pending) rhoe = shifted_rhoe(g, rho, rhou, rhov, rhow, rhoe, a.tbdiff, ts);
     const double uu = rhou / rho, vv = rhov / rho, ww = rhow / rho;
     const double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-    const double tt = t_from_e(g, rhoe / rho - qq);
+    const double tt = t_from_e(g, rhoe / rho - qq, ts);
     const double pp = rho * tt * g.rgas0;
     const double tg = 2.0 * g.t_wall - tt;
     const double rg = pp / tg / g.rgas0;
@@ -92,51 +94,62 @@ __device__ __forceinline__ void stat_point(const Geom& g, const double* __restri
   v[0] = w[s]; v[1] = w[n + s]; v[2] = w[2 * n + s]; v[3] = w[3 * n + s];
 }
 
+// Velocities u = (rho u)/rho, ... of every interior and face-ghost point of the sampled state
+// (stat_point), each formed once: the derivative stencils of compute_stats divide
+// w(.,2:4)/w(.,1) at the neighbour points, the same quotients.
+template <class A>
+__global__ void __launch_bounds__(256) k_stats_vel(Geom g, const double* __restrict__ w, const A* __restrict__ aux,
+                                                   const double* __restrict__ fl2, const double* __restrict__ fl3,
+                                                   StatStep a, double* __restrict__ vel) {
+  const long long n = g.nvol;
+  const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (q >= n) return;
+  const int i = (int)(q % g.sx) - g.ng + 1, j = (int)((q / g.sx) % g.sy) - g.ng + 1,
+            k = (int)(q / ((long long)g.sx * g.sy)) - g.ng + 1;
+  const int ox = (i < 1 || i > g.nx), oy = (j < 1 || j > g.ny), oz = (k < 1 || k > g.nz);
+  if (ox + oy + oz > 1) return;  // the derivative stencils use no edge or corner points
+  double v[4];
+  stat_point(g, w, aux, fl2, fl3, a, i, j, k, v);
+  vel[q] = v[1] / v[0];
+  vel[n + q] = v[2] / v[0];
+  vel[2 * n + q] = v[3] / v[0];
+}
+
 template <class A>
 __global__ void __launch_bounds__(ST_NT) k_stats(Geom g, const double* __restrict__ w, const A* __restrict__ aux,
-                                                 const double* __restrict__ fl2, const double* __restrict__ fl3,
-                                                 StatStep a, int itav, double* __restrict__ wstat_z,
-                                                 double* __restrict__ wstat) {
+                                                 const double* __restrict__ vel, int itav,
+                                                 double* __restrict__ wstat_z, double* __restrict__ wstat) {
   const long long q = (long long)blockIdx.x * ST_NT + threadIdx.x;
   if (q >= (long long)g.nx * g.ny) return;
   const int i = (int)(q % g.nx) + 1, j = (int)(q / g.nx) + 1;
-  const long long n = g.nvol;
+  const long long n = g.nvol, sY = g.sx, sZ = (long long)g.sx * g.sy;
   const int lmax = g.lmax_base;  // visc_order / 2 (visc_order = ep_order)
   const double rgas0 = g.rgas0;
-  // get_gamloc (singleideal.F90:4752-4771), calorically perfect
-  const double gamloc = g.cp0 / (g.cp0 - rgas0);
-  const double cploc = gamloc / (gamloc - 1.0) * rgas0;
   const double dxm = g.dcsidx[i], dym = g.detady[j];
   double acc[NV_STAT];
 #pragma unroll
   for (int l = 0; l < NV_STAT; ++l) acc[l] = 0.0;
   for (int k = 1; k <= g.nz; ++k) {
+    const long long c = gidx(g, i, j, k);
     double ux = 0, vx = 0, wx = 0, uy = 0, vy = 0, wy = 0, uz = 0, vz = 0, wz = 0;
     for (int l = 1; l <= lmax; ++l) {
       const double ccl = g.coeff[lmax - 1][l - 1];
-      double p[4], m[4];
-      stat_point(g, w, fl2, fl3, a, i + l, j, k, p);
-      stat_point(g, w, fl2, fl3, a, i - l, j, k, m);
-      ux = ux + ccl * (p[1] / p[0] - m[1] / m[0]);
-      vx = vx + ccl * (p[2] / p[0] - m[2] / m[0]);
-      wx = wx + ccl * (p[3] / p[0] - m[3] / m[0]);
-      stat_point(g, w, fl2, fl3, a, i, j + l, k, p);
-      stat_point(g, w, fl2, fl3, a, i, j - l, k, m);
-      uy = uy + ccl * (p[1] / p[0] - m[1] / m[0]);
-      vy = vy + ccl * (p[2] / p[0] - m[2] / m[0]);
-      wy = wy + ccl * (p[3] / p[0] - m[3] / m[0]);
-      stat_point(g, w, fl2, fl3, a, i, j, k + l, p);
-      stat_point(g, w, fl2, fl3, a, i, j, k - l, m);
-      uz = uz + ccl * (p[1] / p[0] - m[1] / m[0]);
-      vz = vz + ccl * (p[2] / p[0] - m[2] / m[0]);
-      wz = wz + ccl * (p[3] / p[0] - m[3] / m[0]);
+      const long long ox = l, oy = l * sY, oz = l * sZ;
+      ux = ux + ccl * (vel[c + ox] - vel[c - ox]);
+      vx = vx + ccl * (vel[n + c + ox] - vel[n + c - ox]);
+      wx = wx + ccl * (vel[2 * n + c + ox] - vel[2 * n + c - ox]);
+      uy = uy + ccl * (vel[c + oy] - vel[c - oy]);
+      vy = vy + ccl * (vel[n + c + oy] - vel[n + c - oy]);
+      wy = wy + ccl * (vel[2 * n + c + oy] - vel[2 * n + c - oy]);
+      uz = uz + ccl * (vel[c + oz] - vel[c - oz]);
+      vz = vz + ccl * (vel[n + c + oz] - vel[n + c - oz]);
+      wz = wz + ccl * (vel[2 * n + c + oz] - vel[2 * n + c - oz]);
     }
     const double dzm = g.dzitdz[k];
     ux = ux * dxm; vx = vx * dxm; wx = wx * dxm;
     uy = uy * dym; vy = vy * dym; wy = wy * dym;
     uz = uz * dzm; vz = vz * dzm; wz = wz * dzm;
     const double omx = wy - vz, omy = uz - wx, omz = vx - uy;
-    const long long c = gidx(g, i, j, k);
     const double rho = w[c], rhou = w[n + c], rhov = w[2 * n + c], rhow = w[3 * n + c];
     const double ri = 1.0 / rho;
     const double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
@@ -145,6 +158,9 @@ __global__ void __launch_bounds__(ST_NT) k_stats(Geom g, const double* __restric
     const double pp = rho * rgas0 * tt;
     const double mu = double(aux[6 * n + c]);
     const double nu = mu / rho;
+    // get_gamloc (singleideal.F90:4752-4771)
+    const double gamloc = g.calorically_perfect ? g.cp0 / (g.cp0 - rgas0) : gamloc_of_t(g, tt);
+    const double cploc = gamloc / (gamloc - 1.0) * rgas0;
     const double cs = sqrt(gamloc * rgas0 * tt);
     const double mach = sqrt(2.0 * qq) / cs;
     const double t_tot = tt + qq * (gamloc - 1.0) / gamloc;
@@ -194,22 +210,32 @@ __global__ void __launch_bounds__(ST_NT) k_stats(Geom g, const double* __restric
   }
 }
 
+// The block's 256 cells own a contiguous run of 14 x 256 statistics: it is staged through shared
+// memory so that the reads and writes of w_stat_3d are coalesced.
 template <class A>
 __global__ void __launch_bounds__(256) k_stats3d(Geom g, const double* __restrict__ w, const A* __restrict__ aux,
                                                  int itav, double* __restrict__ ws3) {
-  const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
-  if (q >= g.nint) return;
-  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
-  const long long n = g.nvol, c = gidx(g, i, j, k);
-  const double r = w[c], ru = w[n + c], rv = w[2 * n + c], rw = w[3 * n + c];
-  const double t = double(aux[5 * n + c]);
-  const double v[NV_STAT_3D] = {r,           ru,          rv,          rw,          r * t,
-                                r * r,       ru * ru / r, rv * rv / r, rw * rw / r, ru * rv / r,
-                                ru * rw / r, rv * rw / r, r * (t * t), (r * t) * (r * t)};
-  const double rav = (double)itav;
-  double* o = ws3 + q * NV_STAT_3D;
+  __shared__ double buf[256 * NV_STAT_3D];
+  const long long q0 = (long long)blockIdx.x * 256, q = q0 + threadIdx.x;
+  const int cnt = (int)(g.nint - q0 < 256 ? g.nint - q0 : 256);
+  double* base = ws3 + q0 * NV_STAT_3D;
+  for (int e = threadIdx.x; e < cnt * NV_STAT_3D; e += 256) buf[e] = base[e];
+  __syncthreads();
+  if (q < g.nint) {
+    const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+    const long long n = g.nvol, c = gidx(g, i, j, k);
+    const double r = w[c], ru = w[n + c], rv = w[2 * n + c], rw = w[3 * n + c];
+    const double t = double(aux[5 * n + c]);
+    const double v[NV_STAT_3D] = {r,           ru,          rv,          rw,          r * t,
+                                  r * r,       ru * ru / r, rv * rv / r, rw * rw / r, ru * rv / r,
+                                  ru * rw / r, rv * rw / r, r * (t * t), (r * t) * (r * t)};
+    const double rav = (double)itav;
+    double* o = buf + threadIdx.x * NV_STAT_3D;
 #pragma unroll
-  for (int l = 0; l < NV_STAT_3D; ++l) o[l] = (o[l] * rav + v[l]) / (rav + 1.0);
+    for (int l = 0; l < NV_STAT_3D; ++l) o[l] = (o[l] * rav + v[l]) / (rav + 1.0);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < cnt * NV_STAT_3D; e += 256) base[e] = buf[e];
 }
 
 inline unsigned nblk(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
@@ -229,12 +255,15 @@ cudaError_t launch_stats(const Geom& g, DevState& d, const double* fl2, const do
   a.b2 = sc.bulk[1];
   a.tbdiff = sc.tbdiff;
   a.pending = pending;
-  const unsigned nb = nblk((long long)g.nx * g.ny, ST_NT);
-  if (g.precision == 1)
-    SB_LAUNCH(d, K_STATS, s, k_stats<float><<<nb, ST_NT, 0, s>>>(g, d.w, d.auxf, fl2, fl3, a, itav, d.wstat_z, d.wstat));
-  else
-    SB_LAUNCH(d, K_STATS, s, k_stats<double><<<nb, ST_NT, 0, s>>>(g, d.w, d.aux, fl2, fl3, a, itav, d.wstat_z, d.wstat));
-  ++*nl;
+  const unsigned nv = nblk(g.nvol, 256), nb = nblk((long long)g.nx * g.ny, ST_NT);
+  if (g.precision == 1) {
+    SB_LAUNCH(d, K_STATS, s, k_stats_vel<float><<<nv, 256, 0, s>>>(g, d.w, d.auxf, fl2, fl3, a, d.wstat_vel));
+    SB_LAUNCH(d, K_STATS, s, k_stats<float><<<nb, ST_NT, 0, s>>>(g, d.w, d.auxf, d.wstat_vel, itav, d.wstat_z, d.wstat));
+  } else {
+    SB_LAUNCH(d, K_STATS, s, k_stats_vel<double><<<nv, 256, 0, s>>>(g, d.w, d.aux, fl2, fl3, a, d.wstat_vel));
+    SB_LAUNCH(d, K_STATS, s, k_stats<double><<<nb, ST_NT, 0, s>>>(g, d.w, d.aux, d.wstat_vel, itav, d.wstat_z, d.wstat));
+  }
+  *nl += 2;
   return cudaGetLastError();
 }
 

@@ -40,16 +40,39 @@ void get_deriv_coeffs(double c1[4], double c2[5], int order1, int order2) {
   }
 }
 
-// get_e_from_temperature (singleideal.F90:2661-2683), calorically perfect branch
+// x^l for an integer exponent (Fortran's ** with an integer power)
+double ipow(double x, int l) {
+  double r = 1.0;
+  for (int q = 0; q < (l < 0 ? -l : l); ++q) r = r * x;
+  return l < 0 ? 1.0 / r : r;
+}
+
+// get_e_from_temperature (singleideal.F90:2661-2683)
 double e_from_t(const Setup& s, double tt) {
-  double ee = s.cv_coeff[1];
-  ee = ee + s.cv_coeff[0] * (tt / s.t0 - 1.0);
+  const int lo = s.indx_cp_l, hi = s.indx_cp_r;
+  auto cv = [&](int l) { return s.cv_coeff[static_cast<size_t>(l - lo)]; };
+  double ee = cv(hi + 1);
+  if (s.calorically_perfect == 1) {
+    ee = ee + cv(0) * (tt / s.t0 - 1.0);
+  } else {
+    for (int l = lo; l <= hi; ++l) {
+      if (l == -1) ee = ee + cv(l) * std::log(tt / s.t0);
+      else ee = ee + cv(l) / (l + 1.0) * (ipow(tt / s.t0, l + 1) - 1.0);
+    }
+  }
   return ee * s.t0;
 }
 
-// get_gamloc (singleideal.F90:4752-4771), calorically perfect branch
-double gamloc_host(const Setup& s) {
-  double cploc = s.cp_coeff[0];
+// get_gamloc (singleideal.F90:4752-4771)
+double gamloc_host(const Setup& s, double tt) {
+  const int lo = s.indx_cp_l, hi = s.indx_cp_r;
+  double cploc;
+  if (s.calorically_perfect == 1) {
+    cploc = s.cp_coeff[static_cast<size_t>(-lo)];
+  } else {
+    cploc = 0.0;
+    for (int l = lo; l <= hi; ++l) cploc = cploc + s.cp_coeff[static_cast<size_t>(l - lo)] * ipow(tt / s.t0, l);
+  }
   return cploc / (cploc - s.rgas0);
 }
 
@@ -252,7 +275,8 @@ void metrics_1d(const OffsetArray& g, int n, int mm, const double* c, const doub
   }
 }
 
-// set_fluid_prop (singleideal.F90:2685-2774), calorically perfect gas
+// set_fluid_prop (singleideal.F90:2685-2774): constant cp, or the cp(T) polynomial of a
+// thermally perfect gas (coefficients of cp/R in T_ref units, scaled to T/t0 and times rgas0)
 void set_fluid_prop(Setup& s) {
   const IniFile& c = s.ini;
   s.t_ref_dim = c.get_double("flow", "T_ref");
@@ -262,21 +286,59 @@ void set_fluid_prop(Setup& s) {
   s.sutherland_s = c.get_double("fluid", "s_suth");
   s.powerlaw_vtexp = c.get_double("fluid", "vt_exp");
   s.calorically_perfect = c.get_int("fluid", "calorically_perfect");
-  if (s.calorically_perfect != 1)
-    throw InputError("calorically_perfect = 0 (cp(T) polynomial) is not supported by the B200 backend");
-  s.indx_cp_l = 0;
-  s.indx_cp_r = 0;
+  if (s.calorically_perfect == 0) {
+    s.indx_cp_l = c.get_int("fluid", "indx_cp_l");
+    s.indx_cp_r = c.get_int("fluid", "indx_cp_r");
+    if (s.indx_cp_l > 0 || s.indx_cp_r < 0 || s.indx_cp_r - s.indx_cp_l + 2 > STREAMS_B200_MAX_CP)
+      throw InputError("cp polynomial: indx_cp_l <= 0 <= indx_cp_r with at most " +
+                       std::to_string(STREAMS_B200_MAX_CP) + " coefficients");
+  } else if (s.calorically_perfect == 1) {
+    s.indx_cp_l = 0;
+    s.indx_cp_r = 0;
+  } else {
+    throw InputError("calorically_perfect must be 0 or 1");
+  }
   s.rfac_type = c.get_int_or("fluid", "rfac_type", 0);
   s.rfac = (s.rfac_type == 0) ? std::pow(s.prandtl, 1.0 / 3.0) : std::pow(s.prandtl, 1.0 / 2.0);
-  s.cp_coeff.assign(2, 0.0);
-  s.cv_coeff.assign(2, 0.0);
+  const int lo = s.indx_cp_l, hi = s.indx_cp_r;
+  const size_t ncoef = static_cast<size_t>(hi - lo + 2);
+  s.cp_coeff.assign(ncoef, 0.0);
+  s.cv_coeff.assign(ncoef, 0.0);
+  auto cp = [&](int l) -> double& { return s.cp_coeff[static_cast<size_t>(l - lo)]; };
+  auto cv = [&](int l) -> double& { return s.cv_coeff[static_cast<size_t>(l - lo)]; };
+  double bcoeff = 0.0;
+  if (s.calorically_perfect == 0) {
+    const std::vector<double> tmp = c.get_double_array("fluid", "cp_coeff");
+    if (tmp.size() != ncoef)
+      throw InputError("Error! Check number of cp coefficients (" + std::to_string(ncoef) + " expected)");
+    s.cp_coeff = tmp;
+    const double tr = s.t_ref_dim;
+    double hstar = cp(hi + 1);
+    for (int l = lo; l <= hi; ++l) {
+      if (l == -1) hstar = hstar + cp(l) * std::log(tr);
+      else hstar = hstar + cp(l) / (l + 1) * ipow(tr, l + 1);
+    }
+    bcoeff = hstar / tr;
+    double cp_tref = 0.0;
+    for (int l = lo; l <= hi; ++l) cp_tref = cp_tref + cp(l) * ipow(tr, l);
+    cp_tref = cp_tref * s.rgas0;
+    const double cv_tref = cp_tref - s.rgas0;
+    s.gam = cp_tref / cv_tref;
+    for (int l = lo; l <= hi; ++l) {
+      cp(l) = cp(l) * ipow(tr, l);
+      cv(l) = cp(l);
+    }
+    cv(0) = cp(0) - 1.0;
+  }
   s.gm1 = s.gam - 1.0;
   s.gm = 1.0 / s.gm1;
-  s.cv_coeff[0] = s.gm;
-  s.cp_coeff[0] = s.gm * s.gam;
-  double bcoeff = s.cv_coeff[0] + 1.0;
-  s.cp_coeff[1] = bcoeff;
-  s.cv_coeff[1] = bcoeff - 1.0;
+  if (s.calorically_perfect == 1) {
+    cv(0) = s.gm;
+    cp(0) = s.gm * s.gam;
+    bcoeff = cv(0) + 1.0;
+  }
+  cp(hi + 1) = bcoeff;
+  cv(hi + 1) = bcoeff - 1.0;
   for (auto& v : s.cv_coeff) v = v * s.rgas0;
   for (auto& v : s.cp_coeff) v = v * s.rgas0;
 }
@@ -301,7 +363,7 @@ ChanPre chan_prop_pre(Setup& s) {
       tb_over_tw = 1.0 / tw_over_tb;
       tw_over_tr = 1.0 / (trec_over_tb * tb_over_tw);
       s.t_bulk_target = tb_over_tw * s.t_wall;
-      gamloc = gamloc_host(s);
+      gamloc = gamloc_host(s, s.t_bulk_target);
       if (std::fabs(gamloc - gamlocold) < 1.0e-9) break;
     }
     rmtw = rmb * std::sqrt(tb_over_tw);
@@ -1048,7 +1110,13 @@ void Setup::fill_params(streams_b200_params* p, int precision) const {
   p->mu0 = mu0; p->t0 = t0; p->rgas0 = rgas0; p->rho0 = rho0; p->u0 = u0; p->l0 = l0;
   p->sutherland_s = sutherland_s; p->t_ref_dim = t_ref_dim; p->powerlaw_vtexp = powerlaw_vtexp;
   p->prandtl = prandtl;
-  p->cp0 = cp_coeff[0]; p->cv0 = cv_coeff[0]; p->cp_last = cp_coeff[1]; p->cv_last = cv_coeff[1];
+  p->cp0 = cp_coeff[static_cast<size_t>(-indx_cp_l)]; p->cv0 = cv_coeff[static_cast<size_t>(-indx_cp_l)];
+  p->cp_last = cp_coeff.back(); p->cv_last = cv_coeff.back();
+  p->indx_cp_l = indx_cp_l; p->indx_cp_r = indx_cp_r;
+  for (size_t q = 0; q < cp_coeff.size() && q < STREAMS_B200_MAX_CP; ++q) {
+    p->cp_coeff[q] = cp_coeff[q];
+    p->cv_coeff[q] = cv_coeff[q];
+  }
   p->channel_case = channel_case ? 1 : 0;
   p->theta_wall = theta_wall; p->t_wall = t_wall; p->t_bulk_target = t_bulk_target; p->volchan = volchan;
   p->nrk = nrk;

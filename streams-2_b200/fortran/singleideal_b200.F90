@@ -74,6 +74,10 @@ contains
       p%betarecyc = eb%betarecyc
       p%xshock_imp = eb%xshock_imp ; p%shock_angle = eb%shock_angle ; p%tanhfacs = eb%tanhfacs
       p%winf_past_shock = eb%winf_past_shock
+      p%indx_cp_l = eb%indx_cp_l ; p%indx_cp_r = eb%indx_cp_r
+      p%cp_coeff = 0._rkind ; p%cv_coeff = 0._rkind
+      p%cp_coeff(1:eb%indx_cp_r-eb%indx_cp_l+2) = eb%cp_coeff(eb%indx_cp_l:eb%indx_cp_r+1)
+      p%cv_coeff(1:eb%indx_cp_r-eb%indx_cp_l+2) = eb%cv_coeff(eb%indx_cp_l:eb%indx_cp_r+1)
       ! the crandom sequence continues on the device: seed of this rank and the draws taken so far
       p%rng_seed = self%myrank + 1 ; p%rng_draws = self%crandom_draws
       allocate(self%epx(0:f%nx), self%epy(0:f%ny), self%epz(0:f%nz))

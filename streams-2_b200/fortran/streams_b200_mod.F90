@@ -10,6 +10,7 @@ module streams_b200_mod
 
   integer(c_int), parameter :: STREAMS_B200_OK = 0, STREAMS_B200_EINVAL = -1, STREAMS_B200_ECUDA = -2, &
                                STREAMS_B200_ENOMEM = -3, STREAMS_B200_ENAN = -4, STREAMS_B200_ENODEV = -6
+  integer(c_int), parameter :: STREAMS_B200_MAX_CP = 12
 
   type, bind(c) :: streams_b200_params
     integer(c_int) :: nx, ny, nz, ng
@@ -38,6 +39,9 @@ module streams_b200_mod
     integer(c_long_long) :: rng_draws
     real(c_double) :: xshock_imp, shock_angle, tanhfacs
     real(c_double) :: winf_past_shock(5)
+    ! cp(T) polynomial (calorically_perfect = 0): cp_coeff(indx_cp_l:indx_cp_r+1) at 1..
+    integer(c_int) :: indx_cp_l, indx_cp_r
+    real(c_double) :: cp_coeff(STREAMS_B200_MAX_CP), cv_coeff(STREAMS_B200_MAX_CP)
   end type streams_b200_params
 
   type, bind(c) :: streams_b200_grid

@@ -55,6 +55,8 @@ class Params(C.Structure):
         ("betarecyc", C.c_double), ("rng_seed", C.c_uint), ("rng_draws", C.c_longlong),
         ("xshock_imp", C.c_double), ("shock_angle", C.c_double), ("tanhfacs", C.c_double),
         ("winf_past_shock", C.c_double * 5),
+        ("indx_cp_l", C.c_int), ("indx_cp_r", C.c_int),
+        ("cp_coeff", C.c_double * 12), ("cv_coeff", C.c_double * 12),
     ]
 
 

@@ -10,11 +10,29 @@ import math
 import random
 
 
+# A thermally perfect gas for tests and examples: cp/R = sum of a_l T^l (T in kelvin),
+# l = -2..2 (so that the inverse powers and the logarithm of the l = -1 term are exercised),
+# about 3.49 at 220 K and 3.7 at 600 K, and the energy datum a_3 = 0.  Pass cp_poly=SYNTHETIC_CP_POLY
+# (or any (indx_cp_l, indx_cp_r, coefficients) triple) to the case builders.
+SYNTHETIC_CP_POLY = (-2, 2, (1000.0, 10.0, 3.3, 5.0e-4, 2.0e-7, 0.0))
+
+
+def _gas_keys(cp_poly) -> str:
+    """[fluid] keys of the gas model: calorically perfect, or a cp(T) polynomial."""
+    if cp_poly is None:
+        return "calorically_perfect = 1"
+    lo, hi, coef = cp_poly
+    if len(coef) != hi - lo + 2:
+        raise ValueError("cp_poly needs indx_cp_r - indx_cp_l + 2 coefficients")
+    return (f"calorically_perfect = 0\nindx_cp_l = {lo}\nindx_cp_r = {hi}\n"
+            f"cp_coeff = {', '.join(repr(float(c)) for c in coef)}")
+
+
 def channel_ini(nx=32, ny=24, nz=16, *, lx=6.283185307179586, ly=2.0, lz=3.141592653589793, mach=1.5,
                 re_bulk=3000.0, theta_wall=0.0, visc_model=1, vt_exp=0.76, sensor=0.05, ep_order=6,
                 weno_scheme=3, weno_version=0, nkeep=0, amp=0.1, seed=1, y_stretch=1.5, cfl=0.8,
                 num_iter=100, print_control=1, correct_bound_ord=1, reynolds_tau=None,
-                conservative_viscous=1, flux_splitting=0) -> str:
+                conservative_viscous=1, flux_splitting=0, cp_poly=None) -> str:
     """Input file of a seeded synthetic channel case (the shape of the benchmark channel).
 
     A [synthetic] section selects the seeded Poiseuille + uniform-noise initial field and the
@@ -92,7 +110,7 @@ Prandtl = 0.72
 visc_model = {visc_model}
 vt_exp = {vt_exp!r}
 s_suth = 110.4
-calorically_perfect = 1
+{_gas_keys(cp_poly)}
 
 [output]
 print_control = {print_control}
@@ -116,7 +134,7 @@ def bl_ini(nx=64, ny=48, nz=16, *, lx=100.0, ly=12.0, lz=8.0, mach=2.0, reynolds
            weno_scheme=3, weno_version=0, amp=0.05, x_recyc=None, nr_outflow=1, nr_top=1, cfl=0.8,
            jbgrid=None, dyptarget=0.7, nywr=None, lywr=None, ysmoosteps=10, conservative_viscous=1,
            num_iter=100, print_control=1, correct_bound_ord=1, rand_type=1, shock_angle=None,
-           xshock_imp=None, flux_splitting=0) -> str:
+           xshock_imp=None, flux_splitting=0, cp_poly=None) -> str:
     """Input file of a spatially developing supersonic boundary layer (the benchmark's boundary
     layer workload): box lx x ly x lz inflow thicknesses, BL grid (grid_type 4, wall-resolved part
     of nywr points up to lywr), recycling-rescaling inflow at xmin, extrapolation with a
@@ -211,7 +229,7 @@ Prandtl = 0.72
 visc_model = {visc_model}
 vt_exp = {vt_exp!r}
 s_suth = 110.4
-calorically_perfect = 1
+{_gas_keys(cp_poly)}
 
 [output]
 print_control = {print_control}

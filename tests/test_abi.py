@@ -38,7 +38,7 @@ def test_library_is_built_for_sm100a():
 
 def test_abi_version():
     import streams_b200
-    assert streams_b200.lib.streams_b200_abi_version() == 2
+    assert streams_b200.lib.streams_b200_abi_version() == 3
 
 
 def test_case_load_and_params(tmp_path):
