@@ -178,10 +178,6 @@ void fill_geom(streams_b200_ctx* c) {
   g.calorically_perfect = p.calorically_perfect;
   g.cp_l = p.indx_cp_l;
   g.cp_r = p.indx_cp_r;
-  for (int q = 0; q < MAX_CP; ++q) {
-    g.cpc[q] = p.cp_coeff[q];
-    g.cvc[q] = p.cv_coeff[q];
-  }
   g.t_wall = p.t_wall;
   g.channel_case = p.channel_case;
   g.force_var = p.channel_case && p.theta_wall >= -1.0;
@@ -279,6 +275,19 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
   g.epx = ex; g.epy = ey; g.epz = ez;
   for (int lm = 0; lm < 4; ++lm)
     for (int l = 0; l < 4; ++l) g.coeff[lm][l] = gr->coeff_deriv1 ? gr->coeff_deriv1[lm * 4 + l] : 0.0;
+  {
+    // cp(T) / cv(T) polynomial coefficients of the gas (used by the thermally perfect gas)
+    double* poly;
+    if ((e = dev_alloc(c, &poly, 2 * MAX_CP))) return fail(e, "cudaMalloc(gas)");
+    double h[2 * MAX_CP];
+    for (int q = 0; q < MAX_CP; ++q) {
+      h[q] = p->cp_coeff[q];
+      h[MAX_CP + q] = p->cv_coeff[q];
+    }
+    if ((e = cudaMemcpy(poly, h, sizeof(h), cudaMemcpyHostToDevice))) return fail(e, "cudaMemcpy(gas)");
+    g.cpc = poly;
+    g.cvc = poly + MAX_CP;
+  }
   if (p->conservative_viscous == 0) {
     if (!gr->dcsidx2 || !gr->detady2 || !gr->dzitdz2 || !gr->coeff_deriv2) {
       streams_b200_destroy(c);

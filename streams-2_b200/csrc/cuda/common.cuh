@@ -76,7 +76,8 @@ struct Geom {
   // thermally perfect gas (calorically_perfect = 0): cp(T) = sum of cpc[l - cp_l] (T/t0)^l for
   // l = cp_l..cp_r, cv likewise (set_fluid_prop's cp_coeff / cv_coeff, times rgas0)
   int calorically_perfect, cp_l, cp_r;
-  double cpc[MAX_CP], cvc[MAX_CP];
+  const double* cpc;  // device arrays of MAX_CP values (a kernel-parameter array indexed at run
+  const double* cvc;  // time would be copied to local memory)
   double t_wall;
   // channel forcing
   int channel_case, force_var;
@@ -202,15 +203,16 @@ __device__ __forceinline__ double gamloc_of_t(const Geom& g, double tt) {
 
 // Apply force_var_2 (kernels_cpu.F90:3285-3314) to the conserved values of one interior point:
 // temperature from the (unshifted) state as force_var_1 computes it (:3241-3282), shifted by tbdiff.
+template <bool TPA = true>
 __device__ __forceinline__ double shifted_rhoe(const Geom& g, double rho, double rhou, double rhov, double rhow,
                                                double rhoe, double tbdiff, double t_start) {
   double ri = 1.0 / rho;
   double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
   double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
   double ee = rhoe / rho - qq;
-  double tt = t_from_e(g, ee, t_start);
+  double tt = t_from_e<TPA>(g, ee, t_start);
   double ttnew = tt + tbdiff;
-  double en = e_from_t(g, ttnew);
+  double en = e_from_t<TPA>(g, ttnew);
   return rho * en + 0.5 * (rhou * rhou + rhov * rhov + rhow * rhow) / rho;
 }
 

@@ -78,6 +78,7 @@ __device__ __forceinline__ Prim prim_from_w(const Geom& g, const double* __restr
 // (bcswap, code/src/base_cpu.F90:1326-1435) or the staggered-wall mirror of
 // bcwall_staggered_subroutine (kernels_cpu.F90:6612-6678); t_src is the start of the Newton
 // iteration for the mirrored point's temperature (thermally perfect gas).
+template <bool TPA = true>
 __device__ __forceinline__ void point_state(const Geom& g, const double* __restrict__ w, int i, int j, int k,
                                             double (&st)[5], double t_src) {
   const long long n = g.nvol;
@@ -103,10 +104,10 @@ __device__ __forceinline__ void point_state(const Geom& g, const double* __restr
     double uu = rhou / rho, vv = rhov / rho, ww = rhow / rho;
     double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
     double ee = rhoe / rho - qq;
-    double tt = t_from_e(g, ee, t_src);
+    double tt = t_from_e<TPA>(g, ee, t_src);
     double pp = rho * tt * g.rgas0;
     tt = 2.0 * g.t_wall - tt;
-    ee = e_from_t(g, tt);
+    ee = e_from_t<TPA>(g, tt);
     rho = pp / tt / g.rgas0;
     rhou = -rho * uu;
     rhov = -rho * vv;
@@ -119,7 +120,7 @@ __device__ __forceinline__ void point_state(const Geom& g, const double* __restr
 // w -> aux at all interior and face-ghost points (eval_aux_subroutine, kernels_cpu.F90:6960-7011),
 // computed in FP64 and stored as A; with write_ghost_w = 1 the ghost states are also stored into
 // w, with write_ghost_w = 2 only they are (aux is left as it is).
-template <class A>
+template <class A, bool TP = false>
 __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, A* __restrict__ aux,
                                                 int write_ghost_w) {
   const long long n = g.nvol;
@@ -135,12 +136,15 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   const long long dst = gidx(g, i, j, k);
   // Newton starts (thermally perfect gas): the point's previous temperature, as eval_aux starts
   // from w_aux(6); for a wall ghost the mirror of it estimates the interior source point's
-  double t_old = double(aux[5 * n + dst]);
-  if (!(t_old > 0.0)) t_old = g.t0;
-  double t_src = 2.0 * g.t_wall - t_old;
-  if (!(t_src > 0.0)) t_src = g.t0;
+  double t_old = g.t0, t_src = g.t0;
+  if constexpr (TP) {
+    t_old = double(aux[5 * n + dst]);
+    if (!(t_old > 0.0)) t_old = g.t0;
+    t_src = 2.0 * g.t_wall - t_old;
+    if (!(t_src > 0.0)) t_src = g.t0;
+  }
   double st[5];
-  point_state(g, w, i, j, k, st, t_src);
+  point_state<TP>(g, w, i, j, k, st, t_src);
   double rho = st[0], rhou = st[1], rhov = st[2], rhow = st[3], rhoe = st[4];
   if (write_ghost_w && (ox | oy | oz)) {
     w[dst] = rho; w[n + dst] = rhou; w[2 * n + dst] = rhov; w[3 * n + dst] = rhow; w[4 * n + dst] = rhoe;
@@ -150,7 +154,7 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   double uu = rhou * ri, vv = rhov * ri, ww = rhow * ri;
   double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
   double ee = rhoe / rho - qq;
-  double tt = t_from_e(g, ee, t_old);
+  double tt = t_from_e<TP>(g, ee, t_old);
   double pp = rho * tt * g.rgas0;
   aux[dst] = A(rho);
   aux[n + dst] = A(uu);
@@ -224,15 +228,15 @@ __global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restri
 }
 // Pending energy shift on interior points only (before a download).  The Newton start of the
 // thermally perfect gas is the point's temperature in aux, as force_var_1 starts from w_aux(6).
-template <class A>
+template <class A, bool TP = false>
 __global__ void __launch_bounds__(AUX_NT) k_apply_shift(Geom g, double* __restrict__ w, const A* __restrict__ aux,
                                                         const Scalars* __restrict__ sc) {
   const long long q = (long long)blockIdx.x * AUX_NT + threadIdx.x;
   if (q >= g.nint) return;
   const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
   const long long n = g.nvol, s = gidx(g, i, j, k);
-  w[4 * n + s] = shifted_rhoe(g, w[s], w[n + s], w[2 * n + s], w[3 * n + s], w[4 * n + s], sc->tbdiff,
-                              double(aux[5 * n + s]));
+  const double t_start = TP ? double(aux[5 * n + s]) : g.t0;
+  w[4 * n + s] = shifted_rhoe<TP>(g, w[s], w[n + s], w[2 * n + s], w[3 * n + s], w[4 * n + s], sc->tbdiff, t_start);
 }
 
 // Readers of the interior-only sensor and div/3 arrays at a stencil point that may be a ghost.
@@ -466,7 +470,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
             double fln1 = (istep > 1 ? -(rhodt * fl_prev[ic]) : 0.0) - gamdt * f[0];
             double fln2 = (istep > 1 ? -(rhodt * fl_prev[nI + ic]) : 0.0) - gamdt * f[1];
             double dy = g.yn[j + 1] - g.yn[j];
-            const Prim pr = prim_from_w<(FS & 2) != 0>(g, w, a, double(aux[5 * n + a]));
+            const Prim pr = prim_from_w<(FS & 2) != 0>(g, w, a, (FS & 2) != 0 ? double(aux[5 * n + a]) : g.t0);
             double rhou = w[n + a];
             part[0] += fln1 * dy;
             part[1] += fln2 * dy;
@@ -747,7 +751,7 @@ __global__ void __launch_bounds__(256) k_dt(Geom g, const double* __restrict__ w
     if constexpr (sizeof(R) == sizeof(double)) {
       uu = aux[n + c]; vv = aux[2 * n + c]; ww = aux[3 * n + c]; tt = aux[5 * n + c]; mu = aux[6 * n + c];
     } else {
-      const Prim p = prim_from_w<false>(g, w, c, double(aux[5 * n + c]));  // mixed form only
+      const Prim p = prim_from_w<false>(g, w, c, g.t0);  // mixed form only: calorically perfect
       uu = p.uu; vv = p.vv; ww = p.ww; tt = p.tt; mu = viscosity(g, tt);
     }
     double nu = ri * mu;
@@ -831,7 +835,7 @@ __global__ void __launch_bounds__(FIN_NT) k_finish_rhs(Geom g, const double* __r
 // update_flux + force_rhs_2 + update_field (kernels_cpu.F90:3400-3442, 3092-3116) and the
 // partials of force_var_1 (:3241-3282) and of compute_residual / minmax (:6682-6810).  All FP64;
 // the primitive values of the stage's starting state are recomputed from w as eval_aux does.
-template <class R>
+template <class R, bool TP = false>
 __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, const double* __restrict__ fl_prev,
                                                 const double* __restrict__ fl_new, const Scalars* __restrict__ sc,
                                                 double rhork, double gamrk, int istep, int stats,
@@ -850,8 +854,8 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
     const double dt = sc->dt;
     const double rhodt = rhork * dt, gamdt = gamrk * dt;
     // the stage's starting temperature is in aux (Newton start of the thermally perfect gas)
-    const double t_aux = double(aux[5 * n + c]);
-    const Prim old = prim_from_w<sizeof(R) == sizeof(double)>(g, w, c, t_aux);
+    const double t_aux = TP ? double(aux[5 * n + c]) : g.t0;
+    const Prim old = prim_from_w<TP>(g, w, c, t_aux);
     double fln[5];
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
@@ -879,7 +883,7 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
       double uu = wn[1] * ri, vv = wn[2] * ri, ww = wn[3] * ri;
       double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
       double ee = wn[4] / wn[0] - qq;
-      double tt = t_from_e<sizeof(R) == sizeof(double)>(g, ee, t_aux);
+      double tt = t_from_e<TP>(g, ee, t_aux);
       s2[0] = wn[1] * tt * dy;
       tstat = tt;
       // force_var_1 leaves this temperature in w_aux(6), where the statistics read it
@@ -1093,15 +1097,28 @@ template <> float* div3_of<float>(DevState& d) { return d.div3f; }
 
 // A pending energy shift is applied to the interior in its own pass first: the aux pass reads
 // interior points as the sources of ghost states, so it must not rewrite them itself.
+template <class R, bool TP>
+static void aux_launch_tp(const Geom& g, DevState& d, int apply_shift, int write_ghost, int kid, cudaStream_t s,
+                          long long* nl) {
+  if (apply_shift) {
+    SB_LAUNCH(d, K_APPLY_SHIFT, s,
+              k_apply_shift<R, TP><<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), d.sc));
+    ++*nl;
+  }
+  SB_LAUNCH(d, kid, s, k_aux<R, TP><<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), write_ghost));
+  ++*nl;
+}
+// the thermally perfect instantiations exist for the FP64 form only
 template <class R>
 static void aux_launch(const Geom& g, DevState& d, int apply_shift, int write_ghost, int kid, cudaStream_t s,
                        long long* nl) {
-  if (apply_shift) {
-    SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<R><<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), d.sc));
-    ++*nl;
+  if constexpr (sizeof(R) == sizeof(double)) {
+    if (!g.calorically_perfect) {
+      aux_launch_tp<R, true>(g, d, apply_shift, write_ghost, kid, s, nl);
+      return;
+    }
   }
-  SB_LAUNCH(d, kid, s, k_aux<R><<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), write_ghost));
-  ++*nl;
+  aux_launch_tp<R, false>(g, d, apply_shift, write_ghost, kid, s, nl);
 }
 
 cudaError_t launch_aux(const Geom& g, DevState& d, int apply_shift, cudaStream_t s, long long* nl) {
@@ -1119,6 +1136,9 @@ cudaError_t launch_fill_ghosts(const Geom& g, DevState& d, cudaStream_t s, long 
 cudaError_t launch_apply_shift(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
   if (g.precision == 1)
     SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<float><<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.auxf, d.sc));
+  else if (!g.calorically_perfect)
+    SB_LAUNCH(d, K_APPLY_SHIFT, s,
+              k_apply_shift<double, true><<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc));
   else
     SB_LAUNCH(d, K_APPLY_SHIFT, s, k_apply_shift<double><<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, d.aux, d.sc));
   ++*nl;
@@ -1225,7 +1245,7 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   }
   const unsigned nbu = nblocks(g.nint, 256);
   SB_LAUNCH(d, K_UPDATE, s,
-            k_update<R><<<nbu, 256, 0, s>>>(g, d.w, fl_prev, fl_new, d.sc, a.rhork, a.gamrk, a.istep,
+            k_update<R, (FS & 2) != 0><<<nbu, 256, 0, s>>>(g, d.w, fl_prev, fl_new, d.sc, a.rhork, a.gamrk, a.istep,
                                             a.want_stats, d.red, sensor_next, sensor, aux));
   SB_LAUNCH(d, K_FINISH_UPD, s, k_finish_upd<<<1, FIN_NT, 0, s>>>(g, d.red, nbu, a.want_stats, a.add_time, d.sc));
   *nl += 2;
