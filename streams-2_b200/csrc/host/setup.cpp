@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <fstream>
 #include <sstream>
+#include <utility>
 
 namespace streams_b200 {
 
@@ -1237,8 +1238,27 @@ void write_restart_state(const Setup& s, const double* w, int icyc, double time,
   std::fclose(fin);
 }
 
+// flow_params.dat as set_flow_params writes it (singleideal.F90:2818-2852): the reference values
+// that post-processing (tools/postpro) reads beside stat.bin
+void write_flow_params(const Setup& s, const std::string& dir) {
+  FILE* f = std::fopen((dir + "/flow_params.dat").c_str(), "w");
+  if (!f) throw InputError("cannot write flow_params.dat");
+  const double cp0 = s.cp_coeff[static_cast<size_t>(-s.indx_cp_l)];
+  const double cv0 = s.cv_coeff[static_cast<size_t>(-s.indx_cp_l)];
+  const double k0 = s.mu0 * cp0 / s.prandtl;
+  std::fprintf(f, "[flow_params]\n");
+  const std::pair<const char*, double> kv[] = {
+      {"u0", s.u0}, {"p0", s.p0}, {"rho0", s.rho0}, {"t0", s.t0}, {"c0", s.c0}, {"l0", s.l0},
+      {"cp0", cp0}, {"cv0", cv0}, {"mu0", s.mu0}, {"k0", k0}, {"gam", s.gam}, {"T_wall", s.t_wall},
+      {"theta_wall", s.theta_wall}, {"rfac", s.rfac}, {"powerlaw_vtexp", s.powerlaw_vtexp},
+      {"T_ref_dim", s.t_ref_dim}, {"Reynolds", s.reynolds}, {"Mach", s.mach}, {"Prandtl", s.prandtl}};
+  for (const auto& p : kv) std::fprintf(f, "%s = %.17e\n", p.first, p.second);
+  std::fclose(f);
+}
+
 void write_run_output(const Setup& s, const double* w, int icyc, double time, const std::string& dir,
                       const StatsOut* st) {
+  write_flow_params(s, dir);
   write_rst(s, w, dir);
   if (st) write_stats_files(s, dir, *st);
   write_field_info(dir, icyc, time, st);
