@@ -33,13 +33,15 @@ constexpr int AUX_NT = 256;
 constexpr int XF_TX = 32, XF_TY = 4, XF_NT = XF_TX * XF_TY;  // x faces: 4 row-warps per block
 constexpr int MT_NT = 128;                                     // march kernels
 // Resident blocks per SM asked of the register allocator for the FP64 and FP32 instantiations
-// of the flux kernels (measured: 3 and 4 blocks of 128 threads beat the unconstrained
-// 2 blocks, although the FP64 march kernels then spill a little; the kernels are latency bound).
+// of the flux kernels (measured on the 1024x256x192 boundary layer: 3 blocks of 128 threads for
+// the FP64 kernels, whose WENO scratch also caps them at 3; for FP32, 5 blocks for the x pass
+// (5.41 against 5.90 ms at 4) and 4 for the march passes (5 blocks: 7.1-7.4 against 5.4-6.5 ms);
+// the kernels are latency bound).
 #ifndef XF_MINB_D
 #define XF_MINB_D 3
 #endif
 #ifndef XF_MINB_F
-#define XF_MINB_F 4
+#define XF_MINB_F 5
 #endif
 #ifndef MT_MINB_D
 #define MT_MINB_D 3
@@ -48,9 +50,12 @@ constexpr int MT_NT = 128;                                     // march kernels
 #define MT_MINB_F 4
 #endif
 // the viscous pass: 4 blocks of 256 threads per SM (64 registers, a little spilling) measured
-// faster than 2 blocks at 128 registers
+// faster than 2 blocks at 128 registers, and for FP32 faster than 3 blocks (2.77 against 3.48 ms)
 #ifndef VISC_MINB
 #define VISC_MINB 4
+#endif
+#ifndef VISC_MINB_F
+#define VISC_MINB_F VISC_MINB
 #endif
 constexpr int FIN_NT = 1024;
 
@@ -502,7 +507,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
 // sensor_subroutine (:4726-4744) into the next sensor buffer.  Arithmetic in R, accumulation
 // into the FP64 register.
 template <class R, bool TP = false>
-__global__ void __launch_bounds__(256, VISC_MINB) k_visc(Geom g, const R* __restrict__ aux, double* __restrict__ fl,
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F) k_visc(Geom g, const R* __restrict__ aux, double* __restrict__ fl,
                                               R* __restrict__ div3, double* __restrict__ sensor_next,
                                               double* __restrict__ wallprop, int do_sensor) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
