@@ -73,6 +73,7 @@ long long footprint(const streams_b200_params* p) {
   long long b = 0;
   b += nvol * 5 * 8;   // w
   b += nvol * 7 * fb;  // aux
+  if (p->precision == 1) b += nvol * 3 * 8;  // FP64 velocities for the stage-3 sensor
   b += nint * fb;      // div3
   b += nint * 2 * 8;   // sensor, sensor_next
   b += nint * 10 * 8;  // two RK registers
@@ -333,7 +334,8 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
   DevState& d = c->d;
   const bool mixed = p->precision == 1;
   if (mixed) {
-    if ((e = dev_alloc(c, &d.auxf, g.nvol * 7)) || (e = dev_alloc(c, &d.div3f, g.nint)))
+    if ((e = dev_alloc(c, &d.auxf, g.nvol * 7)) || (e = dev_alloc(c, &d.div3f, g.nint)) ||
+        (e = dev_alloc(c, &d.vel64, g.nvol * 3)))
       return fail(e, "cudaMalloc(state)");
   } else {
     if ((e = dev_alloc(c, &d.aux, g.nvol * 7)) || (e = dev_alloc(c, &d.div3, g.nint)))

@@ -41,6 +41,7 @@ struct DevState {
   // mixed form: primitive fields and div/3 in FP32 (the sensor stays FP64 in both forms)
   float* auxf = nullptr;
   float* div3f = nullptr;
+  double* vel64 = nullptr;    // FP64 velocities of the stage-3 aux pass (3 x nvol): the stage-3 sensor
   double* fl_a = nullptr;     // interior, 5 variables (two RK registers, ping-pong)
   double* fl_b = nullptr;
   double* wallprop = nullptr; // nx*nz*3

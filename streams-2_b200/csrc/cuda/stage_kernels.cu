@@ -124,10 +124,11 @@ __device__ __forceinline__ void point_state(const Geom& g, const double* __restr
 
 // w -> aux at all interior and face-ghost points (eval_aux_subroutine, kernels_cpu.F90:6960-7011),
 // computed in FP64 and stored as A; with write_ghost_w = 1 the ghost states are also stored into
-// w, with write_ghost_w = 2 only they are (aux is left as it is).
+// w, with write_ghost_w = 2 only they are (aux is left as it is).  With vel non-null the FP64
+// velocities are stored too (the mixed form's stage-3 sensor reads them).
 template <class A, bool TP = false>
 __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, A* __restrict__ aux,
-                                                int write_ghost_w) {
+                                                int write_ghost_w, double* __restrict__ vel) {
   const long long n = g.nvol;
   const long long q = (long long)blockIdx.x * AUX_NT + threadIdx.x;
   if (q >= n) return;
@@ -161,6 +162,11 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   double ee = rhoe / rho - qq;
   double tt = t_from_e<TP>(g, ee, t_old);
   double pp = rho * tt * g.rgas0;
+  if (vel) {  // FP64 velocities, as the sensor forms them from w
+    vel[dst] = uu;
+    vel[n + dst] = vv;
+    vel[2 * n + dst] = ww;
+  }
   aux[dst] = A(rho);
   aux[n + dst] = A(uu);
   aux[2 * n + dst] = A(vv);
@@ -231,6 +237,51 @@ __global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restri
   double t = fmax(-div / sqrt(omod2 + div * div + u0l0 * u0l0), 0.0);
   out[q] = t * t;
 }
+// The stage-3 Ducros sensor of the mixed form (k_sensor64 modes 1 and 2) from the FP64 velocities
+// that the stage's aux pass stored at the interior and face-ghost points: the same quotients and
+// the same arithmetic, without re-forming six neighbours' states per point.
+__global__ void __launch_bounds__(256) k_sensor_vel(Geom g, const double* __restrict__ vel, double* __restrict__ out,
+                                                    int mode) {
+  const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (q >= g.nint) return;
+  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+  const long long n = g.nvol, c = gidx(g, i, j, k), sY = g.sx, sZ = (long long)g.sx * g.sy;
+  auto V = [&](long long a, int m) { return vel[m * n + a]; };
+  double ux, vx, wx, uy, vy, wy, uz, vz, wz;
+  if (mode == 1) {
+    double dxl = 1.0 / (g.x[i + 1] - g.x[i - 1]);
+    double dyl = 1.0 / (g.y[j + 1] - g.y[j - 1]);
+    double dzl = 1.0 / (g.z[k + 1] - g.z[k - 1]);
+    ux = dxl * (V(c + 1, 0) - V(c - 1, 0)); vx = dxl * (V(c + 1, 1) - V(c - 1, 1)); wx = dxl * (V(c + 1, 2) - V(c - 1, 2));
+    uy = dyl * (V(c + sY, 0) - V(c - sY, 0)); vy = dyl * (V(c + sY, 1) - V(c - sY, 1));
+    wy = dyl * (V(c + sY, 2) - V(c - sY, 2));
+    uz = dzl * (V(c + sZ, 0) - V(c - sZ, 0)); vz = dzl * (V(c + sZ, 1) - V(c - sZ, 1));
+    wz = dzl * (V(c + sZ, 2) - V(c - sZ, 2));
+  } else {
+    const int lv = g.lmax_base;
+    double d[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int l = 1; l <= lv; ++l) {
+      const double ccl = g.coeff[lv - 1][l - 1];
+      for (int v = 0; v < 3; ++v) d[0][v] = d[0][v] + ccl * (V(c + l, v) - V(c - l, v));
+      for (int v = 0; v < 3; ++v) d[1][v] = d[1][v] + ccl * (V(c + l * sY, v) - V(c - l * sY, v));
+      for (int v = 0; v < 3; ++v) d[2][v] = d[2][v] + ccl * (V(c + l * sZ, v) - V(c - l * sZ, v));
+    }
+    ux = d[0][0] * g.dcsidx[i]; vx = d[0][1] * g.dcsidx[i]; wx = d[0][2] * g.dcsidx[i];
+    uy = d[1][0] * g.detady[j]; vy = d[1][1] * g.detady[j]; wy = d[1][2] * g.detady[j];
+    uz = d[2][0] * g.dzitdz[k]; vz = d[2][1] * g.dzitdz[k]; wz = d[2][2] * g.dzitdz[k];
+  }
+  double div = ux + vy + wz;
+  double omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
+  double omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
+  double u0l0 = g.u0 / g.l0;
+  double div3l = div / 3.0;
+  double om = sqrt(omod2);
+  omod2 = om * om;
+  div = 3.0 * div3l;
+  double t = fmax(-div / sqrt(omod2 + div * div + u0l0 * u0l0), 0.0);
+  out[q] = t * t;
+}
+
 // Pending energy shift on interior points only (before a download).  The Newton start of the
 // thermally perfect gas is the point's temperature in aux, as force_var_1 starts from w_aux(6).
 template <class A, bool TP = false>
@@ -1104,26 +1155,27 @@ template <> float* div3_of<float>(DevState& d) { return d.div3f; }
 // interior points as the sources of ghost states, so it must not rewrite them itself.
 template <class R, bool TP>
 static void aux_launch_tp(const Geom& g, DevState& d, int apply_shift, int write_ghost, int kid, cudaStream_t s,
-                          long long* nl) {
+                          long long* nl, double* vel) {
   if (apply_shift) {
     SB_LAUNCH(d, K_APPLY_SHIFT, s,
               k_apply_shift<R, TP><<<nblocks(g.nint, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), d.sc));
     ++*nl;
   }
-  SB_LAUNCH(d, kid, s, k_aux<R, TP><<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), write_ghost));
+  SB_LAUNCH(d, kid, s,
+            k_aux<R, TP><<<nblocks(g.nvol, AUX_NT), AUX_NT, 0, s>>>(g, d.w, aux_of<R>(d), write_ghost, vel));
   ++*nl;
 }
 // the thermally perfect instantiations exist for the FP64 form only
 template <class R>
 static void aux_launch(const Geom& g, DevState& d, int apply_shift, int write_ghost, int kid, cudaStream_t s,
-                       long long* nl) {
+                       long long* nl, double* vel = nullptr) {
   if constexpr (sizeof(R) == sizeof(double)) {
     if (!g.calorically_perfect) {
-      aux_launch_tp<R, true>(g, d, apply_shift, write_ghost, kid, s, nl);
+      aux_launch_tp<R, true>(g, d, apply_shift, write_ghost, kid, s, nl, vel);
       return;
     }
   }
-  aux_launch_tp<R, false>(g, d, apply_shift, write_ghost, kid, s, nl);
+  aux_launch_tp<R, false>(g, d, apply_shift, write_ghost, kid, s, nl, vel);
 }
 
 cudaError_t launch_aux(const Geom& g, DevState& d, int apply_shift, cudaStream_t s, long long* nl) {
@@ -1200,7 +1252,9 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   double* sensor_next = d.sensor_next;
   R* div3 = div3_of<R>(d);
   const bool fp64 = sizeof(R) == sizeof(double);
-  if (a.run_aux) aux_launch<R>(g, d, a.apply_shift, 0, K_AUX, s, nl);
+  // the mixed form's stage-3 sensor is taken in FP64 from velocities that this aux pass stores
+  double* vel = (!fp64 && a.istep == 3) ? d.vel64 : nullptr;
+  if (a.run_aux) aux_launch<R>(g, d, a.apply_shift, 0, K_AUX, s, nl, vel);
   const size_t xsm = weno_scratch_bytes<R, WS>(XF_NT), msm = weno_scratch_bytes<R, WS>(MT_NT);
   // per instantiation and device: allow more than 48 KB of dynamic shared memory
   static unsigned long long smem_set = 0;
@@ -1224,8 +1278,13 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
                                                                 fp64 && a.istep == 3));
   if (!fp64 && a.istep == 3) {
     // the mixed form takes the stage-3 sensor in FP64 from the stage's starting state
-    SB_LAUNCH(d, K_INIT_SENSOR, s,
-              k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, sensor_next, g.conservative_viscous ? 1 : 2));
+    if (a.run_aux)
+      SB_LAUNCH(d, K_INIT_SENSOR, s,
+                k_sensor_vel<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.vel64, sensor_next,
+                                                                  g.conservative_viscous ? 1 : 2));
+    else
+      SB_LAUNCH(d, K_INIT_SENSOR, s,
+                k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, sensor_next, g.conservative_viscous ? 1 : 2));
     ++*nl;
   }
   if (gyb > 0)
