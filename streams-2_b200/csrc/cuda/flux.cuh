@@ -231,10 +231,13 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
 }
 
 // Central energy-preserving split-form flux (kernels_cpu.F90:462-612 for x; same in y, z).
-// DIR: 0 x, 1 y, 2 z.  Points of st are at offsets -(S-1)..S (index o + S - 1).
-template <class R, int DIR, int LB, int S>
-__device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>& st, int lmax, int nkeep,
+// DIR: 0 x, 1 y, 2 z.  Points of st are at offsets -(S-1)..S (index o + S - 1).  KG = false
+// instantiates the default nkeep = 0 form at compile time (the general KEEP(n) branch, with its
+// divisions, otherwise shapes the register allocation of the whole flux kernel).
+template <class R, int DIR, int LB, int S, bool KG = true>
+__device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>& st, int lmax, int nkeep_in,
                                              bool zero_flux, R (&fh)[5], R (&fl)[5]) {
+  const int nkeep = KG ? nkeep_in : 0;
   const R rgas0 = R(g.rgas0);
   R pp[2 * S], ee[2 * S];
 #pragma unroll

@@ -332,7 +332,7 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
 // Flux at a face from a loaded stencil window (points p-(S-1) .. p+S of face p):
 // hi + lo is the face flux (lo = 0 in the FP64 form).  FS holds the flux variant flags of a
 // kernel instantiation: bit 0 the component-wise (Rusanov) WENO splitting, bit 1 the thermally
-// perfect gas.
+// perfect gas, bit 2 a central flux with nkeep != 0 (otherwise nkeep = 0 at compile time).
 template <class R, int DIR, int LB, int WS, int S, int FS = 0>
 __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& st, bool ishk, int p,
                                             R (&hi)[5], R (&lo)[5], R* __restrict__ gs, int gstride) {
@@ -341,7 +341,7 @@ __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& 
   if (!ishk) {
     const int lmax = max(g.lmax_base + ep, 1);
     const bool zf = (p == 0 && g.fzf[2 * DIR] == 1) || (p == nd && g.fzf[2 * DIR + 1] == 1);
-    central_flux<R, DIR, LB, S>(g, st, lmax, g.nkeep, zf, hi, lo);
+    central_flux<R, DIR, LB, S, (FS & 4) != 0>(g, st, lmax, g.nkeep, zf, hi, lo);
   } else {
     const int ord = max(WS + ep, 1);
     if constexpr ((FS & 1) != 0)
@@ -1317,6 +1317,14 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   return cudaGetLastError();
 }
 
+// nkeep = 0 (the default) with the central flux specialised at compile time, else the general form
+template <class R, int LB, int WS, int FS>
+static cudaError_t stage_kg(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
+                            cudaStream_t s, long long* nl) {
+  if (g.nkeep != 0) return stage_impl<R, LB, WS, FS | 4>(g, d, a, fl_prev, fl_new, s, nl);
+  return stage_impl<R, LB, WS, FS>(g, d, a, fl_prev, fl_new, s, nl);
+}
+
 template <class R>
 static cudaError_t stage_dispatch(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
                                   cudaStream_t s, long long* nl) {
@@ -1324,20 +1332,20 @@ static cudaError_t stage_dispatch(const Geom& g, DevState& d, const StageArgs& a
     // the thermally perfect gas is instantiated for the FP64 sixth-order central / WENO5 scheme
     if constexpr (sizeof(R) == sizeof(double)) {
       if (g.lmax_base == 3 && g.weno_scheme == 3)
-        return g.flux_splitting == 1 ? stage_impl<R, 3, 3, 3>(g, d, a, fl_prev, fl_new, s, nl)
-                                     : stage_impl<R, 3, 3, 2>(g, d, a, fl_prev, fl_new, s, nl);
+        return g.flux_splitting == 1 ? stage_kg<R, 3, 3, 3>(g, d, a, fl_prev, fl_new, s, nl)
+                                     : stage_kg<R, 3, 3, 2>(g, d, a, fl_prev, fl_new, s, nl);
     }
     return cudaErrorInvalidValue;
   }
   if (g.flux_splitting == 1) {
     // the Rusanov splitting is instantiated for the sixth-order central / WENO5 scheme
-    if (g.lmax_base == 3 && g.weno_scheme == 3) return stage_impl<R, 3, 3, 1>(g, d, a, fl_prev, fl_new, s, nl);
+    if (g.lmax_base == 3 && g.weno_scheme == 3) return stage_kg<R, 3, 3, 1>(g, d, a, fl_prev, fl_new, s, nl);
     return cudaErrorInvalidValue;
   }
-  if (g.lmax_base == 3 && g.weno_scheme == 3) return stage_impl<R, 3, 3>(g, d, a, fl_prev, fl_new, s, nl);
-  if (g.lmax_base == 2 && g.weno_scheme == 2) return stage_impl<R, 2, 2>(g, d, a, fl_prev, fl_new, s, nl);
-  if (g.lmax_base == 4 && g.weno_scheme == 4) return stage_impl<R, 4, 4>(g, d, a, fl_prev, fl_new, s, nl);
-  if (g.lmax_base == 3 && g.weno_scheme == 2) return stage_impl<R, 3, 2>(g, d, a, fl_prev, fl_new, s, nl);
+  if (g.lmax_base == 3 && g.weno_scheme == 3) return stage_kg<R, 3, 3, 0>(g, d, a, fl_prev, fl_new, s, nl);
+  if (g.lmax_base == 2 && g.weno_scheme == 2) return stage_kg<R, 2, 2, 0>(g, d, a, fl_prev, fl_new, s, nl);
+  if (g.lmax_base == 4 && g.weno_scheme == 4) return stage_kg<R, 4, 4, 0>(g, d, a, fl_prev, fl_new, s, nl);
+  if (g.lmax_base == 3 && g.weno_scheme == 2) return stage_kg<R, 3, 2, 0>(g, d, a, fl_prev, fl_new, s, nl);
   return cudaErrorInvalidValue;
 }
 
