@@ -330,7 +330,8 @@ __device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>&
 // (:2728-2782, :2842-2896, :2956-3010), local Lax-Friedrichs splitting with the stencil maximum
 // of |u_n -+ c| (:614-675) and wenorec_1d; back-projection with the right eigenvectors (:677-683).
 // TP: thermally perfect gas (Newton for the Roe-averaged temperature, gamma(T) per point; FP64).
-template <class R, int DIR, int WS, int S, bool TP = false>
+// WZ: WENO-Z weights (weno_version = 1) instead of WENO-JS, fixed at compile time.
+template <class R, int DIR, int WS, int S, bool TP = false, bool WZ = false>
 __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5],
                                           R (&fl)[5], R* __restrict__ gs, int gstride) {
   static_assert(!TP || sizeof(R) == sizeof(double), "the thermally perfect gas is an FP64 path");
@@ -442,7 +443,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
       gm[l] = gs[((m * 2 * WS + l) * 2 + 1) * gstride];
     }
     const R bs = (m == 2 || m == 3) ? betascale_b : betascale_a;
-    const R f = wenorec<R, WS>(gp, gm, ord, g.weno_version, bs);
+    const R f = wenorec<R, WS>(gp, gm, ord, WZ ? 1 : 0, bs);
 #pragma unroll
     for (int mm = 0; mm < 5; ++mm)
       if (mm == m) fi[mm] = f;
@@ -477,7 +478,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
 // Rusanov (component-wise local Lax-Friedrichs) WENO flux of the *_hybrid_rusanov kernels
 // (kernels_cpu.F90:692-941 for x, same in y and z): stencil maximum of |u_n -+ c|, split
 // values of the conserved fluxes, wenorec with the scales of wenorec_1d_rusanov (:2325-2523).
-template <class R, int DIR, int WS, int S, bool TP = false>
+template <class R, int DIR, int WS, int S, bool TP = false, bool WZ = false>
 __device__ __forceinline__ void rusanov_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5], R (&fl)[5]) {
   static_assert(!TP || sizeof(R) == sizeof(double), "the thermally perfect gas is an FP64 path");
   const R rgas0 = R(g.rgas0);
@@ -528,7 +529,7 @@ __device__ __forceinline__ void rusanov_flux(const Geom& g, const Stencil<R, S>&
       gm[l] = evm - c;
     }
     const R bs = m == 0 ? bsc[0] : (m == 4 ? bsc[4] : bsc[1]);
-    const R f = wenorec<R, WS>(gp, gm, ord, g.weno_version, bs);
+    const R f = wenorec<R, WS>(gp, gm, ord, WZ ? 1 : 0, bs);
 #pragma unroll
     for (int mm = 0; mm < 5; ++mm)
       if (mm == m) { fh[mm] = f; fl[mm] = R(0); }

@@ -332,7 +332,10 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
 // Flux at a face from a loaded stencil window (points p-(S-1) .. p+S of face p):
 // hi + lo is the face flux (lo = 0 in the FP64 form).  FS holds the flux variant flags of a
 // kernel instantiation: bit 0 the component-wise (Rusanov) WENO splitting, bit 1 the thermally
-// perfect gas, bit 2 a central flux with nkeep != 0 (otherwise nkeep = 0 at compile time).
+// perfect gas, bit 2 a central flux with nkeep != 0 (otherwise nkeep = 0 at compile time), bit 3
+// the WENO-Z weights (otherwise WENO-JS).  Options fixed per kernel instantiation keep the code
+// of the branches a case does not take out of the register allocation of the ones it does
+// (measured: nkeep 10-18 %, the WENO version 3-10 % of the flux passes).
 template <class R, int DIR, int LB, int WS, int S, int FS = 0>
 __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& st, bool ishk, int p,
                                             R (&hi)[5], R (&lo)[5], R* __restrict__ gs, int gstride) {
@@ -345,9 +348,9 @@ __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& 
   } else {
     const int ord = max(WS + ep, 1);
     if constexpr ((FS & 1) != 0)
-      rusanov_flux<R, DIR, WS, S, (FS & 2) != 0>(g, st, ord, hi, lo);
+      rusanov_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo);
     else
-      weno_flux<R, DIR, WS, S, (FS & 2) != 0>(g, st, ord, hi, lo, gs, gstride);
+      weno_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo, gs, gstride);
   }
 }
 
@@ -1317,10 +1320,17 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   return cudaGetLastError();
 }
 
-// nkeep = 0 (the default) with the central flux specialised at compile time, else the general form
+// nkeep = 0 (the default) with the central flux specialised at compile time, else the general
+// form; WENO-JS or, for the WENO5 scheme, WENO-Z
 template <class R, int LB, int WS, int FS>
 static cudaError_t stage_kg(const Geom& g, DevState& d, const StageArgs& a, double* fl_prev, double* fl_new,
                             cudaStream_t s, long long* nl) {
+  if constexpr (WS == 3) {
+    if (g.weno_version == 1) {
+      if (g.nkeep != 0) return stage_impl<R, LB, WS, FS | 4 | 8>(g, d, a, fl_prev, fl_new, s, nl);
+      return stage_impl<R, LB, WS, FS | 8>(g, d, a, fl_prev, fl_new, s, nl);
+    }
+  }
   if (g.nkeep != 0) return stage_impl<R, LB, WS, FS | 4>(g, d, a, fl_prev, fl_new, s, nl);
   return stage_impl<R, LB, WS, FS>(g, d, a, fl_prev, fl_new, s, nl);
 }
