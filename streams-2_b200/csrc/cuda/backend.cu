@@ -72,7 +72,7 @@ long long footprint(const streams_b200_params* p) {
   const long long fb = p->precision == 1 ? 4 : 8;  // bytes of the flux-input fields
   long long b = 0;
   b += nvol * 5 * 8;   // w
-  b += nvol * 7 * fb;  // aux
+  b += nvol * (p->precision == 1 ? 7 : 8) * fb;  // aux (+ the sound speed in the FP64 form)
   if (p->precision == 1) b += nvol * 3 * 8;  // FP64 velocities for the stage-3 sensor
   b += nint * fb;      // div3
   b += nint * 2 * 8;   // sensor, sensor_next
@@ -338,7 +338,7 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
         (e = dev_alloc(c, &d.vel64, g.nvol * 3)))
       return fail(e, "cudaMalloc(state)");
   } else {
-    if ((e = dev_alloc(c, &d.aux, g.nvol * 7)) || (e = dev_alloc(c, &d.div3, g.nint)))
+    if ((e = dev_alloc(c, &d.aux, g.nvol * 8)) || (e = dev_alloc(c, &d.div3, g.nint)))
       return fail(e, "cudaMalloc(state)");
   }
   if ((e = dev_alloc(c, &d.sensor, g.nint)) || (e = dev_alloc(c, &d.sensor_next, g.nint)))
@@ -370,7 +370,7 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
   const size_t fb = mixed ? 4 : 8;
   void* auxp = mixed ? (void*)d.auxf : (void*)d.aux;
   void* dv = mixed ? (void*)d.div3f : (void*)d.div3;
-  if ((e = cudaMemsetAsync(d.w, 0, g.nvol * 5 * 8, c->stream)) || (e = cudaMemsetAsync(auxp, 0, g.nvol * 7 * fb, c->stream)) ||
+  if ((e = cudaMemsetAsync(d.w, 0, g.nvol * 5 * 8, c->stream)) || (e = cudaMemsetAsync(auxp, 0, g.nvol * (mixed ? 7 : 8) * fb, c->stream)) ||
       (e = cudaMemsetAsync(d.sensor, 0, g.nint * 8, c->stream)) ||
       (e = cudaMemsetAsync(d.sensor_next, 0, g.nint * 8, c->stream)) ||
       (e = cudaMemsetAsync(dv, 0, g.nint * fb, c->stream)) || (e = cudaMemsetAsync(c->fl_a, 0, g.nint * 40, c->stream)) ||

@@ -333,7 +333,8 @@ __device__ __forceinline__ void central_flux(const Geom& g, const Stencil<R, S>&
 // WZ: WENO-Z weights (weno_version = 1) instead of WENO-JS, fixed at compile time.
 template <class R, int DIR, int WS, int S, bool TP = false, bool WZ = false>
 __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5],
-                                          R (&fl)[5], R* __restrict__ gs, int gstride) {
+                                          R (&fl)[5], R* __restrict__ gs, int gstride, const R* __restrict__ cpt,
+                                          long long cstr) {
   static_assert(!TP || sizeof(R) == sizeof(double), "the thermally perfect gas is an FP64 path");
   const R rgas0 = R(g.rgas0);
   const int o0 = S - 1, o1 = S;  // the two points adjacent to the face
@@ -382,8 +383,13 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
     static_assert(!TP, "the cached sound speed assumes a calorically perfect gas");
     const R cs = st.c[q];
 #else
-    const R gq = TP ? R(gamloc_of_t(g, double(st.t[q]))) : R(g.gamloc);
-    const R cs = sqrt(gq * R(g.rgas0) * st.t[q]);
+    R cs;
+    if constexpr (sizeof(R) == sizeof(double)) {
+      cs = __ldg(cpt + q * cstr);  // the aux pass's sound speed of the point (FP64 form)
+    } else {
+      const R gq = TP ? R(gamloc_of_t(g, double(st.t[q]))) : R(g.gamloc);
+      cs = sqrt(gq * R(g.rgas0) * st.t[q]);
+    }
 #endif
     ev0 = fmax(fabs(vnq - cs), ev0);
     ev1 = fmax(fabs(vnq), ev1);
@@ -479,7 +485,8 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
 // (kernels_cpu.F90:692-941 for x, same in y and z): stencil maximum of |u_n -+ c|, split
 // values of the conserved fluxes, wenorec with the scales of wenorec_1d_rusanov (:2325-2523).
 template <class R, int DIR, int WS, int S, bool TP = false, bool WZ = false>
-__device__ __forceinline__ void rusanov_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5], R (&fl)[5]) {
+__device__ __forceinline__ void rusanov_flux(const Geom& g, const Stencil<R, S>& st, int ord, R (&fh)[5], R (&fl)[5],
+                                             const R* __restrict__ cpt, long long cstr) {
   static_assert(!TP || sizeof(R) == sizeof(double), "the thermally perfect gas is an FP64 path");
   const R rgas0 = R(g.rgas0);
   R evmax = R(-1);
@@ -487,8 +494,13 @@ __device__ __forceinline__ void rusanov_flux(const Geom& g, const Stencil<R, S>&
   for (int l = 0; l < 2 * WS; ++l) {
     const int q = l + S - WS;
     const R un = DIR == 0 ? st.u[q] : (DIR == 1 ? st.v[q] : st.w[q]);
-    const R gq = TP ? R(gamloc_of_t(g, double(st.t[q]))) : R(g.gamloc);
-    const R c = sqrt(gq * rgas0 * st.t[q]);
+    R c;
+    if constexpr (sizeof(R) == sizeof(double)) {
+      c = __ldg(cpt + q * cstr);
+    } else {
+      const R gq = TP ? R(gamloc_of_t(g, double(st.t[q]))) : R(g.gamloc);
+      c = sqrt(gq * rgas0 * st.t[q]);
+    }
     const R evm = fmax(fabs(un - c), fabs(un + c));
     evmax = fmax(evm, evmax);
   }

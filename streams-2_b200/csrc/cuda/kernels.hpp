@@ -34,7 +34,7 @@ struct Prof {
 struct DevState {
   double* w = nullptr;        // ghosted, 5 variables
   // FP64 form
-  double* aux = nullptr;      // ghosted, 7 variables: rho, u, v, w, H, T, mu
+  double* aux = nullptr;      // ghosted, 8 variables: rho, u, v, w, H, T, mu, sound speed
   double* sensor = nullptr;   // interior: Ducros theta used by the fluxes (both forms)
   double* sensor_next = nullptr;
   double* div3 = nullptr;     // interior: div/3

@@ -174,6 +174,12 @@ __global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, 
   aux[4 * n + dst] = A((rhoe + pp) / rho);
   aux[5 * n + dst] = A(tt);
   aux[6 * n + dst] = A(viscosity(g, tt));
+  // FP64 form: the sound speed, which the WENO eigenvalue bound of every face reads at its
+  // stencil points (the same expression the flux would form)
+  if constexpr (sizeof(A) == sizeof(double)) {
+    const double gq = TP ? gamloc_of_t(g, tt) : g.gamloc;
+    aux[7 * n + dst] = sqrt(gq * g.rgas0 * tt);
+  }
 }
 
 // Ducros sensor in FP64 from w for the mixed form, so that the central/WENO switch is taken
@@ -338,7 +344,8 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
 // (measured: nkeep 10-18 %, the WENO version 3-10 % of the flux passes).
 template <class R, int DIR, int LB, int WS, int S, int FS = 0>
 __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& st, bool ishk, int p,
-                                            R (&hi)[5], R (&lo)[5], R* __restrict__ gs, int gstride) {
+                                            R (&hi)[5], R (&lo)[5], R* __restrict__ gs, int gstride,
+                                            const R* __restrict__ cpt, long long cstr) {
   const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
   const int ep = face_ep<DIR>(g, p);
   if (!ishk) {
@@ -348,9 +355,9 @@ __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& 
   } else {
     const int ord = max(WS + ep, 1);
     if constexpr ((FS & 1) != 0)
-      rusanov_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo);
+      rusanov_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo, cpt, cstr);
     else
-      weno_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo, gs, gstride);
+      weno_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo, gs, gstride, cpt, cstr);
   }
 }
 
@@ -401,7 +408,10 @@ __global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F)
     const long long base = gidx(g, p, j, k);
 #pragma unroll
     for (int q = 0; q < 2 * S; ++q) load_point<R, S>(g, st, q, aux, g.nvol, base + (q - (S - 1)));
-    window_flux<R, 0, LB, WS, S, FS>(g, st, ishk, p, fh, fo, weno_scratch<R>() + threadIdx.y * XF_TX + lane, XF_NT);
+    // the FP64 form's aux holds the sound speed of every point (field 8): stencil point 0 onwards
+    const R* cpt = sizeof(R) == sizeof(double) ? aux + 7 * g.nvol + base - (S - 1) : nullptr;
+    window_flux<R, 0, LB, WS, S, FS>(g, st, ishk, p, fh, fo, weno_scratch<R>() + threadIdx.y * XF_TX + lane, XF_NT,
+                                     cpt, 1);
   }
   R hu[5], lu[5];
 #pragma unroll
@@ -484,7 +494,9 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
       load_point<R, S>(g, st, NP - 1, aux, n, base0 + (long long)(c + S) * sd);
       mask = (mask >> 1) | (sensor_bit(c + WS) << (2 * WS - 1));
       R hhi[5], lhi[5];
-      window_flux<R, DIR, LB, WS, S, FS>(g, st, mask != 0u, c, hhi, lhi, weno_scratch<R>() + threadIdx.x, MT_NT);
+      const R* cpt = sizeof(R) == sizeof(double) ? aux + 7 * n + base0 + (long long)(c - (S - 1)) * sd : nullptr;
+      window_flux<R, DIR, LB, WS, S, FS>(g, st, mask != 0u, c, hhi, lhi, weno_scratch<R>() + threadIdx.x, MT_NT, cpt,
+                                         sd);
       if (c >= c0) {
         // cell c lies between the faces c-1 (lo) and c (hi)
         const long long ic = DIR == 1 ? iidx(g, i, c, b) : iidx(g, i, b, c);
