@@ -280,6 +280,21 @@ int streams_b200_set_tuning(streams_b200_ctx* ctx, long long march_threads, int 
 int streams_b200_get_tuning(streams_b200_ctx* ctx, long long* march_threads, int* march_minseg);
 
 /*
+ * Where the WENO faces of the hybrid scheme are computed (no counterpart in the reference, whose
+ * euler kernels evaluate the WENO branch in place).  At the first stage of each step the faces
+ * of each direction whose stencil sees the Ducros sensor are listed on the device; when a
+ * direction's list holds at most max_fraction of its faces, their fluxes are computed apart by
+ * a kernel of their own and the direction's hybrid pass reads them from a face buffer, otherwise
+ * the hybrid pass computes them itself.  The choice is made on the device per direction and
+ * step (no host synchronisation).  Default 0.55; 0 keeps every WENO face in the hybrid passes,
+ * 1 always computes them apart.  Both forms evaluate the same arithmetic: FP64 results are
+ * identical up to the compiler's contraction of the WENO arithmetic in the two kernels
+ * (observed: bit-identical, or differences of a few ulp).
+ */
+int streams_b200_set_weno_split(streams_b200_ctx* ctx, double max_fraction);
+int streams_b200_get_weno_split(streams_b200_ctx* ctx, double* max_fraction);
+
+/*
  * Batched form: many independent contexts (boxes of any size and flow parameters, one device,
  * one precision each) advanced together.  The per-box step sequences (compute_dt + rk_sync)
  * are captured once into one CUDA graph whose branches, one per box, run concurrently on the

@@ -2,6 +2,7 @@
 // points declared in include/streams_b200.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -78,12 +79,19 @@ long long footprint(const streams_b200_params* p) {
   b += nint * 2 * 8;   // sensor, sensor_next
   b += nint * 10 * 8;  // two RK registers
   b += (long long)p->nx * p->nz * 3 * 8;
+  // WENO faces apart: the largest direction's face buffer (40 B per face), the three lists and
+  // the ghosted sensor flags (1 B per point)
+  const long long nfx = (p->nx + 1LL) * p->ny * p->nz, nfy = (long long)p->nx * (p->ny + 1LL) * p->nz,
+                  nfz = (long long)p->nx * p->ny * (p->nz + 1LL);
+  b += 40 * std::max(nfx, std::max(nfy, nfz)) + 4 * (nfx + nfy + nfz) + 16 + nvol;
   b += ((nint + 255) / 256) * 9 * 8 + ((p->nx + 31) / 32) * ((p->nz + 7) / 8) * (long long)p->ny * 5 * 8;
   return b + 4096;
 }
 
 std::string validate(const streams_b200_params* p) {
   if (p->nx < 1 || p->ny < 1 || p->nz < 1) return "grid sizes must be positive";
+  // the launch grids carry y lines (ny + 1 faces) and z lines in their y and z dimensions
+  if (p->ny >= 65535 || p->nz >= 65535) return "ny and nz must be below 65535";
   if (p->ep_order < 2 || p->ep_order > 8 || p->ep_order % 2) return "ep_order must be 2, 4, 6 or 8";
   const int lmax = p->ep_order / 2;
   if (p->weno_scheme < 1 || p->weno_scheme > 4) return "weno_scheme must be 1..4";
@@ -140,6 +148,18 @@ std::string validate(const streams_b200_params* p) {
   return "";
 }
 
+// Largest WENO face fraction of a direction at which its hybrid pass reads the WENO faces from
+// the face buffer: measured on the 1024x256x192 boundary layer, the split form is ahead below a
+// fraction of about 0.55 (FP64: 85.2 vs 87.0 ms per step at 0.51, 89.0 vs 87.3 at 0.61; 61.9 vs
+// 78.1 at 0.06) and behind above it (99.8 vs 86.8 at 0.90).
+constexpr double WENO_SPLIT_FRAC_DEFAULT = 0.55;
+
+void set_weno_split(Geom& g, double frac) {
+  const double nf[3] = {(g.nx + 1.0) * g.ny * g.nz, g.nx * (g.ny + 1.0) * g.nz, g.nx * (double)g.ny * (g.nz + 1.0)};
+  g.weno_split_frac = frac;
+  for (int d = 0; d < 3; ++d) g.wthr[d] = (unsigned)std::min(std::floor(frac * nf[d]), 4294967295.0);
+}
+
 void fill_geom(streams_b200_ctx* c) {
   const streams_b200_params& p = c->p;
   Geom& g = c->g;
@@ -189,6 +209,7 @@ void fill_geom(streams_b200_ctx* c) {
   g.flux_splitting = p.flux_splitting;
   g.march_threads = 148LL * 1024;
   g.march_minseg = 16;
+  set_weno_split(g, WENO_SPLIT_FRAC_DEFAULT);
 }
 
 }  // namespace
@@ -329,6 +350,29 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
     g.yplus_inflow = yi + (ng - 1); g.eta_inflow = ei + (ng - 1);
     g.yplus_recyc = yr + (ng - 1); g.eta_recyc = er + (ng - 1);
     g.weta_inflow = we - 1; g.map_j_inn = mi - 1; g.map_j_out = mo - 1;
+  }
+  // WENO faces apart: the face buffer (planes of the largest direction's face count) and the lists
+  {
+    const long long nfx = (p->nx + 1LL) * p->ny * p->nz, nfy = (long long)p->nx * (p->ny + 1LL) * p->nz,
+                    nfz = (long long)p->nx * p->ny * (p->nz + 1LL);
+    const long long nfmax = std::max(nfx, std::max(nfy, nfz));
+    if (nfmax >= (1LL << 32)) {
+      streams_b200_destroy(c);
+      return set_err(nullptr, STREAMS_B200_EINVAL, "more than 2^32 faces in one direction");
+    }
+    double* wf;
+    unsigned* wl;
+    unsigned char* wb;
+    if ((e = dev_alloc(c, &wf, 5 * nfmax)) || (e = dev_alloc(c, &wl, nfx + nfy + nfz + 4)) ||
+        (e = dev_alloc(c, &wb, g.nvol)))
+      return fail(e, "cudaMalloc(weno faces)");
+    g.wbits = wb;
+    g.wface = wf;
+    g.nwface = nfmax;  // plane stride: 5 planes of doubles, or 10 planes of floats in the same bytes
+    g.wlist[0] = wl;
+    g.wlist[1] = wl + nfx;
+    g.wlist[2] = wl + nfx + nfy;
+    g.wcount = wl + nfx + nfy + nfz;
   }
   // state
   DevState& d = c->d;
@@ -758,6 +802,20 @@ int streams_b200_get_tuning(streams_b200_ctx* c, long long* march_threads, int* 
   return STREAMS_B200_OK;
 }
 
+int streams_b200_set_weno_split(streams_b200_ctx* c, double max_fraction) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  if (!(max_fraction >= 0.0 && max_fraction <= 1.0))
+    return set_err(c, STREAMS_B200_EINVAL, "max_fraction must be in [0, 1]");
+  set_weno_split(c->g, max_fraction);
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_get_weno_split(streams_b200_ctx* c, double* max_fraction) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  if (max_fraction) *max_fraction = c->g.weno_split_frac;
+  return STREAMS_B200_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------------------
@@ -768,6 +826,7 @@ struct streams_b200_batch {
   std::vector<long long> launches_per_replay;  // per box
   std::vector<long long> tuned_threads;        // per box tuning the graph was captured with
   std::vector<int> tuned_minseg;
+  std::vector<double> tuned_wsplit;
   int steps_per_graph = 1, dt_every = 1;
   long long step = 0;  // batch steps taken (drives the dt recompute pattern)
   long long replays = 0;
@@ -835,6 +894,7 @@ int capture(streams_b200_batch* b) {
     c->launches = l0;
     b->tuned_threads[i] = c->g.march_threads;
     b->tuned_minseg[i] = c->g.march_minseg;
+    b->tuned_wsplit[i] = c->g.weno_split_frac;
   }
   cudaGraph_t gr = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(b->master, &gr);
@@ -884,6 +944,7 @@ int streams_b200_batch_create(streams_b200_ctx** ctxs, int n, int steps_per_grap
   b->launches_per_replay.assign(n, 0);
   b->tuned_threads.assign(n, 0);
   b->tuned_minseg.assign(n, 0);
+  b->tuned_wsplit.assign(n, -1.0);
   b->ev_box.assign(n, nullptr);
   b->steps_per_graph = steps_per_graph;
   b->dt_every = dt_every;
@@ -925,7 +986,8 @@ int streams_b200_batch_advance(streams_b200_batch* b, int nsteps) {
   const int nrep = nsteps / b->steps_per_graph;
   if (nrep > 0) {
     for (size_t i = 0; i < b->ctxs.size() && b->exec; ++i)
-      if (b->ctxs[i]->g.march_threads != b->tuned_threads[i] || b->ctxs[i]->g.march_minseg != b->tuned_minseg[i])
+      if (b->ctxs[i]->g.march_threads != b->tuned_threads[i] || b->ctxs[i]->g.march_minseg != b->tuned_minseg[i] ||
+          b->ctxs[i]->g.weno_split_frac != b->tuned_wsplit[i])
         drop_graph(b);  // a box was re-tuned since the capture
     if (!b->exec) {
       rc = capture(b);

@@ -84,6 +84,19 @@ struct Geom {
   double volchan, t_bulk_target;
   // arithmetic of the flux and viscous passes: 0 FP64, 1 mixed (FP32 fluxes, FP64 state)
   int precision;
+  // WENO faces computed apart from the hybrid passes: per direction the list of the faces whose
+  // stencil sees the sensor (rebuilt at stage 1, the sensor being fixed for a step) and one face
+  // buffer of their fluxes (planes of nwface values: 5 in FP64, 5 high + 5 low parts in FP32)
+  void* wface;
+  long long nwface;
+  unsigned int* wlist[3];
+  unsigned int* wcount;  // [3]
+  // ghosted flags sensor > threshold of the step (periodic ghosts copied, other ghosts 0)
+  unsigned char* wbits;
+  // a direction's hybrid pass reads the buffer when its list holds at most wthr[d] faces and
+  // computes its WENO faces itself otherwise (wthr = weno_split_frac x the direction's faces)
+  unsigned int wthr[3];
+  double weno_split_frac;  // host side
   // launch shape of the y/z march passes (host side only): the lines are cut into segments so
   // that about march_threads threads run, each segment at least march_minseg cells long
   long long march_threads;

@@ -13,7 +13,7 @@ namespace sb200 {
 enum KernelId {
   K_AUX = 0, K_EULER_X, K_VISC, K_EULER_Y, K_EULER_Z, K_FINISH_RHS, K_UPDATE, K_FINISH_UPD, K_DT, K_DT_FINISH,
   K_INIT_SENSOR, K_APPLY_SHIFT, K_FILL_GHOSTS, K_COUNT_WENO, K_ADD_TIME, K_BC_FILL, K_BC_NR, K_RAND_PLANE,
-  K_STATS, K_STATS3D, K_NUM
+  K_STATS, K_STATS3D, K_WENO_LIST, K_WENO_FACES, K_NUM
 };
 const char* kernel_name(int kid);
 

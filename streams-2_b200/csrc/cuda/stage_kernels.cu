@@ -20,6 +20,7 @@
 // the mixed form, where w, the RK registers fl, the temperature recovery from the total energy,
 // the Ducros sensor, the time step and all reductions stay FP64 and the face fluxes are carried
 // as float-float pairs whose differences are formed in FP64.
+#include <algorithm>
 #include <cfloat>
 
 #include "flux.cuh"
@@ -335,6 +336,58 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
   return DIR == 0 ? g.epx[p] : (DIR == 1 ? g.epy[p] : g.epz[p]);
 }
 
+// WENO faces apart (1) or always inside the hybrid passes (0).  Apart, the faces whose stencil
+// sees the sensor are listed per direction once per step and computed by their own kernel at
+// full occupancy; the hybrid passes read their fluxes from a face buffer.  A warp of the hybrid
+// passes otherwise runs both branches whenever one of its faces is a WENO face, which with
+// scattered WENO faces costs nearly a full WENO pass.  When most faces are WENO faces the
+// buffer's extra traffic and the stencil loads without the passes' sliding window cost more
+// than that, so each direction chooses on the device from its list's length (weno_split), the
+// hybrid passes holding both branches.
+#ifndef SB_WENO_SPLIT
+#define SB_WENO_SPLIT 1
+#endif
+
+// Face index of the WENO face buffer of direction DIR for face p (0..n along DIR) of the line
+// (a, b): x faces p fastest (a = j, b = k), y and z faces i fastest (a = i; b = k for y, j for z).
+template <int DIR>
+__host__ __device__ __forceinline__ long long wface_index(const Geom& g, int p, int a, int b) {
+  if (DIR == 0) return ((long long)(b - 1) * g.ny + (a - 1)) * (g.nx + 1) + p;
+  if (DIR == 1) return ((long long)(b - 1) * (g.ny + 1) + p) * g.nx + (a - 1);
+  return ((long long)p * g.ny + (b - 1)) * g.nx + (a - 1);
+}
+template <int DIR>
+__device__ __forceinline__ void wface_decode(const Geom& g, unsigned f, int& p, int& a, int& b) {
+  // face counts per direction stay below 2^32 (checked at context creation)
+  if (DIR == 0) {
+    const unsigned n0 = g.nx + 1, r = f / n0;
+    p = (int)(f - r * n0);
+    a = (int)(r % (unsigned)g.ny) + 1;
+    b = (int)(r / (unsigned)g.ny) + 1;
+  } else if (DIR == 1) {
+    const unsigned r = f / (unsigned)g.nx;
+    a = (int)(f - r * (unsigned)g.nx) + 1;
+    p = (int)(r % (unsigned)(g.ny + 1));
+    b = (int)(r / (unsigned)(g.ny + 1)) + 1;
+  } else {
+    const unsigned r = f / (unsigned)g.nx;
+    a = (int)(f - r * (unsigned)g.nx) + 1;
+    b = (int)(r % (unsigned)g.ny) + 1;
+    p = (int)(r / (unsigned)g.ny);
+  }
+}
+// Whether the hybrid pass of direction DIR reads its WENO faces from the face buffer this step
+// (the list, built at stage 1, holds at most wthr[DIR] faces) or computes them itself.
+template <int DIR>
+__device__ __forceinline__ bool weno_split(const Geom& g) {
+  return SB_WENO_SPLIT && *(volatile const unsigned*)(g.wcount + DIR) <= g.wthr[DIR];
+}
+template <int DIR>
+__host__ __device__ __forceinline__ long long wface_count(const Geom& g) {
+  return DIR == 0 ? (long long)(g.nx + 1) * g.ny * g.nz
+                  : (DIR == 1 ? (long long)g.nx * (g.ny + 1) * g.nz : (long long)g.nx * g.ny * (g.nz + 1));
+}
+
 // Flux at a face from a loaded stencil window (points p-(S-1) .. p+S of face p):
 // hi + lo is the face flux (lo = 0 in the FP64 form).  FS holds the flux variant flags of a
 // kernel instantiation: bit 0 the component-wise (Rusanov) WENO splitting, bit 1 the thermally
@@ -342,22 +395,40 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
 // the WENO-Z weights (otherwise WENO-JS).  Options fixed per kernel instantiation keep the code
 // of the branches a case does not take out of the register allocation of the ones it does
 // (measured: nkeep 10-18 %, the WENO version 3-10 % of the flux passes).
+// The WENO flux of face p (characteristic or component-wise splitting), order reduced near
+// non-periodic boundaries as ep_ord_change says.
+template <class R, int DIR, int LB, int WS, int S, int FS = 0>
+__device__ __forceinline__ void weno_face(const Geom& g, const Stencil<R, S>& st, int p, R (&hi)[5], R (&lo)[5],
+                                          R* __restrict__ gs, int gstride, const R* __restrict__ cpt, long long cstr) {
+  const int ep = face_ep<DIR>(g, p);
+  const int ord = max(WS + ep, 1);
+  if constexpr ((FS & 1) != 0)
+    rusanov_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo, cpt, cstr);
+  else
+    weno_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo, gs, gstride, cpt, cstr);
+}
+
 template <class R, int DIR, int LB, int WS, int S, int FS = 0>
 __device__ __forceinline__ void window_flux(const Geom& g, const Stencil<R, S>& st, bool ishk, int p,
                                             R (&hi)[5], R (&lo)[5], R* __restrict__ gs, int gstride,
-                                            const R* __restrict__ cpt, long long cstr) {
+                                            const R* __restrict__ cpt, long long cstr, bool split, int wa, int wb) {
   const int nd = DIR == 0 ? g.nx : (DIR == 1 ? g.ny : g.nz);
-  const int ep = face_ep<DIR>(g, p);
   if (!ishk) {
+    const int ep = face_ep<DIR>(g, p);
     const int lmax = max(g.lmax_base + ep, 1);
     const bool zf = (p == 0 && g.fzf[2 * DIR] == 1) || (p == nd && g.fzf[2 * DIR + 1] == 1);
     central_flux<R, DIR, LB, S, (FS & 4) != 0>(g, st, lmax, g.nkeep, zf, hi, lo);
+  } else if (SB_WENO_SPLIT && split) {
+    // the WENO faces come from the face buffer
+    const R* fb = static_cast<const R*>(g.wface);
+    const long long wf = wface_index<DIR>(g, p, wa, wb);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      hi[m] = __ldg(fb + m * g.nwface + wf);
+      lo[m] = sizeof(R) == sizeof(double) ? R(0) : __ldg(fb + (5 + m) * g.nwface + wf);
+    }
   } else {
-    const int ord = max(WS + ep, 1);
-    if constexpr ((FS & 1) != 0)
-      rusanov_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo, cpt, cstr);
-    else
-      weno_flux<R, DIR, WS, S, (FS & 2) != 0, (FS & 8) != 0>(g, st, ord, hi, lo, gs, gstride, cpt, cstr);
+    weno_face<R, DIR, LB, WS, S, FS>(g, st, p, hi, lo, gs, gstride, cpt, cstr);
   }
 }
 
@@ -411,7 +482,7 @@ __global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F)
     // the FP64 form's aux holds the sound speed of every point (field 8): stencil point 0 onwards
     const R* cpt = sizeof(R) == sizeof(double) ? aux + 7 * g.nvol + base - (S - 1) : nullptr;
     window_flux<R, 0, LB, WS, S, FS>(g, st, ishk, p, fh, fo, weno_scratch<R>() + threadIdx.y * XF_TX + lane, XF_NT,
-                                     cpt, 1);
+                                     cpt, 1, weno_split<0>(g), j, k);
   }
   R hu[5], lu[5];
 #pragma unroll
@@ -435,7 +506,7 @@ __global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F)
 // point loaded per face), computes every face of the segment once and adds the divergence to fl.
 // The z pass also applies the grad(mu div/3) term of visflx_div_ord2_subroutine
 // (kernels_cpu.F90:3446-3480) and emits the force_rhs block partials (:3157-3193).
-template <class R, int DIR, int LB, int WS, bool CH = false, int FS = 0>
+template <class R, int DIR, int LB, int WS, bool CH = false, int FS = 0, bool SPLIT = false>
 __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F) k_march(Geom g, const R* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl,
                                                  const R* __restrict__ div3,
@@ -453,6 +524,8 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
   const int emax = DIR == 1 ? g.eul_jmax : g.eul_kmax;
   const long long nlines = (long long)n1 * n2;
   const long long t = (long long)blockIdx.x * MT_NT + threadIdx.x;
+  // both forms are launched; the one that the list length does not select leaves at once
+  if (weno_split<DIR>(g) != SPLIT) return;
   double part[5] = {0, 0, 0, 0, 0};
   if (t < nlines * nseg) {
     const int i = (int)(t % n1) + 1;
@@ -496,7 +569,7 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
       R hhi[5], lhi[5];
       const R* cpt = sizeof(R) == sizeof(double) ? aux + 7 * n + base0 + (long long)(c - (S - 1)) * sd : nullptr;
       window_flux<R, DIR, LB, WS, S, FS>(g, st, mask != 0u, c, hhi, lhi, weno_scratch<R>() + threadIdx.x, MT_NT, cpt,
-                                         sd);
+                                         sd, SPLIT, i, b);
       if (c >= c0) {
         // cell c lies between the faces c-1 (lo) and c (hi)
         const long long ic = DIR == 1 ? iidx(g, i, c, b) : iidx(g, i, b, c);
@@ -1078,6 +1151,95 @@ __global__ void __launch_bounds__(256) k_count_weno(Geom g, const double* __rest
     for (int r = 0; r < 3; ++r) red[(long long)blockIdx.x * 3 + r] = v[r];
 }
 
+// The sensor flags of a step on the ghosted grid: sensor > threshold at interior points, the
+// periodic image at the ghosts of periodic directions and 0 at the others (sensor_at).
+__global__ void __launch_bounds__(256) k_weno_bits(Geom g, const double* __restrict__ sensor) {
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31) + 1 - g.ng;
+  const int j = blockIdx.y * 8 + (threadIdx.x >> 5) + 1 - g.ng;
+  const int k = blockIdx.z + 1 - g.ng;
+  if (i > g.nx + g.ng || j > g.ny + g.ng) return;
+  g.wbits[gidx(g, i, j, k)] = sensor_at(g, sensor, i, j, k) > g.sensor_threshold ? 1 : 0;
+}
+
+// The WENO faces of direction DIR: the faces the hybrid pass computes (eul range) whose stencil
+// sees a sensor flag, appended to the direction's list.  A block covers 32 consecutive faces
+// along the fastest index of the face numbering (x faces: p; y and z faces: i) times 8 along the
+// second, the grid's z the third, so no index is decoded; one atomic per block reserves its
+// entries (the order of the list does not matter, every entry is computed independently).
+constexpr int WL_NT = 256;
+template <int DIR, int WS>
+__global__ void __launch_bounds__(WL_NT) k_weno_list(Geom g) {
+  __shared__ unsigned wsum[WL_NT / 32];
+  __shared__ unsigned base;
+  const int t0 = blockIdx.x * 32 + (threadIdx.x & 31), t1 = blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int t2 = blockIdx.z;
+  // (p, a, b) as wface_index numbers the faces: x (p, j, k), y (p, i, k), z (p, i, j)
+  const int p = DIR == 0 ? t0 : (DIR == 1 ? t1 : t2);
+  const int a = DIR == 0 ? t1 + 1 : t0 + 1;
+  const int b = DIR == 2 ? t1 + 1 : t2 + 1;
+  const int n0 = DIR == 0 ? g.nx + 1 : g.nx, n1 = DIR == 1 ? g.ny + 1 : g.ny;
+  const int emin = DIR == 0 ? g.eul_imin : (DIR == 1 ? g.eul_jmin : g.eul_kmin);
+  const int emax = DIR == 0 ? g.eul_imax : (DIR == 1 ? g.eul_jmax : g.eul_kmax);
+  bool shk = false;
+  if (t0 < n0 && t1 < n1 && p >= emin - 1 && p <= emax) {
+    // the stencil points p-WS+1 .. p+WS of the face, all inside the ghosted grid (ng >= WS)
+    const long long sd = DIR == 0 ? 1 : (DIR == 1 ? (long long)g.sx : (long long)g.sx * g.sy);
+    const long long c = DIR == 0 ? gidx(g, p, a, b) : (DIR == 1 ? gidx(g, a, p, b) : gidx(g, a, b, p));
+    const unsigned char* f = g.wbits + c;
+    unsigned any = 0;
+#pragma unroll
+    for (int o = -WS + 1; o <= WS; ++o) any |= f[o * sd];
+    shk = any != 0;
+  }
+  const unsigned bal = __ballot_sync(0xffffffffu, shk);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) wsum[wid] = (unsigned)__popc(bal);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned tot = 0;
+#pragma unroll
+    for (int q = 0; q < WL_NT / 32; ++q) {
+      const unsigned cq = wsum[q];
+      wsum[q] = tot;
+      tot += cq;
+    }
+    base = tot ? atomicAdd(&g.wcount[DIR], tot) : 0u;
+  }
+  __syncthreads();
+  if (shk)
+    g.wlist[DIR][base + wsum[wid] + (unsigned)__popc(bal & ((1u << lane) - 1u))] = (unsigned)wface_index<DIR>(g, p, a, b);
+}
+
+// The fluxes of the listed WENO faces of direction DIR into the face buffer (grid-stride over the
+// list; each thread loads its face's stencil as the hybrid pass would hold it).
+constexpr int WF_NT = 128;
+template <class R, int DIR, int LB, int WS, int FS>
+__global__ void __launch_bounds__(WF_NT) k_weno_faces(Geom g, const R* __restrict__ aux) {
+  constexpr int S = LB > WS ? LB : WS;
+  const unsigned cnt = g.wcount[DIR];
+  if (cnt > g.wthr[DIR]) return;  // the hybrid pass computes the WENO faces itself
+  const long long n = g.nvol;
+  const long long sd = DIR == 0 ? 1 : (DIR == 1 ? (long long)g.sx : (long long)g.sx * g.sy);
+  R* fb = static_cast<R*>(g.wface);
+  for (unsigned e = blockIdx.x * WF_NT + threadIdx.x; e < cnt; e += gridDim.x * WF_NT) {
+    const unsigned f = g.wlist[DIR][e];
+    int p, a, b;
+    wface_decode<DIR>(g, f, p, a, b);
+    const long long base = DIR == 0 ? gidx(g, p, a, b) : (DIR == 1 ? gidx(g, a, p, b) : gidx(g, a, b, p));
+    Stencil<R, S> st;
+#pragma unroll
+    for (int q = 0; q < 2 * S; ++q) load_point<R, S>(g, st, q, aux, n, base + (q - (S - 1)) * sd);
+    const R* cpt = sizeof(R) == sizeof(double) ? aux + 7 * n + base - (S - 1) * sd : nullptr;
+    R hi[5], lo[5];
+    weno_face<R, DIR, LB, WS, S, FS>(g, st, p, hi, lo, weno_scratch<R>() + threadIdx.x, WF_NT, cpt, sd);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      fb[m * g.nwface + f] = hi[m];
+      if constexpr (sizeof(R) != sizeof(double)) fb[(5 + m) * g.nwface + f] = lo[m];
+    }
+  }
+}
+
 inline unsigned nblocks(long long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
 // Wrap one launch with profiler events when profiling is on.
@@ -1089,7 +1251,8 @@ const char* kernel_name(int kid) {
   static const char* names[K_NUM] = {"k_aux", "k_euler_x", "k_visc", "k_euler_y", "k_euler_z", "k_finish_rhs",
                                      "k_update", "k_finish_upd", "k_dt", "k_dt_finish", "k_init_sensor",
                                      "k_apply_shift", "k_fill_ghosts", "k_count_weno", "k_add_time",
-                                     "k_bc_fill", "k_bc_nr", "k_rand_plane", "k_stats", "k_stats3d"};
+                                     "k_bc_fill", "k_bc_nr", "k_rand_plane", "k_stats", "k_stats3d",
+                                     "k_weno_list", "k_weno_faces"};
   return (kid >= 0 && kid < K_NUM) ? names[kid] : "?";
 }
 
@@ -1270,7 +1433,10 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   // the mixed form's stage-3 sensor is taken in FP64 from velocities that this aux pass stores
   double* vel = (!fp64 && a.istep == 3) ? d.vel64 : nullptr;
   if (a.run_aux) aux_launch<R>(g, d, a.apply_shift, 0, K_AUX, s, nl, vel);
-  const size_t xsm = weno_scratch_bytes<R, WS>(XF_NT), msm = weno_scratch_bytes<R, WS>(MT_NT);
+  // the hybrid passes hold the WENO scratch for the steps at which they compute WENO faces
+  const size_t xsm = weno_scratch_bytes<R, WS>(XF_NT);
+  const size_t msm = weno_scratch_bytes<R, WS>(MT_NT);
+  const size_t wsm = weno_scratch_bytes<R, WS>(WF_NT);
   // per instantiation and device: allow more than 48 KB of dynamic shared memory
   static unsigned long long smem_set = 0;
   int dev = 0;
@@ -1280,7 +1446,31 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
     cudaFuncSetAttribute(k_march<R, 1, LB, WS, false, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
     cudaFuncSetAttribute(k_march<R, 2, LB, WS, false, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
     cudaFuncSetAttribute(k_march<R, 2, LB, WS, true, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+    if (SB_WENO_SPLIT) {
+      cudaFuncSetAttribute(k_weno_faces<R, 0, LB, WS, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+      cudaFuncSetAttribute(k_weno_faces<R, 1, LB, WS, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+      cudaFuncSetAttribute(k_weno_faces<R, 2, LB, WS, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm);
+    }
     smem_set |= 1ULL << dev;
+  }
+  // WENO faces apart: the lists at the first stage of a step (the sensor is fixed for the step),
+  // the face fluxes before each hybrid pass
+  const long long wnf = std::max(wface_count<0>(g), std::max(wface_count<1>(g), wface_count<2>(g)));
+  const unsigned wgrid = (unsigned)std::min<long long>((long long)nblocks(wnf, WF_NT), 148LL * 16);
+  if (SB_WENO_SPLIT && a.istep == 1) {
+    SB_LAUNCH(d, K_WENO_LIST, s, cudaMemsetAsync(g.wcount, 0, 3 * sizeof(unsigned), s));
+    const dim3 gb(nblocks(g.sx, 32), nblocks(g.sy, 8), g.sz);
+    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_bits<<<gb, 256, 0, s>>>(g, sensor));
+    const dim3 gl0(nblocks(g.nx + 1, 32), nblocks(g.ny, 8), g.nz), gl1(nblocks(g.nx, 32), nblocks(g.ny + 1, 8), g.nz),
+        gl2(nblocks(g.nx, 32), nblocks(g.ny, 8), g.nz + 1);
+    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<0, WS><<<gl0, WL_NT, 0, s>>>(g));
+    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<1, WS><<<gl1, WL_NT, 0, s>>>(g));
+    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<2, WS><<<gl2, WL_NT, 0, s>>>(g));
+    *nl += 4;
+  }
+  if (SB_WENO_SPLIT) {
+    SB_LAUNCH(d, K_WENO_FACES, s, k_weno_faces<R, 0, LB, WS, FS><<<wgrid, WF_NT, wsm, s>>>(g, aux));
+    ++*nl;
   }
   SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS, FS><<<xg, xb, xsm, s>>>(g, aux, sensor, fl_new));
   if (g.conservative_viscous)
@@ -1302,19 +1492,44 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
                 k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, sensor_next, g.conservative_viscous ? 1 : 2));
     ++*nl;
   }
-  if (gyb > 0)
+  if (SB_WENO_SPLIT) {
+    SB_LAUNCH(d, K_WENO_FACES, s, k_weno_faces<R, 1, LB, WS, FS><<<wgrid, WF_NT, wsm, s>>>(g, aux));
+    ++*nl;
+  }
+  if (gyb > 0) {
     SB_LAUNCH(d, K_EULER_Y, s,
               k_march<R, 1, LB, WS, false, FS><<<gyb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                           a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
+    if (SB_WENO_SPLIT) {
+      SB_LAUNCH(d, K_EULER_Y, s,
+                k_march<R, 1, LB, WS, false, FS, true><<<gyb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev,
+                                                                   d.sc, a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
+      ++*nl;
+    }
+  }
+  if (SB_WENO_SPLIT) {
+    SB_LAUNCH(d, K_WENO_FACES, s, k_weno_faces<R, 2, LB, WS, FS><<<wgrid, WF_NT, wsm, s>>>(g, aux));
+    ++*nl;
+  }
   // the channel's force_rhs partials are a separate instantiation (fewer registers without them)
-  if (g.channel_case)
+  if (g.channel_case) {
     SB_LAUNCH(d, K_EULER_Z, s,
               k_march<R, 2, LB, WS, true, FS><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                                   a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
-  else
+    if (SB_WENO_SPLIT)
+      SB_LAUNCH(d, K_EULER_Z, s,
+                k_march<R, 2, LB, WS, true, FS, true><<<gzb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev,
+                                                                  d.sc, a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
+  } else {
     SB_LAUNCH(d, K_EULER_Z, s,
               k_march<R, 2, LB, WS, false, FS><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                                    a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
+    if (SB_WENO_SPLIT)
+      SB_LAUNCH(d, K_EULER_Z, s,
+                k_march<R, 2, LB, WS, false, FS, true><<<gzb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev,
+                                                                   d.sc, a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
+  }
+  if (SB_WENO_SPLIT) ++*nl;
   *nl += 4;
   if (g.recyc) launch_rand_plane(g, d, s, nl);  // euler_z draws the inflow plane of the stage
   launch_bc_nr(g, d, fl_new, s, nl);

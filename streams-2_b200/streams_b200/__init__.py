@@ -134,6 +134,8 @@ def _load() -> C.CDLL:
         "streams_b200_case_stats": (I, [P, I, D, LL]),
         "streams_b200_set_tuning": (I, [P, LL, I]),
         "streams_b200_get_tuning": (I, [P, C.POINTER(LL), C.POINTER(I)]),
+        "streams_b200_set_weno_split": (I, [P, C.c_double]),
+        "streams_b200_get_weno_split": (I, [P, D]),
         "streams_b200_batch_create": (I, [C.POINTER(P), I, I, I, C.POINTER(P)]),
         "streams_b200_batch_advance": (I, [P, I]),
         "streams_b200_batch_synchronize": (I, [P]),
@@ -169,7 +171,8 @@ EXPORTED = [
     "streams_b200_run_case_stats", "streams_b200_case_write_state_stats", "streams_b200_case_stats_info",
     "streams_b200_case_stats",
     "streams_b200_set_tuning",
-    "streams_b200_get_tuning", "streams_b200_batch_create", "streams_b200_batch_advance",
+    "streams_b200_get_tuning", "streams_b200_set_weno_split", "streams_b200_get_weno_split",
+    "streams_b200_batch_create", "streams_b200_batch_advance",
     "streams_b200_batch_synchronize", "streams_b200_batch_invalidate", "streams_b200_batch_stats",
     "streams_b200_batch_last_error", "streams_b200_batch_destroy",
 ]
@@ -481,6 +484,17 @@ class Solver:
         t, m = C.c_longlong(), C.c_int()
         self._check(lib.streams_b200_get_tuning(self._h, C.byref(t), C.byref(m)))
         return int(t.value), int(m.value)
+
+    def set_weno_split(self, max_fraction: float) -> None:
+        """Largest WENO face fraction of a direction at which its hybrid pass reads the WENO
+        faces from the face buffer (see streams_b200_set_weno_split): 0 keeps them in the hybrid
+        passes, 1 always computes them apart."""
+        self._check(lib.streams_b200_set_weno_split(self._h, float(max_fraction)))
+
+    def get_weno_split(self) -> float:
+        v = np.zeros(1)
+        self._check(lib.streams_b200_get_weno_split(self._h, _dptr(v)))
+        return float(v[0])
 
 
 class Batch:
