@@ -83,7 +83,7 @@ long long footprint(const streams_b200_params* p) {
   // the ghosted sensor flags (1 B per point)
   const long long nfx = (p->nx + 1LL) * p->ny * p->nz, nfy = (long long)p->nx * (p->ny + 1LL) * p->nz,
                   nfz = (long long)p->nx * p->ny * (p->nz + 1LL);
-  b += 40 * std::max(nfx, std::max(nfy, nfz)) + 4 * (nfx + nfy + nfz) + 16 + nvol;
+  b += 40 * std::max(nfx, std::max(nfy, nfz)) + 4 * (nfx + nfy + nfz) + 32 + nvol;
   b += ((nint + 255) / 256) * 9 * 8 + ((p->nx + 31) / 32) * ((p->nz + 7) / 8) * (long long)p->ny * 5 * 8;
   return b + 4096;
 }
@@ -156,8 +156,15 @@ constexpr double WENO_SPLIT_FRAC_DEFAULT = 0.55;
 
 void set_weno_split(Geom& g, double frac) {
   const double nf[3] = {(g.nx + 1.0) * g.ny * g.nz, g.nx * (g.ny + 1.0) * g.nz, g.nx * (double)g.ny * (g.nz + 1.0)};
+  // the sample: planes 0, WSAMPLE, 2 WSAMPLE, ... of z (x and y faces) or of the z faces
+  const double ns[3] = {(g.nx + 1.0) * g.ny * ((g.nz + WSAMPLE - 1) / WSAMPLE),
+                        g.nx * (g.ny + 1.0) * ((g.nz + WSAMPLE - 1) / WSAMPLE),
+                        g.nx * (double)g.ny * ((g.nz + WSAMPLE) / WSAMPLE)};
   g.weno_split_frac = frac;
-  for (int d = 0; d < 3; ++d) g.wthr[d] = (unsigned)std::min(std::floor(frac * nf[d]), 4294967295.0);
+  for (int d = 0; d < 3; ++d) {
+    g.wthr[d] = (unsigned)std::min(std::floor(frac * nf[d]), 4294967294.0);
+    g.wthr_s[d] = (unsigned)std::min(std::floor(frac * ns[d]), 4294967294.0);
+  }
 }
 
 void fill_geom(streams_b200_ctx* c) {
@@ -363,7 +370,7 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
     double* wf;
     unsigned* wl;
     unsigned char* wb;
-    if ((e = dev_alloc(c, &wf, 5 * nfmax)) || (e = dev_alloc(c, &wl, nfx + nfy + nfz + 4)) ||
+    if ((e = dev_alloc(c, &wf, 5 * nfmax)) || (e = dev_alloc(c, &wl, nfx + nfy + nfz + 8)) ||
         (e = dev_alloc(c, &wb, g.nvol)))
       return fail(e, "cudaMalloc(weno faces)");
     g.wbits = wb;
@@ -372,7 +379,7 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
     g.wlist[0] = wl;
     g.wlist[1] = wl + nfx;
     g.wlist[2] = wl + nfx + nfy;
-    g.wcount = wl + nfx + nfy + nfz;
+    g.wcount = wl + nfx + nfy + nfz;  // [0..2] list lengths, [4..6] sample counts
   }
   // state
   DevState& d = c->d;

@@ -18,6 +18,7 @@ constexpr int NRED_UPD = 8;   // force_var sum rhou*T*dy, residual sum, rho/T/p 
 // running statistics per (i,j) column and per cell (nv_stat, nv_stat_3d of singleideal.F90:474-478)
 constexpr int NV_STAT = 70;
 constexpr int NV_STAT_3D = 14;
+constexpr int WSAMPLE = 16;  // WENO face sample: every 16th plane
 
 struct Geom {
   // block sizes and padded strides (ghosted arrays: index (i,j,k), i in 1-ng..nx+ng)
@@ -96,6 +97,9 @@ struct Geom {
   // a direction's hybrid pass reads the buffer when its list holds at most wthr[d] faces and
   // computes its WENO faces itself otherwise (wthr = weno_split_frac x the direction's faces)
   unsigned int wthr[3];
+  // the lists are built only when a sample of the faces (every WSAMPLE-th plane of the list
+  // kernels' third grid index) holds at most wthr_s[d] WENO faces (wcount[4 + d] on the device)
+  unsigned int wthr_s[3];
   double weno_split_frac;  // host side
   // launch shape of the y/z march passes (host side only): the lines are cut into segments so
   // that about march_threads threads run, each segment at least march_minseg cells long

@@ -342,8 +342,11 @@ __device__ __forceinline__ int face_ep(const Geom& g, int p) {
 // passes otherwise runs both branches whenever one of its faces is a WENO face, which with
 // scattered WENO faces costs nearly a full WENO pass.  When most faces are WENO faces the
 // buffer's extra traffic and the stencil loads without the passes' sliding window cost more
-// than that, so each direction chooses on the device from its list's length (weno_split), the
-// hybrid passes holding both branches.
+// than that, so each direction chooses on the device from its list's length (weno_split): the
+// x pass holds both branches, the y and z passes are launched in both forms and the one not
+// chosen leaves at once (about a thousand blocks; the x pass's grid is too large for that).
+// The lists themselves are built only when a sample of every 16th plane is within the
+// threshold, so a step that keeps its WENO faces in the hybrid passes pays for the sample only.
 #ifndef SB_WENO_SPLIT
 #define SB_WENO_SPLIT 1
 #endif
@@ -1151,63 +1154,132 @@ __global__ void __launch_bounds__(256) k_count_weno(Geom g, const double* __rest
     for (int r = 0; r < 3; ++r) red[(long long)blockIdx.x * 3 + r] = v[r];
 }
 
-// The sensor flags of a step on the ghosted grid: sensor > threshold at interior points, the
-// periodic image at the ghosts of periodic directions and 0 at the others (sensor_at).
-__global__ void __launch_bounds__(256) k_weno_bits(Geom g, const double* __restrict__ sensor) {
-  const int i = blockIdx.x * 32 + (threadIdx.x & 31) + 1 - g.ng;
-  const int j = blockIdx.y * 8 + (threadIdx.x >> 5) + 1 - g.ng;
-  const int k = blockIdx.z + 1 - g.ng;
-  if (i > g.nx + g.ng || j > g.ny + g.ng) return;
-  g.wbits[gidx(g, i, j, k)] = sensor_at(g, sensor, i, j, k) > g.sensor_threshold ? 1 : 0;
+// Face (p, a, b) of direction DIR as wface_index numbers it (x (p, j, k), y (p, i, k), z (p, i, j))
+// from the list kernels' thread coordinates: t0 the fastest index of that numbering (x faces: p;
+// y and z faces: i), t1 the second, t2 the third.
+template <int DIR>
+__device__ __forceinline__ void list_face(int t0, int t1, int t2, int& p, int& a, int& b) {
+  p = DIR == 0 ? t0 : (DIR == 1 ? t1 : t2);
+  a = DIR == 0 ? t1 + 1 : t0 + 1;
+  b = DIR == 2 ? t1 + 1 : t2 + 1;
 }
 
-// The WENO faces of direction DIR: the faces the hybrid pass computes (eul range) whose stencil
-// sees a sensor flag, appended to the direction's list.  A block covers 32 consecutive faces
-// along the fastest index of the face numbering (x faces: p; y and z faces: i) times 8 along the
-// second, the grid's z the third, so no index is decoded; one atomic per block reserves its
-// entries (the order of the list does not matter, every entry is computed independently).
-constexpr int WL_NT = 256;
+// Block-aggregated append: one atomic per block reserves the entries of its faces with shk set
+// (the order of a list does not matter, every entry is computed independently).  Returns the
+// entry of this thread (any value when !shk).  All threads of the block call it; successive
+// calls alternate between the two halves of wsum (2 x warps) and base (2), so that a call
+// needs no barrier after its last read.
+__device__ __forceinline__ unsigned block_append(bool shk, unsigned* counter, unsigned* wsum, unsigned* base,
+                                                 int par) {
+  const int nw = (int)(blockDim.x >> 5);
+  unsigned* ws = wsum + par * nw;
+  const unsigned bal = __ballot_sync(0xffffffffu, shk);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) ws[wid] = (unsigned)__popc(bal);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned tot = 0;
+    for (int q = 0; q < nw; ++q) {
+      const unsigned cq = ws[q];
+      ws[q] = tot;
+      tot += cq;
+    }
+    base[par] = tot ? atomicAdd(counter, tot) : 0u;
+  }
+  __syncthreads();
+  return base[par] + ws[wid] + (unsigned)__popc(bal & ((1u << lane) - 1u));
+}
+
+constexpr int WL_NT = 256;  // list kernels: 32 faces along t0 x 8 along t1
+
+// The sample count of direction DIR: the WENO faces (stencil sees the sensor, eul range) of the
+// planes t2 = 0, WSAMPLE, 2 WSAMPLE, ... read from the sensor itself, into wcount[4 + DIR].
 template <int DIR, int WS>
-__global__ void __launch_bounds__(WL_NT) k_weno_list(Geom g) {
-  __shared__ unsigned wsum[WL_NT / 32];
-  __shared__ unsigned base;
+__global__ void __launch_bounds__(WL_NT) k_weno_sample(Geom g, const double* __restrict__ sensor) {
+  __shared__ unsigned wsum[2 * (WL_NT / 32)];
+  __shared__ unsigned base[2];
   const int t0 = blockIdx.x * 32 + (threadIdx.x & 31), t1 = blockIdx.y * 8 + (threadIdx.x >> 5);
-  const int t2 = blockIdx.z;
-  // (p, a, b) as wface_index numbers the faces: x (p, j, k), y (p, i, k), z (p, i, j)
-  const int p = DIR == 0 ? t0 : (DIR == 1 ? t1 : t2);
-  const int a = DIR == 0 ? t1 + 1 : t0 + 1;
-  const int b = DIR == 2 ? t1 + 1 : t2 + 1;
+  const int t2 = blockIdx.z * WSAMPLE;
+  int p, a, b;
+  list_face<DIR>(t0, t1, t2, p, a, b);
   const int n0 = DIR == 0 ? g.nx + 1 : g.nx, n1 = DIR == 1 ? g.ny + 1 : g.ny;
   const int emin = DIR == 0 ? g.eul_imin : (DIR == 1 ? g.eul_jmin : g.eul_kmin);
   const int emax = DIR == 0 ? g.eul_imax : (DIR == 1 ? g.eul_jmax : g.eul_kmax);
   bool shk = false;
   if (t0 < n0 && t1 < n1 && p >= emin - 1 && p <= emax) {
-    // the stencil points p-WS+1 .. p+WS of the face, all inside the ghosted grid (ng >= WS)
-    const long long sd = DIR == 0 ? 1 : (DIR == 1 ? (long long)g.sx : (long long)g.sx * g.sy);
-    const long long c = DIR == 0 ? gidx(g, p, a, b) : (DIR == 1 ? gidx(g, a, p, b) : gidx(g, a, b, p));
-    const unsigned char* f = g.wbits + c;
-    unsigned any = 0;
 #pragma unroll
-    for (int o = -WS + 1; o <= WS; ++o) any |= f[o * sd];
-    shk = any != 0;
-  }
-  const unsigned bal = __ballot_sync(0xffffffffu, shk);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) wsum[wid] = (unsigned)__popc(bal);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned tot = 0;
-#pragma unroll
-    for (int q = 0; q < WL_NT / 32; ++q) {
-      const unsigned cq = wsum[q];
-      wsum[q] = tot;
-      tot += cq;
+    for (int o = -WS + 1; o <= WS; ++o) {
+      const double th = DIR == 0 ? sensor_at(g, sensor, p + o, a, b)
+                                 : (DIR == 1 ? sensor_at(g, sensor, a, p + o, b) : sensor_at(g, sensor, a, b, p + o));
+      shk = shk || th > g.sensor_threshold;
     }
-    base = tot ? atomicAdd(&g.wcount[DIR], tot) : 0u;
   }
-  __syncthreads();
-  if (shk)
-    g.wlist[DIR][base + wsum[wid] + (unsigned)__popc(bal & ((1u << lane) - 1u))] = (unsigned)wface_index<DIR>(g, p, a, b);
+  block_append(shk, g.wcount + 4 + DIR, wsum, base, 0);
+}
+
+// Whether the lists of direction DIR are built this step (its sample is within the threshold).
+template <int DIR>
+__device__ __forceinline__ bool list_wanted(const Geom& g) {
+  return *(volatile const unsigned*)(g.wcount + 4 + DIR) <= g.wthr_s[DIR];
+}
+
+// The sensor flags of a step on the ghosted grid: sensor > threshold at interior points, the
+// periodic image at the ghosts of periodic directions and 0 at the others (sensor_at).  Only
+// when some direction builds its list; grid-stride over tiles of 32 x 8 points of a z plane.
+__global__ void __launch_bounds__(256) k_weno_bits(Geom g, const double* __restrict__ sensor) {
+  if (!list_wanted<0>(g) && !list_wanted<1>(g) && !list_wanted<2>(g)) return;
+  const unsigned tx = (g.sx + 31) / 32, ty = (g.sy + 7) / 8;
+  const unsigned ntile = tx * ty * (unsigned)g.sz;
+  for (unsigned tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    const unsigned r = tile / tx;
+    const int i = (int)(tile - r * tx) * 32 + (threadIdx.x & 31) + 1 - g.ng;
+    const int j = (int)(r % ty) * 8 + (threadIdx.x >> 5) + 1 - g.ng;
+    const int k = (int)(r / ty) + 1 - g.ng;
+    if (i <= g.nx + g.ng && j <= g.ny + g.ng)
+      g.wbits[gidx(g, i, j, k)] = sensor_at(g, sensor, i, j, k) > g.sensor_threshold ? 1 : 0;
+  }
+}
+
+// The WENO faces of direction DIR: the faces the hybrid pass computes (eul range) whose stencil
+// sees a sensor flag, appended to the direction's list; grid-stride over tiles of 32 faces along
+// t0 x 8 along t1 of one t2 plane.  A direction whose sample is above its threshold builds no
+// list and marks its count as above every threshold (its hybrid pass computes the WENO faces).
+template <int DIR, int WS>
+__global__ void __launch_bounds__(WL_NT) k_weno_list(Geom g) {
+  __shared__ unsigned wsum[2 * (WL_NT / 32)];
+  __shared__ unsigned base[2];
+  if (!list_wanted<DIR>(g)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) g.wcount[DIR] = 0xffffffffu;
+    return;
+  }
+  const int n0 = DIR == 0 ? g.nx + 1 : g.nx, n1 = DIR == 1 ? g.ny + 1 : g.ny;
+  const int n2 = DIR == 2 ? g.nz + 1 : g.nz;
+  const unsigned tx = (unsigned)(n0 + 31) / 32, ty = (unsigned)(n1 + 7) / 8;
+  const unsigned ntile = tx * ty * (unsigned)n2;
+  const int emin = DIR == 0 ? g.eul_imin : (DIR == 1 ? g.eul_jmin : g.eul_kmin);
+  const int emax = DIR == 0 ? g.eul_imax : (DIR == 1 ? g.eul_jmax : g.eul_kmax);
+  const long long sd = DIR == 0 ? 1 : (DIR == 1 ? (long long)g.sx : (long long)g.sx * g.sy);
+  int par = 0;
+  for (unsigned tile = blockIdx.x; tile < ntile; tile += gridDim.x, par ^= 1) {
+    const unsigned r = tile / tx;
+    const int t0 = (int)(tile - r * tx) * 32 + (threadIdx.x & 31);
+    const int t1 = (int)(r % ty) * 8 + (threadIdx.x >> 5);
+    const int t2 = (int)(r / ty);
+    int p, a, b;
+    list_face<DIR>(t0, t1, t2, p, a, b);
+    bool shk = false;
+    if (t0 < n0 && t1 < n1 && p >= emin - 1 && p <= emax) {
+      // the stencil points p-WS+1 .. p+WS of the face, all inside the ghosted grid (ng >= WS)
+      const long long c = DIR == 0 ? gidx(g, p, a, b) : (DIR == 1 ? gidx(g, a, p, b) : gidx(g, a, b, p));
+      const unsigned char* f = g.wbits + c;
+      unsigned any = 0;
+#pragma unroll
+      for (int o = -WS + 1; o <= WS; ++o) any |= f[o * sd];
+      shk = any != 0;
+    }
+    const unsigned e = block_append(shk, g.wcount + DIR, wsum, base, par);
+    if (shk) g.wlist[DIR][e] = (unsigned)wface_index<DIR>(g, p, a, b);
+  }
 }
 
 // The fluxes of the listed WENO faces of direction DIR into the face buffer (grid-stride over the
@@ -1458,15 +1530,25 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   const long long wnf = std::max(wface_count<0>(g), std::max(wface_count<1>(g), wface_count<2>(g)));
   const unsigned wgrid = (unsigned)std::min<long long>((long long)nblocks(wnf, WF_NT), 148LL * 16);
   if (SB_WENO_SPLIT && a.istep == 1) {
-    SB_LAUNCH(d, K_WENO_LIST, s, cudaMemsetAsync(g.wcount, 0, 3 * sizeof(unsigned), s));
-    const dim3 gb(nblocks(g.sx, 32), nblocks(g.sy, 8), g.sz);
+    SB_LAUNCH(d, K_WENO_LIST, s, cudaMemsetAsync(g.wcount, 0, 8 * sizeof(unsigned), s));
+    // the sample counts, then the flags and the lists of the directions whose sample is within
+    // the threshold (the others leave at once)
+    const unsigned ns2 = (unsigned)(g.nz + WSAMPLE - 1) / WSAMPLE, ns2z = (unsigned)(g.nz + WSAMPLE) / WSAMPLE;
+    SB_LAUNCH(d, K_WENO_LIST, s,
+              k_weno_sample<0, WS><<<dim3(nblocks(g.nx + 1, 32), nblocks(g.ny, 8), ns2), WL_NT, 0, s>>>(g, sensor));
+    SB_LAUNCH(d, K_WENO_LIST, s,
+              k_weno_sample<1, WS><<<dim3(nblocks(g.nx, 32), nblocks(g.ny + 1, 8), ns2), WL_NT, 0, s>>>(g, sensor));
+    SB_LAUNCH(d, K_WENO_LIST, s,
+              k_weno_sample<2, WS><<<dim3(nblocks(g.nx, 32), nblocks(g.ny, 8), ns2z), WL_NT, 0, s>>>(g, sensor));
+    // grid-stride over one resident wave (148 SMs x 8 blocks): a grid of one block per tile,
+    // whose blocks leave at once when no list is built, measured 2.5 ms per step of empty
+    // blocks on the 1024x256x192 boundary layer
+    const unsigned gb = 148 * 8;
     SB_LAUNCH(d, K_WENO_LIST, s, k_weno_bits<<<gb, 256, 0, s>>>(g, sensor));
-    const dim3 gl0(nblocks(g.nx + 1, 32), nblocks(g.ny, 8), g.nz), gl1(nblocks(g.nx, 32), nblocks(g.ny + 1, 8), g.nz),
-        gl2(nblocks(g.nx, 32), nblocks(g.ny, 8), g.nz + 1);
-    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<0, WS><<<gl0, WL_NT, 0, s>>>(g));
-    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<1, WS><<<gl1, WL_NT, 0, s>>>(g));
-    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<2, WS><<<gl2, WL_NT, 0, s>>>(g));
-    *nl += 4;
+    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<0, WS><<<gb, WL_NT, 0, s>>>(g));
+    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<1, WS><<<gb, WL_NT, 0, s>>>(g));
+    SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<2, WS><<<gb, WL_NT, 0, s>>>(g));
+    *nl += 7;
   }
   if (SB_WENO_SPLIT) {
     SB_LAUNCH(d, K_WENO_FACES, s, k_weno_faces<R, 0, LB, WS, FS><<<wgrid, WF_NT, wsm, s>>>(g, aux));
