@@ -286,8 +286,12 @@ int streams_b200_get_tuning(streams_b200_ctx* ctx, long long* march_threads, int
  * direction's list holds at most max_fraction of its faces, their fluxes are computed apart by
  * a kernel of their own and the direction's hybrid pass reads them from a face buffer, otherwise
  * the hybrid pass computes them itself.  The choice is made on the device per direction and
- * step (no host synchronisation).  Default 0.55; 0 keeps every WENO face in the hybrid passes,
- * 1 always computes them apart.  Both forms evaluate the same arithmetic: FP64 results are
+ * step (no host synchronisation); the lists are built only when a sample of every 16th plane is
+ * within the fraction.  1 always computes the WENO faces apart; 0 turns the split off (the hybrid
+ * passes alone, no list or face kernel launched).  Default: 0.55 for boxes of at least 2^21
+ * cells, 0 for smaller ones (launch-bound, where the split's extra launches cost more than it
+ * saves).  The face buffers (about 53 bytes per cell) are allocated when the split is first on;
+ * STREAMS_B200_ENOMEM if that fails.  Both forms evaluate the same arithmetic: FP64 results are
  * identical up to the compiler's contraction of the WENO arithmetic in the two kernels
  * (observed: bit-identical, or differences of a few ulp).
  */

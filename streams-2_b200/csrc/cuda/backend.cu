@@ -67,6 +67,17 @@ cudaError_t dev_alloc(streams_b200_ctx* c, T** p, size_t count) {
   return cudaSuccess;
 }
 
+// Largest WENO face fraction of a direction at which its hybrid pass reads the WENO faces from
+// the face buffer: measured on the 1024x256x192 boundary layer, the split form is ahead below a
+// fraction of about 0.55 (FP64: 85.2 vs 87.0 ms per step at 0.51, 89.0 vs 87.3 at 0.61; 61.9 vs
+// 78.1 at 0.06) and behind above it (99.8 vs 86.8 at 0.90).
+constexpr double WENO_SPLIT_FRAC_DEFAULT = 0.55;
+// Boxes below this many cells start with the split off (fraction 0: the hybrid passes alone, no
+// list or face kernels launched and no buffers held).  A small box's step is launch-bound and the
+// split adds about twenty launches per step, most of them leaving at once; measured on the
+// served channel boxes of 0.13 - 1.2 M cells: 501 -> 436 Mcell-steps/s with the split on.
+constexpr long long WENO_SPLIT_MIN_CELLS = 1LL << 21;
+
 long long footprint(const streams_b200_params* p) {
   const long long sx = p->nx + 2LL * p->ng, sy = p->ny + 2LL * p->ng, sz = p->nz + 2LL * p->ng;
   const long long nvol = sx * sy * sz, nint = (long long)p->nx * p->ny * p->nz;
@@ -79,11 +90,11 @@ long long footprint(const streams_b200_params* p) {
   b += nint * 2 * 8;   // sensor, sensor_next
   b += nint * 10 * 8;  // two RK registers
   b += (long long)p->nx * p->nz * 3 * 8;
-  // WENO faces apart: the largest direction's face buffer (40 B per face), the three lists and
-  // the ghosted sensor flags (1 B per point)
+  // WENO faces apart (boxes that start with the split on): the largest direction's face buffer
+  // (40 B per face), the three lists and the ghosted sensor flags (1 B per point)
   const long long nfx = (p->nx + 1LL) * p->ny * p->nz, nfy = (long long)p->nx * (p->ny + 1LL) * p->nz,
                   nfz = (long long)p->nx * p->ny * (p->nz + 1LL);
-  b += 40 * std::max(nfx, std::max(nfy, nfz)) + 4 * (nfx + nfy + nfz) + 32 + nvol;
+  if (nint >= WENO_SPLIT_MIN_CELLS) b += 40 * std::max(nfx, std::max(nfy, nfz)) + 4 * (nfx + nfy + nfz) + 32 + nvol;
   b += ((nint + 255) / 256) * 9 * 8 + ((p->nx + 31) / 32) * ((p->nz + 7) / 8) * (long long)p->ny * 5 * 8;
   return b + 4096;
 }
@@ -148,11 +159,6 @@ std::string validate(const streams_b200_params* p) {
   return "";
 }
 
-// Largest WENO face fraction of a direction at which its hybrid pass reads the WENO faces from
-// the face buffer: measured on the 1024x256x192 boundary layer, the split form is ahead below a
-// fraction of about 0.55 (FP64: 85.2 vs 87.0 ms per step at 0.51, 89.0 vs 87.3 at 0.61; 61.9 vs
-// 78.1 at 0.06) and behind above it (99.8 vs 86.8 at 0.90).
-constexpr double WENO_SPLIT_FRAC_DEFAULT = 0.55;
 
 void set_weno_split(Geom& g, double frac) {
   const double nf[3] = {(g.nx + 1.0) * g.ny * g.nz, g.nx * (g.ny + 1.0) * g.nz, g.nx * (double)g.ny * (g.nz + 1.0)};
@@ -161,6 +167,7 @@ void set_weno_split(Geom& g, double frac) {
                         g.nx * (g.ny + 1.0) * ((g.nz + WSAMPLE - 1) / WSAMPLE),
                         g.nx * (double)g.ny * ((g.nz + WSAMPLE) / WSAMPLE)};
   g.weno_split_frac = frac;
+  g.wsplit_on = frac > 0.0 ? 1 : 0;
   for (int d = 0; d < 3; ++d) {
     g.wthr[d] = (unsigned)std::min(std::floor(frac * nf[d]), 4294967294.0);
     g.wthr_s[d] = (unsigned)std::min(std::floor(frac * ns[d]), 4294967294.0);
@@ -216,7 +223,32 @@ void fill_geom(streams_b200_ctx* c) {
   g.flux_splitting = p.flux_splitting;
   g.march_threads = 148LL * 1024;
   g.march_minseg = 16;
-  set_weno_split(g, WENO_SPLIT_FRAC_DEFAULT);
+  set_weno_split(g, g.nint >= WENO_SPLIT_MIN_CELLS ? WENO_SPLIT_FRAC_DEFAULT : 0.0);
+}
+
+// WENO faces apart: the face buffer (planes of the largest direction's face count), the lists
+// with their counters and the ghosted sensor flags, allocated when the split is first turned on.
+cudaError_t ensure_weno_buffers(streams_b200_ctx* c) {
+  Geom& g = c->g;
+  if (g.wface) return cudaSuccess;
+  const long long nfx = (g.nx + 1LL) * g.ny * g.nz, nfy = (long long)g.nx * (g.ny + 1LL) * g.nz,
+                  nfz = (long long)g.nx * g.ny * (g.nz + 1LL);
+  const long long nfmax = std::max(nfx, std::max(nfy, nfz));
+  double* wf;
+  unsigned* wl;
+  unsigned char* wb;
+  cudaError_t e;
+  if ((e = dev_alloc(c, &wf, 5 * nfmax)) || (e = dev_alloc(c, &wl, nfx + nfy + nfz + 8)) ||
+      (e = dev_alloc(c, &wb, g.nvol)))
+    return e;
+  g.wbits = wb;
+  g.wface = wf;
+  g.nwface = nfmax;  // plane stride: 5 planes of doubles, or 10 planes of floats in the same bytes
+  g.wlist[0] = wl;
+  g.wlist[1] = wl + nfx;
+  g.wlist[2] = wl + nfx + nfy;
+  g.wcount = wl + nfx + nfy + nfz;  // [0..2] list lengths, [4..6] sample counts
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -358,28 +390,16 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
     g.yplus_recyc = yr + (ng - 1); g.eta_recyc = er + (ng - 1);
     g.weta_inflow = we - 1; g.map_j_inn = mi - 1; g.map_j_out = mo - 1;
   }
-  // WENO faces apart: the face buffer (planes of the largest direction's face count) and the lists
+  // WENO faces apart: at most 2^32 faces in a direction (32-bit list entries); buffers when on
   {
-    const long long nfx = (p->nx + 1LL) * p->ny * p->nz, nfy = (long long)p->nx * (p->ny + 1LL) * p->nz,
-                    nfz = (long long)p->nx * p->ny * (p->nz + 1LL);
-    const long long nfmax = std::max(nfx, std::max(nfy, nfz));
+    const long long nfmax = std::max((p->nx + 1LL) * p->ny * p->nz,
+                                     std::max((long long)p->nx * (p->ny + 1LL) * p->nz,
+                                              (long long)p->nx * p->ny * (p->nz + 1LL)));
     if (nfmax >= (1LL << 32)) {
       streams_b200_destroy(c);
       return set_err(nullptr, STREAMS_B200_EINVAL, "more than 2^32 faces in one direction");
     }
-    double* wf;
-    unsigned* wl;
-    unsigned char* wb;
-    if ((e = dev_alloc(c, &wf, 5 * nfmax)) || (e = dev_alloc(c, &wl, nfx + nfy + nfz + 8)) ||
-        (e = dev_alloc(c, &wb, g.nvol)))
-      return fail(e, "cudaMalloc(weno faces)");
-    g.wbits = wb;
-    g.wface = wf;
-    g.nwface = nfmax;  // plane stride: 5 planes of doubles, or 10 planes of floats in the same bytes
-    g.wlist[0] = wl;
-    g.wlist[1] = wl + nfx;
-    g.wlist[2] = wl + nfx + nfy;
-    g.wcount = wl + nfx + nfy + nfz;  // [0..2] list lengths, [4..6] sample counts
+    if (g.wsplit_on && (e = ensure_weno_buffers(c))) return fail(e, "cudaMalloc(weno faces)");
   }
   // state
   DevState& d = c->d;
@@ -813,6 +833,14 @@ int streams_b200_set_weno_split(streams_b200_ctx* c, double max_fraction) {
   if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
   if (!(max_fraction >= 0.0 && max_fraction <= 1.0))
     return set_err(c, STREAMS_B200_EINVAL, "max_fraction must be in [0, 1]");
+  if (max_fraction > 0.0) {
+    cudaSetDevice(c->device);
+    const cudaError_t e = ensure_weno_buffers(c);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(c, STREAMS_B200_ENOMEM, std::string("WENO face buffers: ") + cudaGetErrorString(e));
+    }
+  }
   set_weno_split(c->g, max_fraction);
   return STREAMS_B200_OK;
 }

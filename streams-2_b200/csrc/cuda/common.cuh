@@ -100,6 +100,7 @@ struct Geom {
   // the lists are built only when a sample of the faces (every WSAMPLE-th plane of the list
   // kernels' third grid index) holds at most wthr_s[d] WENO faces (wcount[4 + d] on the device)
   unsigned int wthr_s[3];
+  int wsplit_on;  // weno_split_frac > 0: the lists, face kernels and split forms are launched
   double weno_split_frac;  // host side
   // launch shape of the y/z march passes (host side only): the lines are cut into segments so
   // that about march_threads threads run, each segment at least march_minseg cells long

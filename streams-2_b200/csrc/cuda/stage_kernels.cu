@@ -383,7 +383,7 @@ __device__ __forceinline__ void wface_decode(const Geom& g, unsigned f, int& p, 
 // (the list, built at stage 1, holds at most wthr[DIR] faces) or computes them itself.
 template <int DIR>
 __device__ __forceinline__ bool weno_split(const Geom& g) {
-  return SB_WENO_SPLIT && *(volatile const unsigned*)(g.wcount + DIR) <= g.wthr[DIR];
+  return SB_WENO_SPLIT && g.wsplit_on && *(volatile const unsigned*)(g.wcount + DIR) <= g.wthr[DIR];
 }
 template <int DIR>
 __host__ __device__ __forceinline__ long long wface_count(const Geom& g) {
@@ -1529,7 +1529,8 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
   // the face fluxes before each hybrid pass
   const long long wnf = std::max(wface_count<0>(g), std::max(wface_count<1>(g), wface_count<2>(g)));
   const unsigned wgrid = (unsigned)std::min<long long>((long long)nblocks(wnf, WF_NT), 148LL * 16);
-  if (SB_WENO_SPLIT && a.istep == 1) {
+  const bool split_on = SB_WENO_SPLIT && g.wsplit_on;
+  if (split_on && a.istep == 1) {
     SB_LAUNCH(d, K_WENO_LIST, s, cudaMemsetAsync(g.wcount, 0, 8 * sizeof(unsigned), s));
     // the sample counts, then the flags and the lists of the directions whose sample is within
     // the threshold (the others leave at once)
@@ -1550,7 +1551,7 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
     SB_LAUNCH(d, K_WENO_LIST, s, k_weno_list<2, WS><<<gb, WL_NT, 0, s>>>(g));
     *nl += 7;
   }
-  if (SB_WENO_SPLIT) {
+  if (split_on) {
     SB_LAUNCH(d, K_WENO_FACES, s, k_weno_faces<R, 0, LB, WS, FS><<<wgrid, WF_NT, wsm, s>>>(g, aux));
     ++*nl;
   }
@@ -1574,7 +1575,7 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
                 k_sensor64<<<nblocks(g.nint, 256), 256, 0, s>>>(g, d.w, sensor_next, g.conservative_viscous ? 1 : 2));
     ++*nl;
   }
-  if (SB_WENO_SPLIT) {
+  if (split_on) {
     SB_LAUNCH(d, K_WENO_FACES, s, k_weno_faces<R, 1, LB, WS, FS><<<wgrid, WF_NT, wsm, s>>>(g, aux));
     ++*nl;
   }
@@ -1582,14 +1583,14 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
     SB_LAUNCH(d, K_EULER_Y, s,
               k_march<R, 1, LB, WS, false, FS><<<gyb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                           a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
-    if (SB_WENO_SPLIT) {
+    if (split_on) {
       SB_LAUNCH(d, K_EULER_Y, s,
                 k_march<R, 1, LB, WS, false, FS, true><<<gyb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev,
                                                                    d.sc, a.rhork, a.gamrk, a.istep, sly, nsy, d.red));
       ++*nl;
     }
   }
-  if (SB_WENO_SPLIT) {
+  if (split_on) {
     SB_LAUNCH(d, K_WENO_FACES, s, k_weno_faces<R, 2, LB, WS, FS><<<wgrid, WF_NT, wsm, s>>>(g, aux));
     ++*nl;
   }
@@ -1598,7 +1599,7 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
     SB_LAUNCH(d, K_EULER_Z, s,
               k_march<R, 2, LB, WS, true, FS><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                                   a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
-    if (SB_WENO_SPLIT)
+    if (split_on)
       SB_LAUNCH(d, K_EULER_Z, s,
                 k_march<R, 2, LB, WS, true, FS, true><<<gzb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev,
                                                                   d.sc, a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
@@ -1606,12 +1607,12 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
     SB_LAUNCH(d, K_EULER_Z, s,
               k_march<R, 2, LB, WS, false, FS><<<gzb, MT_NT, msm, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev, d.sc,
                                                                    a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
-    if (SB_WENO_SPLIT)
+    if (split_on)
       SB_LAUNCH(d, K_EULER_Z, s,
                 k_march<R, 2, LB, WS, false, FS, true><<<gzb, MT_NT, 0, s>>>(g, aux, sensor, fl_new, div3, d.w, fl_prev,
                                                                    d.sc, a.rhork, a.gamrk, a.istep, slz, nsz, d.red));
   }
-  if (SB_WENO_SPLIT) ++*nl;
+  if (split_on) ++*nl;
   *nl += 4;
   if (g.recyc) launch_rand_plane(g, d, s, nl);  // euler_z draws the inflow plane of the stage
   launch_bc_nr(g, d, fl_new, s, nl);

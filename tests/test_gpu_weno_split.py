@@ -94,10 +94,14 @@ def test_mixed_forms_agree(tmp_path):
 
 
 def test_the_default_threshold_and_its_limits(tmp_path):
+    """On by default (0.55) from 2^21 cells, off (0) below; turning it on allocates the buffers."""
     from streams_b200 import BackendError, Case, Solver
     from streams_b200.cases import channel_ini
+    big = Solver.from_case(Case(tmp_path, channel_ini(nx=128, ny=128, nz=128)))
+    assert big.get_weno_split() == 0.55
+    big.close()
     s = Solver.from_case(Case(tmp_path, channel_ini(nx=16, ny=12, nz=8)))
-    assert s.get_weno_split() == 0.55
+    assert s.get_weno_split() == 0.0
     for bad in (-0.1, 1.5, float("nan")):
         with pytest.raises(BackendError, match="max_fraction"):
             s.set_weno_split(bad)
