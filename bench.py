@@ -22,7 +22,9 @@ oracle timed on the host cores (cpu_baseline), the SM clocks sampled during the 
 mixed-precision form on the three workloads, the batched form (48 channel boxes) and the served
 form (a Poisson stream of solves).  The headline is timed from step 4 of the synthetic start, a
 transient in which most faces take the WENO branch (weno_face_fraction_xyz); "developed" repeats
-the measurement from step 300, when the hybrid scheme runs mostly central.  With --gpus N > 1 each rank advances an independent replica
+the measurement from step 300, when the hybrid scheme runs mostly central; "full_run" times the
+configuration's whole run (--run-steps, 500, after the warm-up) in event-bracketed segments, the
+headline's and the developed window's steps included.  With --gpus N > 1 each rank advances an independent replica
 (the path has no exchange step).  --impl reference times the CPU restatement of the reference's
 CPU backend (oracle/) on the host.
 """
@@ -325,6 +327,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the served-form measurement")
     ap.add_argument("--no-developed", action="store_true",
                     help="skip the second measurement on the developed flow")
+    ap.add_argument("--run-steps", type=int, default=500,
+                    help="length of the configuration's whole run, timed after the warm-up (full_run)")
     ap.add_argument("--developed-at", type=int, default=300,
                     help="step from which the developed-flow measurement is timed")
     ap.add_argument("--batched-steps", type=int, default=200)
@@ -431,25 +435,39 @@ def main():
                    "share": v[0] / total_prof}
                for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}
 
-    # the same measurement on the developed flow: the synthetic start is a strong transient in
-    # which the Ducros sensor sends most faces to WENO; after a few hundred steps the hybrid
-    # scheme runs mostly central, as a production run does (fraction of WENO faces reported)
+    # the configuration's whole run (run_steps steps after the warm-up) and, inside it, the same
+    # measurement on the developed flow: the synthetic start is a strong transient in which the
+    # Ducros sensor sends most faces to WENO; after a few hundred steps the hybrid scheme runs
+    # mostly central, as a production run does (fraction of WENO faces reported).  The run is
+    # timed in segments, each bracketed by events on the context's stream with nothing else
+    # inside, and the segments are summed with the timed region above.
     developed = None
+    full_run = None
     if not args.no_developed and args.developed_at > icyc:
-        s.advance(args.developed_at - icyc, 1, icyc, 0)
-        icyc = args.developed_at
-        s.synchronize()
+        def timed_advance(n):
+            nonlocal icyc
+            a0_, a1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            barrier()
+            a0_.record(stream)
+            s.advance(n, 1, icyc, 0)
+            a1_.record(stream)
+            s.synchronize()
+            barrier()
+            icyc += n
+            return max_over_ranks(a0_.elapsed_time(a1_))
+
+        seg_ms = [ms, timed_advance(args.developed_at - icyc)]
         weno_dev = [round(x, 4) for x in s.count_weno()]
-        barrier()
-        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        d0.record(stream)
-        s.advance(args.steps, 1, icyc, 0)
-        d1.record(stream)
-        s.synchronize()
-        barrier()
-        icyc += args.steps
-        dms = max_over_ranks(d0.elapsed_time(d1))
-        # per-kernel device time of the steps that follow (the same regime)
+        dms = timed_advance(args.steps)
+        seg_ms.append(dms)
+        run_end = max(args.warmup + args.run_steps, icyc)
+        if run_end > icyc:
+            seg_ms.append(timed_advance(run_end - icyc))
+        run_n = icyc - args.warmup
+        full_run = {"value": ncell * run_n * world / (sum(seg_ms) / 1e3) / 1e6, "unit": "Mcell-steps/s",
+                    "ms_per_step": sum(seg_ms) / run_n, "steps": run_n, "from_step": args.warmup,
+                    "weno_face_fraction_xyz_at_end": [round(x, 4) for x in s.count_weno()]}
+        # per-kernel device time of the steps that follow (the developed regime)
         s.profile(-1)
         s.profile(1)
         s.advance(args.steps, 1, icyc, 0)
@@ -461,7 +479,8 @@ def main():
                      "ms_per_step": dms / args.steps, "timed_from_step": args.developed_at,
                      "weno_face_fraction_xyz": weno_dev,
                      "kernels_ms_per_step": {k: round(v[0] / args.steps, 3)
-                                             for k, v in sorted(dprof.items(), key=lambda kv: -kv[1][0])}}
+                                             for k, v in sorted(dprof.items(), key=lambda kv: -kv[1][0])},
+                     "kernels_from_step": icyc - args.steps}
 
     # end to end through the C ABI with pinned host buffers: upload the field, run, read the
     # progress scalars after every step (the step's metric), download the final field
@@ -585,7 +604,7 @@ def main():
             "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
             "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "mixed": mixed,
             "batched": batched, "serving": serving,
-            "weno_face_fraction_xyz": weno_timed, "developed": developed,
+            "weno_face_fraction_xyz": weno_timed, "developed": developed, "full_run": full_run,
             "state": {"dt": sc["dt"], "rhobulk": sc["rhobulk"], "ubulk": sc["ubulk"], "tbulk": sc["tbulk"],
                       "residual_rhou": res["residual_rhou"], "nan": res["nan"]},
             "u0": info["u0"],
