@@ -107,3 +107,36 @@ def test_the_default_threshold_and_its_limits(tmp_path):
             s.set_weno_split(bad)
     s.set_weno_split(0.3)
     assert s.get_weno_split() == 0.3
+
+
+@pytest.mark.parametrize("frac", [1.0, 0.55])
+def test_batch_with_the_split_equals_alone(frac, tmp_path):
+    """The lists, samples and face kernels replayed from the batch graph (with a change of the
+    fraction between replays, which recaptures it) give the bits of the box advanced alone."""
+    from streams_b200 import Batch, Case, Solver
+    from streams_b200.cases import bl_ini, channel_ini
+    ini = bl_ini(nx=48, ny=40, nz=16, mach=2.28, shock_angle=32.6, lx=60.0)
+    ch = channel_ini(nx=32, ny=24, nz=16)
+    alone = []
+    for case_ini in (ini, ch):
+        a = Solver.from_case(Case(tmp_path, case_ini))
+        a.set_weno_split(frac)
+        a.init_run()
+        a.advance(6)
+        a.set_weno_split(0.3)
+        a.advance(6)
+        alone.append(a.copy_to_field())
+    boxes = []
+    for case_ini in (ini, ch):
+        b = Solver.from_case(Case(tmp_path, case_ini))
+        b.set_weno_split(frac)
+        b.init_run()
+        boxes.append(b)
+    bt = Batch(boxes, steps_per_graph=5)
+    bt.advance(6)
+    for b in boxes:
+        b.set_weno_split(0.3)
+    bt.advance(6)
+    bt.synchronize()
+    for a, b in zip(alone, boxes):
+        assert np.array_equal(a, b.copy_to_field())
