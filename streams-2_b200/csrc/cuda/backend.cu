@@ -101,8 +101,8 @@ long long footprint(const streams_b200_params* p) {
 
 std::string validate(const streams_b200_params* p) {
   if (p->nx < 1 || p->ny < 1 || p->nz < 1) return "grid sizes must be positive";
-  // the launch grids carry y lines (ny + 1 faces) and z lines in their y and z dimensions
-  if (p->ny >= 65535 || p->nz >= 65535) return "ny and nz must be below 65535";
+  // the x pass's launch grid carries ny / 4 rows in its y and nz planes in its z dimension
+  if (p->ny > 4 * 65535 || p->nz > 65535) return "ny must be at most 262140 and nz at most 65535";
   if (p->ep_order < 2 || p->ep_order > 8 || p->ep_order % 2) return "ep_order must be 2, 4, 6 or 8";
   const int lmax = p->ep_order / 2;
   if (p->weno_scheme < 1 || p->weno_scheme > 4) return "weno_scheme must be 1..4";

@@ -84,3 +84,16 @@ def test_create_without_device_fails_loudly(tmp_path):
     with pytest.raises(streams_b200.BackendError) as e:
         streams_b200.Solver(case.params(), case.grid())
     assert e.value.code == streams_b200.ENODEV
+
+
+def test_grid_limits_fail_loudly(tmp_path):
+    """The x pass's launch grid bounds ny (4 rows per block row) and nz (one grid plane each);
+    create rejects larger blocks before touching the device."""
+    from streams_b200 import BackendError, Case, Solver
+    from streams_b200.cases import channel_ini
+    case = Case(tmp_path, channel_ini(16, 12, 8))
+    for field, value in (("nz", 65536), ("ny", 4 * 65535 + 1)):
+        p = case.params()
+        setattr(p, field, value)
+        with pytest.raises(BackendError, match="at most"):
+            Solver(p, case.grid())
