@@ -123,6 +123,17 @@ __host__ __device__ __forceinline__ long long gidx(const Geom& g, int i, int j, 
 __host__ __device__ __forceinline__ long long iidx(const Geom& g, int i, int j, int k) {
   return ((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1);
 }
+// Interior cell (i, j, k) of the interior index q (i fastest).  Interior counts stay below 2^32
+// (no direction may have 2^32 faces, checked at context creation), so the divisions are 32-bit
+// rather than the emulated 64-bit ones.
+__device__ __forceinline__ void cell_of(const Geom& g, long long q, int& i, int& j, int& k) {
+  const unsigned u = (unsigned)q, nx = (unsigned)g.nx, ny = (unsigned)g.ny;
+  const unsigned r = u / nx;
+  i = (int)(u - r * nx) + 1;
+  const unsigned kk = r / ny;
+  j = (int)(r - kk * ny) + 1;
+  k = (int)kk + 1;
+}
 
 // Device-resident scalars of a context (one cache line group).
 struct Scalars {

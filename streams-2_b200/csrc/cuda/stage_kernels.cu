@@ -194,7 +194,8 @@ __global__ void __launch_bounds__(256) k_sensor64(Geom g, const double* __restri
                                                   int mode) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
   if (q >= g.nint) return;
-  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+  int i, j, k;
+  cell_of(g, q, i, j, k);
   auto vel = [&](int a, int b, int c, double (&v)[3]) {
     double st[5];
     point_state(g, w, a, b, c, st, g.t_wall);
@@ -251,7 +252,8 @@ __global__ void __launch_bounds__(256) k_sensor_vel(Geom g, const double* __rest
                                                     int mode) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
   if (q >= g.nint) return;
-  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+  int i, j, k;
+  cell_of(g, q, i, j, k);
   const long long n = g.nvol, c = gidx(g, i, j, k), sY = g.sx, sZ = (long long)g.sx * g.sy;
   auto V = [&](long long a, int m) { return vel[m * n + a]; };
   double ux, vx, wx, uy, vy, wy, uz, vz, wz;
@@ -296,7 +298,8 @@ __global__ void __launch_bounds__(AUX_NT) k_apply_shift(Geom g, double* __restri
                                                         const Scalars* __restrict__ sc) {
   const long long q = (long long)blockIdx.x * AUX_NT + threadIdx.x;
   if (q >= g.nint) return;
-  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+  int i, j, k;
+  cell_of(g, q, i, j, k);
   const long long n = g.nvol, s = gidx(g, i, j, k);
   const double t_start = TP ? double(aux[5 * n + s]) : g.t0;
   w[4 * n + s] = shifted_rhoe<TP>(g, w[s], w[n + s], w[2 * n + s], w[3 * n + s], w[4 * n + s], sc->tbdiff, t_start);
@@ -654,7 +657,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F)
                                               double* __restrict__ wallprop, int do_sensor) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
   if (q >= g.nint) return;
-  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+  int i, j, k;
+  cell_of(g, q, i, j, k);
   const long long n = g.nvol, nI = g.nint;
   const long long c = gidx(g, i, j, k);
   const long long sX = 1, sY = g.sx, sZ = (long long)g.sx * g.sy;
@@ -770,7 +774,8 @@ __global__ void __launch_bounds__(256) k_visc_ns(Geom g, const R* __restrict__ a
                                                  double* __restrict__ wallprop, int do_sensor) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
   if (q >= g.nint) return;
-  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+  int i, j, k;
+  cell_of(g, q, i, j, k);
   const long long n = g.nvol, nI = g.nint;
   const long long c = gidx(g, i, j, k);
   const long long st[3] = {1, g.sx, (long long)g.sx * g.sy};
@@ -858,7 +863,8 @@ __global__ void __launch_bounds__(256) k_init_sensor(Geom g, const R* __restrict
                                                      double* __restrict__ sensor) {
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
   if (q >= g.nint) return;
-  const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+  int i, j, k;
+  cell_of(g, q, i, j, k);
   const long long n = g.nvol, c = gidx(g, i, j, k), sY = g.sx, sZ = (long long)g.sx * g.sy;
   auto A = [&](long long a, int m) -> R { return aux[(m - 1) * n + a]; };
   R dxl = R(1) / R(g.x[i + 1] - g.x[i - 1]);
@@ -890,7 +896,8 @@ __global__ void __launch_bounds__(256) k_dt(Geom g, const double* __restrict__ w
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (q < g.nint) {
-    const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+    int i, j, k;
+    cell_of(g, q, i, j, k);
     const long long n = g.nvol, c = gidx(g, i, j, k);
     double rho = w[c];
     double ri = 1.0 / rho;
@@ -996,7 +1003,8 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
   double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX};
   double mx[3] = {-100.0, -100.0, -100.0};
   if (q < g.nint) {
-    const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+    int i, j, k;
+    cell_of(g, q, i, j, k);
     const long long n = g.nvol, nI = g.nint, c = gidx(g, i, j, k);
     const double dt = sc->dt;
     const double rhodt = rhork * dt, gamdt = gamrk * dt;
@@ -1130,7 +1138,8 @@ __global__ void __launch_bounds__(256) k_count_weno(Geom g, const double* __rest
   const long long q = (long long)blockIdx.x * 256 + threadIdx.x;
   double v[3] = {0.0, 0.0, 0.0};
   if (q < g.nint) {
-    const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+    int i, j, k;
+    cell_of(g, q, i, j, k);
     const int ws = g.weno_scheme;
     const double thr = g.sensor_threshold;
     if (i >= g.eul_imin && i <= g.eul_imax) {

@@ -222,7 +222,8 @@ __global__ void __launch_bounds__(256) k_stats3d(Geom g, const double* __restric
   for (int e = threadIdx.x; e < cnt * NV_STAT_3D; e += 256) buf[e] = base[e];
   __syncthreads();
   if (q < g.nint) {
-    const int i = (int)(q % g.nx) + 1, j = (int)((q / g.nx) % g.ny) + 1, k = (int)(q / ((long long)g.nx * g.ny)) + 1;
+    int i, j, k;
+    cell_of(g, q, i, j, k);
     const long long n = g.nvol, c = gidx(g, i, j, k);
     const double r = w[c], ru = w[n + c], rv = w[2 * n + c], rw = w[3 * n + c];
     const double t = double(aux[5 * n + c]);
