@@ -330,6 +330,33 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
     if ((e = cudaMemcpy(cp.d, cp.h, cp.b, cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e, "cudaMemcpy(grid)");
   }
   g.x = dx + (ng - 1); g.y = dy + (ng - 1); g.z = dz + (ng - 1);
+  {
+    // the viscous pass's grid divisions, one per line instead of one per cell (host IEEE
+    // division: the quotients the device would form)
+    const double* crd[3] = {gr->x, gr->y, gr->z};
+    const int nn[3] = {p->nx, p->ny, p->nz};
+    for (int d = 0; d < 3; ++d) {
+      std::vector<double> r(nn[d]), h(nn[d]);
+      std::vector<float> rf(nn[d]);
+      for (int i = 1; i <= nn[d]; ++i) {
+        const double dd = crd[d][i + ng] - crd[d][i + ng - 2];  // x(i+1) - x(i-1)
+        r[i - 1] = 1.0 / dd;
+        h[i - 1] = 2.0 / dd;
+        rf[i - 1] = 1.0f / static_cast<float>(dd);
+      }
+      double *dr, *dh;
+      float* drf;
+      if ((e = dev_alloc(c, &dr, nn[d])) || (e = dev_alloc(c, &dh, nn[d])) || (e = dev_alloc(c, &drf, nn[d])))
+        return fail(e, "cudaMalloc(grid)");
+      if ((e = cudaMemcpy(dr, r.data(), nn[d] * 8, cudaMemcpyHostToDevice)) ||
+          (e = cudaMemcpy(dh, h.data(), nn[d] * 8, cudaMemcpyHostToDevice)) ||
+          (e = cudaMemcpy(drf, rf.data(), nn[d] * 4, cudaMemcpyHostToDevice)))
+        return fail(e, "cudaMemcpy(grid)");
+      g.vrl[d] = dr - 1;
+      g.vhl[d] = dh - 1;
+      g.vrlf[d] = drf - 1;
+    }
+  }
   g.yn = dyn - 1;
   g.dcsidx = m1 - 1; g.detady = m2 - 1; g.dzitdz = m3 - 1;
   g.dcsidxs = m4 - 1; g.detadys = m5 - 1; g.dzitdzs = m6 - 1;

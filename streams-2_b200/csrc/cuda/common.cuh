@@ -28,6 +28,11 @@ struct Geom {
   long long nint;  // nx*ny*nz: stride between variables of an interior array
   // one-dimensional grid (device pointers, already offset so that x[i] is x(i) of the reference)
   const double* x;
+  // per line of each direction, index 1..n: 1/(x(i+1)-x(i-1)) in FP64 and in FP32 and
+  // 2/(x(i+1)-x(i-1)) in FP64, the grid divisions of the viscous pass (the same IEEE quotients)
+  const double* vrl[3];
+  const float* vrlf[3];
+  const double* vhl[3];
   const double* y;
   const double* z;
   const double* yn;       // yn[j], j = 1..ny+1

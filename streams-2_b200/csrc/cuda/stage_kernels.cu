@@ -667,9 +667,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F)
   // cp at the point (visflx_reduced_ord2) and at a face's mean temperature (visflx_x/y/z);
   // a constant for the calorically perfect gas
   const R cploc = TP ? R(cp_of_t(g, double(A(c, 6)))) : R(g.cp0), prandtl = R(g.prandtl);
-  R dxl = R(1) / R(g.x[i + 1] - g.x[i - 1]);
-  R dyl = R(1) / R(g.y[j + 1] - g.y[j - 1]);
-  R dzl = R(1) / R(g.z[k + 1] - g.z[k - 1]);
+  // 1/(x(i+1)-x(i-1)) etc. from the per-line tables (the same quotients as a division here)
+  R dxl, dyl, dzl;
+  if constexpr (sizeof(R) == sizeof(double)) {
+    dxl = R(__ldg(g.vrl[0] + i)); dyl = R(__ldg(g.vrl[1] + j)); dzl = R(__ldg(g.vrl[2] + k));
+  } else {
+    dxl = R(__ldg(g.vrlf[0] + i)); dyl = R(__ldg(g.vrlf[1] + j)); dzl = R(__ldg(g.vrlf[2] + k));
+  }
   R ux = dxl * (A(c + sX, 2) - A(c - sX, 2));
   R vx = dxl * (A(c + sX, 3) - A(c - sX, 3));
   R wx = dxl * (A(c + sX, 4) - A(c - sX, 4));
@@ -736,7 +740,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F)
   // x: fl += dxhl*(fhat(i) - fhat(i-1)), fhat = -sigma
   face(c - sX, c, g.x[i] - g.x[i - 1], lo);
   face(c, c + sX, g.x[i + 1] - g.x[i], hi);
-  double dxhl = 2.0 / (g.x[i + 1] - g.x[i - 1]);
+  double dxhl = __ldg(g.vhl[0] + i);  // 2/(x(i+1)-x(i-1))
   f2 = f2 + dxhl * (-hi[0] - -lo[0]);
   f3 = f3 + dxhl * (-hi[1] - -lo[1]);
   f4 = f4 + dxhl * (-hi[2] - -lo[2]);
@@ -744,14 +748,14 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F)
   // y: fl = (fl + sigma(j-1/2)*dyhl) - sigma(j+1/2)*dyhl
   face(c - sY, c, g.y[j] - g.y[j - 1], lo);
   face(c, c + sY, g.y[j + 1] - g.y[j], hi);
-  double dyhl = 2.0 / (g.y[j + 1] - g.y[j - 1]);
+  double dyhl = __ldg(g.vhl[1] + j);
   f2 = f2 + lo[0] * dyhl - hi[0] * dyhl;
   f3 = f3 + lo[1] * dyhl - hi[1] * dyhl;
   f4 = f4 + lo[2] * dyhl - hi[2] * dyhl;
   f5 = f5 + lo[3] * dyhl - hi[3] * dyhl;
   face(c - sZ, c, g.z[k] - g.z[k - 1], lo);
   face(c, c + sZ, g.z[k + 1] - g.z[k], hi);
-  double dzhl = 2.0 / (g.z[k + 1] - g.z[k - 1]);
+  double dzhl = __ldg(g.vhl[2] + k);
   f2 = f2 + lo[0] * dzhl - hi[0] * dzhl;
   f3 = f3 + lo[1] * dzhl - hi[1] * dzhl;
   f4 = f4 + lo[2] * dzhl - hi[2] * dzhl;
