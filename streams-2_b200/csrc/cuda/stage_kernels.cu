@@ -1057,6 +1057,9 @@ __global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, 
       mx[0] = rho; mx[1] = tstat; mx[2] = pp;
     }
   }
+  // the block partials are read only by the forcing and by a stats sample (the same branch for
+  // the whole grid)
+  if (!g.force_var && !stats) return;
   block_reduce_sum<2, 256>(s2, sm);
   // min / max (exact, order independent)
 #pragma unroll
@@ -1091,7 +1094,9 @@ __global__ void __launch_bounds__(FIN_NT) k_finish_upd(Geom g, const double* __r
   __shared__ double smn[3 * (FIN_NT / 32)], smx[3 * (FIN_NT / 32)];
   double v[2] = {0.0, 0.0};
   double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-100.0, -100.0, -100.0};
-  for (long long b = threadIdx.x; b < nblk; b += FIN_NT) {
+  // k_update wrote block partials only for the forcing or a stats sample
+  const long long nb = (g.force_var || stats) ? nblk : 0;
+  for (long long b = threadIdx.x; b < nb; b += FIN_NT) {
     const double* o = red + b * NRED_UPD;
     v[0] = v[0] + o[0];
     v[1] = v[1] + o[1];
