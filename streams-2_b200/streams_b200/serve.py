@@ -5,10 +5,13 @@ Each is prepared on the host as it arrives (input parsing, grid, initial field: 
 threads, so that set-up overlaps the GPU work), then admitted in arrival order as soon as its
 device footprint fits the HBM budget next to the solves already resident.  A resident solve
 keeps its fields in HBM from admission to completion.  The loop advances all resident solves
-together in ticks: one ``Batch`` (one CUDA graph with a branch per solve) runs a few steps of
-every solve, so the stages of different solves share launches and overlap on the GPU.  Solves
-are admitted while a tick runs (their first step overlaps it), join the next tick, and leave,
-freeing their memory, at the end of the tick in which they complete.  Completion latency is
+together in ticks: every resident solve replays its own CUDA graph of a tick's steps (a one-box
+``Batch``, captured once when the solve joins) on its own stream, so the solves' stages overlap on
+the GPU and a change of the resident set rebuilds nothing (one graph over all resident solves had
+to be captured again whenever a solve joined or left, which at a hundred resident solves cost more
+host time than the tick's GPU work).  Solves are admitted while a tick runs (their first step
+overlaps it), join the next tick, and leave, freeing their memory, at the end of the tick in which
+they complete.  Completion latency is
 measured from a request's arrival to the end of the tick that completes it.
 
 A solve's arithmetic does not depend on what else is resident: with the same launch tuning its
@@ -38,6 +41,7 @@ class Solve:
     footprint: int
     cells: int
     solver: Solver | None = None
+    batch: Batch | None = None      # the solve's own tick graph
     remaining: int = 0
     admitted: float = 0.0
     finished: float = 0.0
@@ -97,7 +101,6 @@ class Server:
         rejected: list[int] = []
         used = 0
         nxt = 0
-        batch, members = None, ()
         busy = 0.0
         host = {"admit_s": 0.0, "batch_build_s": 0.0}
         try:
@@ -124,17 +127,14 @@ class Server:
                 # issue one tick of every resident solve through one shared graph (asynchronous)
                 n = 0
                 if active:
-                    key = tuple(s.rid for s in active)
-                    if key != members:
-                        tc = now()
-                        if batch is not None:
-                            batch.close()
-                        batch = Batch([s.solver for s in active], steps_per_graph=self.tick_steps, dt_every=1)
-                        members = key
-                        host["batch_build_s"] += now() - tc
                     n = tick_length([s.remaining for s in active], self.tick_steps)
                     ta = now()
-                    batch.advance(n)
+                    for s in active:
+                        if s.batch is None:
+                            tc = now()
+                            s.batch = Batch([s.solver], steps_per_graph=self.tick_steps, dt_every=1)
+                            host["batch_build_s"] += now() - tc
+                        s.batch.advance(n)
                 # admission by footprint, first come first served, while the tick runs; the
                 # solves admitted now take their first step on their own streams and join the
                 # next tick (memory of solves finishing in this tick is released after it)
@@ -156,7 +156,8 @@ class Server:
                     joining.append(s)
                 host["admit_s"] += now() - tadm
                 if n:
-                    batch.synchronize()
+                    for s in active:
+                        s.batch.synchronize()
                     tb = now()
                     busy += tb - ta
                     self.log.append((ta, tb, len(active), n))
@@ -167,9 +168,6 @@ class Server:
                             still.append(s)
                         else:
                             used -= self._finish(s, tb, done)
-                    if len(still) != len(active):
-                        batch.close()
-                        batch, members = None, ()
                     active = still
                 # a one-step solve is complete after its first step
                 for s in joining:
@@ -185,9 +183,9 @@ class Server:
                     elif nxt < len(reqs):
                         time.sleep(max(0.0, min(0.05, reqs[nxt]["arrival"] * time_scale - now())))
         finally:
-            if batch is not None:
-                batch.close()
             for s in active:
+                if s.batch is not None:
+                    s.batch.close()
                 if s.solver is not None:
                     s.solver.close()
             pool.shutdown(wait=True)
@@ -202,6 +200,9 @@ class Server:
         s.result["scalars"] = s.solver.scalars()
         if self.keep_fields:
             s.result["w"] = s.solver.copy_to_field()
+        if s.batch is not None:
+            s.batch.close()
+            s.batch = None
         s.solver.close()
         s.solver = None
         done.append(s)
