@@ -124,7 +124,7 @@ class Server:
                         else:
                             waiting.append(s)
                 waiting.sort(key=lambda s: s.arrival)
-                # issue one tick of every resident solve through one shared graph (asynchronous)
+                # issue one tick of every resident solve, each through its own graph (asynchronous)
                 n = 0
                 if active:
                     n = tick_length([s.remaining for s in active], self.tick_steps)
@@ -148,7 +148,7 @@ class Server:
                     if s.tuning:
                         s.solver.set_tuning(*s.tuning)
                     s.solver.init_run()
-                    # the first step runs alone, so that the shared graph only holds steady steps
+                    # the first step runs alone, so that the solve's graph only holds steady steps
                     s.solver.advance(1)
                     s.remaining = s.nsteps - 1
                     s.admitted = now()
