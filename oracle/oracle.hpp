@@ -44,6 +44,10 @@ class Solver {
   void rk_sync();
   void compute_residual();
   ProgressRow progress_row() const;
+  // hybrid convective flux at face (i,j,k) of direction dir (0 x, 1 y, 2 z) from the current
+  // w_aux (fhat of euler_{x,y,z}_*hybrid_kernel); the test suite checks it face by face against
+  // an independent restatement
+  void face_flux_at(int dir, int i, int j, int k, double fh[5]) const { face_flux(dir, i, j, k, fh); }
 
   // running statistics, as manage_output calls them after a step (itav samples already averaged):
   // compute_stats (singleideal.F90:2003-2179) and compute_stats_3d (:2513-2543)

@@ -51,6 +51,11 @@ void oracle_compute_dt(void* hp) {
   s->compute_aux(1, 0);
   s->compute_dt();
 }
+// fhat of nface faces (dir, i, j, k) = ijk[4q .. 4q+3] from the current w_aux into out[5q ..]
+void oracle_face_flux(void* hp, int nface, const int* ijk, double* out) {
+  auto* s = static_cast<Handle*>(hp)->solver;
+  for (int q = 0; q < nface; ++q) s->face_flux_at(ijk[4 * q], ijk[4 * q + 1], ijk[4 * q + 2], ijk[4 * q + 3], out + 5 * q);
+}
 void oracle_set_dt(void* hp, double dt) { static_cast<Handle*>(hp)->solver->dt = dt; }
 void oracle_compute_residual(void* hp) { static_cast<Handle*>(hp)->solver->compute_residual(); }
 

@@ -30,6 +30,7 @@ def _load():
         "oracle_rk_sync": (None, [P]),
         "oracle_compute_dt": (None, [P]),
         "oracle_set_dt": (None, [P, C.c_double]),
+        "oracle_face_flux": (None, [P, I, C.POINTER(C.c_int), D]),
         "oracle_compute_residual": (None, [P]),
         "oracle_sizes": (None, [P, C.POINTER(C.c_int)]),
         "oracle_get_w": (None, [P, D]),
@@ -113,6 +114,13 @@ class Oracle:
         a = np.zeros((10, self.nz + 2 * g, self.ny + 2 * g, self.nx + 2 * g))
         lib.oracle_get_waux(self._h, _d(a))
         return a
+
+    def face_flux(self, faces: np.ndarray) -> np.ndarray:
+        """fhat at the faces (dir, i, j, k), one row each, from the current w_aux: (n, 5)."""
+        f = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 4)
+        out = np.zeros((f.shape[0], 5))
+        lib.oracle_face_flux(self._h, f.shape[0], f.ctypes.data_as(C.POINTER(C.c_int)), _d(out))
+        return out
 
     def fl(self) -> np.ndarray:
         a = np.zeros((5, self.nz, self.ny, self.nx))

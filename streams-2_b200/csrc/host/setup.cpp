@@ -943,6 +943,10 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
   s.nkeep = c.get_int_or("numerics", "nkeep", 0);
   s.weno_scheme = c.get_int("numerics", "weno_scheme");
   if (s.weno_scheme < 1 || s.weno_scheme > 4) throw InputError("weno_scheme must be 1, 2, 3 or 4");
+  // the face stencils reach max(ep_order/2, weno_scheme) points beyond a face into the ghosts
+  if (s.ng < std::max(s.ep_order / 2, s.weno_scheme))
+    throw InputError("ng must be at least max(ep_order/2, weno_scheme) = " +
+                     std::to_string(std::max(s.ep_order / 2, s.weno_scheme)));
   s.weno_version = c.get_int("numerics", "weno_version");
   if (s.weno_scheme != 3 && s.weno_version == 1) throw InputError("weno_version 1 supported only for weno_scheme = 3");
   s.flux_splitting = c.get_int_or("numerics", "flux_splitting", 0);

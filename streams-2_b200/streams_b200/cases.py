@@ -49,7 +49,7 @@ domain_size_z = {lz!r}
 nxmax = {nx}
 nymax = {ny}
 nzmax = {nz}
-ng = 3
+ng = {max(3, ep_order // 2, weno_scheme)}
 metrics_order = {ep_order}
 grid_type = 3
 dyptarget = 0.7
@@ -165,7 +165,7 @@ domain_size_z = {lz!r}
 nxmax = {nx}
 nymax = {ny}
 nzmax = {nz}
-ng = 3
+ng = {max(3, ep_order // 2, weno_scheme)}
 metrics_order = {ep_order}
 grid_type = 4
 jbgrid = {jbgrid!r}

@@ -52,6 +52,9 @@ CASES = {
     # flux_splitting = 1: component-wise (Rusanov) WENO instead of the characteristic one
     "rusanov": dict(nx=32, ny=24, nz=16, flux_splitting=1),
     "rusanov_full_weno": dict(nx=24, ny=16, nz=12, sensor=-1.0, flux_splitting=1),
+    # seventh-order WENO with the eighth-order central flux (ng = 4)
+    "weno7_central8": dict(nx=32, ny=24, nz=16, weno_scheme=4, ep_order=8),
+    "weno7_full": dict(nx=24, ny=16, nz=12, weno_scheme=4, ep_order=8, sensor=-1.0),
 }
 
 
@@ -68,7 +71,7 @@ def test_one_step(name, tmp_path):
 
 
 @pytest.mark.parametrize("name", ["hybrid", "full_weno", "full_central_sutherland", "nonconservative_viscous",
-                                  "rusanov"])
+                                  "rusanov", "weno7_central8"])
 def test_hundred_steps(name, tmp_path):
     o, s = run_pair(tmp_path, channel_ini(**CASES[name]), 100)
     ng = o.ng
@@ -198,3 +201,31 @@ def test_restart_from_device_state(tmp_path):
     for m in range(5):
         assert rel_l2(wg[m], wo[m]) <= 1e-12, (m, rel_l2(wg[m], wo[m]))
     assert abs(s2.scalars()["time"] - o.scalars()["time"]) <= 1e-12 * o.scalars()["time"]
+
+
+def test_channel_128x96x64_hundred_steps(tmp_path):
+    """The plain FP64 channel workload itself: 128x96x64, tanh 1.5 stretching, bulk Mach 1.5,
+    bulk Re 3000, power law 0.76, Ducros threshold 0.05, CFL 0.8, +-10 % seeded noise (seed 1),
+    T_b held by force_var; 100 steps.  Every conserved variable within 1e-11 relative L2 of the
+    oracle, the bulk values and dpdx within 1e-11, the wall shear within 1e-11, and the bulk
+    temperature held at its target by the device's force_var."""
+    ini = channel_ini(nx=128, ny=96, nz=64, mach=1.5, re_bulk=3000.0, vt_exp=0.76, sensor=0.05, cfl=0.8,
+                      seed=1, y_stretch=1.5, amp=0.1, theta_wall=0.0)
+    o, s = run_pair(tmp_path, ini, 100)
+    ng = o.ng
+    wo, wg = interior(o.w(), ng), interior(s.copy_to_field(), ng)
+    errs = [rel_l2(wg[m], wo[m]) for m in range(5)]
+    assert max(errs) <= 1e-11, errs
+    so, sg = o.scalars(), s.scalars()
+    for k in ("dt", "time", "dpdx", "rhobulk", "ubulk", "tbulk"):
+        assert abs(sg[k] - so[k]) <= 1e-11 * max(abs(so[k]), 1e-30), (k, sg[k], so[k])
+    assert rel_l2(s.wallprop(), o.wallprop()) <= 1e-11
+    # force_var on the device: sum(rho u T dy) / (volchan rho_b u_b) at the target
+    from streams_b200 import Case
+    case = Case(tmp_path, ini)
+    p = case.params()
+    dy = np.diff(np.ctypeslib.as_array(case.grid().yn, shape=(p.ny + 1,)))
+    rho, ru, rv, rw, re = wg
+    tt = p.t0 + (re / rho - 0.5 * ((ru / rho) ** 2 + (rv / rho) ** 2 + (rw / rho) ** 2) - p.cv_last * p.t0) / p.cv0
+    tb = (ru * tt * dy[None, :, None]).sum() / p.volchan / sg["rhobulk"] / sg["ubulk"]
+    assert abs(tb - p.t_bulk_target) <= 1e-12 * p.t_bulk_target, (tb, p.t_bulk_target)
