@@ -53,8 +53,10 @@ typedef struct streams_b200_params {
   int nkeep;                /* KEEP(n) variant: 0 internal-energy split, <0 enthalpy split, >0 KEEP(n) */
   int weno_scheme;          /* WENO order = 2*weno_scheme-1 (1..4) */
   int weno_version;         /* 0 Jiang-Shu, 1 WENO-Z (weno_scheme 3 only) */
-  int flux_splitting;       /* 0 Roe characteristic splitting (the only one on the device path) */
-  int conservative_viscous; /* 1 conservative 2nd-order viscous form (the only one on the device path) */
+  int flux_splitting;       /* 0 Roe characteristic splitting, 1 component-wise Rusanov splitting
+                               (sixth-order central / WENO5; tests/test_gpu_parity.py rusanov cases) */
+  int conservative_viscous; /* 1 conservative 2nd-order viscous form, 0 non-conservative form at
+                               visc_order (tests/test_gpu_parity.py nonconservative cases) */
   double sensor_threshold;  /* Ducros threshold; <0 full WENO, >1 full central */
   /* boundary conditions (bctags after the periodic normalisation, singleideal.F90:379-403) */
   int bctags[6];            /* xmin xmax ymin ymax zmin zmax: 0 periodic, 6 viscous wall */
@@ -257,6 +259,13 @@ int streams_b200_profile_enable(streams_b200_ctx* ctx, int on);
 int streams_b200_profile_read(streams_b200_ctx* ctx, int kid, double* total_ms, long long* count);
 int streams_b200_kernel_count(void);
 const char* streams_b200_kernel_name(int kid);
+/*
+ * Architecture of the loaded device code: cudaFuncGetAttributes(...).binaryVersion of one kernel
+ * of each CUDA source of the library (100 for sm_100a) into out[0 .. min(max, n) - 1]; returns
+ * n, the number of sources (3), or STREAMS_B200_EINVAL.  A value of -1 means the driver could not
+ * load that source's kernels on the current device.  No counterpart in the reference.
+ */
+int streams_b200_kernel_binary_versions(int* out, int max);
 
 /*
  * Diagnostics: copy an internal device array to the host (synchronous).  which =
@@ -344,7 +353,10 @@ int streams_b200_batch_destroy(streams_b200_batch* b);
  *   aux      device aux fields rho,u,v,w,H,T,mu, 7 arrays of the same ghosted shape
  *            (the layout of streams_b200_debug_fetch(ctx, 0, ...)), current for w
  *   dcsidx.. device metric arrays of nx, ny, nz entries (set_local_grid, field.F90:456-516)
- *   gamma    cp/(cp - rgas0) of the calorically perfect gas
+ *   gamma    cp/(cp - rgas0) of the calorically perfect gas, > 1.  The time step of a thermally
+ *            perfect gas (calorically_perfect = 0) takes gamma(T) per cell: such cases must use
+ *            the context's streams_b200_compute_dt.  gamma <= 1, rgas0 <= 0 or prandtl <= 0
+ *            return STREAMS_B200_EINVAL.
  *   dt       device address that receives cfl / max(inverse time scales)
  *   stream   cudaStream_t on which both kernels run (asynchronous; NULL = default stream)
  *

@@ -717,6 +717,13 @@ int streams_b200_profile_read(streams_b200_ctx* c, int kid, double* total_ms, lo
 int streams_b200_kernel_count(void) { return K_NUM; }
 const char* streams_b200_kernel_name(int kid) { return kernel_name(kid); }
 
+int streams_b200_kernel_binary_versions(int* out, int max) {
+  if (!out || max < 0) return STREAMS_B200_EINVAL;
+  const int v[3] = {binary_version_stage(), binary_version_bc(), binary_version_stats()};
+  for (int q = 0; q < 3 && q < max; ++q) out[q] = v[q];
+  return 3;
+}
+
 int streams_b200_debug_fetch(streams_b200_ctx* c, int which, double* out, long long n) {
   if (!c || !out) return set_err(c, STREAMS_B200_EINVAL, "null argument");
   cudaSetDevice(c->device);

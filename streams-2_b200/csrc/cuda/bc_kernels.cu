@@ -430,4 +430,10 @@ cudaError_t launch_bc_nr(const Geom& g, DevState& d, double* fl, cudaStream_t s,
   return cudaGetLastError();
 }
 
+// binaryVersion of this file's kernels as the driver loaded them (architecture check)
+int binary_version_bc() {
+  cudaFuncAttributes a;
+  return cudaFuncGetAttributes(&a, k_bc_extr) == cudaSuccess ? a.binaryVersion : -1;
+}
+
 }  // namespace sb200

@@ -16,6 +16,10 @@ enum KernelId {
   K_STATS, K_STATS3D, K_WENO_LIST, K_WENO_FACES, K_NUM
 };
 const char* kernel_name(int kid);
+// binaryVersion (10 * major + minor) of one kernel of each CUDA source, as loaded by the driver
+int binary_version_stage();
+int binary_version_bc();
+int binary_version_stats();
 
 // Per-kernel CUDA-event timing (off unless enabled on the context).
 struct Prof {

@@ -132,6 +132,11 @@ int streams_b200_compute_dt_noalloc(int nx, int ny, int nz, int ng, const double
   if (!w || !aux || !dcsidx || !detady || !dzitdz || !dcsidxs || !detadys || !dzitdzs || !dt)
     return fail(STREAMS_B200_EINVAL, "compute_dt_noalloc: null array pointer");
   if (!(cfl > 0)) return fail(STREAMS_B200_EINVAL, "compute_dt_noalloc: cfl must be positive");
+  // one constant gamma: a thermally perfect gas (gamma(T) per cell) must use the context's
+  // streams_b200_compute_dt; nonsense constants are refused rather than giving a wrong dt
+  if (!(gamma > 1)) return fail(STREAMS_B200_EINVAL, "compute_dt_noalloc: gamma must exceed 1 (calorically perfect gas)");
+  if (!(rgas0 > 0)) return fail(STREAMS_B200_EINVAL, "compute_dt_noalloc: rgas0 must be positive");
+  if (!(prandtl > 0)) return fail(STREAMS_B200_EINVAL, "compute_dt_noalloc: prandtl must be positive");
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(STREAMS_B200_ENODEV, std::string("cudaGetDevice: ") + cudaGetErrorString(e));

@@ -1698,4 +1698,10 @@ bool stage_supported(int lmax_base, int weno_scheme) {
          (lmax_base == 4 && weno_scheme == 4) || (lmax_base == 3 && weno_scheme == 2);
 }
 
+// binaryVersion of this file's kernels as the driver loaded them (architecture check)
+int binary_version_stage() {
+  cudaFuncAttributes a;
+  return cudaFuncGetAttributes(&a, k_add_time) == cudaSuccess ? a.binaryVersion : -1;
+}
+
 }  // namespace sb200

@@ -278,4 +278,10 @@ cudaError_t launch_stats3d(const Geom& g, DevState& d, int itav, cudaStream_t s,
   return cudaGetLastError();
 }
 
+// binaryVersion of this file's kernels as the driver loaded them (architecture check)
+int binary_version_stats() {
+  cudaFuncAttributes a;
+  return cudaFuncGetAttributes(&a, k_stats_vel<double>) == cudaSuccess ? a.binaryVersion : -1;
+}
+
 }  // namespace sb200

@@ -19,16 +19,42 @@ module streams_equation_singleideal_b200_object
     integer, allocatable, dimension(:) :: epx, epy, epz
     ! recycling inflow: wmean(1-i, j, 1:4), i = 1..ng, of the equation object, contiguous
     real(c_double), allocatable, dimension(:,:,:) :: wmean_inflow
-    ! rank of this process and the crandom draws the set-up took (init_bl: 3 per cell)
+    ! rank of this process and the crandom draws the set-up took (setup_draws)
     integer(c_int) :: myrank = 0
     integer(c_long_long) :: crandom_draws = 0
   contains
     procedure, pass(self) :: initialize
     procedure, pass(self) :: run
     procedure, pass(self) :: check
+    procedure, pass(self) :: setup_draws
   endtype equation_singleideal_b200_object
 
 contains
+
+  ! crandom draws that the equation object's set-up took on this rank before the first step.
+  ! initial_conditions runs on restarts too (singleideal.F90:710-712), so the count does not
+  ! depend on restart_type.  The boundary layer (flow_init = 1, turbulent) draws 3 per interior
+  ! cell in init_bl (singleideal.F90:3386-3392), then add_synthetic_perturbations draws the 4
+  ! streak phases (:3631) and 3 per cell below the local thickness deltavec (:3663-3666).
+  ! Other initialisations draw nothing that a later step depends on (no recycling inflow).
+  function setup_draws(self) result(nd)
+    class(equation_singleideal_b200_object), intent(in) :: self
+    integer(c_long_long) :: nd
+    integer :: i, j, k, ii
+    nd = 0_c_long_long
+    associate(eb => self%equation_base, f => self%equation_base%field)
+      if (eb%flow_init /= 1 .or. eb%bl_laminar) return
+      nd = 3_c_long_long * f%nx * f%ny * f%nz + 4_c_long_long
+      do k = 1, f%nz
+        do j = 1, f%ny
+          do i = 1, f%nx
+            ii = f%ncoords(1) * f%nx + i
+            if (f%y(j) < eb%deltavec(ii)) nd = nd + 3_c_long_long
+          enddo
+        enddo
+      enddo
+    endassociate
+  endfunction setup_draws
 
   subroutine check(self, rc, what)
     class(equation_singleideal_b200_object), intent(inout) :: self
@@ -78,8 +104,12 @@ contains
       p%cp_coeff = 0._rkind ; p%cv_coeff = 0._rkind
       p%cp_coeff(1:eb%indx_cp_r-eb%indx_cp_l+2) = eb%cp_coeff(eb%indx_cp_l:eb%indx_cp_r+1)
       p%cv_coeff(1:eb%indx_cp_r-eb%indx_cp_l+2) = eb%cv_coeff(eb%indx_cp_l:eb%indx_cp_r+1)
-      ! the crandom sequence continues on the device: seed of this rank and the draws taken so far
-      p%rng_seed = self%myrank + 1 ; p%rng_draws = self%crandom_draws
+      ! the crandom sequence continues on the device: the seed of this rank (init_crandom_f,
+      ! singleideal.F90:314-323) and the draws the set-up took, both known before create
+      self%myrank = eb%myrank
+      self%crandom_draws = self%setup_draws()
+      ! (rand_type = 0 seeds 0, which the device takes as draws rescaled to zero)
+      p%rng_seed = merge(0, self%myrank + 1, eb%rand_type == 0) ; p%rng_draws = self%crandom_draws
       allocate(self%epx(0:f%nx), self%epy(0:f%ny), self%epz(0:f%nz))
       do i = 0, f%nx ; self%epx(i) = eb%ep_ord_change(i,1,1,1) ; enddo
       do j = 0, f%ny ; self%epy(j) = eb%ep_ord_change(1,j,1,2) ; enddo
@@ -96,7 +126,6 @@ contains
         do i = 1, f%grid%ng
           self%wmean_inflow(i, :, :) = eb%wmean(1-i, 1:f%ny, 1:4)
         enddo
-        self%crandom_draws = 3_c_long_long * f%nx * f%ny * f%nz
         g%wmean_inflow = c_loc(self%wmean_inflow) ; g%weta_inflow = c_loc(eb%weta_inflow)
         g%yplus_inflow = c_loc(eb%yplus_inflow) ; g%eta_inflow = c_loc(eb%eta_inflow)
         g%yplus_recyc = c_loc(eb%yplus_recyc) ; g%eta_recyc = c_loc(eb%eta_recyc)

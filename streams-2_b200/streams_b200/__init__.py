@@ -5,8 +5,8 @@ This is a thin host-side mirror of the solver-object interface of STREAmS-2
 ``Solver`` wraps one device context and exposes ``init_run``, ``compute_dt``, ``rk_sync``,
 ``compute_residual``, ``copy_from_field``/``copy_to_field`` and a no-sync ``advance`` loop;
 ``Case`` wraps the host set-up of a ``singleideal.ini`` case.  All compute happens in the
-compiled library ``lib/libstreams_b200.so``; importing this module fails loudly when the
-library is missing.
+compiled library ``lib/libstreams_b200.so``, mapped on the first call into it; that call fails
+loudly when the library is missing.
 """
 from __future__ import annotations
 
@@ -117,6 +117,7 @@ def _load() -> C.CDLL:
         "streams_b200_profile_read": (I, [P, I, D, C.POINTER(LL)]),
         "streams_b200_kernel_count": (I, []),
         "streams_b200_kernel_name": (C.c_char_p, [I]),
+        "streams_b200_kernel_binary_versions": (I, [C.POINTER(C.c_int), I]),
         "streams_b200_compute_dt_noalloc": (I, [I, I, I, I] + [V] * 8 + [C.c_double] * 4 + [V, V]),
         "streams_b200_case_load": (I, [C.c_char_p, C.c_char_p, C.POINTER(P)]),
         "streams_b200_case_free": (I, [P]),
@@ -151,7 +152,24 @@ def _load() -> C.CDLL:
     return lib
 
 
-lib = _load()
+class _Library:
+    """The compiled library, mapped on first use: importing the package (for example for the
+    input-file builders of ``streams_b200.cases``) maps no shared object, and the first call
+    into the C ABI fails loudly when the library is missing.  There is no CPU fallback."""
+
+    def __init__(self):
+        self._cdll = None
+
+    def _get(self) -> C.CDLL:
+        if self._cdll is None:
+            self._cdll = _load()
+        return self._cdll
+
+    def __getattr__(self, name):
+        return getattr(self._get(), name)
+
+
+lib = _Library()
 
 # Every symbol the C headers declare (checked by the CPU test suite).
 EXPORTED = [
@@ -165,7 +183,7 @@ EXPORTED = [
     "streams_b200_set_stats",
     "streams_b200_launch_count", "streams_b200_debug_fetch", "streams_b200_get_stream",
     "streams_b200_profile_enable", "streams_b200_profile_read", "streams_b200_kernel_count",
-    "streams_b200_kernel_name", "streams_b200_compute_dt_noalloc", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
+    "streams_b200_kernel_name", "streams_b200_kernel_binary_versions", "streams_b200_compute_dt_noalloc", "streams_b200_case_load", "streams_b200_case_free", "streams_b200_case_error",
     "streams_b200_case_params", "streams_b200_case_grid", "streams_b200_case_field", "streams_b200_case_info",
     "streams_b200_case_write_restart", "streams_b200_case_write_state", "streams_b200_run_case",
     "streams_b200_run_case_stats", "streams_b200_case_write_state_stats", "streams_b200_case_stats_info",

@@ -12,7 +12,7 @@ The runner splits each patch on the first ',' of every ';'-separated item, so th
 ``controls,num_iter=10,controls,rand_type=0`` sets num_iter to "10,controls,rand_type=0"
 (read back as 10 by Fortran list-directed input) and leaves rand_type at its example value.
 
-Usage:  python tests/golden/make_golden.py [reference root]   (default /root/reference)
+Usage:  python tests/golden/make_golden.py <reference root>   (the STREAmS-2 source tree)
 """
 import json
 import sys
@@ -50,7 +50,9 @@ def patch_items(line):
 
 
 def main():
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the STREAmS-2 source tree>")
+    ref = Path(sys.argv[1])
     tests = (ref / "tests" / "tests.ini").read_text().splitlines()
     tests = [t.strip() for t in tests if t.strip()]
     i = tests.index("[subsonic_channel]")

@@ -28,12 +28,25 @@ def test_library_exports_every_declared_symbol():
     assert set(streams_b200.EXPORTED) <= set(names)
 
 
-def test_library_is_built_for_sm100a():
-    import subprocess
+def test_library_build_targets_sm100a():
+    """The build recipe compiles every CUDA source for sm_100a only (no other architecture, no
+    PTX for JIT); the device-side check of the loaded image is test_loaded_kernels_are_sm100."""
+    text = (ROOT / "streams-2_b200" / "Makefile").read_text()
+    flags = re.findall(r"-gencode\s+arch=(\S+),code=(\S+)", text)
+    assert flags and all(f == ("compute_100a", "sm_100a") for f in flags), flags
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not gpu_available(), reason="no CUDA device")
+def test_loaded_kernels_are_sm100():
+    """The kernels the driver loaded from the library are sm_100 binaries (binaryVersion 100,
+    from cudaFuncGetAttributes on one kernel of every source file)."""
     import streams_b200
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", str(streams_b200.LIB_PATH)],
-                         capture_output=True, text=True)
-    assert "sm_100a" in out.stdout, out.stdout[-500:]
+    streams_b200.Solver  # noqa: B018  (the library is mapped on first use)
+    versions = (C.c_int * 8)()
+    n = streams_b200.lib.streams_b200_kernel_binary_versions(versions, 8)
+    assert n == 3, n
+    assert all(versions[q] == 100 for q in range(n)), list(versions)[:n]
 
 
 def test_abi_version():

@@ -52,3 +52,14 @@ def test_compute_dt_noalloc_rejects_oversized_input():
     rc = lib.streams_b200_compute_dt_noalloc(n, n, n, 3, *([1] * 8), 1.0, 0.72, 1.4, 0.8, 1, None)
     assert rc == EINVAL
     assert "static scratch limit" in lib.streams_b200_global_error().decode()
+
+
+@pytest.mark.parametrize("gamma,rgas0,prandtl", [(1.0, 1.0, 0.72), (0.5, 1.0, 0.72), (float("nan"), 1.0, 0.72),
+                                                  (1.4, 0.0, 0.72), (1.4, 1.0, -1.0)])
+def test_compute_dt_noalloc_rejects_bad_gas_constants(gamma, rgas0, prandtl):
+    # one constant gamma serves only a calorically perfect gas; nonsense constants are refused
+    # before any device work (a thermally perfect case must call the context's compute_dt)
+    from streams_b200 import EINVAL, lib
+    rc = lib.streams_b200_compute_dt_noalloc(8, 8, 8, 3, *([1] * 8), rgas0, prandtl, gamma, 0.8, 1, None)
+    assert rc == EINVAL
+    assert "compute_dt_noalloc" in lib.streams_b200_global_error().decode()
