@@ -127,6 +127,7 @@ def test_bl_inflow_draws_continue_the_setup_sequence(tmp_path):
     assert p.rng_draws > 0 and p.rng_seed == 1
     p.rng_draws = 0
     s0 = Solver(p, case.grid(), keepalive=case)
+    s0.copy_from_field(case.field())
     s0.init_run()
     s0.advance(3)
     g = o.ng
