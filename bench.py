@@ -59,6 +59,46 @@ ALG_BYTES_PER_CELL = {
 PASSES_PER_STEP = {"k_aux": 3, "k_euler_x": 3, "k_visc": 3, "k_euler_y": 3, "k_euler_z": 3, "k_update": 3, "k_dt": 1}
 # Compulsory traffic of a whole RK3 step per cell (state read/written once per stage, RK register).
 STEP_BYTES_PER_CELL = 440
+# FP64 roofline of the flux passes: operations per WENO face and per central face counted
+# through the oracle's face-flux code (profiles/fp64_flops.json, written by
+# oracle/count_flops.py), plus the divergence (10 per cell), times the faces of the direction
+FLUX_DIR = {"k_euler_x": 0, "k_euler_y": 1, "k_euler_z": 2}
+# nominal FP64 rate of a B200: 148 SMs x 64 FMA lanes x 2 flops x 1.965 GHz
+NOMINAL_FP64_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+
+
+def flux_flops(kernel, nx, ny, nz, weno_fraction, scheme="weno5_central6"):
+    f = ROOT / "profiles" / "fp64_flops.json"
+    if kernel not in FLUX_DIR or not f.exists():
+        return None
+    d = json.loads(f.read_text())
+    sc = d["schemes"][scheme]
+    dr = FLUX_DIR[kernel]
+    faces = nx * ny * nz * ((nx, ny, nz)[dr] + 1) / (nx, ny, nz)[dr]
+    fw = weno_fraction[dr]
+    per_face = fw * sc["weno_face"]["flops"] + (1 - fw) * sc["central_face"]["flops"]
+    return faces * per_face + nx * ny * nz * d["divergence_per_cell_per_direction"]
+
+
+def fp64_peak(torch):
+    """Measured FP64 rate of this GPU: cuBLAS DGEMM (torch.matmul, float64, 8192^3), best of 5
+    by CUDA events; the nominal rate is reported beside it."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
 
 
 def parse_size(s):
@@ -233,8 +273,10 @@ def run_serving(torch, duration_s, step_scale, single_rate, tune_cache):
             "p50_s": out["p50_s"], "p99_s": out["p99_s"], "mean_s": out["mean_s"],
             "mcell_steps_per_s": out["mcell_steps_per_s"], "mcell_steps_per_busy_s": out["mcell_steps_per_busy_s"],
             "max_resident": out["max_resident"], "ticks": out["ticks"], "budget_gb": budget / 1e9,
-            "offered_mcell_steps_per_s": work / duration_s / 1e6, "host_admit_s": out["admit_s"],
-            "host_batch_build_s": out["batch_build_s"]}
+            "offered_mcell_steps_per_s": work / duration_s / 1e6, "loop_admit_wait_s": out["admit_wait_s"],
+            "loop_iterations": out["loop_iterations"],
+            "loop": "admission (tuning, context, first step, graph capture) on 2 admission threads; each "
+                    "resident solve gets its next 10-step tick when its stream reports the last one done"}
 
 
 def cpu_oracle_rate(workload, nx, ny, nz, nsteps, budget_s=20.0):
@@ -387,6 +429,7 @@ def main():
     # timed region: device-resident state, CUDA events on the context's stream
     barrier()
     l0 = s.launches
+    weno_before = s.count_weno()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         ev0.record(stream)
@@ -396,6 +439,8 @@ def main():
         barrier()
     icyc += args.steps
     launches = s.launches - l0
+    weno_after = s.count_weno()
+    weno_mean = [(a_ + b_) / 2 for a_, b_ in zip(weno_before, weno_after)]
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     value = ncell * args.steps * world / (ms / 1e3) / 1e6
 
@@ -428,6 +473,22 @@ def main():
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                 "alg_bytes_per_cell": ALG_BYTES_PER_CELL[dom], "launch_ms": dom_ms,
                 "share": prof[dom][0] / total_prof}
+    # the flux passes are FP64-bound: their counted operations against the measured DGEMM rate
+    roofline_fp64 = None
+    dflops = flux_flops(dom, nx, ny, nz, weno_mean)
+    if dflops is not None:
+        pk = fp64_peak(torch)
+        ach = dflops / (dom_ms / 1e3) / 1e12
+        step_flux = sum(flux_flops(k, nx, ny, nz, weno_mean) for k in FLUX_DIR)
+        step_ms_flux = sum(prof[k][0] for k in FLUX_DIR if k in prof) / args.steps
+        roofline_fp64 = {"bound": "fp64", "kernel": dom, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                         "frac": ach / pk, "peak_kind": "measured (cuBLAS DGEMM 8192^3, float64)",
+                         "nominal_peak": NOMINAL_FP64_TFLOPS, "frac_of_nominal": ach / NOMINAL_FP64_TFLOPS,
+                         "flops_per_launch": dflops, "weno_face_fraction_xyz": [round(x, 4) for x in weno_mean],
+                         "flops_source": "profiles/fp64_flops.json (oracle/count_flops.py)",
+                         "three_flux_passes": {"tflops": step_flux * 3 / (step_ms_flux / 1e3) / 1e12,
+                                               "ms_per_step": step_ms_flux}}
+        roofline["binding"] = "fp64 (see roofline_fp64): the flux passes do ~10 FP64 operations per byte"
     step_gbs = STEP_BYTES_PER_CELL * ncell * args.steps / (ms / 1e3) / 1e9
     step_roofline = {"bytes_per_cell_step": STEP_BYTES_PER_CELL, "achieved": step_gbs, "peak": peak,
                      "frac": step_gbs / peak, "unit": "GB/s", "peak_kind": peak_kind}
@@ -601,7 +662,7 @@ def main():
             "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": nbytes / args.steps,
                     "d2h_bytes_per_step": (nbytes + 56 * args.steps) / args.steps, "wall_s": wall,
                     "what": "copy_from_field (pinned) + init_run + K x (rk step + scalar read) + copy_to_field"},
-            "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
+            "roofline": roofline, "roofline_fp64": roofline_fp64, "step_roofline": step_roofline, "kernels": kernels,
             "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "mixed": mixed,
             "batched": batched, "serving": serving,
             "weno_face_fraction_xyz": weno_timed, "developed": developed, "full_run": full_run,

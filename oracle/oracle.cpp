@@ -6,6 +6,7 @@
 #include <cmath>
 #include <limits>
 
+#include "flops.hpp"
 #include "par_for.hpp"
 
 namespace streams_oracle {
@@ -13,8 +14,10 @@ namespace streams_oracle {
 namespace {
 
 // wenorec_1d (kernels_cpu.F90:2526-2724).  vp, vm: [5][8] with Fortran index l = 1..8 at [m][l-1].
-void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], int iweno, int ord, int version,
-                double rho0, double u0, bool rusanov = false) {
+template <class T>
+void wenorec_1d(const T vp[5][8], const T vm[5][8], T vhat[5], int iweno, int ord, int version, double rho0,
+                double u0, bool rusanov = false) {
+  using std::fabs;
   auto VP = [&](int m, int l) { return vp[m][l - 1]; };
   auto VM = [&](int m, int l) { return vm[m][l - 1]; };
   double u0_2 = u0 * u0;
@@ -40,7 +43,7 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
   } else if (ord == 2) {
     double dwe[2] = {1.0 / 3.0, 2.0 / 3.0};
     for (int m = 0; m < 5; ++m) {
-      double bp[2], bm[2];
+      T bp[2], bm[2];
       bp[0] = (VP(m, i) - VP(m, i - 1)) * (VP(m, i) - VP(m, i - 1));
       bp[1] = (VP(m, i + 1) - VP(m, i)) * (VP(m, i + 1) - VP(m, i));
       bp[1] = betascale[m] * bp[1];
@@ -49,9 +52,9 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
       bm[1] = (VM(m, i + 1) - VM(m, i)) * (VM(m, i + 1) - VM(m, i));
       bm[1] = betascale[m] * bm[1];
       bm[0] = betascale[m] * bm[0];
-      double sump = 0.0, summ = 0.0;
+      T sump = 0.0, summ = 0.0;
       for (int l = 0; l < 2; ++l) {
-        double tp = 0.000001 + bp[l], tm = 0.000001 + bm[l];
+        T tp = 0.000001 + bp[l], tm = 0.000001 + bm[l];
         bp[l] = dwe[l] / (tp * tp);
         bm[l] = dwe[l] / (tm * tm);
         sump = sump + bp[l];
@@ -61,17 +64,17 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
         bp[l] = bp[l] / sump;
         bm[l] = bm[l] / summ;
       }
-      double vminus = bp[0] * (-VP(m, i - 1) + 3 * VP(m, i)) + bp[1] * (VP(m, i) + VP(m, i + 1));
-      double vplus = bm[0] * (-VM(m, i + 2) + 3 * VM(m, i + 1)) + bm[1] * (VM(m, i) + VM(m, i + 1));
+      T vminus = bp[0] * (-VP(m, i - 1) + 3 * VP(m, i)) + bp[1] * (VP(m, i) + VP(m, i + 1));
+      T vplus = bm[0] * (-VM(m, i + 2) + 3 * VM(m, i + 1)) + bm[1] * (VM(m, i) + VM(m, i + 1));
       vhat[m] = 0.5 * (vminus + vplus);
     }
   } else if (ord == 3) {
     const double dwe[3] = {1.0 / 10.0, 6.0 / 10.0, 3.0 / 10.0};
     const double d0 = 13.0 / 12.0, d1 = 1.0 / 4.0;
     const double c0 = 1.0 / 3.0, c1 = 5.0 / 6.0, c2 = -1.0 / 6.0, c3 = -7.0 / 6.0, c4 = 11.0 / 6.0;
-    auto sq = [](double a) { return a * a; };
+    auto sq = [](T a) { return a * a; };
     for (int m = 0; m < 5; ++m) {
-      double bp[3], bm[3];
+      T bp[3], bm[3];
       bp[2] = d0 * sq(VP(m, i) - 2.0 * VP(m, i + 1) + VP(m, i + 2)) +
               d1 * sq(3.0 * VP(m, i) - 4.0 * VP(m, i + 1) + VP(m, i + 2));
       bp[1] = d0 * sq(VP(m, i - 1) - 2.0 * VP(m, i) + VP(m, i + 1)) + d1 * sq(VP(m, i - 1) - VP(m, i + 1));
@@ -89,9 +92,9 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
       bm[1] = betascale[m] * bm[1];
       bm[0] = betascale[m] * bm[0];
       if (version == 0) {
-        double sump = 0.0, summ = 0.0;
+        T sump = 0.0, summ = 0.0;
         for (int l = 0; l < 3; ++l) {
-          double tp = 0.000001 + bp[l], tm = 0.000001 + bm[l];
+          T tp = 0.000001 + bp[l], tm = 0.000001 + bm[l];
           bp[l] = dwe[l] / (tp * tp);
           bm[l] = dwe[l] / (tm * tm);
           sump = sump + bp[l];
@@ -104,13 +107,13 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
       } else {
         // eps40 is a default-kind (single precision) literal in the reference
         const double eps40 = static_cast<double>(1.e-35f);
-        double tau5p = std::fabs(bp[0] - bp[2]) + eps40;
-        double tau5m = std::fabs(bm[0] - bm[2]) + eps40;
+        T tau5p = fabs(bp[0] - bp[2]) + eps40;
+        T tau5m = fabs(bm[0] - bm[2]) + eps40;
         for (int l = 0; l < 3; ++l) {
           bp[l] = (bp[l] + eps40) / (bp[l] + tau5p);
           bm[l] = (bm[l] + eps40) / (bm[l] + tau5m);
         }
-        double sump = 0.0, summ = 0.0;
+        T sump = 0.0, summ = 0.0;
         for (int l = 0; l < 3; ++l) {
           bp[l] = dwe[l] / bp[l];
           bm[l] = dwe[l] / bm[l];
@@ -122,10 +125,10 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
           bm[l] = bm[l] / summ;
         }
       }
-      double vminus = bp[2] * (c0 * VP(m, i) + c1 * VP(m, i + 1) + c2 * VP(m, i + 2)) +
+      T vminus = bp[2] * (c0 * VP(m, i) + c1 * VP(m, i + 1) + c2 * VP(m, i + 2)) +
                       bp[1] * (c2 * VP(m, i - 1) + c1 * VP(m, i) + c0 * VP(m, i + 1)) +
                       bp[0] * (c0 * VP(m, i - 2) + c3 * VP(m, i - 1) + c4 * VP(m, i));
-      double vplus = bm[2] * (c0 * VM(m, i + 1) + c1 * VM(m, i) + c2 * VM(m, i - 1)) +
+      T vplus = bm[2] * (c0 * VM(m, i + 1) + c1 * VM(m, i) + c2 * VM(m, i - 1)) +
                      bm[1] * (c2 * VM(m, i + 2) + c1 * VM(m, i + 1) + c0 * VM(m, i)) +
                      bm[0] * (c0 * VM(m, i + 3) + c3 * VM(m, i + 2) + c4 * VM(m, i + 1));
       vhat[m] = vminus + vplus;
@@ -133,9 +136,9 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
   } else if (ord == 4) {
     const double dwe[4] = {1.0 / 35.0, 12.0 / 35.0, 18.0 / 35.0, 4.0 / 35.0};
     const double d1 = 1.0 / 36.0, d2 = 13.0 / 12.0, d3 = 781.0 / 720.0;
-    auto sq = [](double a) { return a * a; };
+    auto sq = [](T a) { return a * a; };
     for (int m = 0; m < 5; ++m) {
-      double bp[4], bm[4];
+      T bp[4], bm[4];
       bp[3] = d1 * sq(-11 * VP(m, i) + 18 * VP(m, i + 1) - 9 * VP(m, i + 2) + 2 * VP(m, i + 3)) +
               d2 * sq(2 * VP(m, i) - 5 * VP(m, i + 1) + 4 * VP(m, i + 2) - VP(m, i + 3)) +
               d3 * sq(-VP(m, i) + 3 * VP(m, i + 1) - 3 * VP(m, i + 2) + VP(m, i + 3));
@@ -162,9 +165,9 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
               d2 * sq(-VM(m, i + 4) + 4 * VM(m, i + 3) - 5 * VM(m, i + 2) + 2 * VM(m, i + 1)) +
               d3 * sq(-VM(m, i + 4) + 3 * VM(m, i + 3) - 3 * VM(m, i + 2) + VM(m, i + 1));
       for (int l = 3; l >= 0; --l) bm[l] = betascale[m] * bm[l];
-      double sump = 0.0, summ = 0.0;
+      T sump = 0.0, summ = 0.0;
       for (int l = 0; l < 4; ++l) {
-        double tp = 0.000001 + bp[l], tm = 0.000001 + bm[l];
+        T tp = 0.000001 + bp[l], tm = 0.000001 + bm[l];
         bp[l] = dwe[l] / (tp * tp);
         bm[l] = dwe[l] / (tm * tm);
         sump = sump + bp[l];
@@ -174,11 +177,11 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
         bp[l] = bp[l] / sump;
         bm[l] = bm[l] / summ;
       }
-      double vminus = bp[3] * (6 * VP(m, i) + 26 * VP(m, i + 1) - 10 * VP(m, i + 2) + 2 * VP(m, i + 3)) +
+      T vminus = bp[3] * (6 * VP(m, i) + 26 * VP(m, i + 1) - 10 * VP(m, i + 2) + 2 * VP(m, i + 3)) +
                       bp[2] * (-2 * VP(m, i - 1) + 14 * VP(m, i) + 14 * VP(m, i + 1) - 2 * VP(m, i + 2)) +
                       bp[1] * (2 * VP(m, i - 2) - 10 * VP(m, i - 1) + 26 * VP(m, i) + 6 * VP(m, i + 1)) +
                       bp[0] * (-6 * VP(m, i - 3) + 26 * VP(m, i - 2) - 46 * VP(m, i - 1) + 50 * VP(m, i));
-      double vplus = bm[3] * (6 * VM(m, i + 1) + 26 * VM(m, i) - 10 * VM(m, i - 1) + 2 * VM(m, i - 2)) +
+      T vplus = bm[3] * (6 * VM(m, i + 1) + 26 * VM(m, i) - 10 * VM(m, i - 1) + 2 * VM(m, i - 2)) +
                      bm[2] * (-2 * VM(m, i + 2) + 14 * VM(m, i + 1) + 14 * VM(m, i) - 2 * VM(m, i - 1)) +
                      bm[1] * (2 * VM(m, i + 3) - 10 * VM(m, i + 2) + 26 * VM(m, i + 1) + 6 * VM(m, i)) +
                      bm[0] * (-6 * VM(m, i + 4) + 26 * VM(m, i + 3) - 46 * VM(m, i + 2) + 50 * VM(m, i + 1));
@@ -189,10 +192,11 @@ void wenorec_1d(const double vp[5][8], const double vm[5][8], double vhat[5], in
 
 // eigenvectors_x / _y / _z (kernels_cpu.F90:2728-2782, 2842-2896, 2956-3010).
 // el[r][c], er[r][c] hold the reference's el(r+1,c+1), er(r+1,c+1).
-void eigenvectors(int dir, double b1, double b2, double b3, double uu, double vv, double ww, double c, double ci,
-                  double h, double el[5][5], double er[5][5]) {
-  const double vel[3] = {uu, vv, ww};
-  const double vn = vel[dir];
+template <class T>
+void eigenvectors(int dir, T b1, T b2, T b3, T uu, T vv, T ww, T c, T ci,
+                  T h, T el[5][5], T er[5][5]) {
+  const T vel[3] = {uu, vv, ww};
+  const T vn = vel[dir];
   // left eigenvectors: columns 1 and 5 (acoustic), 2 (entropy), 3 and 4 (tangential)
   el[0][0] = 0.5 * (b1 + vn * ci);
   el[1][0] = -0.5 * (dir == 0 ? b2 * uu + ci : b2 * uu);
@@ -652,9 +656,15 @@ void Solver::compute_aux(int central, int ghost) {
 // Hybrid convective flux at one face (euler_x_fluxes_hybrid_kernel kernels_cpu.F90:425-689,
 // euler_z_hybrid_kernel :1063-1325, euler_y_hybrid_kernel :1808-2071).  The face lies between
 // the point (i,j,k) and its neighbour +1 along dir.
-void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
+template <class T>
+void Solver::face_flux_t(int dir, int i, int j, int k, T fh[5]) const {
+  using std::fabs;
+  using std::log;
+  using std::max;
+  using std::pow;
+  using std::sqrt;
   const int ex = dir == 0, ey = dir == 1, ez = dir == 2;
-  auto at = [&](int o, int m) { return A(i + o * ex, j + o * ey, k + o * ez, m); };
+  auto at = [&](int o, int m) { return T(A(i + o * ex, j + o * ey, k + o * ez, m)); };
   const int pos = dir == 0 ? i : (dir == 1 ? j : k);
   const int nd = dir == 0 ? nx : (dir == 1 ? ny : nz);
   const int ws = s.weno_scheme;
@@ -664,35 +674,35 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
     if (at(o, 8) > s.sensor_threshold) ishk = 1;
   const int epo = s.ep_ord[dir][pos];
   if (ishk == 0) {
-    double ft1 = 0, ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
-    const int lmax = std::max(s.ep_order / 2 + epo, 1);
+    T ft1 = 0, ft2 = 0, ft3 = 0, ft4 = 0, ft5 = 0, ft6 = 0;
+    const int lmax = max(s.ep_order / 2 + epo, 1);
     for (int l = 1; l <= lmax; ++l) {
-      double uvs1 = 0, uvs2 = 0, uvs3 = 0, uvs4 = 0, uvs5 = 0, uvs5_i = 0, uvs5_k = 0, uvs5_p = 0, uvs6 = 0;
+      T uvs1 = 0, uvs2 = 0, uvs3 = 0, uvs4 = 0, uvs5 = 0, uvs5_i = 0, uvs5_k = 0, uvs5_p = 0, uvs6 = 0;
       for (int m = 0; m <= l - 1; ++m) {
-        double rhoi = at(-m, 1), uui = at(-m, 2), vvi = at(-m, 3), wwi = at(-m, 4), enti = at(-m, 5),
+        T rhoi = at(-m, 1), uui = at(-m, 2), vvi = at(-m, 3), wwi = at(-m, 4), enti = at(-m, 5),
                tti = at(-m, 6);
-        double ppi = tti * rhoi * rgas0;
-        double rhoip = at(-m + l, 1), uuip = at(-m + l, 2), vvip = at(-m + l, 3), wwip = at(-m + l, 4),
+        T ppi = tti * rhoi * rgas0;
+        T rhoip = at(-m + l, 1), uuip = at(-m + l, 2), vvip = at(-m + l, 3), wwip = at(-m + l, 4),
                entip = at(-m + l, 5), ttip = at(-m + l, 6);
-        double ppip = ttip * rhoip * rgas0;
-        const double vni = dir == 0 ? uui : (dir == 1 ? vvi : wwi);
-        const double vnip = dir == 0 ? uuip : (dir == 1 ? vvip : wwip);
-        double rhom = rhoi + rhoip;
+        T ppip = ttip * rhoip * rgas0;
+        const T vni = dir == 0 ? uui : (dir == 1 ? vvi : wwi);
+        const T vnip = dir == 0 ? uuip : (dir == 1 ? vvip : wwip);
+        T rhom = rhoi + rhoip;
         if (s.nkeep >= 0) {
-          double eei = enti - ppi / rhoi - 0.5 * (uui * uui + vvi * vvi + wwi * wwi);
-          double eeip = entip - ppip / rhoip - 0.5 * (uuip * uuip + vvip * vvip + wwip * wwip);
-          double eem = eei + eeip;
-          double drhof = 1.0, deef = 1.0;
+          T eei = enti - ppi / rhoi - 0.5 * (uui * uui + vvi * vvi + wwi * wwi);
+          T eeip = entip - ppip / rhoip - 0.5 * (uuip * uuip + vvip * vvip + wwip * wwip);
+          T eem = eei + eeip;
+          T drhof = 1.0, deef = 1.0;
           if (s.nkeep != 0) {
-            double sumnumrho = 1.0;
-            double drho = 2.0 * (rhoip - rhoi) / rhom;
-            double dee = 2.0 * (eeip - eei) / eem;
-            double t_sumdenrho = (0.5 * drho) * (0.5 * drho);
-            double t_sumdenee = (0.5 * dee) * (0.5 * dee);
-            double t2_sumdenrho = t_sumdenrho, t2_sumdenee = t_sumdenee;
-            double sumdenrho = 1.0 + t_sumdenrho / 3.0;
-            double sumdenee = 1.0 + t_sumdenee;
-            double sumnumee = 1.0 + t_sumdenee / 3.0;
+            T sumnumrho = 1.0;
+            T drho = 2.0 * (rhoip - rhoi) / rhom;
+            T dee = 2.0 * (eeip - eei) / eem;
+            T t_sumdenrho = (0.5 * drho) * (0.5 * drho);
+            T t_sumdenee = (0.5 * dee) * (0.5 * dee);
+            T t2_sumdenrho = t_sumdenrho, t2_sumdenee = t_sumdenee;
+            T sumdenrho = 1.0 + t_sumdenrho / 3.0;
+            T sumdenee = 1.0 + t_sumdenee;
+            T sumnumee = 1.0 + t_sumdenee / 3.0;
             for (int n = 2; n <= s.nkeep; ++n) {
               int n2 = 2 * n;
               t_sumdenrho = t2_sumdenrho * t_sumdenrho;
@@ -704,7 +714,7 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
             drhof = sumnumrho / sumdenrho;
             deef = sumnumee / sumdenee;
           }
-          double uv_part = (vni + vnip) * rhom * drhof;
+          T uv_part = (vni + vnip) * rhom * drhof;
           uvs1 = uvs1 + uv_part * 2.0;
           uvs2 = uvs2 + uv_part * (uui + uuip);
           uvs3 = uvs3 + uv_part * (vvi + vvip);
@@ -714,7 +724,7 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
           uvs5_p = uvs5_p + 4.0 * (vni * ppip + vnip * ppi);
           uvs6 = uvs6 + 2.0 * (ppi + ppip);
         } else {
-          double uv_part = (vni + vnip) * rhom;
+          T uv_part = (vni + vnip) * rhom;
           uvs1 = uvs1 + uv_part * 2.0;
           uvs2 = uvs2 + uv_part * (uui + uuip);
           uvs3 = uvs3 + uv_part * (vvi + vvip);
@@ -746,24 +756,24 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
     // Rusanov (component-wise local Lax-Friedrichs) WENO branch of the *_hybrid_rusanov kernels
     // (kernels_cpu.F90:692-941 for x): stencil maximum of |u_n -+ c|, split of the conserved
     // fluxes, wenorec_1d_rusanov
-    double evmax = -1.0;
+    T evmax = -1.0;
     for (int l = 1; l <= 2 * ws; ++l) {
       const int o = l - ws;
-      const double un = at(o, 2 + dir), tt = at(o, 6);
-      const double c = std::sqrt(gamloc_at(tt) * rgas0 * tt);
-      const double evm = std::max(std::fabs(un - c), std::fabs(un + c));
-      evmax = std::max(evm, evmax);
+      const T un = at(o, 2 + dir), tt = at(o, 6);
+      const T c = sqrt(T(gamloc_at(static_cast<double>(tt))) * rgas0 * tt);
+      const T evm = max(fabs(un - c), fabs(un + c));
+      evmax = max(evm, evmax);
     }
-    double gp[5][8], gm[5][8];
+    T gp[5][8], gm[5][8];
     for (int l = 1; l <= 2 * ws; ++l) {
       const int o = l - ws;
-      const double rho = at(o, 1), h = at(o, 5);
-      const double vel[3] = {at(o, 2), at(o, 3), at(o, 4)};
-      const double rhou = rho * vel[dir];
-      const double pp = rho * at(o, 6) * rgas0;
-      const double rhoevm = rho * evmax;
-      double evm = rhou;
-      double c = 0.5 * (evm + rhoevm);
+      const T rho = at(o, 1), h = at(o, 5);
+      const T vel[3] = {at(o, 2), at(o, 3), at(o, 4)};
+      const T rhou = rho * vel[dir];
+      const T pp = rho * at(o, 6) * rgas0;
+      const T rhoevm = rho * evmax;
+      T evm = rhou;
+      T c = 0.5 * (evm + rhoevm);
       gp[0][l - 1] = c;
       gm[0][l - 1] = evm - c;
       for (int d = 0; d < 3; ++d) {
@@ -778,88 +788,88 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
       gp[4][l - 1] = c;
       gm[4][l - 1] = evm - c;
     }
-    const int ord = std::max(ws + epo, 1);
+    const int ord = max(ws + epo, 1);
     wenorec_1d(gp, gm, fh, ws, ord, s.weno_version, s.rho0, s.u0, true);
   } else {
     // compute_roe_average (kernels_cpu.F90:3013-3089)
-    double uu = at(0, 2), vv = at(0, 3), ww = at(0, 4);
-    double h = at(0, 5);
-    double up = at(1, 2), vp = at(1, 3), wp = at(1, 4);
-    double hp = at(1, 5);
-    double r = at(1, 1) / at(0, 1);
-    r = std::sqrt(r);
-    double rho = r * at(0, 1);
-    double rp1 = 1.0 / (r + 1.0);
+    T uu = at(0, 2), vv = at(0, 3), ww = at(0, 4);
+    T h = at(0, 5);
+    T up = at(1, 2), vp = at(1, 3), wp = at(1, 4);
+    T hp = at(1, 5);
+    T r = at(1, 1) / at(0, 1);
+    r = sqrt(r);
+    T rho = r * at(0, 1);
+    T rp1 = 1.0 / (r + 1.0);
     uu = (r * up + uu) * rp1;
     vv = (r * vp + vv) * rp1;
     ww = (r * wp + ww) * rp1;
     h = (r * hp + h) * rp1;
-    double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
-    double hbar = h - qq - cp(s.indx_cp_r + 1) * s.t0;
-    double tt, gamloc;
+    T qq = 0.5 * (uu * uu + vv * vv + ww * ww);
+    T hbar = h - qq - cp(s.indx_cp_r + 1) * s.t0;
+    T tt, gamloc;
     if (s.calorically_perfect == 1) {
-      tt = s.t0 + hbar / cp(0);
+      tt = s.t0 + hbar / T(cp(0));
       gamloc = cp(0) / (cp(0) - rgas0);
     } else {
       tt = at(0, 6);
-      const double ttp = at(1, 6);
+      const T ttp = at(1, 6);
       tt = (r * ttp + tt) * rp1;
-      double told = tt;
+      T told = tt;
       for (int iter = 1; iter <= 50; ++iter) {
-        double num = 0.0, den = 0.0;
+        T num = 0.0, den = 0.0;
         for (int ll = s.indx_cp_l; ll <= s.indx_cp_r; ++ll) {
-          const double tpow = std::pow(told / s.t0, ll);
+          const T tpow = pow(told / s.t0, ll);
           if (ll == -1) {
             den = den + cp(ll) * tpow;
-            num = num + cp(ll) * std::log(told / s.t0);
+            num = num + cp(ll) * log(told / s.t0);
           } else {
-            const double tpowp = (told / s.t0) * tpow;
+            const T tpowp = (told / s.t0) * tpow;
             den = den + cp(ll) * tpow;
             num = num + cp(ll) * (tpowp - 1.0) / (ll + 1.0);
           }
         }
         num = num * s.t0;
         tt = told + (hbar - num) / den;
-        if (std::fabs(tt - told) < 1e-12) break;
+        if (fabs(tt - told) < 1e-12) break;
         told = tt;
       }
-      gamloc = gamloc_at(tt);
+      gamloc = T(gamloc_at(static_cast<double>(tt)));
     }
-    double cc = gamloc * tt * rgas0;
-    double gm1loc = gamloc - 1.0;
-    double c = std::sqrt(cc);
-    double ci = 1.0 / c;
-    double p_rho = tt * rgas0;
-    double p_e = rho * gm1loc;
-    double etot = h - tt * rgas0;
-    double b3 = etot - rho * p_rho / p_e;
-    double b2 = p_e / (rho * cc);
-    double b1 = p_rho / cc - b2 * (etot - 2.0 * qq);
-    double el[5][5], er[5][5];
+    T cc = gamloc * tt * rgas0;
+    T gm1loc = gamloc - 1.0;
+    T c = sqrt(cc);
+    T ci = 1.0 / c;
+    T p_rho = tt * rgas0;
+    T p_e = rho * gm1loc;
+    T etot = h - tt * rgas0;
+    T b3 = etot - rho * p_rho / p_e;
+    T b2 = p_e / (rho * cc);
+    T b1 = p_rho / cc - b2 * (etot - 2.0 * qq);
+    T el[5][5], er[5][5];
     eigenvectors(dir, b1, b2, b3, uu, vv, ww, c, ci, h, el, er);
-    double evmax[5];
+    T evmax[5];
     for (int m = 0; m < 5; ++m) evmax[m] = -1.0;
     const int wsz = 2 * ws;
     for (int l = 1; l <= wsz; ++l) {
       const int o = l - ws;
-      double vn = at(o, 2 + dir);
-      double t = at(o, 6);
-      double gl = gamloc_at(t);
-      double cs = std::sqrt(gl * rgas0 * t);
-      evmax[0] = std::max(std::fabs(vn - cs), evmax[0]);
-      evmax[1] = std::max(std::fabs(vn), evmax[1]);
+      T vn = at(o, 2 + dir);
+      T t = at(o, 6);
+      T gl = T(gamloc_at(static_cast<double>(t)));
+      T cs = sqrt(gl * rgas0 * t);
+      evmax[0] = max(fabs(vn - cs), evmax[0]);
+      evmax[1] = max(fabs(vn), evmax[1]);
       evmax[2] = evmax[1];
       evmax[3] = evmax[1];
-      evmax[4] = std::max(std::fabs(vn + cs), evmax[4]);
+      evmax[4] = max(fabs(vn + cs), evmax[4]);
     }
-    double gp[5][8], gm[5][8];
+    T gp[5][8], gm[5][8];
     for (int l = 1; l <= wsz; ++l) {
       const int o = l - ws;
-      double rr = at(o, 1), u1 = at(o, 2), v1 = at(o, 3), w1 = at(o, 4), h1 = at(o, 5);
-      double vn = dir == 0 ? u1 : (dir == 1 ? v1 : w1);
-      double rhovn = rr * vn;
-      double pp = rr * at(o, 6) * rgas0;
-      double fi[5];
+      T rr = at(o, 1), u1 = at(o, 2), v1 = at(o, 3), w1 = at(o, 4), h1 = at(o, 5);
+      T vn = dir == 0 ? u1 : (dir == 1 ? v1 : w1);
+      T rhovn = rr * vn;
+      T pp = rr * at(o, 6) * rgas0;
+      T fi[5];
       fi[0] = rhovn;
       fi[1] = u1 * rhovn;
       fi[2] = v1 * rhovn;
@@ -867,7 +877,7 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
       fi[1 + dir] = fi[1 + dir] + pp;
       fi[4] = h1 * rhovn;
       for (int m = 0; m < 5; ++m) {
-        double wc = 0.0, gc = 0.0;
+        T wc = 0.0, gc = 0.0;
         wc = wc + el[0][m] * rr;
         gc = gc + el[0][m] * fi[0];
         wc = wc + el[1][m] * rr * u1;
@@ -878,21 +888,25 @@ void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const {
         gc = gc + el[3][m] * fi[3];
         wc = wc + el[4][m] * (rr * h1 - pp);
         gc = gc + el[4][m] * fi[4];
-        double cm = 0.5 * (gc + evmax[m] * wc);
+        T cm = 0.5 * (gc + evmax[m] * wc);
         gp[m][l - 1] = cm;
         gm[m][l - 1] = gc - cm;
       }
     }
-    const int ord = std::max(ws + epo, 1);
-    double fi[5];
+    const int ord = max(ws + epo, 1);
+    T fi[5];
     wenorec_1d(gp, gm, fi, ws, ord, s.weno_version, s.rho0, s.u0);
     for (int m = 0; m < 5; ++m) {
-      double acc = 0.0;
+      T acc = 0.0;
       for (int mm = 0; mm < 5; ++mm) acc = acc + er[mm][m] * fi[mm];
       fh[m] = acc;
     }
   }
 }
+
+void Solver::face_flux(int dir, int i, int j, int k, double fh[5]) const { face_flux_t<double>(dir, i, j, k, fh); }
+
+template void Solver::face_flux_t<Counted>(int, int, int, int, Counted*) const;
 
 // euler_x / euler_y / euler_z (singleideal_cpu.F90:674-843) = hybrid flux kernel + update
 // (euler_{x,y,z}_update_subroutine, kernels_cpu.F90:944-963, 991-1010, 1039-1058)

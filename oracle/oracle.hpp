@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 
+#include "flops.hpp"
 #include "glibc_rand.hpp"
 #include "setup.hpp"
 
@@ -109,6 +110,12 @@ class Solver {
   void force_rhs();
   void force_var();
   void face_flux(int dir, int i, int j, int k, double fh[5]) const;
+ public:
+  // the same face flux in any scalar type (Counted of flops.hpp tallies its operations)
+  template <class T>
+  void face_flux_t(int dir, int i, int j, int k, T fh[5]) const;
+
+ private:
   void bcextr(int ilat);
   void bcwall(int ilat);
   void bcwall_staggered(int ilat);

@@ -56,6 +56,16 @@ void oracle_face_flux(void* hp, int nface, const int* ijk, double* out) {
   auto* s = static_cast<Handle*>(hp)->solver;
   for (int q = 0; q < nface; ++q) s->face_flux_at(ijk[4 * q], ijk[4 * q + 1], ijk[4 * q + 2], ijk[4 * q + 3], out + 5 * q);
 }
+// FP64 operations of the face flux at (dir, i, j, k) from the current w_aux, counted through the
+// oracle's own code (flops.hpp): out = add/sub, mul, div, sqrt, pow/log, comparisons and max
+void oracle_face_flops(void* hp, int dir, int i, int j, int k, long long* out) {
+  auto* s = static_cast<Handle*>(hp)->solver;
+  streams_oracle::flop_tally() = streams_oracle::FlopTally();
+  streams_oracle::Counted fh[5];
+  s->face_flux_t(dir, i, j, k, fh);
+  const auto& t = streams_oracle::flop_tally();
+  out[0] = t.add; out[1] = t.mul; out[2] = t.div; out[3] = t.sqrt; out[4] = t.special; out[5] = t.cmp;
+}
 void oracle_set_dt(void* hp, double dt) { static_cast<Handle*>(hp)->solver->dt = dt; }
 void oracle_compute_residual(void* hp) { static_cast<Handle*>(hp)->solver->compute_residual(); }
 

@@ -31,6 +31,7 @@ def _load():
         "oracle_compute_dt": (None, [P]),
         "oracle_set_dt": (None, [P, C.c_double]),
         "oracle_face_flux": (None, [P, I, C.POINTER(C.c_int), D]),
+        "oracle_face_flops": (None, [P, I, I, I, I, C.POINTER(C.c_longlong)]),
         "oracle_compute_residual": (None, [P]),
         "oracle_sizes": (None, [P, C.POINTER(C.c_int)]),
         "oracle_get_w": (None, [P, D]),
@@ -121,6 +122,15 @@ class Oracle:
         out = np.zeros((f.shape[0], 5))
         lib.oracle_face_flux(self._h, f.shape[0], f.ctypes.data_as(C.POINTER(C.c_int)), _d(out))
         return out
+
+    def face_flops(self, direction: int, i: int, j: int, k: int) -> dict:
+        """FP64 operations of one face flux as the oracle's code performs them (flops.hpp)."""
+        out = (C.c_longlong * 6)()
+        lib.oracle_face_flops(self._h, direction, i, j, k, out)
+        names = ["add", "mul", "div", "sqrt", "special", "cmp"]
+        d = dict(zip(names, list(out)))
+        d["flops"] = d["add"] + d["mul"] + d["div"] + d["sqrt"] + d["special"]
+        return d
 
     def fl(self) -> np.ndarray:
         a = np.zeros((5, self.nz, self.ny, self.nx))
