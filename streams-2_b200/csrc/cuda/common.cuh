@@ -79,6 +79,10 @@ struct Geom {
   int visc_model;
   double mu0, t0, rgas0, rho0, u0, l0, sutherland_s, t_ref_dim, vtexp, prandtl;
   double cp0, cv0, cp_last, cv_last, gamloc;
+  // constants of the WENO faces formed once on the host: gamma - 1 and 1/(gamma - 1) of the
+  // calorically perfect gas, the smoothness-indicator scales 1/(rho0^2 u0^2) and
+  // 1/(rho0^2 u0^4) of wenorec_1d (kernels_cpu.F90:2539-2546) and 1/(rho0^2 u0^6)
+  double gm1, rgm1, wbs_a, wbs_b, wbs_c;
   // thermally perfect gas (calorically_perfect = 0): cp(T) = sum of cpc[l - cp_l] (T/t0)^l for
   // l = cp_l..cp_r, cv likewise (set_fluid_prop's cp_coeff / cv_coeff, times rgas0)
   int calorically_perfect, cp_l, cp_r;

@@ -47,6 +47,22 @@ __device__ __forceinline__ void acc_add(double& hi, double& lo, double b) {
   (void)lo;
 }
 
+// 1/a and 1/b from one division in FP64, 1/(a b) times the other factor: the weight sums of
+// the two sides of a WENO reconstruction are positive and stay far inside the FP64 exponent
+// range (products of (eps + beta)^2 terms, eps = 1e-6, or WENO-Z ratios), so the product neither
+// overflows nor underflows.  FP32 keeps two divisions (its range is too narrow for the product).
+template <class R>
+__device__ __forceinline__ void recip_pair(R a, R b, R& ra, R& rb) {
+  if constexpr (sizeof(R) == sizeof(double)) {
+    const R r = R(1) / (a * b);
+    ra = b * r;
+    rb = a * r;
+  } else {
+    ra = R(1) / a;
+    rb = R(1) / b;
+  }
+}
+
 // Stencil of a face: NP = 2*S points at offsets o = -(S-1) .. S from the face's lower point.
 template <class R, int S>
 struct Stencil {
@@ -82,7 +98,8 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
       bm0 = dwe0 / (tm0 * tm0);
       bp1 = dwe1 / (tp1 * tp1);
       bm1 = dwe1 / (tm1 * tm1);
-      const R rsp = R(1) / ((R(0) + bp0) + bp1), rsm = R(1) / ((R(0) + bm0) + bm1);
+      R rsp, rsm;
+      recip_pair((R(0) + bp0) + bp1, (R(0) + bm0) + bm1, rsp, rsm);
       bp0 = bp0 * rsp; bp1 = bp1 * rsp; bm0 = bm0 * rsm; bm1 = bm1 * rsm;
       R vminus = bp0 * (-VP(i - 1) + R(3) * VP(i)) + bp1 * (VP(i) + VP(i + 1));
       R vplus = bm0 * (-VM(i + 2) + R(3) * VM(i + 1)) + bm1 * (VM(i) + VM(i + 1));
@@ -133,7 +150,8 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
         }
         const R np0 = dwe[0] * (tp[1] * tp[2]), np1 = dwe[1] * (tp[0] * tp[2]), np2 = dwe[2] * (tp[0] * tp[1]);
         const R nm0 = dwe[0] * (tm[1] * tm[2]), nm1 = dwe[1] * (tm[0] * tm[2]), nm2 = dwe[2] * (tm[0] * tm[1]);
-        const R rsp = R(1) / ((np0 + np1) + np2), rsm = R(1) / ((nm0 + nm1) + nm2);
+        R rsp, rsm;
+        recip_pair((np0 + np1) + np2, (nm0 + nm1) + nm2, rsp, rsm);
         bp[0] = np0 * rsp; bp[1] = np1 * rsp; bp[2] = np2 * rsp;
         bm[0] = nm0 * rsm; bm[1] = nm1 * rsm; bm[2] = nm2 * rsm;
       } else {
@@ -154,7 +172,8 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
           sump = sump + bp[l];
           summ = summ + bm[l];
         }
-        const R rsp = R(1) / sump, rsm = R(1) / summ;
+        R rsp, rsm;
+        recip_pair(sump, summ, rsp, rsm);
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
           bp[l] = bp[l] * rsp;
@@ -210,7 +229,8 @@ __device__ __forceinline__ R wenorec(const R (&vp)[2 * WS], const R (&vm)[2 * WS
         sump = sump + bp[l];
         summ = summ + bm[l];
       }
-      const R rsp = R(1) / sump, rsm = R(1) / summ;
+      R rsp, rsm;
+      recip_pair(sump, summ, rsp, rsm);
 #pragma unroll
       for (int l = 0; l < 4; ++l) {
         bp[l] = bp[l] * rsp;
@@ -361,15 +381,28 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
     gamloc = R(g.gamloc);
   }
   R cc = gamloc * tt * rgas0;
-  R gm1loc = gamloc - R(1);
-  R c = sqrt(cc);
-  R ci = R(1) / c;
-  R p_rho = tt * rgas0;
-  R p_e = rho * gm1loc;
-  R etot = h - tt * rgas0;
-  R b3 = etot - rho * p_rho / p_e;
-  R b2 = p_e / (rho * cc);
-  R b1 = p_rho / cc - b2 * (etot - R(2) * qq);
+  R c, ci, b1, b2, b3;
+  const R p_rho = tt * rgas0;
+  const R etot = h - tt * rgas0;
+  if constexpr (TP) {
+    const R gm1loc = gamloc - R(1);
+    c = sqrt(cc);
+    ci = R(1) / c;
+    const R p_e = rho * gm1loc;
+    b3 = etot - rho * p_rho / p_e;
+    b2 = p_e / (rho * cc);
+    b1 = p_rho / cc - b2 * (etot - R(2) * qq);
+  } else {
+    // constant gamma: p_e = rho (gamma - 1), so b2 = (gamma - 1)/c^2 and rho p_rho/p_e =
+    // p_rho/(gamma - 1); one reciprocal square root gives c and 1/c (the reference forms three
+    // quotients and a square root here: the results differ in the last bits)
+    ci = rsqrt(cc);
+    c = cc * ci;
+    const R ci2 = ci * ci;
+    b2 = R(g.gm1) * ci2;
+    b1 = p_rho * ci2 - b2 * (etot - R(2) * qq);
+    b3 = etot - p_rho * R(g.rgm1);
+  }
   const R vn = DIR == 0 ? uu : (DIR == 1 ? vv : ww);
   constexpr int t1 = DIR == 0 ? 1 : 0;
   constexpr int t2 = DIR == 2 ? 1 : 2;
@@ -395,15 +428,16 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
     ev1 = fmax(fabs(vnq), ev1);
     ev4 = fmax(fabs(vnq + cs), ev4);
   }
-  const R betascale_a = R(1) / (R(g.rho0) * R(g.rho0) * (R(g.u0) * R(g.u0)));
-  const R betascale_b = R(1) / (R(g.rho0) * R(g.rho0) * (R(g.u0) * R(g.u0)) * (R(g.u0) * R(g.u0)));
+  const R betascale_a = R(g.wbs_a), betascale_b = R(g.wbs_b);
   // Projection of the stencil's conserved states U and fluxes F onto the five characteristic
   // fields, point by point, using the structure of the left eigenvectors (the reference forms
   // the five dot products el(:,m).U one field at a time): with dq = Roe velocity . X(2:4),
   // s = b1 X1 + b2 (X5 - dq) and a = ci (vn X1 - X(normal momentum)),
   //   P1 = (s + a)/2, P2 = X1 - s, P3 = X(t1) - v_t1 X1, P4 = X(t2) - v_t2 X1, P5 = (s - a)/2.
   // The split values g+- = (P(F) +- lambda_m P(U))/2 of every point and field go to this
-  // thread's scratch gs[((m*2WS + l)*2 + side) * gstride].
+  // thread's scratch.  wenorec_1d reads g+ at the points l = 1 .. 2WS-1 and g- at l = 2 .. 2WS
+  // whatever its order (vp(i-WS+1 .. i+WS-1), vm(i-WS+2 .. i+WS) with i = WS), so each side keeps
+  // 2WS-1 values: gs[((m*(2WS-1) + l)*2 + side) * gstride], l counted from the first point used.
   const R lam[5] = {ev0, ev1, ev1, ev1, ev4};
   const R vel[3] = {uu, vv, ww};
 #pragma unroll
@@ -434,8 +468,8 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
 #pragma unroll
     for (int m = 0; m < 5; ++m) {
       const R cm = R(0.5) * (PF[m] + lam[m] * PU[m]);
-      gs[((m * 2 * WS + l) * 2) * gstride] = cm;
-      gs[((m * 2 * WS + l) * 2 + 1) * gstride] = PF[m] - cm;
+      if (l < 2 * WS - 1) gs[((m * (2 * WS - 1) + l) * 2) * gstride] = cm;
+      if (l > 0) gs[((m * (2 * WS - 1) + l - 1) * 2 + 1) * gstride] = PF[m] - cm;
     }
   }
   // reconstruction, one characteristic field per iteration (rolled: one copy of wenorec)
@@ -445,8 +479,8 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
     R gp[2 * WS], gm[2 * WS];
 #pragma unroll
     for (int l = 0; l < 2 * WS; ++l) {
-      gp[l] = gs[((m * 2 * WS + l) * 2) * gstride];
-      gm[l] = gs[((m * 2 * WS + l) * 2 + 1) * gstride];
+      gp[l] = l < 2 * WS - 1 ? gs[((m * (2 * WS - 1) + l) * 2) * gstride] : R(0);
+      gm[l] = l > 0 ? gs[((m * (2 * WS - 1) + l - 1) * 2 + 1) * gstride] : R(0);
     }
     const R bs = (m == 2 || m == 3) ? betascale_b : betascale_a;
     const R f = wenorec<R, WS>(gp, gm, ord, WZ ? 1 : 0, bs);
@@ -504,15 +538,12 @@ __device__ __forceinline__ void rusanov_flux(const Geom& g, const Stencil<R, S>&
     const R evm = fmax(fabs(un - c), fabs(un + c));
     evmax = fmax(evm, evmax);
   }
-  const R u02 = R(g.u0) * R(g.u0);
-  const R r2u2 = R(g.rho0) * R(g.rho0) * u02;
-  const R r2u4 = r2u2 * u02;
   R bsc[5];
-  bsc[0] = R(1) / r2u2;
-  bsc[1] = R(1) / r2u4;
+  bsc[0] = R(g.wbs_a);
+  bsc[1] = R(g.wbs_b);
   bsc[2] = bsc[1];
   bsc[3] = bsc[1];
-  bsc[4] = bsc[1] / u02;
+  bsc[4] = R(g.wbs_c);
 #pragma unroll 1
   for (int m = 0; m < 5; ++m) {
     R gp[2 * WS], gm[2 * WS];

@@ -34,18 +34,27 @@ constexpr int AUX_NT = 256;
 constexpr int XF_TX = 32, XF_TY = 4, XF_NT = XF_TX * XF_TY;  // x faces: 4 row-warps per block
 constexpr int MT_NT = 128;                                     // march kernels
 // Resident blocks per SM asked of the register allocator for the FP64 and FP32 instantiations
-// of the flux kernels (measured on the 1024x256x192 boundary layer: 3 blocks of 128 threads for
-// the FP64 kernels, whose WENO scratch also caps them at 3; for FP32, 5 blocks for the x pass
-// (5.41 against 5.90 ms at 4) and 4 for the march passes (5 blocks: 7.1-7.4 against 5.4-6.5 ms);
-// the kernels are latency bound).
+// of the flux kernels (measured on the 1024x256x192 boundary layer; the kernels are FP64-latency
+// bound, so resident warps pay).  FP64 x pass: 4 blocks of 128 threads (128 registers, no
+// spills; 16.5 against 18.6 ms per step at 3 blocks), which the WENO scratch of 2WS-1 values a
+// side allows (51 KB a block).  FP64 march passes: 3 blocks, each face loading its stencil
+// afresh (y 17.3 against 18.2 ms per step with the sliding register window, which spills
+// 176-228 bytes at 4 blocks; with reloads at 4 blocks y takes 18.8 ms: the reloads then miss
+// L1).  FP32: 5 blocks for the x pass (5.41 against 5.90 ms at 4) and 4 for the march passes
+// (5 blocks: 7.1-7.4 against 5.4-6.5 ms).
 #ifndef XF_MINB_D
-#define XF_MINB_D 3
+#define XF_MINB_D 4
 #endif
 #ifndef XF_MINB_F
 #define XF_MINB_F 5
 #endif
 #ifndef MT_MINB_D
 #define MT_MINB_D 3
+#endif
+// y/z passes: the stencil window slides along the line in registers (1), or every face loads
+// its stencil afresh (0: no window held across the WENO branch, fewer registers)
+#ifndef SB_MARCH_WINDOW
+#define SB_MARCH_WINDOW 0
 #endif
 #ifndef MT_MINB_F
 #define MT_MINB_F 4
@@ -323,7 +332,7 @@ __device__ __forceinline__ R div3_at(const Geom& g, const R* __restrict__ d, int
 }
 
 // Per-thread scratch of the WENO characteristic projections (dynamic shared memory of the flux
-// kernels, 5 fields x 2WS points x 2 sides per thread, thread-interleaved)
+// kernels, 5 fields x (2WS-1) points x 2 sides per thread, thread-interleaved)
 template <class R>
 __device__ __forceinline__ R* weno_scratch() {
   extern __shared__ __align__(16) unsigned char sb_dyn_smem[];
@@ -331,7 +340,7 @@ __device__ __forceinline__ R* weno_scratch() {
 }
 template <class R, int WS>
 constexpr size_t weno_scratch_bytes(int nthreads) {
-  return (size_t)nthreads * 5 * 2 * WS * 2 * sizeof(R);
+  return (size_t)nthreads * 5 * (2 * WS - 1) * 2 * sizeof(R);
 }
 
 template <int DIR>
@@ -554,13 +563,16 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
     // preload the window and sensor bits of the face c0-2; the loop starts at the face c0-1
     Stencil<R, S> st;
     const int p = c0 - 2;
+#if SB_MARCH_WINDOW
 #pragma unroll
     for (int q = 1; q < NP; ++q) load_point<R, S>(g, st, q, aux, n, base0 + (long long)(p - (S - 1) + q) * sd);
+#endif
     unsigned mask = 0;
 #pragma unroll
     for (int bq = 1; bq < 2 * WS; ++bq) mask |= sensor_bit(p - WS + 1 + bq) << bq;
     R hlo[5] = {0, 0, 0, 0, 0}, llo[5] = {0, 0, 0, 0, 0};
     for (int c = c0 - 1; c <= c1; ++c) {
+#if SB_MARCH_WINDOW
       // slide the window to the face c
 #pragma unroll
       for (int q = 0; q < NP - 1; ++q) {
@@ -571,6 +583,12 @@ __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
 #endif
       }
       load_point<R, S>(g, st, NP - 1, aux, n, base0 + (long long)(c + S) * sd);
+#else
+      // the face's stencil, loaded afresh: the lanes of a warp hold consecutive i, so every load
+      // is one coalesced row, and the points shared with the previous face come from L1 / L2
+#pragma unroll
+      for (int q = 0; q < NP; ++q) load_point<R, S>(g, st, q, aux, n, base0 + (long long)(c - (S - 1) + q) * sd);
+#endif
       mask = (mask >> 1) | (sensor_bit(c + WS) << (2 * WS - 1));
       R hhi[5], lhi[5];
       const R* cpt = sizeof(R) == sizeof(double) ? aux + 7 * n + base0 + (long long)(c - (S - 1)) * sd : nullptr;
