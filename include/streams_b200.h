@@ -242,6 +242,10 @@ int streams_b200_set_stats(streams_b200_ctx* ctx, int which, const double* in, l
 
 /* Synchronise the context's stream and report any asynchronous error. */
 int streams_b200_synchronize(streams_b200_ctx* ctx);
+/* Non-blocking completion check (no counterpart in the reference): 1 while work issued on the
+ * context's stream is pending, 0 once it has completed, a negative status on a device error.
+ * The serving loop polls it instead of waiting on every resident solve. */
+int streams_b200_query(streams_b200_ctx* ctx);
 
 /* Number of kernel launches issued by this context since creation (instrumentation). */
 long long streams_b200_launch_count(const streams_b200_ctx* ctx);

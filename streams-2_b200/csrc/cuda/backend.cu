@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -57,10 +58,30 @@ int cuda_err(streams_b200_ctx* c, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_err((ctx), e_, #call); \
   } while (0)
 
+// Device memory comes from the device's stream-ordered pool (cudaMallocAsync on the context's
+// stream, cudaFreeAsync at destroy): creating and destroying contexts while others run, as the
+// serving loop does, then neither synchronises the device (cudaFree does) nor returns memory to
+// the driver between them (the pool keeps what it has: release threshold raised once per device).
+void keep_pool_memory(int device) {
+  static std::mutex mu;
+  static unsigned long long done = 0;
+  std::lock_guard<std::mutex> lk(mu);
+  if (device < 0 || device >= 64 || (done & (1ULL << device))) return;
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long keep = ~0ULL;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done |= 1ULL << device;
+}
+
 template <class T>
 cudaError_t dev_alloc(streams_b200_ctx* c, T** p, size_t count) {
   void* v = nullptr;
-  cudaError_t e = cudaMalloc(&v, count * sizeof(T) > 0 ? count * sizeof(T) : 16);
+  cudaError_t e = cudaMallocAsync(&v, count * sizeof(T) > 0 ? count * sizeof(T) : 16, c->stream);
+  // the buffers are filled by copies outside the stream (set-up), so the allocation completes first
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return e;
   c->allocs.push_back(v);
   *p = static_cast<T*>(v);
@@ -210,6 +231,15 @@ void fill_geom(streams_b200_ctx* c) {
   g.sutherland_s = p.sutherland_s; g.t_ref_dim = p.t_ref_dim; g.vtexp = p.powerlaw_vtexp; g.prandtl = p.prandtl;
   g.cp0 = p.cp0; g.cv0 = p.cv0; g.cp_last = p.cp_last; g.cv_last = p.cv_last;
   g.gamloc = p.cp0 / (p.cp0 - p.rgas0);
+  g.gm1 = g.gamloc - 1.0;
+  g.rgm1 = 1.0 / g.gm1;
+  {
+    // the same products and quotients the reference forms in wenorec_1d (u0_2, rho0_2u0_2, ...)
+    const double u0_2 = p.u0 * p.u0, r2u2 = p.rho0 * p.rho0 * u0_2, r2u4 = r2u2 * u0_2;
+    g.wbs_a = 1.0 / r2u2;
+    g.wbs_b = 1.0 / r2u4;
+    g.wbs_c = g.wbs_b / u0_2;
+  }
   g.calorically_perfect = p.calorically_perfect;
   g.cp_l = p.indx_cp_l;
   g.cp_r = p.indx_cp_r;
@@ -270,8 +300,11 @@ int streams_b200_destroy(streams_b200_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   ctx->prof.resolve();
-  for (void* a : ctx->allocs) cudaFree(a);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  for (void* a : ctx->allocs) cudaFreeAsync(a, ctx->stream);
+  if (ctx->stream) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+  }
   delete ctx;
   return STREAMS_B200_OK;
 }
@@ -305,6 +338,7 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
   };
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return fail(e, "cudaStreamCreate");
+  keep_pool_memory(c->device);
   // 1-D grid data
   const int ng = p->ng;
   double *dx, *dy, *dz, *dyn, *m1, *m2, *m3, *m4, *m5, *m6;
@@ -757,6 +791,15 @@ int streams_b200_synchronize(streams_b200_ctx* c) {
   SB_CHECK(c, cudaStreamSynchronize(c->stream));
   SB_CHECK(c, cudaGetLastError());
   return STREAMS_B200_OK;
+}
+
+int streams_b200_query(streams_b200_ctx* c) {
+  if (!c) return set_err(c, STREAMS_B200_EINVAL, "null context");
+  cudaSetDevice(c->device);
+  const cudaError_t e = cudaStreamQuery(c->stream);
+  if (e == cudaErrorNotReady) return 1;
+  SB_CHECK(c, e);
+  return 0;
 }
 
 static int ensure_stats(streams_b200_ctx* c, bool three_d) {

@@ -110,6 +110,7 @@ def _load() -> C.CDLL:
         "streams_b200_get_stats": (I, [P, I, D, LL]),
         "streams_b200_set_stats": (I, [P, I, D, LL]),
         "streams_b200_synchronize": (I, [P]),
+        "streams_b200_query": (I, [P]),
         "streams_b200_launch_count": (LL, [P]),
         "streams_b200_debug_fetch": (I, [P, I, D, LL]),
         "streams_b200_get_stream": (I, [P, C.POINTER(P)]),
@@ -178,7 +179,7 @@ EXPORTED = [
     "streams_b200_copy_to_field", "streams_b200_copy_from_device", "streams_b200_copy_to_device",
     "streams_b200_init_run", "streams_b200_compute_dt", "streams_b200_set_dt", "streams_b200_rk_sync",
     "streams_b200_advance", "streams_b200_get_scalars", "streams_b200_set_time", "streams_b200_compute_residual",
-    "streams_b200_count_weno", "streams_b200_get_wallprop", "streams_b200_synchronize",
+    "streams_b200_count_weno", "streams_b200_get_wallprop", "streams_b200_synchronize", "streams_b200_query",
     "streams_b200_compute_stats", "streams_b200_compute_stats_3d", "streams_b200_get_stats",
     "streams_b200_set_stats",
     "streams_b200_launch_count", "streams_b200_debug_fetch", "streams_b200_get_stream",
@@ -430,6 +431,13 @@ class Solver:
 
     def synchronize(self):
         self._check(lib.streams_b200_synchronize(self._h))
+
+    def busy(self) -> bool:
+        """Whether work issued on the context's stream is still pending (non-blocking)."""
+        rc = lib.streams_b200_query(self._h)
+        if rc < 0:
+            self._check(rc)
+        return rc == 1
 
     NV_STAT, NV_STAT_3D = 70, 14
 

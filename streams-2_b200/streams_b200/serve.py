@@ -1,18 +1,15 @@
 """Serving form: a request loop over resident solves with continuous batching.
 
-Requests (channel solves of any size, Mach number, step count and precision) arrive over time.
-Each is prepared on the host as it arrives (input parsing, grid, initial field: worker
-threads, so that set-up overlaps the GPU work), then admitted in arrival order as soon as its
-device footprint fits the HBM budget next to the solves already resident.  A resident solve
-keeps its fields in HBM from admission to completion.  The loop advances all resident solves
-together in ticks: every resident solve replays its own CUDA graph of a tick's steps (a one-box
-``Batch``, captured once when the solve joins) on its own stream, so the solves' stages overlap on
-the GPU and a change of the resident set rebuilds nothing (one graph over all resident solves had
-to be captured again whenever a solve joined or left, which at a hundred resident solves cost more
-host time than the tick's GPU work).  Solves are admitted while a tick runs (their first step
-overlaps it), join the next tick, and leave, freeing their memory, at the end of the tick in which
-they complete.  Completion latency is
-measured from a request's arrival to the end of the tick that completes it.
+Requests (channel and shock-interaction solves of any size, Mach number, step count and
+precision) arrive over time.  Each is prepared on the host as it arrives (input parsing, grid,
+initial field: worker threads, so that set-up overlaps the GPU work), then admitted in arrival
+order as soon as its device footprint fits the HBM budget next to the solves already resident;
+its device set-up runs on an admission thread, off the loop.  A resident solve keeps its fields in
+HBM from admission to completion and advances in ticks: it replays its own CUDA graph of a tick's
+steps (a one-box ``Batch``, captured once when the solve joins) on its own stream, and the loop
+gives it its next tick as soon as its stream reports the previous one complete, so the solves'
+stages overlap on the GPU and none waits for another.  A solve leaves, freeing its memory, when its
+last tick is seen complete; completion latency is measured from the request's arrival to then.
 
 A solve's arithmetic does not depend on what else is resident: with the same launch tuning its
 result is bit-identical alone and in any mix.
@@ -46,6 +43,7 @@ class Solve:
     admitted: float = 0.0
     finished: float = 0.0
     tuning: tuple | None = None
+    inflight: int = 0               # steps issued on the solve's stream and not yet seen complete
     result: dict = field(default_factory=dict)
 
 
@@ -69,32 +67,63 @@ class Server:
     """Continuous-batching solve server on one GPU.
 
     budget_bytes  device memory the resident solves may hold together
-    tick_steps    steps of every resident solve per tick (fewer when a solve completes sooner)
+    tick_steps    steps a resident solve is given at a time (fewer when it completes sooner)
     tune          autotune each new (grid, precision) class before its first admission
     keep_fields   download each completed solve's conserved field into Solve.result["w"]
+
+    The loop thread only decides and polls.  Host set-up runs on the preparation threads; an
+    admitted solve's device set-up (tuning of a new class, context creation and upload,
+    run() preamble, first step, capture of its tick graph and its first tick) runs on an
+    admission thread; resident solves advance independently, each given its next tick as soon
+    as its previous one has completed (a non-blocking query of its stream), so no solve waits
+    for the others and a finishing solve releases its memory (stream-ordered, no device-wide
+    synchronisation) the moment it is seen complete.
     """
 
     def __init__(self, budget_bytes: int, tick_steps: int = 10, tune: bool = True, keep_fields: bool = False,
-                 prep_threads: int = 4, tune_cache: dict | None = None):
+                 prep_threads: int = 4, tune_cache: dict | None = None, admit_threads: int = 2):
         self.budget = int(budget_bytes)
         self.tick_steps = int(tick_steps)
         self.tune = tune
         self.keep_fields = keep_fields
         self.prep_threads = prep_threads
+        self.admit_threads = admit_threads
         self.tune_cache = {} if tune_cache is None else tune_cache
         self.log: list[tuple] = []
+
+    def _admit(self, s: Solve) -> Solve:
+        """Device set-up of an admitted solve (admission thread): the solve is resident when this
+        returns, with its first step and first tick issued on its own stream."""
+        from .tune import autotune
+        if self.tune:
+            s.tuning = autotune(s.case, precision=s.precision, cache=self.tune_cache)
+        s.solver = Solver.from_case(s.case, precision=s.precision)
+        if s.tuning:
+            s.solver.set_tuning(*s.tuning)
+        s.solver.init_run()
+        # the first step runs alone, so that the solve's graph only holds steady steps
+        s.solver.advance(1)
+        s.remaining = s.nsteps - 1
+        s.inflight = 0
+        if s.remaining > 0:
+            s.batch = Batch([s.solver], steps_per_graph=self.tick_steps, dt_every=1)
+            n = min(self.tick_steps, s.remaining)
+            s.batch.advance(n)
+            s.inflight = n
+        return s
 
     def run(self, requests: list[dict], time_scale: float = 1.0) -> dict:
         """Serve `requests` (dicts with rid, arrival [s], nsteps, precision and channel
         parameters) with arrivals replayed in real time (scaled by time_scale); returns the
         per-request records and the latency / throughput summary."""
-        from .tune import autotune
         reqs = sorted(requests, key=lambda r: r["arrival"])
         workdir = tempfile.mkdtemp(prefix="streams_b200_serve_")
         pool = cf.ThreadPoolExecutor(max_workers=self.prep_threads)
+        admit_pool = cf.ThreadPoolExecutor(max_workers=self.admit_threads)
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
         futures: dict[int, cf.Future] = {}
+        admitting: dict[int, cf.Future] = {}
         waiting: list[Solve] = []      # prepared, not admitted (arrival order)
         active: list[Solve] = []
         done: list[Solve] = []
@@ -102,97 +131,93 @@ class Server:
         used = 0
         nxt = 0
         busy = 0.0
-        host = {"admit_s": 0.0, "batch_build_s": 0.0}
+        last = None  # start of the current interval with resident solves
+        host = {"admit_wait_s": 0.0, "loop_iterations": 0}
         try:
-            while nxt < len(reqs) or futures or waiting or active:
+            while nxt < len(reqs) or futures or waiting or admitting or active:
+                host["loop_iterations"] += 1
+                progressed = False
                 # arrivals: start host set-up of every request whose arrival time has come
                 while nxt < len(reqs) and reqs[nxt]["arrival"] * time_scale <= now():
                     r = reqs[nxt]
                     futures[r["rid"]] = pool.submit(prepare, r, workdir)
                     nxt += 1
                 # prepared requests join the admission queue in arrival order
-                for r in reqs:
-                    f = futures.get(r["rid"])
-                    if f is not None and f.done():
-                        case = f.result()
-                        del futures[r["rid"]]
-                        nx, ny, nz, _ = case.shape
-                        s = Solve(r["rid"], r["arrival"] * time_scale, r["nsteps"], r["precision"], case,
-                                  footprint_of(case, r["precision"]), nx * ny * nz)
-                        if s.footprint > self.budget:
-                            rejected.append(s.rid)
-                        else:
-                            waiting.append(s)
-                waiting.sort(key=lambda s: s.arrival)
-                # issue one tick of every resident solve, each through its own graph (asynchronous)
-                n = 0
-                if active:
-                    n = tick_length([s.remaining for s in active], self.tick_steps)
-                    ta = now()
-                    for s in active:
-                        if s.batch is None:
-                            tc = now()
-                            s.batch = Batch([s.solver], steps_per_graph=self.tick_steps, dt_every=1)
-                            host["batch_build_s"] += now() - tc
-                        s.batch.advance(n)
-                # admission by footprint, first come first served, while the tick runs; the
-                # solves admitted now take their first step on their own streams and join the
-                # next tick (memory of solves finishing in this tick is released after it)
-                tadm = now()
-                joining = []
-                for _ in range(admit_fifo([w.footprint for w in waiting], used, self.budget)):
-                    s = waiting.pop(0)
-                    if self.tune:
-                        s.tuning = autotune(s.case, precision=s.precision, cache=self.tune_cache)
-                    s.solver = Solver.from_case(s.case, precision=s.precision)
-                    if s.tuning:
-                        s.solver.set_tuning(*s.tuning)
-                    s.solver.init_run()
-                    # the first step runs alone, so that the solve's graph only holds steady steps
-                    s.solver.advance(1)
-                    s.remaining = s.nsteps - 1
-                    s.admitted = now()
-                    used += s.footprint
-                    joining.append(s)
-                host["admit_s"] += now() - tadm
-                if n:
-                    for s in active:
-                        s.batch.synchronize()
-                    tb = now()
-                    busy += tb - ta
-                    self.log.append((ta, tb, len(active), n))
-                    still = []
-                    for s in active:
-                        s.remaining -= n
-                        if s.remaining > 0:
-                            still.append(s)
-                        else:
-                            used -= self._finish(s, tb, done)
-                    active = still
-                # a one-step solve is complete after its first step
-                for s in joining:
-                    if s.remaining <= 0:
-                        s.solver.synchronize()
-                        used -= self._finish(s, now(), done)
+                for rid in [rid for rid, f in futures.items() if f.done()]:
+                    r = next(q for q in reqs if q["rid"] == rid)
+                    case = futures.pop(rid).result()
+                    nx, ny, nz, _ = case.shape
+                    sv = Solve(r["rid"], r["arrival"] * time_scale, r["nsteps"], r["precision"], case,
+                               footprint_of(case, r["precision"]), nx * ny * nz)
+                    if sv.footprint > self.budget:
+                        rejected.append(sv.rid)
                     else:
-                        active.append(s)
-                if not active and not joining:
-                    # idle until the next arrival or finished set-up
-                    if futures:
+                        waiting.append(sv)
+                    progressed = True
+                waiting.sort(key=lambda q: q.arrival)
+                # admission by footprint, first come first served: the memory is reserved now,
+                # the device set-up runs on an admission thread
+                for _ in range(admit_fifo([q.footprint for q in waiting], used, self.budget)):
+                    sv = waiting.pop(0)
+                    used += sv.footprint
+                    admitting[sv.rid] = admit_pool.submit(self._admit, sv)
+                    progressed = True
+                for rid in [rid for rid, f in admitting.items() if f.done()]:
+                    sv = admitting.pop(rid).result()
+                    sv.admitted = now()
+                    active.append(sv)
+                    progressed = True
+                if active and last is None:
+                    last = now()
+                # every resident solve whose tick has completed gets its next one, or leaves
+                still = []
+                for sv in active:
+                    if sv.inflight and sv.solver.busy():
+                        still.append(sv)
+                        continue
+                    sv.remaining -= sv.inflight
+                    sv.inflight = 0
+                    progressed = True
+                    if sv.remaining <= 0:
+                        used -= self._finish(sv, now(), done)
+                        continue
+                    n = tick_length([sv.remaining], self.tick_steps)
+                    sv.batch.advance(n)
+                    sv.inflight = n
+                    still.append(sv)
+                if len(still) != len(active) or progressed:
+                    self.log.append((now(), len(still)))
+                active = still
+                if not active and last is not None:
+                    busy += now() - last
+                    last = None
+                if not progressed:
+                    if admitting and not active:
+                        tw = now()
+                        cf.wait(list(admitting.values()), timeout=0.05, return_when=cf.FIRST_COMPLETED)
+                        host["admit_wait_s"] += now() - tw
+                    elif futures and not active:
                         cf.wait(list(futures.values()), timeout=0.05, return_when=cf.FIRST_COMPLETED)
-                    elif nxt < len(reqs):
+                    elif not active and nxt < len(reqs):
                         time.sleep(max(0.0, min(0.05, reqs[nxt]["arrival"] * time_scale - now())))
+                    else:
+                        time.sleep(0.0002)
+            if last is not None:
+                busy += now() - last
         finally:
-            for s in active:
-                if s.batch is not None:
-                    s.batch.close()
-                if s.solver is not None:
-                    s.solver.close()
+            for f in admitting.values():
+                sv = f.result()
+                active.append(sv)
+            for sv in active:
+                if sv.batch is not None:
+                    sv.batch.close()
+                if sv.solver is not None:
+                    sv.solver.close()
+            admit_pool.shutdown(wait=True)
             pool.shutdown(wait=True)
         out = summarize(done, rejected, busy, self.log)
         out.update(host)
         return out
-
 
     def _finish(self, s: Solve, t: float, done: list) -> int:
         """Record a completed solve, release its device memory; returns the bytes freed."""
@@ -240,6 +265,6 @@ def summarize(done: list[Solve], rejected: list[int], busy: float, log: list) ->
         "mcell_steps_per_busy_s": cell_steps / busy / 1e6 if busy > 0 else None,
         "span_s": span,
         "ticks": len(log),
-        "max_resident": max((x[2] for x in log), default=0),
+        "max_resident": max((x[1] for x in log), default=0),
         "solves": {s.rid: s for s in done},
     }
