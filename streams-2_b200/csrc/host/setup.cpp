@@ -4,13 +4,18 @@
 
 #include "glibc_rand.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
 #include <sstream>
+#include <limits>
+#include <string>
+#include <thread>
 #include <utility>
+#include <vector>
 
 namespace streams_b200 {
 
@@ -422,6 +427,8 @@ void set_oblique_shock(Setup& s) {
 }
 
 // set_flow_params (singleideal.F90:2776-2856) for the channel
+void set_bl_prop(Setup& s);
+
 void set_flow_params(Setup& s, double reynolds_bulk_target) {
   const IniFile& c = s.ini;
   s.reynolds = c.get_double("flow", "Reynolds");
@@ -458,10 +465,13 @@ void set_flow_params(Setup& s, double reynolds_bulk_target) {
     // set_bl_prop (singleideal.F90:2858-2892) converts the input friction Reynolds number into
     // the free-stream one with hasan_meanprofile; the synthetic boundary layer states both
     const IniFile& ci = s.ini;
-    if (!ci.has_section("synthetic"))
-      throw InputError("flow_init = 1 needs the [synthetic] boundary-layer initialisation");
-    s.reynolds_friction = ci.get_double_or("synthetic", "reynolds_tau", s.reynolds);
-    s.reynolds = ci.get_double("synthetic", "reynolds_delta");
+    if (s.bctags[0] == 9) throw InputError("the laminar boundary layer (xmin = 9) is not supported");
+    if (ci.has_section("synthetic")) {
+      s.reynolds_friction = ci.get_double_or("synthetic", "reynolds_tau", s.reynolds);
+      s.reynolds = ci.get_double("synthetic", "reynolds_delta");
+    } else {
+      set_bl_prop(s);
+    }
   } else {
     throw InputError("flow_init other than 0 (channel) or 1 (boundary layer) is not supported");
   }
@@ -639,6 +649,382 @@ void init_bl_synthetic(Setup& s, double amp) {
       }
   s.rng_seed = seed;
   s.rng_draws = 3LL * nx * ny * nz;
+}
+
+// hasan_meanprofile (singleideal.F90:4090-4249): mean velocity, temperature, density and
+// viscosity of a compressible turbulent boundary layer of thickness d99 on a fine uniform grid of
+// 10000 intervals (inner law with a van Driest damped mixing length, Coles wake of strength from
+// Re_theta, Crocco-Busemann-type temperature with spr), iterated until Re_theta (imode 0, Re_tau
+// given) or Re_tau (imode 1, Re_theta given) changes by less than 1e-5; with icompute /= 0 the
+// profiles are interpolated linearly (pol_int with m = 2) onto ye(1:n).  Same operations and
+// order as the reference: the profiles and the thicknesses are reproducible bit for bit.
+struct HasanState {
+  double retau = 0, retheta = 0, redelta = 0, th = 0, cf = 0, ch = 0, mtau = 0, deltav = 0;
+};
+void hasan_meanprofile(int n, double d99, double mach, double theta, HasanState& h, double pr, double spr,
+                       double rfac, double gam, double vtexp, bool visc_exp, double s2tinf, const double* ye,
+                       double* ue, double* te, double* rhoe, double* mue, int imode, int icompute) {
+  constexpr int ny = 10000, nyext = 2 * ny;
+  const double pi_h = 4.0 * std::atan(1.0);
+  const double gm1h = 0.5 * (gam - 1.0);
+  const double tr = 1.0 + gm1h * rfac * (mach * mach);
+  const double tw = 1.0 + theta * (tr - 1.0);
+  const double apl = 17.0, vkc = 0.41;
+  const int nitermax = 10000;
+  const double tol = 0.00001;
+  const double dy = d99 / ny;
+  // index j = 1..ny+1 of the reference at [j-1]
+  std::vector<double> y(ny + 1), u(ny + 1), t(ny + 1), rho(ny + 1), mu(ny + 1), ypl(ny + 1), upl(ny + 1),
+      yst(ny + 1), d(ny + 1), mut(ny + 1), wake(ny + 1), swake(ny + 1);
+  std::vector<double> yext(nyext + 1), uext(nyext + 1), text(nyext + 1), rhoext(nyext + 1), muext(nyext + 1);
+  for (int j = 1; j <= ny + 1; ++j) y[j - 1] = (j - 1) * dy;
+  for (int j = 1; j <= nyext + 1; ++j) yext[j - 1] = (j - 1) * dy;
+  // sin(pi y/d99) of the wake function does not change between iterations
+  for (int j = 0; j <= ny; ++j) swake[j] = std::sin(pi_h * (y[j] / d99));
+  const double ufac = 0.99;
+  for (int j = 0; j <= ny; ++j) u[j] = std::min(1.0, y[j] / d99);
+  const double uinf = u[ny] / ufac;
+  for (int j = 0; j <= ny; ++j) u[j] = u[j] / uinf;
+  int niter = 0;
+  double& retau = h.retau;
+  double& retheta = h.retheta;
+  if (imode == 0) retheta = 1000.0; else retau = 200.0;
+  h.mtau = 0.1;
+  double absdiff = std::numeric_limits<double>::max();
+  auto visc = [&](double tt) {
+    return visc_exp ? std::pow(tt, vtexp) : std::pow(tt, 1.5) * (1.0 + s2tinf) / (tt + s2tinf);
+  };
+  double uinf_plus = 0.0;
+  while (absdiff > tol) {
+    ++niter;
+    if (niter > nitermax) break;
+    const double rethetaold = retheta, retauold = retau;
+    // the Coles wake strength depends on retheta only (the reference forms it at every point)
+    const double z1 = retheta / 425.0 - 1.0;
+    const double picole = 0.69 * (1.0 - std::exp(-0.243 * std::sqrt(z1) - 0.15 * z1));
+    for (int j = 0; j <= ny; ++j) {
+      t[j] = tw + (tr - tw) * (spr * u[j] + (1.0 - spr) * (u[j] * u[j])) + (1.0 - tr) * (u[j] * u[j]);
+      rho[j] = 1.0 / t[j];
+      mu[j] = visc(t[j]);
+      ypl[j] = (y[j] / d99) * retau;
+      yst[j] = ypl[j] * std::sqrt(rho[j] / rho[0]) * mu[0] / mu[j];
+      const double e = 1.0 - std::exp(-yst[j] / (apl + 19.3 * h.mtau));
+      d[j] = e * e;
+      mut[j] = mu[j] / mu[0] * vkc * yst[j] * d[j];
+      wake[j] = picole / vkc * pi_h * swake[j];
+    }
+    upl[0] = 0.0;
+    for (int j = 1; j <= ny; ++j) {
+      const double uint_inn_j = 1.0 / (mu[j] / mu[0] + mut[j]);
+      const double uint_inn_jm = 1.0 / (mu[j - 1] / mu[0] + mut[j - 1]);
+      const double uint_out_j = std::sqrt(rho[0] / rho[j]) / retau * wake[j];
+      const double uint_out_jm = std::sqrt(rho[0] / rho[j - 1]) / retau * wake[j - 1];
+      const double uint_j = uint_inn_j + uint_out_j;
+      const double uint_jm = uint_inn_jm + uint_out_jm;
+      const double uint = 0.5 * (uint_j + uint_jm);
+      upl[j] = upl[j - 1] + uint * (ypl[j] - ypl[j - 1]);
+    }
+    uinf_plus = upl[ny] / ufac;
+    for (int j = 0; j <= ny; ++j) u[j] = upl[j] / uinf_plus;
+    h.th = 0.0;
+    for (int j = 1; j <= ny; ++j) {
+      const double thint_j = rho[j] * u[j] * (1.0 - u[j]);
+      const double thint_jm = rho[j - 1] * u[j - 1] * (1.0 - u[j - 1]);
+      const double thint = 0.5 * (thint_j + thint_jm);
+      h.th = h.th + thint * (y[j] - y[j - 1]);
+    }
+    h.cf = 2.0 / (uinf_plus * uinf_plus) * rho[0];
+    h.ch = 0.5 * h.cf * spr / pr;
+    h.mtau = mach * std::sqrt(0.5 * h.cf);
+    if (imode == 0) {
+      retheta = retau * h.th / d99 * mu[0] / rho[0] * uinf_plus;
+      absdiff = std::fabs(retheta - rethetaold);
+    } else {
+      retau = retheta * d99 / h.th / mu[0] * rho[0] / uinf_plus;
+      absdiff = std::fabs(retau - retauold);
+    }
+    h.redelta = retheta * d99 / h.th;
+  }
+  h.deltav = d99 / retau;
+  if (icompute == 0) return;
+  for (int j = 0; j <= ny; ++j) {
+    uext[j] = u[j];
+    text[j] = t[j];
+  }
+  const double dudy = (uext[ny] - uext[ny - 1]) / (yext[ny] - yext[ny - 1]);
+  for (int j = ny + 1; j <= nyext; ++j) {
+    uext[j] = uext[ny] + dudy * (yext[j] - yext[ny]);
+    uext[j] = std::min(uext[j], 1.0);
+    text[j] = tw + (tr - tw) * (spr * uext[j] + (1.0 - spr) * (uext[j] * uext[j])) + (1.0 - tr) * (uext[j] * uext[j]);
+  }
+  for (int j = 0; j <= nyext; ++j) {
+    rhoext[j] = 1.0 / text[j];
+    muext[j] = visc(text[j]);
+  }
+  for (int j = 0; j < n; ++j) ue[j] = rhoe[j] = te[j] = mue[j] = 1.0;
+  ue[0] = uext[0];
+  rhoe[0] = rhoext[0];
+  te[0] = text[0];
+  mue[0] = muext[0];
+  for (int j = 0; j < n; ++j) {
+    const double yy = ye[j];
+    if (!(yy < yext[nyext])) continue;
+    // locateval (parameters.F90:145-164) on the uniform yext, then pol_int (Neville, :120-143)
+    // with m = 2 on the pair jjj, jjj+1
+    int il = 0, juu = nyext + 2;
+    while (juu - il > 1) {
+      const int jm = (juu + il) / 2;
+      if ((yext[nyext] > yext[0]) == (yy > yext[jm - 1])) il = jm; else juu = jm;
+    }
+    const int jjj = std::min(std::max(il, 1), nyext + 1 + 1 - 2);
+    const double x1 = yext[jjj - 1], x2 = yext[jjj];
+    auto lin = [&](const std::vector<double>& f) {
+      double v = (yy - x2) * f[jjj - 1] + (x1 - yy) * f[jjj];
+      return v / (x1 - x2);
+    };
+    ue[j] = lin(uext);
+    rhoe[j] = lin(rhoext);
+    te[j] = lin(text);
+    mue[j] = lin(muext);
+  }
+}
+
+// set_bl_prop (singleideal.F90:2858-2892): the input Reynolds number of a turbulent boundary
+// layer is the friction one; the free-stream (thickness-based) one follows from the mean profile
+void set_bl_prop(Setup& s) {
+  const bool visc_exp = s.visc_model == 1;
+  const double s2tinf = s.sutherland_s / s.t_ref_dim;
+  s.reynolds_friction = s.reynolds;
+  const int ny = s.nymax;
+  std::vector<double> yvec(ny), uv(ny), tv(ny), rv(ny), mv(ny);
+  for (int j = 1; j <= ny; ++j) yvec[j - 1] = s.yg(j);
+  HasanState h;
+  h.retau = s.reynolds_friction;
+  hasan_meanprofile(ny, s.l0, s.mach, s.theta_wall, h, s.prandtl, 0.8, s.rfac, s.gam, s.powerlaw_vtexp, visc_exp,
+                    s2tinf, yvec.data(), uv.data(), tv.data(), rv.data(), mv.data(), 0, 0);
+  s.reynolds = h.redelta;
+}
+
+// blvec.bin (init_bl, singleideal.F90:3293-3297, 3360-3364): one Fortran unformatted record
+// holding cfvec, thvec, deltavec, deltavvec over xg(1-ng .. nxmax+ng+1)
+bool read_blvec(const std::string& path, size_t n, std::vector<double>& cf, std::vector<double>& th,
+                std::vector<double>& de, std::vector<double>& dv) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return false;
+  int32_t len = 0;
+  f.read(reinterpret_cast<char*>(&len), 4);
+  if (!f || static_cast<size_t>(len) != 4 * n * 8) throw InputError(path + ": unexpected record length");
+  for (auto* v : {&cf, &th, &de, &dv}) {
+    v->resize(n);
+    f.read(reinterpret_cast<char*>(v->data()), static_cast<std::streamsize>(n * 8));
+  }
+  if (!f) throw InputError(path + ": short read");
+  return true;
+}
+void write_blvec(const std::string& path, const std::vector<double>& cf, const std::vector<double>& th,
+                 const std::vector<double>& de, const std::vector<double>& dv) {
+  std::ofstream f(path, std::ios::binary);
+  if (!f) return;  // the file is a cache of the reference's; a read-only directory only loses it
+  const int32_t len = static_cast<int32_t>(4 * cf.size() * 8);
+  f.write(reinterpret_cast<const char*>(&len), 4);
+  for (const auto* v : {&cf, &th, &de, &dv}) f.write(reinterpret_cast<const char*>(v->data()), v->size() * 8);
+  f.write(reinterpret_cast<const char*>(&len), 4);
+}
+
+// init_bl (singleideal.F90:3252-3423) and add_synthetic_perturbations (:3587-3685) for the single
+// block: the thickness delta(x) and viscous length along x from the mean profile at the inflow
+// (Re_tau given) and a momentum-thickness march in both directions (Re_theta given, delta
+// iterated to 1e-9), the mean field wmean from the profile at every station, v from continuity,
+// +-1 % random velocity perturbations (3 draws per cell in k, j, i order), then the streak /
+// vortex perturbations of add_synthetic_perturbations (4 phase draws) with +-1.5 % random
+// perturbations scaled by y/l0 below the local thickness (3 draws per such cell).
+void init_bl(Setup& s) {
+  const int nx = s.nxmax, ny = s.nymax, nz = s.nzmax, ng = s.ng;
+  const int nxt = nx + 2 * ng + 1;  // stations 1-ng .. nx+ng+1
+  auto X = [&](int i) { return i + ng - 1; };
+  const bool visc_exp = s.visc_model == 1;
+  const double s2tinf = s.sutherland_s / s.t_ref_dim, vtexp = s.powerlaw_vtexp, spr = 0.8;
+  std::vector<double> yvec(ny), uvec(ny), tvec(ny), rhovec(ny), viscvec(ny);
+  for (int j = 1; j <= ny; ++j) yvec[j - 1] = s.yg(j);
+  std::vector<double> cfvec, thvec, deltavec, deltavvec;
+  const std::string blvec = s.dir + "/blvec.bin";
+  if (!read_blvec(blvec, nxt, cfvec, thvec, deltavec, deltavvec)) {
+    cfvec.assign(nxt, 0.0);
+    thvec.assign(nxt, 0.0);
+    deltavec.assign(nxt, 0.0);
+    deltavvec.assign(nxt, 0.0);
+    std::vector<double> retauvec(nxt, 0.0);
+    auto hasan = [&](double d99, HasanState& h, int imode) {
+      hasan_meanprofile(ny, d99, s.mach, s.theta_wall, h, s.prandtl, spr, s.rfac, s.gam, vtexp, visc_exp, s2tinf,
+                        yvec.data(), uvec.data(), tvec.data(), rhovec.data(), viscvec.data(), imode, 0);
+    };
+    HasanState h;
+    h.retau = s.reynolds_friction;
+    hasan(s.l0, h, 0);
+    const double retheta_inflow = h.retheta;
+    deltavec[X(1)] = s.l0;
+    deltavvec[X(1)] = h.deltav;
+    cfvec[X(1)] = h.cf;
+    thvec[X(1)] = h.th;
+    retauvec[X(1)] = s.reynolds_friction;
+    // one station from its neighbour nb (the previous one of the march)
+    auto station = [&](int i, int nb, double& retheta) {
+      thvec[X(i)] = thvec[X(nb)] + (i > nb ? 1.0 : -1.0) * 0.5 * std::fabs(s.xg(i) - s.xg(nb)) * cfvec[X(nb)];
+      retheta = retheta / thvec[X(nb)] * thvec[X(i)];
+      double delta = deltavec[X(nb)] / thvec[X(nb)] * thvec[X(i)];
+      HasanState hs;
+      while (true) {
+        const double deltaold = delta;
+        hs = HasanState();
+        hs.retheta = retheta;
+        hasan(delta, hs, 1);
+        delta = deltavec[X(nb)] * hs.retau / retauvec[X(nb)] * std::sqrt(cfvec[X(nb)] / hs.cf);
+        if (std::fabs(delta - deltaold) < 0.000000001) break;
+      }
+      deltavec[X(i)] = delta;
+      cfvec[X(i)] = hs.cf;
+      deltavvec[X(i)] = hs.deltav;
+      retauvec[X(i)] = hs.retau;
+    };
+    double retheta = retheta_inflow;
+    for (int i = 1; i <= ng; ++i) station(1 - i, 2 - i, retheta);
+    retheta = retheta_inflow;
+    for (int i = 2; i <= nx + ng + 1; ++i) station(i, i - 1, retheta);
+    write_blvec(blvec, cfvec, thvec, deltavec, deltavvec);
+  }
+  s.deltavec = deltavec;
+  s.deltavvec = deltavvec;
+  // wmean(1-ng:nx+ng+1, 1:ny, 4) from the profile of every station (independent stations)
+  s.wmean.assign(static_cast<size_t>(nxt) * ny * 4, 0.0);
+  auto WM = [&](int i, int j, int m) -> double& {
+    return s.wmean[(static_cast<size_t>(m - 1) * ny + (j - 1)) * nxt + X(i)];
+  };
+  {
+    const unsigned nthr = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < nthr; ++t)
+      pool.emplace_back([&, t] {
+        std::vector<double> uv(ny), tv(ny), rv(ny), mv(ny);
+        for (int i = 1 - ng + static_cast<int>(t); i <= nx + ng + 1; i += static_cast<int>(nthr)) {
+          HasanState hs;
+          hs.retau = deltavec[X(i)] / deltavvec[X(i)];
+          hasan_meanprofile(ny, deltavec[X(i)], s.mach, s.theta_wall, hs, s.prandtl, spr, s.rfac, s.gam, vtexp,
+                            visc_exp, s2tinf, yvec.data(), uv.data(), tv.data(), rv.data(), mv.data(), 0, 1);
+          for (int j = 1; j <= ny; ++j) {
+            WM(i, j, 1) = rv[j - 1] * s.rho0;
+            WM(i, j, 2) = rv[j - 1] * uv[j - 1] * s.u0 * s.rho0;
+          }
+        }
+      });
+    for (auto& th : pool) th.join();
+  }
+  for (int i = 1 - ng; i <= nx + ng; ++i)
+    for (int j = 2; j <= ny; ++j) {
+      const double vi_j = -(WM(i + 1, j, 2) - WM(i, j, 2)) / (s.xg(i + 1) - s.xg(i));
+      const double vi_jm = -(WM(i + 1, j - 1, 2) - WM(i, j - 1, 2)) / (s.xg(i + 1) - s.xg(i));
+      const double vi = 0.5 * (vi_j + vi_jm);
+      WM(i, j, 3) = WM(i, j - 1, 3) + vi * (s.yg(j) - s.yg(j - 1));
+    }
+  const unsigned seed = s.rand_type == 0 ? 0u : 1u;
+  const double rescale = s.rand_type == 0 ? 0.0 : 1.0;
+  GlibcRand rnd(seed);
+  long long draws = 0;
+  auto crandom = [&]() {
+    ++draws;
+    return rescale * static_cast<double>(rnd()) / RAND_MAX;
+  };
+  const double u0_02 = s.rand_type == 0 ? 0.0 : 0.02 * s.u0;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const double rho = WM(i, j, 1);
+        double rr[3];
+        for (int l = 0; l < 3; ++l) rr[l] = crandom();
+        for (int l = 0; l < 3; ++l) rr[l] = rr[l] - 0.5;
+        const double uu = WM(i, j, 2) / rho + u0_02 * rr[0];
+        const double vv = WM(i, j, 3) / rho + u0_02 * rr[1];
+        const double ww = WM(i, j, 4) / rho + u0_02 * rr[2];
+        const double rhouu = rho * uu, rhovv = rho * vv, rhoww = rho * ww;
+        s.w[s.widx(i, j, k, 0)] = rho;
+        s.w[s.widx(i, j, k, 1)] = rhouu;
+        s.w[s.widx(i, j, k, 2)] = rhovv;
+        s.w[s.widx(i, j, k, 3)] = rhoww;
+        const double tt = s.p0 / s.rgas0 / rho;
+        const double ee = e_from_t(s, tt);
+        s.w[s.widx(i, j, k, 4)] = rho * ee + 0.5 * (rhouu * rhouu + rhovv * rhovv + rhoww * rhoww) / rho;
+      }
+  // add_synthetic_perturbations
+  double sp[5][7] = {{12.0, 1.2, -0.25, 0.12, 10.0, 120.0, 0.0},
+                     {0.3, 0.3, -0.06, 1.2, 0.9, 0.333, 1.0},
+                     {0.45, 0.2, -0.05, 0.6, 0.9, 0.25, 1.0},
+                     {0.6, 0.08, -0.04, 0.4, 0.9, 0.2, 1.0},
+                     {0.5, 0.04, -0.03, 0.2, 0.9, 0.166, 1.0}};
+  const double pi_p = pi();
+  const double lz = s.domain_size[2];
+  const double rho_wall = WM(1, 1, 1);
+  const double tau_wall = cfvec[X(1)] * s.rho0 * (s.u0 * s.u0) * 0.5;
+  const double u_tau = std::sqrt(tau_wall / rho_wall);
+  sp[0][0] = sp[0][0] * deltavvec[X(1)];
+  sp[0][3] = sp[0][3] * u_tau / deltavvec[X(1)];
+  sp[0][4] = sp[0][4] * u_tau;
+  const double lz_plus = lz / deltavvec[X(1)];
+  const long long n_streaks = std::llround(lz_plus / sp[0][5]);
+  sp[0][5] = lz / static_cast<double>(n_streaks);
+  for (int l = 1; l < 5; ++l) {
+    sp[l][0] = sp[l][0] * deltavec[X(1)];
+    sp[l][3] = sp[l][3] * s.u0 / deltavec[X(1)];
+    sp[l][4] = sp[l][4] * s.u0;
+    sp[l][5] = sp[l][5] * lz;
+    const double rr = crandom();
+    sp[l][6] = sp[l][6] * 2.0 * pi_p * rr;
+  }
+  const double u0_03 = s.rand_type == 0 ? 0.0 : 0.03 * s.u0;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        double rhofac = WM(i, 1, 1) / WM(i, j, 1);
+        rhofac = std::sqrt(rhofac) * s.u0;
+        double up = 0.0, vp = 0.0, wp = 0.0;
+        const double xx = s.xg(i), yy = s.yg(j), zz = s.zg(k);
+        for (int l = 1; l < 5; ++l) {
+          const double arg_sin = sp[l][3] * xx / sp[l][4];
+          const double arg_cos = 2.0 * pi_p * zz / sp[l][5] + sp[l][6];
+          const double ys = yy / sp[l][0];
+          const double ufy = ys * std::exp(-ys);
+          const double vfy = (ys * ys) * std::exp(-(ys * ys));
+          up = up + sp[l][1] * ufy * std::sin(arg_sin) * std::cos(arg_cos);
+          vp = vp + sp[l][2] * vfy * std::sin(arg_sin) * std::cos(arg_cos);
+          const double dup_dx = sp[l][1] * ufy * sp[l][3] / sp[l][4] * std::cos(arg_sin);
+          const double dvfy_dy = 2.0 * ys / sp[l][0] * std::exp(-(ys * ys)) * (1.0 - (ys * ys));
+          const double dvp_dy = sp[l][2] * dvfy_dy * std::sin(arg_sin);
+          wp = wp - (dup_dx + dvp_dy) * std::sin(arg_cos) * sp[l][5] / (2.0 * pi_p);
+        }
+        up = up * rhofac;
+        vp = vp * rhofac;
+        wp = wp * rhofac;
+        const double delta = deltavec[X(i)];
+        if (yy < delta) {
+          double rr3[3];
+          for (int l = 0; l < 3; ++l) rr3[l] = crandom();
+          for (int l = 0; l < 3; ++l) rr3[l] = rr3[l] - 0.5;
+          up = up + u0_03 * rr3[0] * (yy / s.l0);
+          vp = vp + u0_03 * rr3[1] * (yy / s.l0);
+          wp = wp + u0_03 * rr3[2] * (yy / s.l0);
+        }
+        double* w1 = &s.w[s.widx(i, j, k, 0)];
+        double& w2 = s.w[s.widx(i, j, k, 1)];
+        double& w3 = s.w[s.widx(i, j, k, 2)];
+        double& w4 = s.w[s.widx(i, j, k, 3)];
+        const double rho = *w1;
+        w2 = w2 + up * *w1;
+        w3 = w3 + vp * *w1;
+        w4 = w4 + wp * *w1;
+        const double tt = s.p0 / s.rgas0 / rho;
+        const double ee = e_from_t(s, tt);
+        s.w[s.widx(i, j, k, 4)] = rho * ee + 0.5 * (w2 * w2 + w3 * w3 + w4 * w4) / *w1;
+      }
+  s.rng_seed = seed;
+  s.rng_draws = draws;
 }
 
 // recyc_prepare (singleideal.F90:1512-1588), single block
@@ -1078,7 +1464,8 @@ Setup setup_from_ini(const IniFile& ini, const std::string& dir) {
       read_field_info(s);
     }
   } else {
-    init_channel(s);
+    if (s.flow_init == 1) init_bl(s);
+    else init_channel(s);
     if (s.restart_type == 1) {
       read_rst(s);
       read_field_info(s);

@@ -7,6 +7,9 @@ row stored in tests/tests.ini.  This script reproduces that patching for the Car
 
   subsonic_channel.ini   the patched input (values only, comments dropped)
   subsonic_channel.json  the expected 14-column progress row and its tolerance
+  supersonic_bl.ini,     the reference's boundary-layer and shock-interaction example inputs
+  supersonic_sbli.ini    (init_bl with hasan_meanprofile and add_synthetic_perturbations), with the
+                         grid reduced to 256 x 64 x 32 (nywr 40) and 10 steps so a test runs them
 
 The runner splits each patch on the first ',' of every ';'-separated item, so the item
 ``controls,num_iter=10,controls,rand_type=0`` sets num_iter to "10,controls,rand_type=0"
@@ -74,6 +77,19 @@ def main():
         "expected": expected,
     }, indent=1))
     print("wrote", HERE / "subsonic_channel.ini", HERE / "subsonic_channel.json")
+    for ex in ("supersonic_bl", "supersonic_sbli"):
+        sections, order = parse_ini((ref / "examples" / ex / "singleideal.ini").read_text())
+        reduced = {("grid", "nxmax"): "256", ("grid", "nymax"): "64", ("grid", "nzmax"): "32",
+                   ("grid", "nywr"): "40", ("controls", "num_iter"): "10", ("output", "print_control"): "1"}
+        for (sec, key), val in reduced.items():
+            sections[sec][key] = val
+        out = []
+        for sec in order:
+            out.append(f"[{sec}]")
+            out += [f"{k} = {v}" for k, v in sections[sec].items()]
+            out.append("")
+        (HERE / f"{ex}.ini").write_text("\n".join(out))
+        print("wrote", HERE / f"{ex}.ini")
 
 
 if __name__ == "__main__":

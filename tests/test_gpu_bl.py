@@ -133,3 +133,17 @@ def test_bl_inflow_draws_continue_the_setup_sequence(tmp_path):
     g = o.ng
     a, b = s0.copy_to_field()[:, g:-g, g:-g, :g], s.copy_to_field()[:, g:-g, g:-g, :g]
     assert rel_l2(a, b) > 1e-6  # the inflow ghosts carry other random numbers
+
+
+@pytest.mark.parametrize("example", ["supersonic_bl", "supersonic_sbli"])
+def test_reference_example_inputs_ten_steps(example, tmp_path):
+    """The reference's own boundary-layer and shock-interaction inputs (examples/supersonic_bl,
+    supersonic_sbli: init_bl with hasan_meanprofile and the synthetic streaks, Sutherland
+    viscosity, recycling inflow, NR outflow and top, impinging shock) with the grid reduced to
+    256x64x32: 10 steps on the device against the oracle within 1e-12."""
+    from conftest import ROOT
+    ini = (ROOT / "tests" / "golden" / f"{example}.ini").read_text()
+    o, s = pair(tmp_path, ini, 10)
+    compare(o, s, 1e-12)
+    so, sg = o.scalars(), s.scalars()
+    assert abs(sg["dt"] - so["dt"]) <= 1e-12 * so["dt"]
