@@ -609,6 +609,15 @@ def main():
                  "max_rel_l2": max(errs),
                  "precision": "FP32 flux/viscous arithmetic, FP64 state, RK register, T recovery, sensor, dt, "
                               "reductions"}
+        # the long-run check of the mean flow (5000 steps of the channel at 512x256x256 and the
+        # shock interaction at 1024x256x128 in both precisions, statistics post-processed as
+        # tools/postpro does): too long for this run, measured by streams_b200.mean_profile_check
+        mp = ROOT / "profiles" / "mixed_mean_profile_5000.json"
+        if mp.exists():
+            mixed["mean_profile_err_5000"] = {
+                k: {"max_rel_diff": v["max_rel_diff_mixed_vs_fp64"], "stat_samples": v["stat_samples"],
+                    "source": "profiles/mixed_mean_profile_5000.json"}
+                for k, v in json.loads(mp.read_text()).items()}
         for wl in ("channel", "sbli"):
             if wl == args.workload:
                 continue
