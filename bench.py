@@ -571,7 +571,7 @@ def main():
     # mixed form (FP32 fluxes, FP64 state): throughput on the headline workload and on the two
     # mixed-precision workloads (the channel at 512x256x256, the shock / boundary-layer interaction at
     # 1024x256x128), each with its error against the FP64 form after 100 steps of a smaller case
-    def device_rate(cs, precision):
+    def device_rate(cs, precision, kernel_table=None):
         sv = Solver.from_case(cs, precision=precision)
         sv.init_run()
         sv.advance(args.warmup, 1, 0, 0)
@@ -585,6 +585,20 @@ def main():
         t_ms = max_over_ranks(a0.elapsed_time(a1))
         n_ = cs.shape[0] * cs.shape[1] * cs.shape[2]
         sv.close()
+        if kernel_table is not None:
+            # per-kernel device time of the same steps replayed with the event profiler
+            sp_ = Solver.from_case(cs, precision=precision)
+            sp_.init_run()
+            sp_.advance(args.warmup, 1, 0, 0)
+            sp_.profile(-1)
+            sp_.profile(1)
+            sp_.advance(args.steps, 1, args.warmup, 0)
+            sp_.synchronize()
+            sp_.profile(0)
+            rep = sp_.profile_report()
+            sp_.close()
+            kernel_table.update({k: round(v[0] / args.steps, 3)
+                                 for k, v in sorted(rep.items(), key=lambda kv: -kv[1][0])})
         return n_ * args.steps * world / (t_ms / 1e3) / 1e6, t_ms
 
     def mixed_error(wl, dims):
@@ -602,11 +616,12 @@ def main():
     small = {"bl": (128, 64, 32), "channel": (128, 96, 64), "sbli": (128, 64, 32)}
     mixed = None
     if not args.no_mixed:
-        mval, mms = device_rate(case, 1)
+        mkern = {}
+        mval, mms = device_rate(case, 1, mkern)
         errs = mixed_error(args.workload, small[args.workload])
         mixed = {"value": mval, "unit": "Mcell-steps/s", "ms_per_step": mms / args.steps, "speedup_vs_fp64": mval / value,
                  "rel_l2_vs_fp64_100_steps": errs, "error_case": "x".join(map(str, small[args.workload])),
-                 "max_rel_l2": max(errs),
+                 "max_rel_l2": max(errs), "kernels_ms_per_step": mkern,
                  "precision": "FP32 flux/viscous arithmetic, FP64 state, RK register, T recovery, sensor, dt, "
                               "reductions"}
         # the long-run check of the mean flow (5000 steps of the channel at 512x256x256 and the

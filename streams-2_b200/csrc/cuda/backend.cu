@@ -490,8 +490,12 @@ int streams_b200_create(const streams_b200_params* p, const streams_b200_grid* g
     RngState hs;
     for (int q = 0; q < 34; ++q) hs.ring[q] = r.ring()[q];
     hs.pos = r.position();
+    std::vector<unsigned int> jump;
+    rand_jump_table((long long)(p->jbl_inflow - 1) * p->nz * 3, jump);
+    if ((e = dev_alloc(c, &d.rcoef, jump.size() + 1))) return fail(e, "cudaMalloc(inflow state)");
     if ((e = cudaMemcpy(d.rplane, half.data(), npl * 8, cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy(d.rng, &hs, sizeof(RngState), cudaMemcpyHostToDevice)))
+        (e = cudaMemcpy(d.rng, &hs, sizeof(RngState), cudaMemcpyHostToDevice)) ||
+        (!jump.empty() && (e = cudaMemcpy(d.rcoef, jump.data(), jump.size() * 4, cudaMemcpyHostToDevice))))
       return fail(e, "cudaMemcpy(inflow state)");
   }
   d.red_capacity = reduction_slots(g);

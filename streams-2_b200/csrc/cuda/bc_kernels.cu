@@ -190,50 +190,39 @@ __global__ void __launch_bounds__(BC_NT) k_recyc_fill(Geom g, double* __restrict
   }
 }
 
-// The random plane of one stage (euler_z's get_crandom_f on inflow_random_plane(2:jbl_inflow,
-// 1:nz, 1:3), singleideal_cpu.F90:841; first index outermost, code/third-party/crandom/
-// crandom_f.F90:81-93), drawn from the continued glibc sequence.  The draws are strictly
-// sequential, so one thread produces the raw words (k_rand_words) and a second kernel converts
-// and scatters them in parallel (k_rand_scatter).  The 34-word ring is rotated into registers
-// so that slot s holds the word of the positions congruent to pos + s (mod 34); blocks of 34
-// draws are unrolled with compile-time slots: new word of slot s = slot (s+3) + slot (s+31).
-__global__ void k_rand_words(RngState* __restrict__ st, unsigned int* __restrict__ words, long long total) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  unsigned int r[34];
-  const long long pos0 = st->pos;
-  const int p0 = (int)(pos0 % 34);
+// The random inflow plane of a stage continues the glibc sequence (random(): additive feedback
+// x_n = x_(n-31) + x_(n-3) mod 2^32, output x_n >> 1; crandom.c, crandom_f.F90:81-93), but is
+// drawn in parallel: the recurrence is linear, so with y_k the 31 words before the stage
+// (y_0 .. y_30) every later word is y_m = sum_i c_i y_i, c the coefficients of t^m mod
+// (t^31 - t^28 - 1) over the integers mod 2^32.  Thread c starts from the host-made
+// coefficients of its chunk's first word and steps them by t (one shift and one addition) for
+// each further word of its chunk: every draw is the reference's, bit for bit.  The 32-bit words
+// go to `words`; the scatter kernel converts them and advances the ring.
+__global__ void __launch_bounds__(128) k_rand_words(const RngState* __restrict__ st, const unsigned int* __restrict__ coef,
+                                                    unsigned int* __restrict__ words, long long total) {
+  const long long c = (long long)blockIdx.x * 128 + threadIdx.x;
+  const long long i0 = c * RAND_CHUNK;
+  if (i0 >= total) return;
+  const long long pos0 = st->pos;  // >= 344: the generator discards 310 words at seeding
+  unsigned int y[31], cv[31];
 #pragma unroll
-  for (int s = 0; s < 34; ++s) {
-    int idx = p0 + s;
-    if (idx >= 34) idx -= 34;
-    r[s] = st->ring[idx];
+  for (int i = 0; i < 31; ++i) {
+    y[i] = st->ring[(pos0 - 31 + i) % 34];
+    cv[i] = coef[c * 31 + i];
   }
-  const long long nblk = total / 34;
-  for (long long b = 0; b < nblk; ++b) {
+  const int n = (int)(total - i0 < RAND_CHUNK ? total - i0 : RAND_CHUNK);
+  for (int r = 0; r < n; ++r) {
+    unsigned int v = 0;
 #pragma unroll
-    for (int s = 0; s < 34; ++s) {
-      r[s] = r[(s + 3) % 34] + r[(s + 31) % 34];
-      words[b * 34 + s] = r[s] >> 1;
-    }
-  }
-  const int rem = (int)(total - nblk * 34);
+    for (int i = 0; i < 31; ++i) v += cv[i] * y[i];
+    words[i0 + r] = v;
+    // cv <- t cv mod (t^31 - t^28 - 1): the t^31 term becomes t^28 + 1
+    const unsigned int top = cv[30];
 #pragma unroll
-  for (int s = 0; s < 34; ++s) {
-    if (s < rem) {
-      r[s] = r[(s + 3) % 34] + r[(s + 31) % 34];
-      words[nblk * 34 + s] = r[s] >> 1;
-    }
+    for (int i = 30; i > 0; --i) cv[i] = cv[i - 1];
+    cv[0] = top;
+    cv[28] += top;
   }
-  // the ring after `total` draws: slot s now holds the latest word of its residue class except
-  // for the slots >= rem of the last (partial) block, which still hold the block before; both
-  // are the words of the last 34 positions, stored at ring[(position) mod 34]
-#pragma unroll
-  for (int s = 0; s < 34; ++s) {
-    int idx = p0 + s;
-    if (idx >= 34) idx -= 34;
-    st->ring[idx] = r[s];
-  }
-  st->pos = pos0 + total;
 }
 
 // draw d of the stage: component c = d mod 3, k = (d / 3) mod nz + 1, j = d / (3 nz) + 2
@@ -244,8 +233,20 @@ __global__ void __launch_bounds__(256) k_rand_scatter(Geom g, const unsigned int
   const int c = (int)(d % 3);
   const long long jk = d / 3;
   const int k = (int)(jk % g.nz) + 1, j = (int)(jk / g.nz) + 2;
-  const int v = (int)words[d];
+  const int v = (int)(words[d] >> 1);
   rplane[(long long)c * g.ny * g.nz + (long long)(k - 1) * g.ny + (j - 1)] = g.rand_scale * (double)v / 2147483647.0;
+}
+
+// the generator's ring after the stage's draws: the last 34 words at their positions mod 34
+__global__ void __launch_bounds__(64) k_rand_advance(RngState* __restrict__ st, const unsigned int* __restrict__ words,
+                                                     long long total) {
+  const long long pos0 = st->pos;
+  __syncthreads();
+  if (threadIdx.x < 34) {
+    const long long idx = total - 34 + threadIdx.x;
+    if (idx >= 0) st->ring[(pos0 + idx) % 34] = words[idx];
+  }
+  if (threadIdx.x == 0) st->pos = pos0 + total;
 }
 
 // bc_nr_lat_x_kernel / bc_nr_lat_y_kernel (kernels_cpu.F90:5169-5283, 5420-5540): characteristic
@@ -406,13 +407,55 @@ bool has_stored_ghosts(const Geom& g) {
   return false;
 }
 
+namespace {
+// a b mod (t^31 - t^28 - 1), coefficients mod 2^32 (t^k = t^(k-3) + t^(k-31) for k >= 31)
+void polymulmod(const unsigned int* a, const unsigned int* b, unsigned int* out) {
+  unsigned int prod[61] = {};
+  for (int i = 0; i < 31; ++i)
+    for (int j = 0; j < 31; ++j) prod[i + j] += a[i] * b[j];
+  for (int k = 60; k >= 31; --k) {
+    const unsigned int c = prod[k];
+    prod[k] = 0;
+    prod[k - 3] += c;
+    prod[k - 31] += c;
+  }
+  for (int i = 0; i < 31; ++i) out[i] = prod[i];
+}
+}  // namespace
+
+void rand_jump_table(long long total, std::vector<unsigned int>& table) {
+  const long long nchunk = (total + RAND_CHUNK - 1) / RAND_CHUNK;
+  table.assign((size_t)nchunk * 31, 0u);
+  if (nchunk == 0) return;
+  // t^RAND_CHUNK by repeated multiplication with t, the first chunk's t^31 = t^28 + 1
+  unsigned int step[31] = {}, t1[31] = {}, cur[31] = {};
+  step[0] = 1;
+  t1[1] = 1;
+  for (int q = 0; q < RAND_CHUNK; ++q) {
+    unsigned int nx[31];
+    polymulmod(step, t1, nx);
+    for (int i = 0; i < 31; ++i) step[i] = nx[i];
+  }
+  cur[0] = 1;
+  cur[28] = 1;
+  for (long long c = 0; c < nchunk; ++c) {
+    for (int i = 0; i < 31; ++i) table[(size_t)c * 31 + i] = cur[i];
+    unsigned int nx[31];
+    polymulmod(cur, step, nx);
+    for (int i = 0; i < 31; ++i) cur[i] = nx[i];
+  }
+}
+
 cudaError_t launch_rand_plane(const Geom& g, DevState& d, cudaStream_t s, long long* nl) {
   const long long total = (long long)(g.jbl_inflow - 1) * g.nz * 3;
   if (total <= 0) return cudaSuccess;
-  SB_LAUNCH(d, K_RAND_PLANE, s, k_rand_words<<<1, 32, 0, s>>>(d.rng, d.rwords, total));
+  const long long nchunk = (total + RAND_CHUNK - 1) / RAND_CHUNK;
+  SB_LAUNCH(d, K_RAND_PLANE, s,
+            k_rand_words<<<(unsigned)((nchunk + 127) / 128), 128, 0, s>>>(d.rng, d.rcoef, d.rwords, total));
   SB_LAUNCH(d, K_RAND_PLANE, s,
             k_rand_scatter<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(g, d.rwords, d.rplane, total));
-  *nl += 2;
+  SB_LAUNCH(d, K_RAND_PLANE, s, k_rand_advance<<<1, 64, 0, s>>>(d.rng, d.rwords, total));
+  *nl += 3;
   return cudaGetLastError();
 }
 

@@ -55,7 +55,10 @@ struct DevState {
   // recycling inflow: the random plane inflow_random_plane(j,k,c) at [(c*nz + k-1)*ny + j-1],
   // the spanwise means of the recycling plane [(m*ny + j-1)*ng + i-1], the generator state
   double* rplane = nullptr;
-  unsigned int* rwords = nullptr;  // raw draws of one stage
+  unsigned int* rwords = nullptr;  // raw draws of one stage (the full 32-bit words)
+  // jump-ahead table of the parallel generator: for chunk c of RAND_CHUNK draws, the 31
+  // coefficients of t^(31 + c RAND_CHUNK) mod (t^31 - t^28 - 1) over the integers mod 2^32
+  unsigned int* rcoef = nullptr;
   double* recyc_av = nullptr;
   RngState* rng = nullptr;
   // running statistics (allocated on first use), statistic index fastest:
@@ -101,6 +104,10 @@ cudaError_t launch_add_time(DevState& d, cudaStream_t s, long long* nl);
 // partial-sum slots needed for a geometry
 // open boundaries (bc_kernels.cu)
 cudaError_t launch_bc_fill(const Geom& g, DevState& d, cudaStream_t s, long long* nl);
+// draws per chunk of the parallel inflow-plane generator
+constexpr int RAND_CHUNK = 64;
+// The jump-ahead table (nchunk x 31 words) of a stage's draws, built on the host at create.
+void rand_jump_table(long long total, std::vector<unsigned int>& table);
 cudaError_t launch_rand_plane(const Geom& g, DevState& d, cudaStream_t s, long long* nl);
 cudaError_t launch_bc_nr(const Geom& g, DevState& d, double* fl, cudaStream_t s, long long* nl);
 bool has_stored_ghosts(const Geom& g);
