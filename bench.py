@@ -196,10 +196,12 @@ def case_ini(workload, nx, ny, nz, steps):
 DEFAULT_SIZE = {"bl": "1024x256x192", "channel": "512x256x256", "sbli": "1024x256x128"}
 
 
-def run_batched(torch, precision, steps, warmup, tune_cache):
+def run_batched(torch, precision, steps, warmup, tune_cache, shared=1):
     """The batched form: 48 channel boxes of uneven grids and flow parameters (seeded mix),
-    autotuned launch shapes, one CUDA graph per 10 steps of all boxes.  Device time from CUDA
-    events recorded on every box's stream (start on the first box, max over the ends)."""
+    autotuned launch shapes, one CUDA graph per 10 steps of all boxes: with shared launches (one
+    launch per kernel kind and stage over the box table of all 48 boxes; shared=2: the boxes in
+    two such groups on parallel graph branches) or, shared=0, one graph branch per box.  Device time from CUDA events recorded on every box's stream (start on
+    the first box, max over the ends)."""
     from streams_b200 import Batch, Case, Solver
     from streams_b200.cases import batch_mix
     from streams_b200.tune import autotune
@@ -219,6 +221,8 @@ def run_batched(torch, precision, steps, warmup, tune_cache):
             solvers.append(sv)
             cells += nx * ny * nz
     batch = Batch(solvers, steps_per_graph=10)
+    batch.set_shared_launches(shared)
+    groups = batch.groups()
     batch.advance(1 + warmup)
     batch.synchronize()
     streams = [torch.cuda.ExternalStream(sv.stream_handle) for sv in solvers]
@@ -239,7 +243,7 @@ def run_batched(torch, precision, steps, warmup, tune_cache):
         sv.close()
     return {"value": cells * steps / (ms / 1e3) / 1e6, "unit": "Mcell-steps/s", "boxes": len(boxes),
             "cells": cells, "steps": steps, "ms": ms, "graph_replays": replays, "launches_per_replay": per,
-            "gpu_launches": launches}
+            "gpu_launches": launches, "shared_launches": shared, "groups": groups[0], "boxes_in_groups": groups[1]}
 
 
 def run_serving(torch, duration_s, step_scale, single_rate, tune_cache):
@@ -274,9 +278,11 @@ def run_serving(torch, duration_s, step_scale, single_rate, tune_cache):
             "mcell_steps_per_s": out["mcell_steps_per_s"], "mcell_steps_per_busy_s": out["mcell_steps_per_busy_s"],
             "max_resident": out["max_resident"], "ticks": out["ticks"], "budget_gb": budget / 1e9,
             "offered_mcell_steps_per_s": work / duration_s / 1e6, "loop_admit_wait_s": out["admit_wait_s"],
-            "loop_iterations": out["loop_iterations"],
-            "loop": "admission (tuning, context, first step, graph capture) on 2 admission threads; each "
-                    "resident solve gets its next 10-step tick when its stream reports the last one done"}
+            "loop_iterations": out["loop_iterations"], "cohort_ticks": out["cohort_ticks"],
+            "max_cohort": out["max_cohort"],
+            "loop": "admission (tuning, context, first step, first tick) on 2 admission threads; the resident "
+                    "solves of a class take their next 10-step tick together (a cohort: shared launches over their "
+                    "box table) once all of them are seen done, a solve without a class on its own"}
 
 
 def cpu_oracle_rate(workload, nx, ny, nz, nsteps, budget_s=20.0):
@@ -653,11 +659,17 @@ def main():
     if not args.no_batched:
         batched = {"fp64": run_batched(torch, 0, args.batched_steps, args.warmup, tune_cache),
                    "mixed": run_batched(torch, 1, args.batched_steps, args.warmup, tune_cache)}
+        # the same boxes in two groups on parallel branches, and with a graph branch per box
+        for name, shared in (("two_groups", 2), ("separate_branches", 0)):
+            for k, prec in (("fp64", 0), ("mixed", 1)):
+                o = run_batched(torch, prec, args.batched_steps, args.warmup, tune_cache, shared=shared)
+                batched[k][name] = {q: o[q] for q in ("value", "ms", "launches_per_replay", "groups")}
         batched["fp64"]["vs_single_box"] = batched["fp64"]["value"] / value
         if mixed:
             batched["mixed"]["vs_single_box"] = batched["mixed"]["value"] / mixed["value"]
         batched["workload"] = ("48 channel boxes, grids from {64,96,128}x{64,96}x{32,64,96}, Mach U[0.3,2], "
-                               "Re_b U[2000,6000], seeded; one CUDA graph per 10 steps of all boxes")
+                               "Re_b U[2000,6000], seeded; one CUDA graph per 10 steps of all boxes, shared launches over "
+                               "the box table (one launch per kernel kind and stage)")
     serving = None
     if not args.no_serve:
         serving = run_serving(torch, args.serve_seconds, args.serve_step_scale, value, tune_cache)

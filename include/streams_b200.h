@@ -313,10 +313,14 @@ int streams_b200_get_weno_split(streams_b200_ctx* ctx, double* max_fraction);
 
 /*
  * Batched form: many independent contexts (boxes of any size and flow parameters, one device,
- * one precision each) advanced together.  The per-box step sequences (compute_dt + rk_sync)
- * are captured once into one CUDA graph whose branches, one per box, run concurrently on the
- * GPU; each streams_b200_batch_advance replays it.  No counterpart in the reference (one box
- * per MPI rank there).
+ * one precision each) advanced together.  The step sequences (compute_dt + rk_sync) of
+ * steps_per_graph steps are captured once into one CUDA graph; each streams_b200_batch_advance
+ * replays it.  Boxes whose stages take the same kernels (precision, scheme orders and form,
+ * channel forcing, viscous form; periodic or staggered-wall faces only, WENO faces computed
+ * inside the hybrid passes) form a group that advances by shared launches: one launch per
+ * kernel kind and stage covers every box of the group, each block working on one box in the
+ * block partition the box uses alone.  Other boxes keep their own step sequence as a parallel
+ * branch of the graph.  No counterpart in the reference (one box per MPI rank there).
  *
  *   steps_per_graph  time steps per graph replay (>= 1)
  *   dt_every         dt is recomputed at batch steps s with s % dt_every == 0 (contexts with
@@ -338,8 +342,18 @@ int streams_b200_batch_create(streams_b200_ctx** ctxs, int n, int steps_per_grap
 int streams_b200_batch_advance(streams_b200_batch* b, int nsteps);
 int streams_b200_batch_synchronize(streams_b200_batch* b);
 int streams_b200_batch_invalidate(streams_b200_batch* b);
+/* Class of a context for shared launches: contexts of one batch with equal non-negative
+ * classes (and equal RK coefficients) form a group; -1 for a context that always advances on
+ * its own branch. */
+int streams_b200_batch_class(streams_b200_ctx* ctx, long long* cls);
 /* Graph replays issued and kernel launches they contain (instrumentation). */
 int streams_b200_batch_stats(streams_b200_batch* b, long long* replays, long long* launches_per_replay);
+/* Shared launches: the boxes of a class in groups_per_class groups (1, the default: one group per
+ * class; the groups' launch chains are parallel branches of the graph), or 0: every box its own
+ * branch. */
+int streams_b200_batch_set_shared_launches(streams_b200_batch* b, int groups_per_class);
+/* Groups that share launches and the boxes they hold. */
+int streams_b200_batch_groups(streams_b200_batch* b, int* ngroups, int* nshared);
 const char* streams_b200_batch_last_error(streams_b200_batch* b);
 int streams_b200_batch_destroy(streams_b200_batch* b);
 

@@ -806,6 +806,13 @@ int streams_b200_query(streams_b200_ctx* c) {
   return 0;
 }
 
+int streams_b200_batch_class(streams_b200_ctx* c, long long* cls) {
+  if (!c || !cls) return set_err(c, STREAMS_B200_EINVAL, "null argument");
+  const long long k = batch_key(c->g);
+  *cls = k < 0 ? -1 : 2 * k + (c->p.cfl > 0 ? 1 : 0);
+  return STREAMS_B200_OK;
+}
+
 static int ensure_stats(streams_b200_ctx* c, bool three_d) {
   const size_t n2 = (size_t)NV_STAT * c->p.nx * c->p.ny;
   if (!c->d.wstat) {
@@ -935,14 +942,28 @@ int streams_b200_get_weno_split(streams_b200_ctx* c, double* max_fraction) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------------------------
-// Batched form: one CUDA graph holding every box's step sequence as a parallel branch.
+// Batched form: one CUDA graph per replay of steps_per_graph steps of every box.  Boxes whose
+// stages take the same kernels form a group that advances by launches over a box table
+// (batch_kernels.cu): one launch per kernel kind and stage for the whole group.  A box that
+// belongs to no group (a configuration the table form does not cover, or the only box of its
+// kind) keeps its own step sequence as a parallel branch of the graph.
+
+// A branch of the batch: one box alone, or a group of boxes sharing launches (table != -1)
+struct BatchBranch {
+  std::vector<int> boxes;
+  int table = -1;
+};
 
 struct streams_b200_batch {
   std::vector<streams_b200_ctx*> ctxs;
-  std::vector<long long> launches_per_replay;  // per box
+  std::vector<long long> launches_per_replay;  // per box (a group's launches count on its first box)
   std::vector<long long> tuned_threads;        // per box tuning the graph was captured with
   std::vector<int> tuned_minseg;
   std::vector<double> tuned_wsplit;
+  int groups_per_class = 1;                    // 0: no shared launches; n: a class's boxes in n groups
+  std::vector<BatchBranch> branches;
+  std::vector<BoxTable> tables;
+  bool grouped = false;                        // branches and tables match the boxes' tuning
   int steps_per_graph = 1, dt_every = 1;
   long long step = 0;  // batch steps taken (drives the dt recompute pattern)
   long long replays = 0;
@@ -990,27 +1011,193 @@ void drop_graph(streams_b200_batch* b) {
   b->graph = nullptr;
 }
 
+void drop_groups(streams_b200_batch* b) {
+  // eager group steps run on the boxes' streams: the tables may be freed once those are done
+  if (!b->tables.empty())
+    for (auto* c : b->ctxs) cudaStreamSynchronize(c->stream);
+  for (auto& t : b->tables) box_table_free(t, b->master);
+  b->tables.clear();
+  b->branches.clear();
+  b->grouped = false;
+}
+
+// Group key of a box: the stage kernels it takes (batch_key) and the host-side step sequence
+// (time step computed or fixed, RK coefficients); -1 when it advances alone.
+std::string group_key(const streams_b200_ctx* c) {
+  const long long k = batch_key(c->g);
+  if (k < 0) return std::string();
+  std::string out = std::to_string(k) + (c->p.cfl > 0 ? "+" : "-");
+  out.append(reinterpret_cast<const char*>(c->p.rhork), sizeof(c->p.rhork));
+  out.append(reinterpret_cast<const char*>(c->p.gamrk), sizeof(c->p.gamrk));
+  return out;
+}
+
+// Branches of the batch and the box tables of its groups, from the boxes' current tuning.
+int make_groups(streams_b200_batch* b) {
+  drop_groups(b);
+  const int n = (int)b->ctxs.size();
+  std::vector<std::string> keys(n);
+  for (int i = 0; i < n; ++i) keys[i] = b->groups_per_class > 0 ? group_key(b->ctxs[i]) : std::string();
+  std::vector<bool> done(n, false);
+  std::vector<BatchBranch> cand;
+  for (int i = 0; i < n; ++i) {
+    if (done[i]) continue;
+    std::vector<int> cls{i};
+    done[i] = true;
+    if (!keys[i].empty())
+      for (int k = i + 1; k < n; ++k)
+        if (!done[k] && keys[k] == keys[i]) {
+          cls.push_back(k);
+          done[k] = true;
+        }
+    // a class's boxes in groups_per_class groups of about equal cell counts (largest box first
+    // into the lightest group), so that the groups' launches, on their own graph branches,
+    // overlap one another's memory-bound and arithmetic-bound passes
+    const int ng = std::max(1, std::min<int>(b->groups_per_class, (int)cls.size() / 2));
+    std::vector<BatchBranch> parts(ng);
+    std::vector<long long> load(ng, 0);
+    std::vector<int> order = cls;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int c) { return b->ctxs[a]->g.nint > b->ctxs[c]->g.nint; });
+    for (int q : order) {
+      const int t = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      parts[t].boxes.push_back(q);
+      load[t] += b->ctxs[q]->g.nint;
+    }
+    for (auto& pt : parts) {
+      std::sort(pt.boxes.begin(), pt.boxes.end());
+      cand.push_back(pt);
+    }
+  }
+  for (BatchBranch& br : cand) {
+    if (br.boxes.size() > 1) {
+      std::vector<BoxRec> recs;
+      for (int q : br.boxes) {
+        streams_b200_ctx* c = b->ctxs[q];
+        recs.push_back(box_rec(c->g, c->d, c->fl_a, c->fl_b, c->p.cfl));
+      }
+      BoxTable t;
+      cudaError_t e = box_table_build(t, recs, b->master);
+      if (e != cudaSuccess) {
+        drop_groups(b);
+        return batch_err(b, STREAMS_B200_ECUDA, std::string("box table: ") + cudaGetErrorString(e));
+      }
+      br.table = (int)b->tables.size();
+      b->tables.push_back(t);
+    }
+    b->branches.push_back(br);
+  }
+  for (int i = 0; i < n; ++i) {
+    b->tuned_threads[i] = b->ctxs[i]->g.march_threads;
+    b->tuned_minseg[i] = b->ctxs[i]->g.march_minseg;
+    b->tuned_wsplit[i] = b->ctxs[i]->g.weno_split_frac;
+  }
+  b->grouped = true;
+  return STREAMS_B200_OK;
+}
+
+// a box was re-tuned since the groups were formed (or the graph captured)
+bool tuning_changed(const streams_b200_batch* b) {
+  for (size_t i = 0; i < b->ctxs.size(); ++i)
+    if (b->ctxs[i]->g.march_threads != b->tuned_threads[i] || b->ctxs[i]->g.march_minseg != b->tuned_minseg[i] ||
+        b->ctxs[i]->g.weno_split_frac != b->tuned_wsplit[i])
+      return true;
+  return false;
+}
+
+// The host flags of a group's boxes agree (they do from the first completed step on).
+bool flags_agree(const streams_b200_batch* b, const BatchBranch& br) {
+  const streams_b200_ctx* c0 = b->ctxs[br.boxes[0]];
+  for (int q : br.boxes) {
+    const streams_b200_ctx* c = b->ctxs[q];
+    if (c->aux_current != c0->aux_current || c->shift_pending != c0->shift_pending) return false;
+  }
+  return true;
+}
+
+// One step of a group on the stream s, as box_step issues it for each box (do_compute_dt and
+// do_rk_sync, with the same host flags), by launches over the group's box table.
+int group_step(streams_b200_batch* b, const BatchBranch& br, long long step, cudaStream_t s) {
+  const BoxTable& t = b->tables[br.table];
+  streams_b200_ctx* c0 = b->ctxs[br.boxes[0]];
+  long long nl = 0;
+  cudaError_t e = cudaSuccess;
+  if (c0->p.cfl > 0 && step % b->dt_every == 0) {
+    if (!c0->aux_current || c0->shift_pending) {
+      e = batch_launch_aux(t, c0->shift_pending ? 1 : 0, s, &nl);
+      for (int q : br.boxes) {
+        streams_b200_ctx* c = b->ctxs[q];
+        c->shift_pending = false;
+        c->aux_current = true;
+        c->stats_ready = false;
+      }
+    }
+    if (e == cudaSuccess) e = batch_launch_dt(t, s, &nl);
+  }
+  const bool fv = c0->g.force_var != 0;
+  for (int istep = 1; istep <= 3 && e == cudaSuccess; ++istep) {
+    StageArgs a{};
+    a.istep = istep;
+    a.rhork = c0->p.rhork[istep - 1];
+    a.gamrk = c0->p.gamrk[istep - 1];
+    a.apply_shift = c0->shift_pending ? 1 : 0;
+    a.run_aux = (c0->aux_current && !c0->shift_pending) ? 0 : 1;
+    a.want_stats = istep == 3;
+    a.add_time = istep == 3;
+    e = batch_launch_stage(t, a, s, &nl);
+    for (int q : br.boxes) {
+      streams_b200_ctx* c = b->ctxs[q];
+      c->last_fl = istep == 2 ? c->fl_b : c->fl_a;
+      c->shift_pending = fv;
+      c->aux_current = false;
+    }
+  }
+  if (e != cudaSuccess)
+    return batch_err(b, STREAMS_B200_ECUDA, std::string("group step: ") + cudaGetErrorString(e));
+  for (int q : br.boxes) {
+    streams_b200_ctx* c = b->ctxs[q];
+    c->have_stats = true;
+    c->stats_ready = true;
+  }
+  c0->launches += nl;
+  return STREAMS_B200_OK;
+}
+
 int capture(streams_b200_batch* b) {
   drop_graph(b);
+  if (!b->grouped) {
+    int rc = make_groups(b);
+    if (rc) return rc;
+  }
   SB_BCHECK(b, cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
   int rc = STREAMS_B200_OK;
   std::string why;
   cudaError_t e = cudaEventRecord(b->ev_master, b->master);
-  for (size_t i = 0; i < b->ctxs.size() && e == cudaSuccess && rc == STREAMS_B200_OK; ++i) {
+  for (size_t r = 0; r < b->branches.size() && e == cudaSuccess && rc == STREAMS_B200_OK; ++r) {
+    const BatchBranch& br = b->branches[r];
+    const int i = br.boxes[0];
     streams_b200_ctx* c = b->ctxs[i];
     const long long l0 = c->launches;
     e = cudaStreamWaitEvent(c->stream, b->ev_master, 0);
     for (int s = 0; s < b->steps_per_graph && e == cudaSuccess && rc == STREAMS_B200_OK; ++s) {
-      rc = box_step(c, s, b->dt_every);
-      if (rc) why = "box " + std::to_string(i) + ": " + c->err;
+      if (br.table >= 0) {
+        rc = group_step(b, br, s, c->stream);
+        if (rc) why = "group of box " + std::to_string(i) + ": " + b->err;
+      } else {
+        rc = box_step(c, s, b->dt_every);
+        if (rc) why = "box " + std::to_string(i) + ": " + c->err;
+      }
     }
     if (e == cudaSuccess && rc == STREAMS_B200_OK) e = cudaEventRecord(b->ev_box[i], c->stream);
     if (e == cudaSuccess && rc == STREAMS_B200_OK) e = cudaStreamWaitEvent(b->master, b->ev_box[i], 0);
+    for (int q : br.boxes) b->launches_per_replay[q] = 0;
     b->launches_per_replay[i] = c->launches - l0;
     c->launches = l0;
-    b->tuned_threads[i] = c->g.march_threads;
-    b->tuned_minseg[i] = c->g.march_minseg;
-    b->tuned_wsplit[i] = c->g.weno_split_frac;
+  }
+  for (size_t i = 0; i < b->ctxs.size(); ++i) {
+    b->tuned_threads[i] = b->ctxs[i]->g.march_threads;
+    b->tuned_minseg[i] = b->ctxs[i]->g.march_minseg;
+    b->tuned_wsplit[i] = b->ctxs[i]->g.weno_split_frac;
   }
   cudaGraph_t gr = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(b->master, &gr);
@@ -1026,12 +1213,33 @@ int capture(streams_b200_batch* b) {
   return STREAMS_B200_OK;
 }
 
-// eager steps of every box on its own stream
+// eager steps: every lone box on its own stream, every group on its first box's stream (the
+// other boxes' streams joined before and after)
 int eager_steps(streams_b200_batch* b, int n) {
+  if (n > 0 && !b->grouped) {
+    int rc = make_groups(b);
+    if (rc) return rc;
+  }
   for (int s = 0; s < n; ++s) {
-    for (size_t i = 0; i < b->ctxs.size(); ++i) {
-      int rc = box_step(b->ctxs[i], b->step, b->dt_every);
-      if (rc) return batch_err(b, rc, "box " + std::to_string(i) + ": " + b->ctxs[i]->err);
+    for (const BatchBranch& br : b->branches) {
+      if (br.table >= 0 && flags_agree(b, br)) {
+        streams_b200_ctx* c0 = b->ctxs[br.boxes[0]];
+        for (size_t q = 1; q < br.boxes.size(); ++q) {
+          streams_b200_ctx* c = b->ctxs[br.boxes[q]];
+          SB_BCHECK(b, cudaEventRecord(b->ev_box[br.boxes[q]], c->stream));
+          SB_BCHECK(b, cudaStreamWaitEvent(c0->stream, b->ev_box[br.boxes[q]], 0));
+        }
+        int rc = group_step(b, br, b->step, c0->stream);
+        if (rc) return rc;
+        SB_BCHECK(b, cudaEventRecord(b->ev_box[br.boxes[0]], c0->stream));
+        for (size_t q = 1; q < br.boxes.size(); ++q)
+          SB_BCHECK(b, cudaStreamWaitEvent(b->ctxs[br.boxes[q]]->stream, b->ev_box[br.boxes[0]], 0));
+        continue;
+      }
+      for (int i : br.boxes) {
+        int rc = box_step(b->ctxs[i], b->step, b->dt_every);
+        if (rc) return batch_err(b, rc, "box " + std::to_string(i) + ": " + b->ctxs[i]->err);
+      }
     }
     ++b->step;
   }
@@ -1084,6 +1292,10 @@ int streams_b200_batch_advance(streams_b200_batch* b, int nsteps) {
   cudaSetDevice(b->device);
   for (auto* c : b->ctxs)
     if (c->prof.on) return batch_err(b, STREAMS_B200_EINVAL, "a profiled context cannot run in a batch");
+  if ((b->exec || b->grouped) && tuning_changed(b)) {
+    drop_graph(b);  // a box was re-tuned since the capture
+    drop_groups(b);
+  }
   bool all_steady = true;
   for (auto* c : b->ctxs) all_steady = all_steady && steady(c);
   if (!all_steady && nsteps > 0) {
@@ -1101,10 +1313,6 @@ int streams_b200_batch_advance(streams_b200_batch* b, int nsteps) {
   nsteps -= lead;
   const int nrep = nsteps / b->steps_per_graph;
   if (nrep > 0) {
-    for (size_t i = 0; i < b->ctxs.size() && b->exec; ++i)
-      if (b->ctxs[i]->g.march_threads != b->tuned_threads[i] || b->ctxs[i]->g.march_minseg != b->tuned_minseg[i] ||
-          b->ctxs[i]->g.weno_split_frac != b->tuned_wsplit[i])
-        drop_graph(b);  // a box was re-tuned since the capture
     if (!b->exec) {
       rc = capture(b);
       if (rc) return rc;
@@ -1137,6 +1345,37 @@ int streams_b200_batch_invalidate(streams_b200_batch* b) {
   if (!b) return batch_err(b, STREAMS_B200_EINVAL, "null batch");
   cudaSetDevice(b->device);
   drop_graph(b);
+  drop_groups(b);
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_batch_set_shared_launches(streams_b200_batch* b, int groups_per_class) {
+  if (!b) return batch_err(b, STREAMS_B200_EINVAL, "null batch");
+  if (groups_per_class < 0) return batch_err(b, STREAMS_B200_EINVAL, "negative groups_per_class");
+  cudaSetDevice(b->device);
+  if (b->groups_per_class != groups_per_class) {
+    drop_graph(b);
+    drop_groups(b);
+    b->groups_per_class = groups_per_class;
+  }
+  return STREAMS_B200_OK;
+}
+
+int streams_b200_batch_groups(streams_b200_batch* b, int* ngroups, int* nshared) {
+  if (!b) return batch_err(b, STREAMS_B200_EINVAL, "null batch");
+  cudaSetDevice(b->device);
+  if (!b->grouped) {
+    int rc = make_groups(b);
+    if (rc) return rc;
+  }
+  int g = 0, n = 0;
+  for (const BatchBranch& br : b->branches)
+    if (br.table >= 0) {
+      ++g;
+      n += (int)br.boxes.size();
+    }
+  if (ngroups) *ngroups = g;
+  if (nshared) *nshared = n;
   return STREAMS_B200_OK;
 }
 
@@ -1156,6 +1395,8 @@ int streams_b200_batch_destroy(streams_b200_batch* b) {
   cudaSetDevice(b->device);
   if (b->master) cudaStreamSynchronize(b->master);
   drop_graph(b);
+  for (auto* c : b->ctxs) cudaStreamSynchronize(c->stream);
+  drop_groups(b);
   for (auto ev : b->ev_box)
     if (ev) cudaEventDestroy(ev);
   if (b->ev_master) cudaEventDestroy(b->ev_master);

@@ -12,6 +12,14 @@
 #define SB_CACHE_C 0
 #endif
 
+// characteristic fields reconstructed per iteration of the WENO branch's field loop (1: one copy
+// of wenorec, the loop rolled; the unrolled loop overflowed the instruction cache)
+#ifndef SB_WENO_UNROLL
+#define SB_WENO_UNROLL 1
+#endif
+#define SB_PRAGMA_(x) _Pragma(#x)
+#define SB_UNROLL_(n) SB_PRAGMA_(unroll n)
+
 namespace sb200 {
 
 // Error-free transformations for the mixed form: the face fluxes are accumulated as float-float
@@ -474,7 +482,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   }
   // reconstruction, one characteristic field per iteration (rolled: one copy of wenorec)
   R fi[5];
-#pragma unroll 1
+  SB_UNROLL_(SB_WENO_UNROLL)
   for (int m = 0; m < 5; ++m) {
     R gp[2 * WS], gm[2 * WS];
 #pragma unroll

@@ -118,4 +118,48 @@ cudaError_t launch_stats(const Geom& g, DevState& d, const double* fl2, const do
 cudaError_t launch_stats3d(const Geom& g, DevState& d, int itav, cudaStream_t s, long long* nl);
 long long reduction_slots(const Geom& g);
 
+// Launches over a box table (batch_kernels.cu): the stages of a group of boxes, one launch per
+// kernel kind for all of them.  Per box: its geometry, device buffers and launch shapes.
+struct BoxRec {
+  Geom g;
+  double* w;
+  void* aux;   // double (FP64 form) or float (mixed form)
+  void* div3;
+  double* sensor;
+  double* sensor_next;
+  double* vel64;
+  double* fl_a;  // RK registers: stage 2 writes fl_b, stages 1 and 3 write fl_a
+  double* fl_b;
+  double* wallprop;
+  double* red;
+  Scalars* sc;
+  double cfl;
+  int sly, nsy, slz, nsz;  // march segments (length, count) of the y and z passes
+  unsigned xg[3];          // grid of the x pass (one-dimensional)
+  unsigned nb_vol, nb_pt, nb_y, nb_z;  // blocks of the aux pass, pointwise passes, y and z passes
+};
+// block of a launch over a box table: the box and the block's index in the box's own grid
+struct BlockRef {
+  unsigned box, local;
+};
+enum BatchKind { BK_VOL = 0, BK_PT, BK_X, BK_Y, BK_Z, BK_NUM };
+struct BoxTable {
+  int nbox = 0;
+  BoxRec* rec = nullptr;       // device
+  BlockRef* blocks = nullptr;  // device: the blocks of each kind, box after box
+  long long off[BK_NUM] = {};
+  unsigned cnt[BK_NUM] = {};
+  Geom g0{};  // host copy of the first box's geometry: the group's common configuration
+};
+// Group key of a geometry (boxes with equal keys share launches), -1 for a box whose stage
+// needs launches that the table form does not have (stored ghosts, recycling inflow,
+// non-reflecting faces, WENO faces computed apart).
+long long batch_key(const Geom& g);
+BoxRec box_rec(const Geom& g, const DevState& d, double* fl_a, double* fl_b, double cfl);
+cudaError_t box_table_build(BoxTable& t, const std::vector<BoxRec>& recs, cudaStream_t s);
+void box_table_free(BoxTable& t, cudaStream_t s);
+cudaError_t batch_launch_aux(const BoxTable& t, int apply_shift, cudaStream_t s, long long* nl);
+cudaError_t batch_launch_dt(const BoxTable& t, cudaStream_t s, long long* nl);
+cudaError_t batch_launch_stage(const BoxTable& t, const StageArgs& a, cudaStream_t s, long long* nl);
+
 }  // namespace sb200

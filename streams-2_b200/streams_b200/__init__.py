@@ -143,6 +143,9 @@ def _load() -> C.CDLL:
         "streams_b200_batch_synchronize": (I, [P]),
         "streams_b200_batch_invalidate": (I, [P]),
         "streams_b200_batch_stats": (I, [P, C.POINTER(LL), C.POINTER(LL)]),
+        "streams_b200_batch_set_shared_launches": (I, [P, I]),
+        "streams_b200_batch_class": (I, [P, C.POINTER(LL)]),
+        "streams_b200_batch_groups": (I, [P, C.POINTER(I), C.POINTER(I)]),
         "streams_b200_batch_last_error": (C.c_char_p, [P]),
         "streams_b200_batch_destroy": (I, [P]),
     }
@@ -193,6 +196,7 @@ EXPORTED = [
     "streams_b200_get_tuning", "streams_b200_set_weno_split", "streams_b200_get_weno_split",
     "streams_b200_batch_create", "streams_b200_batch_advance",
     "streams_b200_batch_synchronize", "streams_b200_batch_invalidate", "streams_b200_batch_stats",
+    "streams_b200_batch_set_shared_launches", "streams_b200_batch_groups", "streams_b200_batch_class",
     "streams_b200_batch_last_error", "streams_b200_batch_destroy",
 ]
 
@@ -432,6 +436,13 @@ class Solver:
     def synchronize(self):
         self._check(lib.streams_b200_synchronize(self._h))
 
+    def batch_class(self) -> int | None:
+        """Class for shared launches in a Batch (solvers of one class form a group), or None
+        for a solver that always advances on its own branch."""
+        k = C.c_longlong()
+        self._check(lib.streams_b200_batch_class(self._h, C.byref(k)))
+        return None if k.value < 0 else int(k.value)
+
     def busy(self) -> bool:
         """Whether work issued on the context's stream is still pending (non-blocking)."""
         rc = lib.streams_b200_query(self._h)
@@ -560,6 +571,17 @@ class Batch:
         r, n = C.c_longlong(), C.c_longlong()
         self._check(lib.streams_b200_batch_stats(self._h, C.byref(r), C.byref(n)))
         return int(r.value), int(n.value)
+
+    def set_shared_launches(self, groups_per_class: int) -> None:
+        """Boxes of a class advance by shared launches in ``groups_per_class`` groups (1, the
+        default), or each on its own branch (0)."""
+        self._check(lib.streams_b200_batch_set_shared_launches(self._h, int(groups_per_class)))
+
+    def groups(self) -> tuple[int, int]:
+        """(groups sharing launches, boxes in them)."""
+        g, n = C.c_int(), C.c_int()
+        self._check(lib.streams_b200_batch_groups(self._h, C.byref(g), C.byref(n)))
+        return int(g.value), int(n.value)
 
     def close(self):
         h = getattr(self, "_h", None)

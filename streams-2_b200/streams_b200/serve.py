@@ -5,11 +5,16 @@ precision) arrive over time.  Each is prepared on the host as it arrives (input 
 initial field: worker threads, so that set-up overlaps the GPU work), then admitted in arrival
 order as soon as its device footprint fits the HBM budget next to the solves already resident;
 its device set-up runs on an admission thread, off the loop.  A resident solve keeps its fields in
-HBM from admission to completion and advances in ticks: it replays its own CUDA graph of a tick's
-steps (a one-box ``Batch``, captured once when the solve joins) on its own stream, and the loop
-gives it its next tick as soon as its stream reports the previous one complete, so the solves'
-stages overlap on the GPU and none waits for another.  A solve leaves, freeing its memory, when its
-last tick is seen complete; completion latency is measured from the request's arrival to then.
+HBM from admission to completion and advances in ticks.  Resident solves of one class (the same
+stage kernels: precision, scheme, channel forcing; Solver.batch_class) advance together: when the
+class's previous tick is seen complete, its solves take their next tick as one cohort, a
+``Batch`` over them whose stages run as shared launches (one launch per kernel kind and stage for
+all of them, over a table of the solves' boxes), captured once per cohort membership.  A solve of
+a class of its own, or of none (shock interactions: stored ghosts, non-reflecting faces), replays
+its own CUDA graph of a tick's steps (a one-box ``Batch``) as soon as its stream reports the
+previous tick complete.  Cohorts and lone solves overlap on the GPU.  A solve leaves, freeing its
+memory, when its last tick is seen complete; completion latency is measured from the request's
+arrival to then.
 
 A solve's arithmetic does not depend on what else is resident: with the same launch tuning its
 result is bit-identical alone and in any mix.
@@ -39,6 +44,7 @@ class Solve:
     cells: int
     solver: Solver | None = None
     batch: Batch | None = None      # the solve's own tick graph
+    cls: int | None = None          # class for shared launches (None: always alone)
     remaining: int = 0
     admitted: float = 0.0
     finished: float = 0.0
@@ -70,19 +76,24 @@ class Server:
     tick_steps    steps a resident solve is given at a time (fewer when it completes sooner)
     tune          autotune each new (grid, precision) class before its first admission
     keep_fields   download each completed solve's conserved field into Solve.result["w"]
+    shared        advance the resident solves of a class as one cohort with shared launches
+                  (False: every solve on its own tick graph)
 
     The loop thread only decides and polls.  Host set-up runs on the preparation threads; an
     admitted solve's device set-up (tuning of a new class, context creation and upload,
     run() preamble, first step, capture of its tick graph and its first tick) runs on an
-    admission thread; resident solves advance independently, each given its next tick as soon
-    as its previous one has completed (a non-blocking query of its stream), so no solve waits
-    for the others and a finishing solve releases its memory (stream-ordered, no device-wide
+    admission thread.  A class's cohort (or a lone solve) is given its next tick as soon as its
+    previous one has completed (non-blocking queries of the solves' streams), so no class waits
+    for another, and a finishing solve releases its memory (stream-ordered, no device-wide
     synchronisation) the moment it is seen complete.
     """
 
     def __init__(self, budget_bytes: int, tick_steps: int = 10, tune: bool = True, keep_fields: bool = False,
-                 prep_threads: int = 4, tune_cache: dict | None = None, admit_threads: int = 2):
+                 prep_threads: int = 4, tune_cache: dict | None = None, admit_threads: int = 2,
+                 shared: bool = True):
         self.budget = int(budget_bytes)
+        self.shared = shared
+        self._cohorts: dict[int, tuple[tuple[int, ...], Batch]] = {}  # class -> (members, batch)
         self.tick_steps = int(tick_steps)
         self.tune = tune
         self.keep_fields = keep_fields
@@ -101,6 +112,7 @@ class Server:
         if s.tuning:
             s.solver.set_tuning(*s.tuning)
         s.solver.init_run()
+        s.cls = s.solver.batch_class() if self.shared else None
         # the first step runs alone, so that the solve's graph only holds steady steps
         s.solver.advance(1)
         s.remaining = s.nsteps - 1
@@ -132,7 +144,7 @@ class Server:
         nxt = 0
         busy = 0.0
         last = None  # start of the current interval with resident solves
-        host = {"admit_wait_s": 0.0, "loop_iterations": 0}
+        host = {"admit_wait_s": 0.0, "loop_iterations": 0, "cohort_ticks": 0, "max_cohort": 0}
         try:
             while nxt < len(reqs) or futures or waiting or admitting or active:
                 host["loop_iterations"] += 1
@@ -169,9 +181,14 @@ class Server:
                     progressed = True
                 if active and last is None:
                     last = now()
-                # every resident solve whose tick has completed gets its next one, or leaves
+                # every resident solve whose tick has completed gets its next one, or leaves; the
+                # solves of a class move together, once all of them are seen complete
                 still = []
+                classes: dict[int, list[Solve]] = {}
                 for sv in active:
+                    if sv.cls is not None:
+                        classes.setdefault(sv.cls, []).append(sv)
+                        continue
                     if sv.inflight and sv.solver.busy():
                         still.append(sv)
                         continue
@@ -185,6 +202,34 @@ class Server:
                     sv.batch.advance(n)
                     sv.inflight = n
                     still.append(sv)
+                for cls, members in classes.items():
+                    if any(sv.inflight and sv.solver.busy() for sv in members):
+                        still.extend(members)
+                        continue
+                    progressed = True
+                    live = []
+                    for sv in members:
+                        sv.remaining -= sv.inflight
+                        sv.inflight = 0
+                        if sv.remaining > 0:
+                            live.append(sv)
+                    if len(live) != len(members):
+                        self._drop_cohort(cls)  # before its finished solves' contexts go
+                        for sv in members:
+                            if sv.remaining <= 0:
+                                used -= self._finish(sv, now(), done)
+                    if not live:
+                        continue
+                    n = tick_length([sv.remaining for sv in live], self.tick_steps)
+                    if len(live) == 1:
+                        live[0].batch.advance(n)
+                    else:
+                        self._cohort(cls, live).advance(n)
+                        host["cohort_ticks"] += 1
+                        host["max_cohort"] = max(host["max_cohort"], len(live))
+                    for sv in live:
+                        sv.inflight = n
+                    still.extend(live)
                 if len(still) != len(active) or progressed:
                     self.log.append((now(), len(still)))
                 active = still
@@ -208,6 +253,8 @@ class Server:
             for f in admitting.values():
                 sv = f.result()
                 active.append(sv)
+            for cls in list(self._cohorts):
+                self._drop_cohort(cls)
             for sv in active:
                 if sv.batch is not None:
                     sv.batch.close()
@@ -218,6 +265,22 @@ class Server:
         out = summarize(done, rejected, busy, self.log)
         out.update(host)
         return out
+
+    def _cohort(self, cls: int, live: list[Solve]) -> Batch:
+        """The class's cohort batch over exactly the solves `live` (rebuilt when they change)."""
+        key = tuple(sv.rid for sv in live)
+        cur = self._cohorts.get(cls)
+        if cur is not None and cur[0] == key:
+            return cur[1]
+        self._drop_cohort(cls)
+        b = Batch([sv.solver for sv in live], steps_per_graph=self.tick_steps, dt_every=1)
+        self._cohorts[cls] = (key, b)
+        return b
+
+    def _drop_cohort(self, cls: int) -> None:
+        cur = self._cohorts.pop(cls, None)
+        if cur is not None:
+            cur[1].close()
 
     def _finish(self, s: Solve, t: float, done: list) -> int:
         """Record a completed solve, release its device memory; returns the bytes freed."""

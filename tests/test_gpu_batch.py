@@ -41,6 +41,7 @@ def test_batch_equals_alone(tmp_path, nsteps, spg):
         s.close()
     solvers = [make(tmp_path, i, kw) for i, kw in enumerate(BOXES)]
     b = Batch(solvers, steps_per_graph=spg)
+    assert b.groups() == (2, 4)  # the FP64 pair and the mixed pair share launches
     b.advance(nsteps)
     b.synchronize()
     replays, per = b.stats()
@@ -49,6 +50,93 @@ def test_batch_equals_alone(tmp_path, nsteps, spg):
     for s, (w, sc) in zip(solvers, alone):
         assert np.array_equal(s.copy_to_field(), w)
         assert s.scalars() == sc
+    b.close()
+
+
+def test_shared_launches_equal_separate_branches(tmp_path):
+    """A group's shared launches (one launch per kernel kind and stage for all its boxes) give
+    the boxes' own results, with fewer launches per replay than a branch per box."""
+    from streams_b200 import Batch
+    boxes = BOXES + [dict(nx=64, ny=32, nz=24, mach=1.1, re_bulk=4000.0, seed=9, precision=0),
+                     dict(nx=40, ny=24, nz=20, mach=0.5, seed=11, precision=1),
+                     dict(nx=48, ny=32, nz=32, mach=1.3, seed=13, precision=0)]
+    out = {}
+    for shared in (0, 1, 2):
+        solvers = [make(tmp_path, i, kw) for i, kw in enumerate(boxes)]
+        b = Batch(solvers, steps_per_graph=5)
+        b.set_shared_launches(shared)
+        # 4 FP64 boxes, 3 mixed: one group per class, or the FP64 class in two groups of two
+        # (equal cell counts: 64x32x24 with 32x24x16, 48x32x32 with 48x32x16)
+        assert b.groups() == {0: (0, 0), 1: (2, 7), 2: (3, 7)}[shared]
+        b.advance(16)
+        b.synchronize()
+        out[shared] = ([s.copy_to_field() for s in solvers], [s.scalars() for s in solvers], b.stats())
+        b.close()
+        for s in solvers:
+            s.close()
+    for shared in (1, 2):
+        for wa, wb in zip(out[0][0], out[shared][0]):
+            assert np.array_equal(wa, wb)
+        assert out[0][1] == out[shared][1]
+    (ra, pa), (rb, pb) = out[0][2], out[1][2]
+    assert ra == rb == 3 and pb < pa / 2, (pa, pb)
+
+
+def test_a_box_outside_the_groups_keeps_its_branch(tmp_path):
+    """A boundary-layer box (stored ghosts, recycling inflow, non-reflecting faces) advances on
+    its own branch beside a group of channels; every box equals its run alone."""
+    from streams_b200 import Batch, Case, Solver
+    from streams_b200.cases import bl_ini
+
+    def bl():
+        d = tmp_path / "bl"
+        d.mkdir(exist_ok=True)
+        s = Solver.from_case(Case(d, bl_ini(nx=48, ny=40, nz=16)), precision=0)
+        s.init_run()
+        return s
+
+    kws = [BOXES[0], BOXES[2]]
+    alone = []
+    for i, kw in enumerate(kws):
+        s = make(tmp_path, i, kw)
+        s.advance(9)
+        alone.append(s.copy_to_field())
+        s.close()
+    s = bl()
+    s.advance(9)
+    alone.append(s.copy_to_field())
+    s.close()
+    solvers = [make(tmp_path, i, kw) for i, kw in enumerate(kws)] + [bl()]
+    b = Batch(solvers, steps_per_graph=4)
+    assert b.groups() == (1, 2)
+    b.advance(9)
+    b.synchronize()
+    for s, w in zip(solvers, alone):
+        assert np.array_equal(s.copy_to_field(), w)
+    b.close()
+
+
+def test_a_retuned_box_rebuilds_its_group(tmp_path):
+    from streams_b200 import Batch
+    kws = [BOXES[0], BOXES[2]]
+    ref = []
+    for i, kw in enumerate(kws):
+        s = make(tmp_path, i, kw)
+        s.advance(7)
+        if i == 1:
+            s.set_tuning(37888, 8)
+        s.advance(8)
+        ref.append(s.copy_to_field())
+        s.close()
+    solvers = [make(tmp_path, i, kw) for i, kw in enumerate(kws)]
+    b = Batch(solvers, steps_per_graph=3)
+    b.advance(7)
+    solvers[1].set_tuning(37888, 8)
+    b.advance(8)
+    b.synchronize()
+    assert b.groups() == (1, 2)
+    for s, w in zip(solvers, ref):
+        assert np.array_equal(s.copy_to_field(), w)
     b.close()
 
 
@@ -107,6 +195,30 @@ def test_serving_alone_equals_in_the_mix():
         alone = Server(budget_bytes=1 << 34, tick_steps=5, keep_fields=True, tune_cache=cache).run([dict(r, arrival=0.0)])
         a, m = alone["solves"][r["rid"]], mix["solves"][r["rid"]]
         assert np.array_equal(a.result["w"], m.result["w"]), r["rid"]
+        assert a.result["scalars"] == m.result["scalars"]
+
+
+def test_serving_cohorts_share_launches_and_equal_alone():
+    """Solves of one class resident together advance as a cohort (shared launches); each result
+    equals the solve served alone, bit for bit, and the same mix served without cohorts."""
+    from streams_b200.serve import Server
+    # long enough (and untuned, so that admission is quick) for the solves to be resident together
+    reqs = [dict(rid=0, arrival=0.0, nx=48, ny=32, nz=32, mach=1.2, nsteps=400, precision=0, seed=1),
+            dict(rid=1, arrival=0.0, nx=32, ny=24, nz=16, mach=2.0, nsteps=270, precision=0, seed=2),
+            dict(rid=2, arrival=0.0, nx=64, ny=32, nz=16, mach=0.7, nsteps=330, precision=0, seed=3),
+            dict(rid=3, arrival=0.0, nx=32, ny=32, nz=16, mach=0.9, nsteps=350, precision=1, seed=4),
+            dict(rid=4, arrival=0.0, nx=48, ny=24, nz=16, mach=1.4, nsteps=220, precision=1, seed=5),
+            dict(rid=5, arrival=0.0, nx=32, ny=32, nz=32, mach=0.8, nsteps=300, precision=1, seed=6)]
+    kw = dict(budget_bytes=1 << 34, tick_steps=5, keep_fields=True, tune=False)
+    mix = Server(**kw).run(reqs)
+    assert mix["completed"] == 6 and mix["cohort_ticks"] > 0 and mix["max_cohort"] >= 2, mix
+    apart = Server(shared=False, **kw).run(reqs)
+    assert apart["cohort_ticks"] == 0
+    for r in reqs:
+        alone = Server(**kw).run([r])
+        a, m, p = alone["solves"][r["rid"]], mix["solves"][r["rid"]], apart["solves"][r["rid"]]
+        assert np.array_equal(a.result["w"], m.result["w"]), r["rid"]
+        assert np.array_equal(a.result["w"], p.result["w"]), r["rid"]
         assert a.result["scalars"] == m.result["scalars"]
 
 
