@@ -22,36 +22,56 @@ namespace {
 
 static_assert(sizeof(Geom) % 8 == 0, "Geom is copied to shared memory in 8-byte words");
 
-// Tiles of one launch: CTA c works through the tiles [c span, (c + 1) span) of the block table
-// (consecutive tiles, mostly of one box, so that a CTA copies a box's geometry into shared memory
-// once and the cost of entering a box is shared by span tiles); each tile runs the kernel body
-// with the tile's block index in its box's grid.
-__device__ __forceinline__ void copy_geom(const Geom& src_g, Geom& gs) {
+// Where a CTA reads its box's record: 2 copies the whole record (geometry and buffer pointers)
+// into shared memory, 1 the geometry only, 0 reads both from the table in global memory (48-box
+// channel mix, FP64 / mixed Mcell-steps/s: 608.0 / 762.3, 600.6 / 756.0, 588.6 / 754.6).
+#ifndef SB_BOX_SMEM
+#define SB_BOX_SMEM 2
+#endif
+
+__device__ __forceinline__ void copy_words(const void* src_p, void* dst_p, int nwords) {
   const int tid = threadIdx.x + blockDim.x * threadIdx.y, nt = blockDim.x * blockDim.y;
-  const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&src_g);
-  unsigned long long* dst = reinterpret_cast<unsigned long long*>(&gs);
-  for (int q = tid; q < (int)(sizeof(Geom) / 8); q += nt) dst[q] = src[q];
+  const unsigned long long* src = static_cast<const unsigned long long*>(src_p);
+  unsigned long long* dst = static_cast<unsigned long long*>(dst_p);
+  for (int q = tid; q < nwords; q += nt) dst[q] = src[q];
 }
+static_assert(sizeof(BoxRec) % 8 == 0, "BoxRec is copied in 8-byte words");
+
+// Tiles of one launch: CTA c works through the tiles [c SPAN, (c + 1) SPAN) of the block table
+// (consecutive tiles, mostly of one box, so that a CTA enters a box once for SPAN tiles); each
+// tile runs body(record, geometry, block index in the box's grid).
 template <unsigned SPAN, class F>
 __device__ __forceinline__ void for_tiles(const BoxRec* __restrict__ rec, const BlockRef* __restrict__ blocks,
-                                          unsigned ntile, Geom& gs, F&& body) {
+                                          unsigned ntile, F&& body) {
+#if SB_BOX_SMEM == 2
+  __shared__ BoxRec rs;
+  auto enter = [&](unsigned box) { copy_words(rec + box, &rs, (int)(sizeof(BoxRec) / 8)); };
+  auto run = [&](unsigned, unsigned l) { body(static_cast<const BoxRec*>(&rs), static_cast<const Geom&>(rs.g), l); };
+#elif SB_BOX_SMEM == 1
+  __shared__ Geom gs;
+  auto enter = [&](unsigned box) { copy_words(&rec[box].g, &gs, (int)(sizeof(Geom) / 8)); };
+  auto run = [&](unsigned box, unsigned l) { body(rec + box, static_cast<const Geom&>(gs), l); };
+#else
+  auto enter = [&](unsigned) {};
+  auto run = [&](unsigned box, unsigned l) { body(rec + box, rec[box].g, l); };
+#endif
   if constexpr (SPAN == 1) {
     const BlockRef b = blocks[blockIdx.x];
-    copy_geom(rec[b.box].g, gs);
-    __syncthreads();
-    body(rec + b.box, b.local);
+    enter(b.box);
+    if (SB_BOX_SMEM) __syncthreads();
+    run(b.box, b.local);
   } else {
     const unsigned t0 = blockIdx.x * SPAN, t1 = min(ntile, t0 + SPAN);
     unsigned cur = 0xffffffffu;
     for (unsigned t = t0; t < t1; ++t) {
       const BlockRef b = blocks[t];
-      if (b.box != cur) {  // uniform over the CTA
-        __syncthreads();   // the previous box's tiles are done with gs
-        copy_geom(rec[b.box].g, gs);
+      if (SB_BOX_SMEM && b.box != cur) {  // uniform over the CTA
+        __syncthreads();                   // the previous box's tiles are done with the copy
+        enter(b.box);
         __syncthreads();
         cur = b.box;
       }
-      body(rec + b.box, b.local);
+      run(b.box, b.local);
       // the bodies end with block reductions through shared memory: the next tile may not write
       // those buffers before every thread has read this tile's result
       if (t + 1 < t1) __syncthreads();
@@ -61,7 +81,7 @@ __device__ __forceinline__ void for_tiles(const BoxRec* __restrict__ rec, const 
 // one block per box (the per-box reductions)
 __device__ __forceinline__ const BoxRec* enter_box_direct(const BoxRec* __restrict__ rec, Geom& gs) {
   const BoxRec* r = rec + blockIdx.x;
-  copy_geom(r->g, gs);
+  copy_words(&r->g, &gs, (int)(sizeof(Geom) / 8));
   __syncthreads();
   return r;
 }
@@ -72,27 +92,24 @@ __device__ __forceinline__ double* fl_prev_of(const BoxRec* r, int istep) { retu
 template <unsigned SPAN, class A, bool TP>
 __global__ void __launch_bounds__(AUX_NT) kb_apply_shift(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile) {
-  __shared__ Geom gs;
-  for_tiles<SPAN>(rec, blocks, ntile, gs, [&](const BoxRec* r, unsigned l) {
-    d_apply_shift<A, TP>(gs, r->w, static_cast<const A*>(r->aux), r->sc, Blk{l, 0, 0});
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
+    d_apply_shift<A, TP>(g, r->w, static_cast<const A*>(r->aux), r->sc, Blk{l, 0, 0});
   });
 }
 
 template <unsigned SPAN, class A, bool TP>
 __global__ void __launch_bounds__(AUX_NT) kb_aux(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile, int want_vel) {
-  __shared__ Geom gs;
-  for_tiles<SPAN>(rec, blocks, ntile, gs, [&](const BoxRec* r, unsigned l) {
-    d_aux<A, TP>(gs, r->w, static_cast<A*>(r->aux), 0, want_vel ? r->vel64 : nullptr, Blk{l, 0, 0});
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
+    d_aux<A, TP>(g, r->w, static_cast<A*>(r->aux), 0, want_vel ? r->vel64 : nullptr, Blk{l, 0, 0});
   });
 }
 
 template <unsigned SPAN, class R, int LB, int WS, int FS>
 __global__ void __launch_bounds__(XF_NT, sizeof(R) == 8 ? XF_MINB_D : XF_MINB_F)
     kb_xflux(const BoxRec* __restrict__ rec, const BlockRef* __restrict__ blocks, unsigned ntile, int istep) {
-  __shared__ Geom gs;
-  for_tiles<SPAN>(rec, blocks, ntile, gs, [&](const BoxRec* r, unsigned l) {
-    d_xflux<R, LB, WS, FS>(gs, static_cast<const R*>(r->aux), r->sensor, fl_new_of(r, istep), Blk{l, 0, 0});
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
+    d_xflux<R, LB, WS, FS>(g, static_cast<const R*>(r->aux), r->sensor, fl_new_of(r, istep), Blk{l, 0, 0});
   });
 }
 
@@ -100,9 +117,8 @@ template <unsigned SPAN, class R, bool TP>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F)
     kb_visc(const BoxRec* __restrict__ rec, const BlockRef* __restrict__ blocks, unsigned ntile,
     int istep, int do_sensor) {
-  __shared__ Geom gs;
-  for_tiles<SPAN>(rec, blocks, ntile, gs, [&](const BoxRec* r, unsigned l) {
-    d_visc<R, TP>(gs, static_cast<const R*>(r->aux), fl_new_of(r, istep), static_cast<R*>(r->div3), r->sensor_next,
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
+    d_visc<R, TP>(g, static_cast<const R*>(r->aux), fl_new_of(r, istep), static_cast<R*>(r->div3), r->sensor_next,
                   r->wallprop, do_sensor, Blk{l, 0, 0});
   });
 }
@@ -110,9 +126,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F)
 template <unsigned SPAN, class R, bool TP>
 __global__ void __launch_bounds__(256) kb_visc_ns(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile, int istep, int do_sensor) {
-  __shared__ Geom gs;
-  for_tiles<SPAN>(rec, blocks, ntile, gs, [&](const BoxRec* r, unsigned l) {
-    d_visc_ns<R, TP>(gs, static_cast<const R*>(r->aux), fl_new_of(r, istep), static_cast<R*>(r->div3), r->sensor_next,
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
+    d_visc_ns<R, TP>(g, static_cast<const R*>(r->aux), fl_new_of(r, istep), static_cast<R*>(r->div3), r->sensor_next,
                      r->wallprop, do_sensor, Blk{l, 0, 0});
   });
 }
@@ -121,23 +136,21 @@ __global__ void __launch_bounds__(256) kb_visc_ns(const BoxRec* __restrict__ rec
 template <unsigned SPAN>
 __global__ void __launch_bounds__(256) kb_sensor(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile, int from_vel) {
-  __shared__ Geom gs;
-  for_tiles<SPAN>(rec, blocks, ntile, gs, [&](const BoxRec* r, unsigned l) {
-    const int mode = gs.conservative_viscous ? 1 : 2;
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
+    const int mode = g.conservative_viscous ? 1 : 2;
     if (from_vel)
-      d_sensor_vel(gs, r->vel64, r->sensor_next, mode, Blk{l, 0, 0});
+      d_sensor_vel(g, r->vel64, r->sensor_next, mode, Blk{l, 0, 0});
     else
-      d_sensor64(gs, r->w, r->sensor_next, mode, Blk{l, 0, 0});
+      d_sensor64(g, r->w, r->sensor_next, mode, Blk{l, 0, 0});
   });
 }
 
 template <unsigned SPAN, class R, int DIR, int LB, int WS, bool CH, int FS>
 __global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
     kb_march(const BoxRec* __restrict__ rec, const BlockRef* __restrict__ blocks, unsigned ntile, double rhork, double gamrk, int istep) {
-  __shared__ Geom gs;
-  for_tiles<SPAN>(rec, blocks, ntile, gs, [&](const BoxRec* r, unsigned l) {
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
     const int seglen = DIR == 1 ? r->sly : r->slz, nseg = DIR == 1 ? r->nsy : r->nsz;
-    d_march<R, DIR, LB, WS, CH, FS, false>(gs, static_cast<const R*>(r->aux), r->sensor, fl_new_of(r, istep),
+    d_march<R, DIR, LB, WS, CH, FS, false>(g, static_cast<const R*>(r->aux), r->sensor, fl_new_of(r, istep),
                                            static_cast<const R*>(r->div3), r->w, fl_prev_of(r, istep), r->sc, rhork,
                                            gamrk, istep, seglen, nseg, r->red, Blk{l, 0, 0});
   });
@@ -153,9 +166,8 @@ template <unsigned SPAN, class R, bool TP>
 __global__ void __launch_bounds__(256) kb_update(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile, double rhork, double gamrk, int istep,
     int stats) {
-  __shared__ Geom gs;
-  for_tiles<SPAN>(rec, blocks, ntile, gs, [&](const BoxRec* r, unsigned l) {
-    d_update<R, TP>(gs, r->w, fl_prev_of(r, istep), fl_new_of(r, istep), r->sc, rhork, gamrk, istep, stats, r->red,
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
+    d_update<R, TP>(g, r->w, fl_prev_of(r, istep), fl_new_of(r, istep), r->sc, rhork, gamrk, istep, stats, r->red,
                     r->sensor_next, r->sensor, static_cast<R*>(r->aux), Blk{l, 0, 0});
   });
 }
@@ -169,9 +181,8 @@ __global__ void __launch_bounds__(FIN_NT) kb_finish_upd(const BoxRec* __restrict
 template <unsigned SPAN, class R>
 __global__ void __launch_bounds__(256) kb_dt(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile) {
-  __shared__ Geom gs;
-  for_tiles<SPAN>(rec, blocks, ntile, gs, [&](const BoxRec* r, unsigned l) {
-    d_dt<R>(gs, r->w, static_cast<const R*>(r->aux), r->red, Blk{l, 0, 0});
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
+    d_dt<R>(g, r->w, static_cast<const R*>(r->aux), r->red, Blk{l, 0, 0});
   });
 }
 

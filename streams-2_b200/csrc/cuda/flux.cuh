@@ -20,7 +20,27 @@
 #define SB_PRAGMA_(x) _Pragma(#x)
 #define SB_UNROLL_(n) SB_PRAGMA_(unroll n)
 
+// quotients and square roots of the mixed form's FP32 flux arithmetic from the hardware
+// approximations (1) or IEEE (0)
+#ifndef SB_FP32_FAST
+#define SB_FP32_FAST 0
+#endif
+
 namespace sb200 {
+
+// Quotient and square root (of a positive value) in the flux arithmetic: IEEE in FP64, where the
+// reference's operations are kept; with SB_FP32_FAST the FP32 form takes the hardware reciprocal
+// and reciprocal square root (at most 2 ulp: the mixed form's error is set by FP32 rounding).
+template <class R>
+__device__ __forceinline__ R fdiv(R a, R b) {
+  if constexpr (sizeof(R) == sizeof(double) || !SB_FP32_FAST) return a / b;
+  else return __fdividef(a, b);
+}
+template <class R>
+__device__ __forceinline__ R fsqrt_pos(R x) {
+  if constexpr (sizeof(R) == sizeof(double) || !SB_FP32_FAST) return sqrt(x);
+  else return x * rsqrtf(x);
+}
 
 // Error-free transformations for the mixed form: the face fluxes are accumulated as float-float
 // pairs (hi + lo) so that the flux differences of neighbouring faces can be formed in FP64
@@ -66,8 +86,8 @@ __device__ __forceinline__ void recip_pair(R a, R b, R& ra, R& rb) {
     ra = b * r;
     rb = a * r;
   } else {
-    ra = R(1) / a;
-    rb = R(1) / b;
+    ra = fdiv(R(1), a);
+    rb = fdiv(R(1), b);
   }
 }
 
@@ -368,10 +388,10 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
   const int o0 = S - 1, o1 = S;  // the two points adjacent to the face
   // Roe average
   R uu = st.u[o0], vv = st.v[o0], ww = st.w[o0], h = st.h[o0];
-  R r = st.rho[o1] / st.rho[o0];
-  r = sqrt(r);
+  R r = fdiv(st.rho[o1], st.rho[o0]);
+  r = fsqrt_pos(r);
   R rho = r * st.rho[o0];
-  R rp1 = R(1) / (r + R(1));
+  R rp1 = fdiv(R(1), r + R(1));
   uu = (r * st.u[o1] + uu) * rp1;
   vv = (r * st.v[o1] + vv) * rp1;
   ww = (r * st.w[o1] + ww) * rp1;
@@ -385,7 +405,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
     tt = tp_newton(g, g.cpc, hbar, t_start);
     gamloc = gamloc_of_t(g, tt);
   } else {
-    tt = R(g.t0) + hbar / R(g.cp0);
+    tt = R(g.t0) + fdiv(hbar, R(g.cp0));
     gamloc = R(g.gamloc);
   }
   R cc = gamloc * tt * rgas0;
@@ -429,7 +449,7 @@ __device__ __forceinline__ void weno_flux(const Geom& g, const Stencil<R, S>& st
       cs = __ldg(cpt + q * cstr);  // the aux pass's sound speed of the point (FP64 form)
     } else {
       const R gq = TP ? R(gamloc_of_t(g, double(st.t[q]))) : R(g.gamloc);
-      cs = sqrt(gq * R(g.rgas0) * st.t[q]);
+      cs = fsqrt_pos(gq * R(g.rgas0) * st.t[q]);
     }
 #endif
     ev0 = fmax(fabs(vnq - cs), ev0);
@@ -541,7 +561,7 @@ __device__ __forceinline__ void rusanov_flux(const Geom& g, const Stencil<R, S>&
       c = __ldg(cpt + q * cstr);
     } else {
       const R gq = TP ? R(gamloc_of_t(g, double(st.t[q]))) : R(g.gamloc);
-      c = sqrt(gq * rgas0 * st.t[q]);
+      c = fsqrt_pos(gq * rgas0 * st.t[q]);
     }
     const R evm = fmax(fabs(un - c), fabs(un + c));
     evmax = fmax(evm, evmax);
