@@ -265,6 +265,17 @@ __device__ __forceinline__ double viscosity(const Geom& g, double tt) {
   return 0.0;
 }
 
+// the same law in FP32 (the mixed form's stored viscosity)
+__device__ __forceinline__ float viscosity_f(const Geom& g, float tt) {
+  const float tr = tt / float(g.t0);
+  if (g.visc_model == 1) return float(g.mu0) * powf(tr, float(g.vtexp));
+  if (g.visc_model == 2) {
+    const float st = float(g.sutherland_s / g.t_ref_dim);
+    return float(g.mu0) * (tr * sqrtf(tr)) * (1.0f + st) / (tr + st);
+  }
+  return 0.0f;
+}
+
 // Index of a stencil point along one axis of the sensor / div arrays (stored interior only):
 // periodic directions wrap; otherwise the caller decides (sensor: 0, div: clamp).
 __device__ __forceinline__ int wrap(int i, int n) { return i < 1 ? i + n : (i > n ? i - n : i); }

@@ -202,7 +202,11 @@ __device__ __forceinline__ void d_aux(const Geom& g, double* __restrict__ w, A* 
   aux[3 * n + dst] = A(ww);
   aux[4 * n + dst] = A((rhoe + pp) / rho);
   aux[5 * n + dst] = A(tt);
-  aux[6 * n + dst] = A(viscosity(g, tt));
+  // the mixed form's viscous arithmetic is FP32, and so is its viscosity law (with SB_FP32_FAST)
+  if constexpr (sizeof(A) == sizeof(float) && SB_FP32_FAST != 0)
+    aux[6 * n + dst] = viscosity_f(g, float(tt));
+  else
+    aux[6 * n + dst] = A(viscosity(g, tt));
   // FP64 form: the sound speed, which the WENO eigenvalue bound of every face reads at its
   // stencil points (the same expression the flux would form)
   if constexpr (sizeof(A) == sizeof(double)) {
