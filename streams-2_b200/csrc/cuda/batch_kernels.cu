@@ -124,6 +124,16 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F)
 }
 
 template <unsigned SPAN, class R, bool TP>
+__global__ void __launch_bounds__(VT_NT, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F)
+    kb_visc_tiled(const BoxRec* __restrict__ rec, const BlockRef* __restrict__ blocks, unsigned ntile,
+    int istep, int do_sensor) {
+  for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
+    d_visc_tiled<R, TP>(g, static_cast<const R*>(r->aux), fl_new_of(r, istep), static_cast<R*>(r->div3),
+                        r->sensor_next, r->wallprop, do_sensor, Blk{l, 0, 0});
+  });
+}
+
+template <unsigned SPAN, class R, bool TP>
 __global__ void __launch_bounds__(256) kb_visc_ns(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile, int istep, int do_sensor) {
   for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
@@ -248,7 +258,10 @@ cudaError_t batch_stage_impl(const BoxTable& t, const StageArgs& a, cudaStream_t
   const Launch X = launch_of(t, BK_X), P = launch_of(t, BK_PT), Y = launch_of(t, BK_Y), Z = launch_of(t, BK_Z);
   kb_xflux<1, R, LB, WS, FS><<<X.grid(1), dim3(XF_TX, XF_TY), xsm, s>>>(t.rec, X.blocks, X.ntile, a.istep);
   const int do_sensor = fp64 && a.istep == 3;
-  if (g.conservative_viscous)
+  if (g.conservative_viscous && SB_VISC_TILED) {
+    const Launch V = launch_of(t, BK_VS);
+    kb_visc_tiled<1, R, TP><<<V.grid(1), VT_NT, 0, s>>>(t.rec, V.blocks, V.ntile, a.istep, do_sensor);
+  } else if (g.conservative_viscous)
     kb_visc<1, R, TP><<<P.grid(1), 256, 0, s>>>(t.rec, P.blocks, P.ntile, a.istep, do_sensor);
   else
     kb_visc_ns<1, R, TP><<<P.grid(1), 256, 0, s>>>(t.rec, P.blocks, P.ntile, a.istep, do_sensor);
@@ -362,6 +375,7 @@ BoxRec box_rec(const Geom& g, const DevState& d, double* fl_a, double* fl_b, dou
   r.nb_z = nblocks(ntz, MT_NT);
   r.nb_pt = nblocks(g.nint, 256);
   r.nb_vol = nblocks(g.nvol, AUX_NT);
+  r.nb_vs = visc_tiled_blocks(g);
   return r;
 }
 
@@ -387,7 +401,8 @@ cudaError_t box_table_build(BoxTable& t, const std::vector<BoxRec>& recs, cudaSt
                                    : k == BK_PT ? r.nb_pt
                                    : k == BK_X  ? (unsigned long long)r.xg[0] * r.xg[1] * r.xg[2]
                                    : k == BK_Y  ? r.nb_y
-                                                : r.nb_z;
+                                   : k == BK_Z  ? r.nb_z
+                                                : r.nb_vs;
       for (unsigned long long q = 0; q < n; ++q) blocks.push_back(BlockRef{(unsigned)b, (unsigned)q});
     }
     const long long c = (long long)blocks.size() - t.off[k];

@@ -63,6 +63,10 @@ constexpr int MT_NT = 128;                                     // march kernels
 #ifndef SB_MARCH_WINDOW_Z
 #define SB_MARCH_WINDOW_Z 1
 #endif
+// the viscous pass with its operands staged in shared memory (1) or read per use (0)
+#ifndef SB_VISC_TILED
+#define SB_VISC_TILED 1
+#endif
 // shared-memory carve-out (percent) preferred by the WENO face kernels: their listed faces'
 // stencil loads are scattered and live on L1 hits (developed boundary layer 1024x256x192: 5.0
 // against 8.1 ms per step of face kernels with the largest carve-out, which fits a fourth block)
@@ -847,6 +851,172 @@ __device__ __forceinline__ void d_visc(const Geom& g, const R* __restrict__ aux,
   fl[3 * nI + q] = f4;
   fl[4 * nI + q] = f5;
 }
+// The same viscous pass with its operands staged in shared memory: a block of 32 x 8 threads
+// owns a 32 x 8 column of cells and marches VT_K cells along z; the five fields the pass reads
+// (u, v, w, T, mu) of the planes k-1, k, k+1 sit in a ring of three tiles of 34 x 10 points (the
+// column and its x / y halo), so that every point is loaded once per block (and its halo once
+// more) with coalesced rows instead of once per use, and the x / y / z neighbours come from
+// shared memory.  The arithmetic is d_visc's, in its order.
+constexpr int VT_X = 32, VT_Y = 8, VT_NT = VT_X * VT_Y, VT_K = 16;
+constexpr int VT_PX = VT_X + 2, VT_PY = VT_Y + 2, VT_PP = VT_PX * VT_PY;
+// blocks of the staged viscous pass: 32 x 8 columns x segments of VT_K cells in z
+inline unsigned visc_tiled_blocks(const Geom& g) {
+  return (unsigned)((g.nx + VT_X - 1) / VT_X) * (unsigned)((g.ny + VT_Y - 1) / VT_Y) *
+         (unsigned)((g.nz + VT_K - 1) / VT_K);
+}
+template <class R, bool TP = false>
+__device__ __forceinline__ void d_visc_tiled(const Geom& g, const R* __restrict__ aux, double* __restrict__ fl,
+                                             R* __restrict__ div3, double* __restrict__ sensor_next,
+                                             double* __restrict__ wallprop, int do_sensor, const Blk blk) {
+  __shared__ R pl[3][5][VT_PP];
+  const unsigned nbx = (unsigned)(g.nx + VT_X - 1) / VT_X, nby = (unsigned)(g.ny + VT_Y - 1) / VT_Y;
+  const unsigned bx = blk.x % nbx, rest = blk.x / nbx, by = rest % nby, bk = rest / nby;
+  const int tx = (int)threadIdx.x % VT_X, ty = (int)threadIdx.x / VT_X;
+  const int i0 = (int)bx * VT_X, j0 = (int)by * VT_Y;  // the tile's points are i0 .. i0+VT_X+1
+  const int i = i0 + 1 + tx, j = j0 + 1 + ty;
+  const bool own = i <= g.nx && j <= g.ny;
+  const int k0 = (int)bk * VT_K + 1, k1 = min(k0 + VT_K - 1, g.nz);
+  const long long n = g.nvol, nI = g.nint;
+  // plane k of the tile into slot k % 3 (points beyond the face ghosts are left unread: no cell
+  // of the column uses them)
+  auto load_plane = [&](int k) {
+    R(*dst)[VT_PP] = pl[k % 3];
+    for (int t = threadIdx.x; t < VT_PP; t += VT_NT) {
+      const int ii = i0 + t % VT_PX, jj = j0 + t / VT_PX;
+      if (ii <= g.nx + 1 && jj <= g.ny + 1) {
+        const long long a = gidx(g, ii, jj, k);
+        dst[0][t] = __ldg(aux + n + a);
+        dst[1][t] = __ldg(aux + 2 * n + a);
+        dst[2][t] = __ldg(aux + 3 * n + a);
+        dst[3][t] = __ldg(aux + 5 * n + a);
+        dst[4][t] = __ldg(aux + 6 * n + a);
+      }
+    }
+  };
+  load_plane(k0 - 1);
+  load_plane(k0);
+  const R prandtl = R(g.prandtl);
+  R dxl = R(0), dyl = R(0);
+  if (own) {
+    if constexpr (sizeof(R) == sizeof(double)) {
+      dxl = R(__ldg(g.vrl[0] + i)); dyl = R(__ldg(g.vrl[1] + j));
+    } else {
+      dxl = R(__ldg(g.vrlf[0] + i)); dyl = R(__ldg(g.vrlf[1] + j));
+    }
+  }
+  for (int k = k0; k <= k1; ++k) {
+    load_plane(k + 1);
+    __syncthreads();
+    if (own) {
+      const int sm = (k - 1) % 3, s0 = k % 3, sp = (k + 1) % 3;
+      const int c0 = (tx + 1) + (ty + 1) * VT_PX;
+      // field f (0 u, 1 v, 2 w, 3 T, 4 mu) at the cell's point offset by (di, dj) in plane slot sl
+      auto F = [&](int sl, int di, int dj, int f) -> R { return pl[sl][f][c0 + di + dj * VT_PX]; };
+      const long long q = iidx(g, i, j, k);
+      const R uu = F(s0, 0, 0, 0), vv = F(s0, 0, 0, 1), ww = F(s0, 0, 0, 2), mu = F(s0, 0, 0, 4);
+      const R cploc = TP ? R(cp_of_t(g, double(F(s0, 0, 0, 3)))) : R(g.cp0);
+      R dzl;
+      if constexpr (sizeof(R) == sizeof(double)) dzl = R(__ldg(g.vrl[2] + k));
+      else dzl = R(__ldg(g.vrlf[2] + k));
+      R ux = dxl * (F(s0, 1, 0, 0) - F(s0, -1, 0, 0));
+      R vx = dxl * (F(s0, 1, 0, 1) - F(s0, -1, 0, 1));
+      R wx = dxl * (F(s0, 1, 0, 2) - F(s0, -1, 0, 2));
+      R mux = dxl * (F(s0, 1, 0, 4) - F(s0, -1, 0, 4));
+      R uy = dyl * (F(s0, 0, 1, 0) - F(s0, 0, -1, 0));
+      R vy = dyl * (F(s0, 0, 1, 1) - F(s0, 0, -1, 1));
+      R wy = dyl * (F(s0, 0, 1, 2) - F(s0, 0, -1, 2));
+      R ty_ = dyl * (F(s0, 0, 1, 3) - F(s0, 0, -1, 3));
+      R muy = dyl * (F(s0, 0, 1, 4) - F(s0, 0, -1, 4));
+      R uz = dzl * (F(sp, 0, 0, 0) - F(sm, 0, 0, 0));
+      R vz = dzl * (F(sp, 0, 0, 1) - F(sm, 0, 0, 1));
+      R wz = dzl * (F(sp, 0, 0, 2) - F(sm, 0, 0, 2));
+      R muz = dzl * (F(sp, 0, 0, 4) - F(sm, 0, 0, 4));
+      if (j == 1) {
+        const long long wp = (long long)(k - 1) * g.nx + (i - 1);
+        const long long nw = (long long)g.nx * g.nz;
+        wallprop[wp] = double(mu * uy);
+        wallprop[nw + wp] = double(mu * wy);
+        wallprop[2 * nw + wp] = double(mu * ty_ * cploc / prandtl);
+      }
+      R div = ux + vy + wz;
+      R div3l = div / R(3);
+      div3[q] = div3l;
+      R omegax = wy - vz, omegay = uz - wx, omegaz = vx - uy;
+      R omod2 = omegax * omegax + omegay * omegay + omegaz * omegaz;
+      if (do_sensor) {
+        R om = sqrt(omod2);
+        R om2 = om * om;
+        R dv = R(3) * div3l;
+        R u0l0 = R(g.u0 / g.l0);
+        R t = fmax(-dv / sqrt(om2 + dv * dv + u0l0 * u0l0), R(0));
+        sensor_next[q] = double(t * t);
+      }
+      R sig11 = ux - R(2) * div3l, sig12 = vx, sig13 = wx;
+      R sig21 = uy, sig22 = vy - R(2) * div3l, sig23 = wy;
+      R sig31 = uz, sig32 = vz, sig33 = wz - R(2) * div3l;
+      R sigx = mux * sig11 + muy * sig12 + muz * sig13;
+      R sigy = mux * sig21 + muy * sig22 + muz * sig23;
+      R sigz = mux * sig31 + muy * sig32 + muz * sig33;
+      R sigah = (sig11 * ux + sig12 * uy + sig13 * uz + sig21 * vx + sig22 * vy + sig23 * vz + sig31 * wx +
+                 sig32 * wy + sig33 * wz) * mu;
+      R sigq = sigx * uu + sigy * vv + sigz * ww + sigah;
+      double f2 = fl[nI + q], f3 = fl[2 * nI + q], f4 = fl[3 * nI + q], f5 = fl[4 * nI + q];
+      f2 = f2 - double(sigx);
+      f3 = f3 - double(sigy);
+      f4 = f4 - double(sigz);
+      f5 = f5 - double(sigq);
+      // conservative face Laplacian: face sigma between points a (lower) and b (upper)
+      auto face = [&](int sla, int dia, int dja, int slb, int dib, int djb, double d, double (&sf)[4]) {
+        R u1 = F(sla, dia, dja, 0), u2 = F(slb, dib, djb, 0), v1 = F(sla, dia, dja, 1), v2 = F(slb, dib, djb, 1);
+        R w1 = F(sla, dia, dja, 2), w2 = F(slb, dib, djb, 2);
+        R t1 = F(sla, dia, dja, 3), t2 = F(slb, dib, djb, 3), m1 = F(sla, dia, dja, 4), m2 = F(slb, dib, djb, 4);
+        R qq1 = R(0.5) * (u1 * u1 + v1 * v1 + w1 * w1);
+        R qq2 = R(0.5) * (u2 * u2 + v2 * v2 + w2 * w2);
+        R muf = m1 + m2;
+        muf = R(0.5) * muf / R(d);
+        sf[0] = double((u2 - u1) * muf);
+        sf[1] = double((v2 - v1) * muf);
+        sf[2] = double((w2 - w1) * muf);
+        const R cpf = TP ? R(cp_of_t(g, double(R(0.5) * (t1 + t2)))) : R(g.cp0);
+        sf[3] = double(((t2 - t1) * cpf / prandtl + (qq2 - qq1)) * muf);
+      };
+      double lo[4], hi[4];
+      face(s0, -1, 0, s0, 0, 0, g.x[i] - g.x[i - 1], lo);
+      face(s0, 0, 0, s0, 1, 0, g.x[i + 1] - g.x[i], hi);
+      double dxhl = __ldg(g.vhl[0] + i);
+      f2 = f2 + dxhl * (-hi[0] - -lo[0]);
+      f3 = f3 + dxhl * (-hi[1] - -lo[1]);
+      f4 = f4 + dxhl * (-hi[2] - -lo[2]);
+      f5 = f5 + dxhl * (-hi[3] - -lo[3]);
+      face(s0, 0, -1, s0, 0, 0, g.y[j] - g.y[j - 1], lo);
+      face(s0, 0, 0, s0, 0, 1, g.y[j + 1] - g.y[j], hi);
+      double dyhl = __ldg(g.vhl[1] + j);
+      f2 = f2 + lo[0] * dyhl - hi[0] * dyhl;
+      f3 = f3 + lo[1] * dyhl - hi[1] * dyhl;
+      f4 = f4 + lo[2] * dyhl - hi[2] * dyhl;
+      f5 = f5 + lo[3] * dyhl - hi[3] * dyhl;
+      face(sm, 0, 0, s0, 0, 0, g.z[k] - g.z[k - 1], lo);
+      face(s0, 0, 0, sp, 0, 0, g.z[k + 1] - g.z[k], hi);
+      double dzhl = __ldg(g.vhl[2] + k);
+      f2 = f2 + lo[0] * dzhl - hi[0] * dzhl;
+      f3 = f3 + lo[1] * dzhl - hi[1] * dzhl;
+      f4 = f4 + lo[2] * dzhl - hi[2] * dzhl;
+      f5 = f5 + lo[3] * dzhl - hi[3] * dzhl;
+      fl[nI + q] = f2;
+      fl[2 * nI + q] = f3;
+      fl[3 * nI + q] = f4;
+      fl[4 * nI + q] = f5;
+    }
+    __syncthreads();  // the slot of plane k-1 is overwritten by plane k+2 next
+  }
+}
+template <class R, bool TP = false>
+__global__ void __launch_bounds__(VT_NT, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F)
+    k_visc_tiled(Geom g, const R* __restrict__ aux, double* __restrict__ fl, R* __restrict__ div3,
+                 double* __restrict__ sensor_next, double* __restrict__ wallprop, int do_sensor) {
+  d_visc_tiled<R, TP>(g, aux, fl, div3, sensor_next, wallprop, do_sensor, Blk{blockIdx.x, blockIdx.y, blockIdx.z});
+}
+
 template <class R, bool TP = false>
 __global__ void __launch_bounds__(256, sizeof(R) == 8 ? VISC_MINB : VISC_MINB_F) k_visc(Geom g, const R* __restrict__ aux, double* __restrict__ fl,
                                               R* __restrict__ div3, double* __restrict__ sensor_next,

@@ -220,7 +220,11 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
     ++*nl;
   }
   SB_LAUNCH(d, K_EULER_X, s, k_xflux<R, LB, WS, FS><<<xg, xb, xsm, s>>>(g, aux, sensor, fl_new));
-  if (g.conservative_viscous)
+  if (g.conservative_viscous && SB_VISC_TILED)
+    SB_LAUNCH(d, K_VISC, s,
+              k_visc_tiled<R, (FS & 2) != 0><<<visc_tiled_blocks(g), VT_NT, 0, s>>>(
+                  g, aux, fl_new, div3, sensor_next, d.wallprop, fp64 && a.istep == 3));
+  else if (g.conservative_viscous)
     SB_LAUNCH(d, K_VISC, s,
               k_visc<R, (FS & 2) != 0><<<nblocks(g.nint, 256), 256, 0, s>>>(g, aux, fl_new, div3, sensor_next, d.wallprop,
                                                              fp64 && a.istep == 3));
