@@ -76,13 +76,15 @@ constexpr int MT_NT = 128;                                     // march kernels
 #ifndef MT_MINB_F
 #define MT_MINB_F 4
 #endif
-// the viscous pass: 4 blocks of 256 threads per SM (64 registers, a little spilling) measured
-// faster than 2 blocks at 128 registers, and for FP32 faster than 3 blocks (2.77 against 3.48 ms)
+// the viscous pass: the staged FP64 pass at 3 blocks of 256 threads per SM (80 registers; 7.42
+// against 7.57 ms per step at 4 blocks and 64 registers on the 1024x256x192 boundary layer), the
+// FP32 one at 4 (5.02 against 5.62 ms at 3); the direct pass at 4 blocks measured faster than 2
+// blocks at 128 registers
 #ifndef VISC_MINB
-#define VISC_MINB 4
+#define VISC_MINB 3
 #endif
 #ifndef VISC_MINB_F
-#define VISC_MINB_F VISC_MINB
+#define VISC_MINB_F 4
 #endif
 constexpr int FIN_NT = 1024;
 
@@ -857,7 +859,10 @@ __device__ __forceinline__ void d_visc(const Geom& g, const R* __restrict__ aux,
 // column and its x / y halo), so that every point is loaded once per block (and its halo once
 // more) with coalesced rows instead of once per use, and the x / y / z neighbours come from
 // shared memory.  The arithmetic is d_visc's, in its order.
-constexpr int VT_X = 32, VT_Y = 8, VT_NT = VT_X * VT_Y, VT_K = 16;
+#ifndef SB_VT_K
+#define SB_VT_K 16
+#endif
+constexpr int VT_X = 32, VT_Y = 8, VT_NT = VT_X * VT_Y, VT_K = SB_VT_K;
 constexpr int VT_PX = VT_X + 2, VT_PY = VT_Y + 2, VT_PP = VT_PX * VT_PY;
 // blocks of the staged viscous pass: 32 x 8 columns x segments of VT_K cells in z
 inline unsigned visc_tiled_blocks(const Geom& g) {
