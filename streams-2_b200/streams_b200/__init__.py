@@ -583,6 +583,30 @@ class Batch:
         self._check(lib.streams_b200_batch_groups(self._h, C.byref(g), C.byref(n)))
         return int(g.value), int(n.value)
 
+    def tune_form(self, forms=(1, 0, 2), replays: int = 2) -> tuple[int, int, dict]:
+        """Pick the launch form (``set_shared_launches`` groups per class; 0: a graph branch per
+        box) by timing ``replays`` graph replays of each on the live boxes, after one replay of
+        warm-up (the capture); the batch is left in the fastest form.  The steps taken are steps
+        of the solves (every form gives the same results), so the caller counts them.  Returns
+        (form, steps advanced, seconds per replay of each form)."""
+        import time
+        spg = self.steps_per_graph
+        self.advance(1)  # leave the first-step / lead phase before timing replays
+        done = 1
+        times = {}
+        for f in forms:
+            self.set_shared_launches(f)
+            self.advance(spg)
+            self.synchronize()
+            t0 = time.perf_counter()
+            self.advance(replays * spg)
+            self.synchronize()
+            times[f] = (time.perf_counter() - t0) / replays
+            done += (1 + replays) * spg
+        best = min(times, key=times.get)
+        self.set_shared_launches(best)
+        return best, done, times
+
     def close(self):
         h = getattr(self, "_h", None)
         if h:

@@ -82,6 +82,25 @@ def test_shared_launches_equal_separate_branches(tmp_path):
     assert ra == rb == 3 and pb < pa / 2, (pa, pb)
 
 
+def test_launch_form_tuning_keeps_the_results(tmp_path):
+    """The launch-form tuner advances the live boxes through every form; they still equal their
+    runs alone, and the batch is left in the fastest form."""
+    from streams_b200 import Batch
+    solvers = [make(tmp_path, i, kw) for i, kw in enumerate(BOXES)]
+    b = Batch(solvers, steps_per_graph=3)
+    form, done, times = b.tune_form(forms=(1, 0), replays=1)
+    assert form in (1, 0) and set(times) == {1, 0} and done == 1 + 2 * 2 * 3
+    b.advance(5)
+    b.synchronize()
+    total = done + 5
+    for i, kw in enumerate(BOXES):
+        s = make(tmp_path, 10 + i, kw)
+        s.advance(total)
+        assert np.array_equal(s.copy_to_field(), solvers[i].copy_to_field()), i
+        s.close()
+    b.close()
+
+
 def test_a_box_outside_the_groups_keeps_its_branch(tmp_path):
     """A boundary-layer box (stored ghosts, recycling inflow, non-reflecting faces) advances on
     its own branch beside a group of channels; every box equals its run alone."""
