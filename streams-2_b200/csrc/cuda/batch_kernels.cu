@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(AUX_NT) kb_apply_shift(const BoxRec* __restric
 }
 
 template <unsigned SPAN, class A, bool TP>
-__global__ void __launch_bounds__(AUX_NT) kb_aux(const BoxRec* __restrict__ rec,
+__global__ void __launch_bounds__(AUX_NT, AUX_MINB) kb_aux(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile, int want_vel) {
   for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
     d_aux<A, TP>(g, r->w, static_cast<A*>(r->aux), 0, want_vel ? r->vel64 : nullptr, Blk{l, 0, 0});
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(FIN_NT) kb_finish_rhs(const BoxRec* __restrict
 }
 
 template <unsigned SPAN, class R, bool TP>
-__global__ void __launch_bounds__(256) kb_update(const BoxRec* __restrict__ rec,
+__global__ void __launch_bounds__(256, UPD_MINB) kb_update(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile, double rhork, double gamrk, int istep,
     int stats) {
   for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(FIN_NT) kb_finish_upd(const BoxRec* __restrict
 }
 
 template <unsigned SPAN, class R>
-__global__ void __launch_bounds__(256) kb_dt(const BoxRec* __restrict__ rec,
+__global__ void __launch_bounds__(256, DT_MINB) kb_dt(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile) {
   for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
     d_dt<R>(g, r->w, static_cast<const R*>(r->aux), r->red, Blk{l, 0, 0});

@@ -83,6 +83,20 @@ constexpr int MT_NT = 128;                                     // march kernels
 #ifndef VISC_MINB
 #define VISC_MINB 3
 #endif
+// resident blocks of 256 threads per SM asked of the register allocator for the memory-bound
+// pointwise passes: 8 (32 registers, a little spilling in the update pass), for more loads in
+// flight (1024x256x192 boundary layer, ms per step against the allocator's own choice: update
+// 4.24 against 5.02 at 60 registers, 4.51 at 6 blocks; aux 3.01 against 3.23; dt 1.12 against
+// 1.27)
+#ifndef UPD_MINB
+#define UPD_MINB 8
+#endif
+#ifndef AUX_MINB
+#define AUX_MINB 8
+#endif
+#ifndef DT_MINB
+#define DT_MINB 8
+#endif
 #ifndef VISC_MINB_F
 #define VISC_MINB_F 4
 #endif
@@ -221,7 +235,7 @@ __device__ __forceinline__ void d_aux(const Geom& g, double* __restrict__ w, A* 
   }
 }
 template <class A, bool TP = false>
-__global__ void __launch_bounds__(AUX_NT) k_aux(Geom g, double* __restrict__ w, A* __restrict__ aux,
+__global__ void __launch_bounds__(AUX_NT, AUX_MINB) k_aux(Geom g, double* __restrict__ w, A* __restrict__ aux,
                                                 int write_ghost_w, double* __restrict__ vel) {
   d_aux<A, TP>(g, w, aux, write_ghost_w, vel, Blk{blockIdx.x, blockIdx.y, blockIdx.z});
 }
@@ -1215,7 +1229,7 @@ __device__ __forceinline__ void d_dt(const Geom& g, const double* __restrict__ w
   }
 }
 template <class R>
-__global__ void __launch_bounds__(256) k_dt(Geom g, const double* __restrict__ w, const R* __restrict__ aux,
+__global__ void __launch_bounds__(256, DT_MINB) k_dt(Geom g, const double* __restrict__ w, const R* __restrict__ aux,
                                             double* __restrict__ red) {
   d_dt<R>(g, w, aux, red, Blk{blockIdx.x, blockIdx.y, blockIdx.z});
 }
@@ -1374,7 +1388,7 @@ __device__ __forceinline__ void d_update(const Geom& g, double* __restrict__ w, 
   }
 }
 template <class R, bool TP = false>
-__global__ void __launch_bounds__(256) k_update(Geom g, double* __restrict__ w, const double* __restrict__ fl_prev,
+__global__ void __launch_bounds__(256, UPD_MINB) k_update(Geom g, double* __restrict__ w, const double* __restrict__ fl_prev,
                                                 const double* __restrict__ fl_new, const Scalars* __restrict__ sc,
                                                 double rhork, double gamrk, int istep, int stats,
                                                 double* __restrict__ red, const double* __restrict__ sensor_next,
