@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(FIN_NT) kb_finish_rhs(const BoxRec* __restrict
 }
 
 template <unsigned SPAN, class R, bool TP>
-__global__ void __launch_bounds__(256, UPD_MINB) kb_update(const BoxRec* __restrict__ rec,
+__global__ void __launch_bounds__(UPD_NT, UPD_MINB) kb_update(const BoxRec* __restrict__ rec,
     const BlockRef* __restrict__ blocks, unsigned ntile, double rhork, double gamrk, int istep,
     int stats) {
   for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(256, UPD_MINB) kb_update(const BoxRec* __restr
 __global__ void __launch_bounds__(FIN_NT) kb_finish_upd(const BoxRec* __restrict__ rec, int stats, int add_time) {
   __shared__ Geom gs;
   const BoxRec* r = enter_box_direct(rec, gs);
-  d_finish_upd(gs, r->red, r->nb_pt, stats, add_time, r->sc, Blk{0, 0, 0});
+  d_finish_upd(gs, r->red, r->nb_up, stats, add_time, r->sc, Blk{0, 0, 0});
 }
 
 template <unsigned SPAN, class R>
@@ -198,13 +198,12 @@ __global__ void __launch_bounds__(256, DT_MINB) kb_dt(const BoxRec* __restrict__
 
 __global__ void __launch_bounds__(FIN_NT) kb_dt_finish(const BoxRec* __restrict__ rec) {
   const BoxRec* r = rec + blockIdx.x;
-  d_dt_finish(r->red, r->nb_pt, r->cfl, r->sc, Blk{0, 0, 0});
+  d_dt_finish(r->red, r->nb_up, r->cfl, r->sc, Blk{0, 0, 0});
 }
 
-// Tiles per CTA: the short tiles of the aux, update, time-step and sensor passes are taken four
-// at a time so that a CTA enters a box (table entry, geometry copy) once for several; the
-// viscous and flux passes, whose tiles carry more work and whose bodies are register bound,
-// take one.
+// Tiles per CTA: the short tiles of the aux, shift and sensor passes are taken four at a time so
+// that a CTA enters a box (table entry, record copy) once for several; the update and time-step
+// passes (1024 cells a tile), the viscous and the flux passes take one.
 constexpr unsigned SPAN_PT = 4;
 struct Launch {
   unsigned ntile;
@@ -285,8 +284,9 @@ cudaError_t batch_stage_impl(const BoxTable& t, const StageArgs& a, cudaStream_t
                                                                        a.istep);
     ++*nl;
   }
-  kb_update<SPAN_PT, R, TP><<<P.grid(SPAN_PT), 256, 0, s>>>(t.rec, P.blocks, P.ntile, a.rhork, a.gamrk, a.istep,
-                                                         a.want_stats);
+  const Launch U = launch_of(t, BK_UP);
+  kb_update<1, R, TP><<<U.grid(1), UPD_NT, 0, s>>>(t.rec, U.blocks, U.ntile, a.rhork, a.gamrk, a.istep,
+                                                     a.want_stats);
   kb_finish_upd<<<nbox, FIN_NT, 0, s>>>(t.rec, a.want_stats, a.add_time);
   *nl += 2;
   return cudaGetLastError();
@@ -376,6 +376,7 @@ BoxRec box_rec(const Geom& g, const DevState& d, double* fl_a, double* fl_b, dou
   r.nb_pt = nblocks(g.nint, 256);
   r.nb_vol = nblocks(g.nvol, AUX_NT);
   r.nb_vs = visc_tiled_blocks(g);
+  r.nb_up = pt_blocks(g.nint);
   return r;
 }
 
@@ -402,7 +403,8 @@ cudaError_t box_table_build(BoxTable& t, const std::vector<BoxRec>& recs, cudaSt
                                    : k == BK_X  ? (unsigned long long)r.xg[0] * r.xg[1] * r.xg[2]
                                    : k == BK_Y  ? r.nb_y
                                    : k == BK_Z  ? r.nb_z
-                                                : r.nb_vs;
+                                   : k == BK_VS ? r.nb_vs
+                                                : r.nb_up;
       for (unsigned long long q = 0; q < n; ++q) blocks.push_back(BlockRef{(unsigned)b, (unsigned)q});
     }
     const long long c = (long long)blocks.size() - t.off[k];
@@ -432,11 +434,11 @@ cudaError_t batch_launch_aux(const BoxTable& t, int apply_shift, cudaStream_t s,
 }
 
 cudaError_t batch_launch_dt(const BoxTable& t, cudaStream_t s, long long* nl) {
-  const Launch P = launch_of(t, BK_PT);
+  const Launch U = launch_of(t, BK_UP);
   if (t.g0.precision == 1)
-    kb_dt<SPAN_PT, float><<<P.grid(SPAN_PT), 256, 0, s>>>(t.rec, P.blocks, P.ntile);
+    kb_dt<1, float><<<U.grid(1), 256, 0, s>>>(t.rec, U.blocks, U.ntile);
   else
-    kb_dt<SPAN_PT, double><<<P.grid(SPAN_PT), 256, 0, s>>>(t.rec, P.blocks, P.ntile);
+    kb_dt<1, double><<<U.grid(1), 256, 0, s>>>(t.rec, U.blocks, U.ntile);
   kb_dt_finish<<<t.nbox, FIN_NT, 0, s>>>(t.rec);
   *nl += 2;
   return cudaGetLastError();

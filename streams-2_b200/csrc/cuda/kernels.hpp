@@ -138,12 +138,13 @@ struct BoxRec {
   unsigned xg[3];          // grid of the x pass (one-dimensional)
   unsigned nb_vol, nb_pt, nb_y, nb_z;  // blocks of the aux pass, pointwise passes, y and z passes
   unsigned nb_vs;                      // blocks of the staged viscous pass
+  unsigned nb_up;                      // blocks of the update and time-step passes
 };
 // block of a launch over a box table: the box and the block's index in the box's own grid
 struct BlockRef {
   unsigned box, local;
 };
-enum BatchKind { BK_VOL = 0, BK_PT, BK_X, BK_Y, BK_Z, BK_VS, BK_NUM };
+enum BatchKind { BK_VOL = 0, BK_PT, BK_X, BK_Y, BK_Z, BK_VS, BK_UP, BK_NUM };
 struct BoxTable {
   int nbox = 0;
   BoxRec* rec = nullptr;       // device

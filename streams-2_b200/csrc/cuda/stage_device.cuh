@@ -83,13 +83,13 @@ constexpr int MT_NT = 128;                                     // march kernels
 #ifndef VISC_MINB
 #define VISC_MINB 3
 #endif
-// resident blocks of 256 threads per SM asked of the register allocator for the memory-bound
-// pointwise passes: 8 (32 registers, a little spilling in the update pass), for more loads in
-// flight (1024x256x192 boundary layer, ms per step against the allocator's own choice: update
-// 4.24 against 5.02 at 60 registers, 4.51 at 6 blocks; aux 3.01 against 3.23; dt 1.12 against
-// 1.27)
+// resident threads per SM asked of the register allocator for the memory-bound pointwise passes:
+// 2048 (32 registers, a little spilling in the update pass), for more loads in flight
+// (1024x256x192 boundary layer, ms per step against the allocator's own choice: update 4.24
+// against 5.02 at 60 registers, 4.51 at 1536 threads; aux 3.01 against 3.23; dt 1.12 against
+// 1.27).  The update pass's blocks are 1024 threads (UPD_MINB of them), the others 256.
 #ifndef UPD_MINB
-#define UPD_MINB 8
+#define UPD_MINB 2
 #endif
 #ifndef AUX_MINB
 #define AUX_MINB 8
@@ -101,6 +101,16 @@ constexpr int MT_NT = 128;                                     // march kernels
 #define VISC_MINB_F 4
 #endif
 constexpr int FIN_NT = 1024;
+// cells per block of the update and time-step passes: 1024 (the time-step pass: 4 per thread of
+// 256), a quarter of the block partials for their one-block finishing reductions (1024x256x192:
+// 0.43 -> 0.13 and 0.17 -> 0.05 ms per step)
+#ifndef SB_PT_CELLS
+#define SB_PT_CELLS 4
+#endif
+constexpr int PT_CELLS = SB_PT_CELLS;
+// the update pass: one cell per thread in blocks of 1024 (the same count of block partials)
+constexpr int UPD_NT = 256 * PT_CELLS;
+inline unsigned pt_blocks(long long nint) { return (unsigned)((nint + 256 * PT_CELLS - 1) / (256 * PT_CELLS)); }
 
 // Block coordinates seen by a kernel body (d_*): the hardware block index in a plain launch
 // (k_*), the block's place in its own box's grid in a launch over a box table (kb_*)
@@ -1185,9 +1195,11 @@ template <class R>
 __device__ __forceinline__ void d_dt(const Geom& g, const double* __restrict__ w, const R* __restrict__ aux,
                                             double* __restrict__ red, const Blk blk) {
   __shared__ double sm[9 * 8];
-  const long long q = (long long)blk.x * 256 + threadIdx.x;
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  if (q < g.nint) {
+#pragma unroll 1
+  for (int cq = 0; cq < PT_CELLS; ++cq) {
+    const long long q = (long long)blk.x * (256 * PT_CELLS) + cq * 256 + threadIdx.x;
+    if (q >= g.nint) break;
     int i, j, k;
     cell_of(g, q, i, j, k);
     const long long n = g.nvol, c = gidx(g, i, j, k);
@@ -1203,15 +1215,15 @@ __device__ __forceinline__ void d_dt(const Geom& g, const double* __restrict__ w
     double nu = ri * mu;
     double kr = nu / g.prandtl;
     double cs = sqrt(gamloc_of_t(g, tt) * g.rgas0 * tt);
-    v[0] = (fabs(uu) + cs) * g.dcsidx[i];
-    v[1] = (fabs(vv) + cs) * g.detady[j];
-    v[2] = (fabs(ww) + cs) * g.dzitdz[k];
-    v[3] = nu * g.dcsidxs[i];
-    v[4] = nu * g.detadys[j];
-    v[5] = nu * g.dzitdzs[k];
-    v[6] = kr * g.dcsidxs[i];
-    v[7] = kr * g.detadys[j];
-    v[8] = kr * g.dzitdzs[k];
+    v[0] = fmax(v[0], (fabs(uu) + cs) * g.dcsidx[i]);
+    v[1] = fmax(v[1], (fabs(vv) + cs) * g.detady[j]);
+    v[2] = fmax(v[2], (fabs(ww) + cs) * g.dzitdz[k]);
+    v[3] = fmax(v[3], nu * g.dcsidxs[i]);
+    v[4] = fmax(v[4], nu * g.detadys[j]);
+    v[5] = fmax(v[5], nu * g.dzitdzs[k]);
+    v[6] = fmax(v[6], kr * g.dcsidxs[i]);
+    v[7] = fmax(v[7], kr * g.detadys[j]);
+    v[8] = fmax(v[8], kr * g.dzitdzs[k]);
   }
 #pragma unroll
   for (int r = 0; r < 9; ++r)
@@ -1300,13 +1312,14 @@ __device__ __forceinline__ void d_update(const Geom& g, double* __restrict__ w, 
                                                 double rhork, double gamrk, int istep, int stats,
                                                 double* __restrict__ red, const double* __restrict__ sensor_next,
                                                 double* __restrict__ sensor, R* __restrict__ aux, const Blk blk) {
-  __shared__ double sm[2 * 8];
-  __shared__ double smn[3 * 8];
-  __shared__ double smx[3 * 8];
-  const long long q = (long long)blk.x * 256 + threadIdx.x;
+  constexpr int NW = UPD_NT / 32;
+  __shared__ double sm[2 * NW];
+  __shared__ double smn[3 * NW];
+  __shared__ double smx[3 * NW];
   double s2[2] = {0.0, 0.0};
   double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX};
   double mx[3] = {-100.0, -100.0, -100.0};
+  const long long q = (long long)blk.x * UPD_NT + threadIdx.x;
   if (q < g.nint) {
     int i, j, k;
     cell_of(g, q, i, j, k);
@@ -1344,24 +1357,24 @@ __device__ __forceinline__ void d_update(const Geom& g, double* __restrict__ w, 
       double qq = 0.5 * (uu * uu + vv * vv + ww * ww);
       double ee = wn[4] / wn[0] - qq;
       double tt = t_from_e<TP>(g, ee, t_aux);
-      s2[0] = wn[1] * tt * dy;
+      s2[0] = s2[0] + wn[1] * tt * dy;
       tstat = tt;
       // force_var_1 leaves this temperature in w_aux(6), where the statistics read it
       if (istep == 3) aux[5 * n + c] = R(tt);
     }
     if (stats) {
       double r = fln[1] / dt;
-      s2[1] = r * r;
+      s2[1] = s2[1] + r * r;
       double rho = old.rho;
       double pp = rho * tstat * g.rgas0;
-      mn[0] = rho; mn[1] = tstat; mn[2] = pp;
-      mx[0] = rho; mx[1] = tstat; mx[2] = pp;
+      mn[0] = fmin(mn[0], rho); mn[1] = fmin(mn[1], tstat); mn[2] = fmin(mn[2], pp);
+      mx[0] = fmax(mx[0], rho); mx[1] = fmax(mx[1], tstat); mx[2] = fmax(mx[2], pp);
     }
   }
   // the block partials are read only by the forcing and by a stats sample (the same branch for
   // the whole grid)
   if (!g.force_var && !stats) return;
-  block_reduce_sum<2, 256>(s2, sm);
+  block_reduce_sum<2, UPD_NT>(s2, sm);
   // min / max (exact, order independent)
 #pragma unroll
   for (int r = 0; r < 3; ++r)
@@ -1373,7 +1386,7 @@ __device__ __forceinline__ void d_update(const Geom& g, double* __restrict__ w, 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0)
 #pragma unroll
-    for (int r = 0; r < 3; ++r) { smn[r * 8 + warp] = mn[r]; smx[r * 8 + warp] = mx[r]; }
+    for (int r = 0; r < 3; ++r) { smn[r * NW + warp] = mn[r]; smx[r * NW + warp] = mx[r]; }
   __syncthreads();
   if (threadIdx.x == 0) {
     double* o = red + (long long)blk.x * NRED_UPD;
@@ -1381,14 +1394,14 @@ __device__ __forceinline__ void d_update(const Geom& g, double* __restrict__ w, 
     o[1] = s2[1];
     for (int r = 0; r < 3; ++r) {
       double a = DBL_MAX, b = -100.0;
-      for (int wq = 0; wq < 8; ++wq) { a = fmin(a, smn[r * 8 + wq]); b = fmax(b, smx[r * 8 + wq]); }
+      for (int wq = 0; wq < NW; ++wq) { a = fmin(a, smn[r * NW + wq]); b = fmax(b, smx[r * NW + wq]); }
       o[2 + r] = a;
       o[5 + r] = b;
     }
   }
 }
 template <class R, bool TP = false>
-__global__ void __launch_bounds__(256, UPD_MINB) k_update(Geom g, double* __restrict__ w, const double* __restrict__ fl_prev,
+__global__ void __launch_bounds__(UPD_NT, UPD_MINB) k_update(Geom g, double* __restrict__ w, const double* __restrict__ fl_prev,
                                                 const double* __restrict__ fl_new, const Scalars* __restrict__ sc,
                                                 double rhork, double gamrk, int istep, int stats,
                                                 double* __restrict__ red, const double* __restrict__ sensor_next,

@@ -124,7 +124,7 @@ cudaError_t launch_init_sensor(const Geom& g, DevState& d, cudaStream_t s, long 
 }
 
 cudaError_t launch_dt(const Geom& g, DevState& d, double cfl, cudaStream_t s, long long* nl) {
-  const unsigned nb = nblocks(g.nint, 256);
+  const unsigned nb = pt_blocks(g.nint);
   if (g.precision == 1)
     SB_LAUNCH(d, K_DT, s, k_dt<float><<<nb, 256, 0, s>>>(g, d.w, d.auxf, d.red));
   else
@@ -288,9 +288,9 @@ static cudaError_t stage_impl(const Geom& g, DevState& d, const StageArgs& a, do
     SB_LAUNCH(d, K_FINISH_RHS, s, k_finish_rhs<<<1, FIN_NT, 0, s>>>(g, d.red, (long long)gzb, a.istep == 1, d.sc));
     ++*nl;
   }
-  const unsigned nbu = nblocks(g.nint, 256);
+  const unsigned nbu = pt_blocks(g.nint);
   SB_LAUNCH(d, K_UPDATE, s,
-            k_update<R, (FS & 2) != 0><<<nbu, 256, 0, s>>>(g, d.w, fl_prev, fl_new, d.sc, a.rhork, a.gamrk, a.istep,
+            k_update<R, (FS & 2) != 0><<<nbu, UPD_NT, 0, s>>>(g, d.w, fl_prev, fl_new, d.sc, a.rhork, a.gamrk, a.istep,
                                             a.want_stats, d.red, sensor_next, sensor, aux));
   SB_LAUNCH(d, K_FINISH_UPD, s, k_finish_upd<<<1, FIN_NT, 0, s>>>(g, d.red, nbu, a.want_stats, a.add_time, d.sc));
   *nl += 2;
