@@ -42,13 +42,14 @@ constexpr int MT_NT = 128;                                     // march kernels
 // spills; 16.5 against 18.6 ms per step at 3 blocks), which the WENO scratch of 2WS-1 values a
 // side allows (51 KB a block).  FP64 march passes: 3 blocks (the y pass without a register
 // window: at 4 blocks its reloads miss L1, 18.8 against 17.3 ms; the windowed passes spill
-// 176-228 bytes at 4 blocks).  FP32: 5 blocks for the x pass (5.41 against 5.90 ms at 4) and 4 for the march passes
-// (5 blocks: 7.1-7.4 against 5.4-6.5 ms).
+// 176-228 bytes at 4 blocks).  FP32, with the Newton-refined quotients: 6 blocks for the x pass
+// (12.31 against 12.89 ms per step at 5) and 5 for the march passes (y 12.11, z 14.72 against
+// 12.36, 15.33 at 4).
 #ifndef XF_MINB_D
 #define XF_MINB_D 4
 #endif
 #ifndef XF_MINB_F
-#define XF_MINB_F 5
+#define XF_MINB_F 6
 #endif
 #ifndef MT_MINB_D
 #define MT_MINB_D 3
@@ -74,7 +75,7 @@ constexpr int MT_NT = 128;                                     // march kernels
 #define SB_WF_CARVEOUT 72
 #endif
 #ifndef MT_MINB_F
-#define MT_MINB_F 4
+#define MT_MINB_F 5
 #endif
 // the viscous pass: the staged FP64 pass at 3 blocks of 256 threads per SM (80 registers; 7.42
 // against 7.57 ms per step at 4 blocks and 64 registers on the 1024x256x192 boundary layer), the
