@@ -43,8 +43,8 @@ constexpr int MT_NT = 128;                                     // march kernels
 // side allows (51 KB a block).  FP64 march passes: 3 blocks (the y pass without a register
 // window: at 4 blocks its reloads miss L1, 18.8 against 17.3 ms; the windowed passes spill
 // 176-228 bytes at 4 blocks).  FP32, with the Newton-refined quotients: 6 blocks for the x pass
-// (12.31 against 12.89 ms per step at 5) and 5 for the march passes (y 12.11, z 14.72 against
-// 12.36, 15.33 at 4).
+// (12.31 against 12.89 ms per step at 5, the same at 7) and 5 for the march passes (y 12.11,
+// z 14.72 against 12.36, 15.33 at 4; z 17.1 at 6).
 #ifndef XF_MINB_D
 #define XF_MINB_D 4
 #endif
