@@ -657,6 +657,12 @@ __device__ __forceinline__ void d_march(const Geom& g, const R* __restrict__ aux
 #pragma unroll
     for (int bq = 1; bq < 2 * WS; ++bq) mask |= sensor_bit(p - WS + 1 + bq) << bq;
     R hlo[5] = {0, 0, 0, 0, 0}, llo[5] = {0, 0, 0, 0, 0};
+    // x(i+1)-x(i-1) and y(j+1)-y(j-1) of the z line (the grad(mu div/3) term)
+    R xdiff = R(1), ydiff = R(1);
+    if constexpr (DIR == 2) {
+      xdiff = R(g.x[i + 1] - g.x[i - 1]);
+      ydiff = R(g.y[b + 1] - g.y[b - 1]);
+    }
     for (int c = c0 - 1; c <= c1; ++c) {
       if constexpr (WIN) {
         // slide the window to the face c
@@ -690,11 +696,12 @@ __device__ __forceinline__ void d_march(const Geom& g, const R* __restrict__ aux
         if (DIR == 2) {
           const int j = b, k = c;
           const long long a = gidx(g, i, j, k);
-          const R uu = aux[n + a], vv = aux[2 * n + a], ww = aux[3 * n + a], mu = aux[6 * n + a];
+          // the cell's velocities are the stencil's point S-1 (the face c's lower point)
+          const R uu = st.u[S - 1], vv = st.v[S - 1], ww = st.w[S - 1], mu = aux[6 * n + a];
           R sigx, sigy, sigz;
           if (g.conservative_viscous) {
-            const R dxl = mu / R(g.x[i + 1] - g.x[i - 1]);
-            const R dyl = mu / R(g.y[j + 1] - g.y[j - 1]);
+            const R dxl = mu / xdiff;
+            const R dyl = mu / ydiff;
             const R dzl = mu / R(g.z[k + 1] - g.z[k - 1]);
             sigx = dxl * (div3_at(g, div3, i + 1, j, k) - div3_at(g, div3, i - 1, j, k));
             sigy = dyl * (div3_at(g, div3, i, j + 1, k) - div3_at(g, div3, i, j - 1, k));
