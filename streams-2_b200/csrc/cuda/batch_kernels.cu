@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256) kb_sensor(const BoxRec* __restrict__ rec,
 }
 
 template <unsigned SPAN, class R, int DIR, int LB, int WS, bool CH, int FS>
-__global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F)
+__global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : (CH ? MT_MINB_F_CH : MT_MINB_F))
     kb_march(const BoxRec* __restrict__ rec, const BlockRef* __restrict__ blocks, unsigned ntile, double rhork, double gamrk, int istep) {
   for_tiles<SPAN>(rec, blocks, ntile, [&](const BoxRec* r, const Geom& g, unsigned l) {
     const int seglen = DIR == 1 ? r->sly : r->slz, nseg = DIR == 1 ? r->nsy : r->nsz;

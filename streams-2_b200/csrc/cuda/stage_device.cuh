@@ -77,6 +77,10 @@ constexpr int MT_NT = 128;                                     // march kernels
 #ifndef MT_MINB_F
 #define MT_MINB_F 5
 #endif
+// the channel's FP32 z pass (force_rhs partials) keeps 4: at 5 it spills 244 bytes
+#ifndef MT_MINB_F_CH
+#define MT_MINB_F_CH 4
+#endif
 // the viscous pass: the staged FP64 pass at 3 blocks of 256 threads per SM (80 registers; 7.42
 // against 7.57 ms per step at 4 blocks and 64 registers on the 1024x256x192 boundary layer), the
 // FP32 one at 4 (5.02 against 5.62 ms at 3); the direct pass at 4 blocks measured faster than 2
@@ -758,7 +762,7 @@ __device__ __forceinline__ void d_march(const Geom& g, const R* __restrict__ aux
   }
 }
 template <class R, int DIR, int LB, int WS, bool CH = false, int FS = 0, bool SPLIT = false>
-__global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : MT_MINB_F) k_march(Geom g, const R* __restrict__ aux,
+__global__ void __launch_bounds__(MT_NT, sizeof(R) == 8 ? MT_MINB_D : (CH ? MT_MINB_F_CH : MT_MINB_F)) k_march(Geom g, const R* __restrict__ aux,
                                                  const double* __restrict__ sensor, double* __restrict__ fl,
                                                  const R* __restrict__ div3,
                                                  const double* __restrict__ w, const double* __restrict__ fl_prev,
